@@ -1,0 +1,222 @@
+/*
+ * scxpca.h -- C ABI of the B200 randomized-PCA library (libscxpca.so).
+ *
+ * Randomized PCA of a sparse cells x genes CSR matrix with implicit per-gene
+ * centring (and optional unit-variance scaling with clipping), computed by
+ * hand-written sm_100a kernels.  The ABI is plain C: pointers, sizes, status
+ * codes; no exceptions cross it and no call aborts the process.
+ *
+ * Every entry point below replaces one interface of ArcInstitute/scx (paths
+ * inside that tree); the citation is in the comment above each declaration.
+ *
+ * Threading: a plan is used by one host thread at a time.  Separate plans may
+ * be used concurrently from different threads.
+ */
+#ifndef SCXPCA_H
+#define SCXPCA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCXPCA_ABI_VERSION 1
+
+/* Status codes.  They mirror the GpuError classes of scx-gpu/src/error.rs:
+ * ShapeMismatch -> INVALID_ARGUMENT, OutOfMemory -> OUT_OF_MEMORY,
+ * CuSolverError("...non-SPD...") -> NOT_SPD, InvalidShard -> INVALID_CSR,
+ * CudaError/KernelLaunchFailed -> CUDA_ERROR. */
+typedef enum {
+  SCXPCA_OK = 0,
+  SCXPCA_INVALID_ARGUMENT = 1,
+  SCXPCA_OUT_OF_MEMORY = 2,
+  SCXPCA_NOT_SPD = 3,
+  SCXPCA_INVALID_CSR = 4,
+  SCXPCA_CUDA_ERROR = 5,
+  SCXPCA_TIMEOUT = 6,
+  SCXPCA_UNSUPPORTED = 7
+} scxpca_status;
+
+/* Element type of stored nonzero values. */
+typedef enum { SCXPCA_F32 = 0, SCXPCA_BF16 = 1, SCXPCA_F16 = 2 } scxpca_dtype;
+
+/* Where a buffer lives. */
+typedef enum { SCXPCA_MEM_HOST = 0, SCXPCA_MEM_DEVICE = 1 } scxpca_memory;
+
+/* Orthonormalisation failure contract (scx-gpu/src/cusolver.rs:256-262).
+ * CHOLESKY reports SCXPCA_NOT_SPD when a Gram pivot breaks down (the message
+ * contains "non-SPD"); HOUSEHOLDER never fails on finite input: its
+ * Cholesky is shifted when a pivot breaks down. */
+typedef enum { SCXPCA_QR_HOUSEHOLDER = 0, SCXPCA_QR_CHOLESKY = 1 } scxpca_qr_method;
+
+/* Arithmetic (scx-gpu/src/math_policy.rs:45-84, GpuMathMode).
+ * STRICT_FP32: FP32 values, FP32 CUDA-core SpMM, FP64 Gram/Cholesky/SVD.
+ * MIXED_BF16 / MIXED_F16: values stream as 16-bit, SpMM products on tensor
+ * cores with FP32 accumulation, final projection and small factorisations
+ * in FP32/FP64. */
+typedef enum {
+  SCXPCA_MATH_STRICT_FP32 = 0,
+  SCXPCA_MATH_MIXED_BF16 = 1,
+  SCXPCA_MATH_MIXED_F16 = 2
+} scxpca_math_mode;
+
+/* SpMM reduction order (scx-gpu/src/math_policy.rs:86-136, SpmmAlgPolicy).
+ * DETERMINISTIC gives bit-identical results across runs on one device. */
+typedef enum { SCXPCA_SPMM_DEFAULT = 0, SCXPCA_SPMM_DETERMINISTIC = 1 } scxpca_spmm_policy;
+
+/* A CSR matrix: rows are cells, columns are genes.  Replaces the ShardSource /
+ * ScxCsr input (scx-format-io/src/shard_source.rs:86-140,
+ * scx-sparse/src/csr.rs:183-192): int64 indptr (n_obs + 1), int32 indices
+ * (nnz), values (nnz) of `values_dtype`.  Column indices must be in
+ * [0, n_vars); rows need not be sorted for correctness.  `memory` says whether
+ * the three arrays are host or device pointers (device: on `device_ordinal`). */
+typedef struct {
+  int64_t n_obs;
+  int64_t n_vars;
+  int64_t nnz;
+  const int64_t* indptr;
+  const int32_t* indices;
+  const void* values;
+  int32_t values_dtype; /* scxpca_dtype */
+  int32_t memory;       /* scxpca_memory */
+} scxpca_csr;
+
+/* Arguments of scx_gpu::gpu_randomized_pca (scx-gpu/src/gpu_pca.rs:706-716)
+ * and pyscx.accel.pca (pyscx/src/accel/pca.rs:573-605), plus the explicit
+ * test matrix and per-gene scaling, which have no reference counterpart. */
+typedef struct {
+  int64_t n_components;
+  int64_t n_oversamples;
+  int64_t n_power_iterations;
+  int32_t zero_center;    /* subtract per-gene means implicitly */
+  int32_t scale;          /* per-gene unit variance (ddof=1), scanpy pp.scale */
+  double clip_max;        /* > 0: clip scaled values to +-clip_max (upper only
+                             without centring); <= 0: no clip */
+  uint64_t seed;          /* used when omega == NULL */
+  const float* omega;     /* optional explicit test matrix, n_vars x k,
+                             column-major (ld = n_vars), k = min(n_components +
+                             n_oversamples, n_vars, n_obs) */
+  int32_t omega_memory;   /* scxpca_memory of omega */
+  int32_t qr_method;      /* scxpca_qr_method */
+  int32_t math_mode;      /* scxpca_math_mode */
+  int32_t spmm_policy;    /* scxpca_spmm_policy */
+  int32_t device_ordinal;
+  int32_t reserved0;
+  void* stream;           /* cudaStream_t; NULL = a stream owned by the plan */
+} scxpca_params;
+
+/* Outputs, caller-allocated.  Replaces GpuPcaResult (gpu_pca.rs:76-98) and
+ * GpuPcaDeviceResult (gpu_pca.rs:108-128).  `embeddings` is n_obs x
+ * n_components row-major float32 in `embeddings_memory` (device: on the plan's
+ * device, written asynchronously before the call returns synchronised).  All
+ * other arrays are host memory; any of them except `embeddings` may be NULL. */
+typedef struct {
+  float* embeddings;            /* n_obs x n_components, row-major */
+  float* components;            /* n_components x n_vars, row-major */
+  double* variance_explained;   /* n_components: sigma^2 / (n_obs - 1) */
+  double* variance_ratio;       /* n_components */
+  double* singular_values;      /* n_components */
+  double* mean;                 /* n_vars: column means of the input matrix */
+  double* std;                  /* n_vars: per-gene std used for scaling */
+  int32_t embeddings_memory;    /* scxpca_memory */
+  int32_t resident_csr;         /* out: 1, the matrix was resident on device */
+  int32_t total_var_recomputed; /* out: 1 when the cancellation guard fired */
+  int32_t shifted_cholesky;     /* out: number of shifted Gram factorisations */
+  double total_var;             /* out: total variance used for the ratios */
+} scxpca_result;
+
+typedef struct scxpca_plan scxpca_plan;
+
+/* Human-readable name of a status code (static storage). */
+const char* scxpca_status_string(int32_t status);
+
+/* ABI version of the loaded library (SCXPCA_ABI_VERSION). */
+int32_t scxpca_abi_version(void);
+
+/* One-shot randomized PCA.  Replaces scx_gpu::gpu_randomized_pca
+ * (scx-gpu/src/gpu_pca.rs:706-763) and gpu_randomized_pca_device
+ * (gpu_pca.rs:775-838) -- device embeddings when embeddings_memory is DEVICE --
+ * as wrapped by scx_accel::randomized_pca_gpu (scx-accel/src/pca/gpu.rs:51-95).
+ * Builds a plan, runs it, destroys it; all device memory is released on
+ * return.  `err` (may be NULL) receives a NUL-terminated message. */
+int32_t scxpca_randomized(const scxpca_csr* x, const scxpca_params* params,
+                          scxpca_result* out, char* err, size_t err_len);
+
+/* Resident plan: validates the CSR, uploads or borrows it (a device CSR whose
+ * values already have the compute type is borrowed, never copied), applies the
+ * per-gene statistics and value transform once, and allocates every buffer a
+ * run needs.  Replaces try_build_resident_csr + ResidentPcaOperator +
+ * GpuPcaScratch (scx-gpu/src/gpu_pca_resident.rs:87-283,
+ * gpu_pca.rs:57-73).  A borrowed device CSR must outlive the plan. */
+int32_t scxpca_plan_create(const scxpca_csr* x, const scxpca_params* params,
+                           scxpca_plan** plan, char* err, size_t err_len);
+
+/* Run the power loop and the Rayleigh-Ritz step on a resident plan
+ * (run_resident_power_loop, gpu_pca_resident.rs:295-347, then
+ * randomized_pca_core steps 7-8, gpu_pca.rs:590-697).  Only `seed`, `omega`,
+ * `omega_memory` and `n_power_iterations` of `params` may differ from the
+ * values the plan was created with; NULL reuses the creation parameters. */
+int32_t scxpca_plan_run(scxpca_plan* plan, const scxpca_params* params,
+                        scxpca_result* out, char* err, size_t err_len);
+
+void scxpca_plan_destroy(scxpca_plan* plan);
+
+/* Plan geometry: k (sketch width), ld (padded row stride of the tall
+ * buffers), bytes of device memory the plan holds. */
+int32_t scxpca_plan_info(const scxpca_plan* plan, int64_t* k, int64_t* ld,
+                         int64_t* device_bytes);
+
+/* Operator seam (scx-gpu/src/pca_operator.rs:69-79, PcaOperator), on device
+ * buffers of the plan's device, ordered on the plan's stream:
+ *   matmat : Y = (X - 1 mu^T) V      V: n_vars x k row-major (ld_v >= k),
+ *                                    Y: n_obs x k row-major (ld_y >= k)
+ *            (spmm_forward_segment + forward_mean_prefactor +
+ *             mean_correct kernel, gpu_pca.rs:218-289, colmajor_ops.cu:41-57)
+ *   rmatmat: Z = (X - 1 mu^T)^T Q    Q: n_obs x k row-major (ld_q >= k),
+ *                                    Z: n_vars x k row-major double (ld_z >= k)
+ *            (spmm_transpose_segment + transpose_centering_correction,
+ *             gpu_pca.rs:302-346, colmajor_ops.cu:78-134, 248-263)
+ *   qr     : A (m x k row-major float, ld_a >= k) <- Q factor of A, in place
+ *            (gpu_qr_q / gpu_cholesky_qr2, scx-gpu/src/cusolver.rs:87-409)
+ * X here is the plan's working matrix (after scaling, in the compute type).
+ * The calls synchronise the plan's stream before returning. */
+int32_t scxpca_plan_matmat(scxpca_plan* plan, const float* v, int64_t ld_v, float* y,
+                           int64_t ld_y, char* err, size_t err_len);
+int32_t scxpca_plan_rmatmat(scxpca_plan* plan, const float* q, int64_t ld_q, double* z,
+                            int64_t ld_z, char* err, size_t err_len);
+int32_t scxpca_plan_qr(scxpca_plan* plan, float* a, int64_t m, int64_t ld_a,
+                       char* err, size_t err_len);
+
+/* Per-gene statistics of the plan's working matrix: column sums and sums of
+ * squares in FP64, host outputs (n_vars each).  Replaces
+ * col_means_and_sum_sq_prefetched (scx-format-io/src/prefetch.rs:616-650) and
+ * ScxCsr::col_sums_and_sum_sq (scx-sparse/src/csr.rs:570-580). */
+int32_t scxpca_plan_col_stats(scxpca_plan* plan, double* col_sums, double* col_sum_sq,
+                              char* err, size_t err_len);
+
+/* Seeded N(0,1) test matrix, n_rows x n_cols column-major float32, into device
+ * memory `out` on `device_ordinal`.  Replaces random_gaussian_gpu
+ * (scx-gpu/src/curand.rs:76-157); the stream is Philox4x32-10 + Box-Muller,
+ * not cuRAND XORWOW, so values differ from the reference's at equal seeds. */
+int32_t scxpca_gaussian(int32_t device_ordinal, uint64_t seed, int64_t n_rows, int64_t n_cols,
+                        float* out, char* err, size_t err_len);
+
+/* Seeded synthetic negative-binomial CSR generated on the device (benchmark
+ * input; no reference counterpart).  mu_g ~ LogNormal(loc, 1.5), s_c ~
+ * LogNormal(0, 0.5), counts ~ NB(mu_g s_c, dispersion), values =
+ * log1p(1e4 * count / rowsum) as float32, rows sorted by gene.  Call with
+ * indices == NULL and values == NULL first to obtain *nnz_out and fill
+ * `indptr` (device, n_obs + 1); then again with device buffers of *nnz_out
+ * entries. */
+int32_t scxpca_synth_nb_csr(int32_t device_ordinal, uint64_t seed, int64_t n_obs,
+                            int64_t n_vars, double loc, double dispersion, int64_t* indptr,
+                            int32_t* indices, float* values, int64_t* nnz_out, char* err,
+                            size_t err_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCXPCA_H */

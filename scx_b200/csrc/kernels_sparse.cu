@@ -1,0 +1,395 @@
+// Sparse-side kernels: per-gene statistics, value transforms, the forward
+// product Y = (X - 1 mu^T) V and the transposed product W = X^T Q on the
+// CUDA cores (FP32 products, FP32/FP64 accumulation).
+//
+// Layouts (all device memory):
+//   CSR    : int64 indptr[n+1], int32 indices[nnz], values[nnz] (f32/bf16/f16)
+//   V      : float [n_vars][ld]   gene-major, ld = k padded to 32, pad = 0
+//   Y, Q   : float [n_obs][ld]    cell-major
+//   partial: float [n_chunks][n_vars][ld] per-chunk partial X^T Q
+#include "common.cuh"
+#include "launch.h"
+
+namespace scx {
+
+// ---------------------------------------------------------------------------
+// Per-gene sums and sums of squares (FP64).  The nnz range is split evenly
+// across blocks; each block accumulates in shared memory and writes one
+// partial row pair, reduced in fixed block order by reduce_rows_f64.
+// Restates ScxCsr::col_sums_and_sum_sq (scx-sparse/src/csr.rs:570-580).
+// ---------------------------------------------------------------------------
+template <typename ValT>
+__global__ void k_col_stats(const int32_t* __restrict__ idx, const ValT* __restrict__ val,
+                            int64_t nnz, int32_t g, double* __restrict__ partial) {
+  extern __shared__ double sm[];  // [2][g]
+  for (int i = threadIdx.x; i < 2 * g; i += blockDim.x) sm[i] = 0.0;
+  __syncthreads();
+  int64_t per = (nnz + gridDim.x - 1) / gridDim.x;
+  int64_t s = (int64_t)blockIdx.x * per;
+  int64_t e = min(nnz, s + per);
+  for (int64_t p = s + threadIdx.x; p < e; p += blockDim.x) {
+    int32_t j = __ldg(idx + p);
+    double x = (double)to_f32(val[p]);
+    atomicAdd(&sm[j], x);
+    atomicAdd(&sm[g + j], x * x);
+  }
+  __syncthreads();
+  double* out = partial + (int64_t)blockIdx.x * 2 * g;
+  for (int i = threadIdx.x; i < 2 * g; i += blockDim.x) out[i] = sm[i];
+}
+
+// Wide matrices (too many genes for shared memory): FP64 global atomics.
+template <typename ValT>
+__global__ void k_col_stats_global(const int32_t* __restrict__ idx, const ValT* __restrict__ val,
+                                   int64_t nnz, int32_t g, double* __restrict__ out) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nnz;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    int32_t j = __ldg(idx + p);
+    double x = (double)to_f32(val[p]);
+    atomicAdd(&out[j], x);
+    atomicAdd(&out[g + j], x * x);
+  }
+}
+
+// out[i] = sum_{b < nparts} part[b * len + i], summed in b order (deterministic).
+template <typename T>
+__global__ void k_reduce_rows(const T* __restrict__ part, int nparts, int64_t len,
+                              double* __restrict__ out, int accumulate) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double acc = accumulate ? out[i] : 0.0;
+    for (int b = 0; b < nparts; ++b) acc += (double)part[(int64_t)b * len + i];
+    out[i] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Value transform: convert to the compute type, optionally scale and clip.
+//   mode 0: p = x
+//   mode 1 (scale, centred):   p = clip((x - mu) * inv_std, +-clip) - c_g
+//   mode 2 (scale, uncentred): p = min(x * inv_std, clip)
+// c_g = clip(-mu * inv_std) is the value every stored zero takes, so the dense
+// scaled matrix is P + 1 c^T with P on X's sparsity pattern.
+// ---------------------------------------------------------------------------
+template <typename InT, typename OutT>
+__global__ void k_transform_values(const int32_t* __restrict__ idx, const InT* __restrict__ in,
+                                   OutT* __restrict__ out, int64_t nnz, int mode,
+                                   const double* __restrict__ mu, const double* __restrict__ inv_std,
+                                   const double* __restrict__ cshift, double clip) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nnz;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    double x = (double)to_f32(in[p]);
+    if (mode != 0) {
+      int32_t j = __ldg(idx + p);
+      double is = __ldg(inv_std + j);
+      if (mode == 1) {
+        double s = (x - __ldg(mu + j)) * is;
+        if (clip > 0.0) s = fmin(fmax(s, -clip), clip);
+        x = s - __ldg(cshift + j);
+      } else {
+        x = x * is;
+        if (clip > 0.0) x = fmin(x, clip);
+      }
+    }
+    out[p] = from_f32<OutT>((float)x);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Forward product Y[i, :] = sum_p x_p V[j_p, :] - mc.  One warp per row; lane
+// l owns columns l + 32 c.  Nonzeros are fetched 32 at a time (coalesced) and
+// broadcast by shuffle; V rows are read through the read-only cache (V is
+// n_vars x ld x 4 bytes, L2-resident).
+// Restates spmm_forward_row (scx-accel/src/pca/cpu.rs:1500-1523) with the
+// mean correction of forward_mean_prefactor (scx-gpu/src/gpu_pca.rs:218-237).
+// ---------------------------------------------------------------------------
+template <int C, typename ValT>
+__global__ void __launch_bounds__(256) k_spmm_fwd(const int64_t* __restrict__ indptr,
+                                                  const int32_t* __restrict__ idx,
+                                                  const ValT* __restrict__ val, int64_t n_obs,
+                                                  const float* __restrict__ V, int ldv,
+                                                  const float* __restrict__ mc,
+                                                  float* __restrict__ Y, int ldy) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  float m[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) m[c] = mc ? mc[lane + 32 * c] : 0.f;
+  for (int64_t row = warp; row < n_obs; row += nwarps) {
+    const int64_t s = indptr[row], e = indptr[row + 1];
+    float acc[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[c] = 0.f;
+    for (int64_t base = s; base < e; base += 32) {
+      const int64_t p = base + lane;
+      int32_t j = 0;
+      float x = 0.f;
+      if (p < e) {
+        j = __ldg(idx + p);
+        x = to_f32(val[p]);
+      }
+      const int cnt = (int)min((int64_t)32, e - base);
+      int t = 0;
+      for (; t + 4 <= cnt; t += 4) {
+        int jj[4];
+        float xx[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          jj[u] = __shfl_sync(0xffffffffu, j, t + u);
+          xx[u] = __shfl_sync(0xffffffffu, x, t + u);
+        }
+        float vv[4][C];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int c = 0; c < C; ++c) vv[u][c] = __ldg(V + (int64_t)jj[u] * ldv + lane + 32 * c);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int c = 0; c < C; ++c) acc[c] = fmaf(xx[u], vv[u][c], acc[c]);
+      }
+      for (; t < cnt; ++t) {
+        const int jt = __shfl_sync(0xffffffffu, j, t);
+        const float xt = __shfl_sync(0xffffffffu, x, t);
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] = fmaf(xt, __ldg(V + (int64_t)jt * ldv + lane + 32 * c), acc[c]);
+      }
+    }
+    float* yr = Y + row * (int64_t)ldy;
+#pragma unroll
+    for (int c = 0; c < C; ++c) yr[lane + 32 * c] = acc[c] - m[c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row-block pointer table for the transposed product: for row i and gene
+// block b, rbp[i * (nb + 1) + b] = offset (from indptr[i]) of the first stored
+// entry of row i whose gene is >= b * gb.  Rows must be sorted by gene.
+// ---------------------------------------------------------------------------
+__global__ void k_row_block_ptr(const int64_t* __restrict__ indptr, const int32_t* __restrict__ idx,
+                                int64_t n_obs, int nb, int gb, int32_t* __restrict__ rbp) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = warp; row < n_obs; row += nwarps) {
+    const int64_t s = indptr[row], e = indptr[row + 1];
+    for (int b = lane; b <= nb; b += 32) {
+      const int32_t key = b * gb;
+      int64_t lo = s, hi = e;  // first position with idx >= key
+      while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (__ldg(idx + mid) < key) lo = mid + 1; else hi = mid;
+      }
+      rbp[row * (nb + 1) + b] = (int32_t)(lo - s);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Transposed product, CUDA-core path: block (chunk, b) owns genes
+// [b*GB, (b+1)*GB) and the rows of one chunk, accumulates W_part[gene, :] in
+// shared memory (FP32 shared atomics) and writes one partial.  Partials are
+// reduced in fixed chunk order into FP64 by k_reduce_rows.
+// Restates spmm_transpose_block (scx-accel/src/pca/cpu.rs:1282-1328).
+// ---------------------------------------------------------------------------
+template <int C, typename ValT, int GB>
+__global__ void __launch_bounds__(512) k_spmm_t(const int64_t* __restrict__ indptr,
+                                                const int32_t* __restrict__ idx,
+                                                const ValT* __restrict__ val, int64_t n_obs,
+                                                int32_t g, const int32_t* __restrict__ rbp, int nb,
+                                                int64_t rows_per_chunk,
+                                                const float* __restrict__ Q, int ldq,
+                                                float* __restrict__ part) {
+  constexpr int LD = 32 * C;
+  extern __shared__ float acc[];  // [GB][LD]
+  const int b = blockIdx.y;
+  const int chunk = blockIdx.x;
+  for (int i = threadIdx.x; i < GB * LD; i += blockDim.x) acc[i] = 0.f;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int wid = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const int64_t r0 = (int64_t)chunk * rows_per_chunk;
+  const int64_t r1 = min(n_obs, r0 + rows_per_chunk);
+  const int g0 = b * GB;
+  for (int64_t row = r0 + wid; row < r1; row += nw) {
+    const int64_t base_row = indptr[row];
+    const int32_t* rb = rbp + row * (nb + 1);
+    const int64_t s = base_row + rb[b], e = base_row + rb[b + 1];
+    if (s >= e) continue;
+    float q[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) q[c] = __ldg(Q + row * (int64_t)ldq + lane + 32 * c);
+    for (int64_t base = s; base < e; base += 32) {
+      const int64_t p = base + lane;
+      int32_t j = 0;
+      float x = 0.f;
+      if (p < e) {
+        j = __ldg(idx + p) - g0;
+        x = to_f32(val[p]);
+      }
+      const int cnt = (int)min((int64_t)32, e - base);
+      for (int t = 0; t < cnt; ++t) {
+        const int jt = __shfl_sync(0xffffffffu, j, t);
+        const float xt = __shfl_sync(0xffffffffu, x, t);
+        float* a = acc + jt * LD + lane;
+#pragma unroll
+        for (int c = 0; c < C; ++c) atomicAdd(a + 32 * c, xt * q[c]);
+      }
+    }
+  }
+  __syncthreads();
+  float* out = part + (int64_t)chunk * g * LD;
+  const int ng = min(GB, g - g0);
+  for (int i = threadIdx.x; i < ng * LD; i += blockDim.x) out[(int64_t)g0 * LD + i] = acc[i];
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+template <typename ValT>
+static cudaError_t col_stats_t(const int32_t* idx, const void* val, int64_t nnz, int32_t g,
+                               double* partial, int nparts, double* out, cudaStream_t st,
+                               int num_sms) {
+  const ValT* v = static_cast<const ValT*>(val);
+  size_t smem = (size_t)2 * g * sizeof(double);
+  if (smem <= kStatsSmemMax) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_col_stats<ValT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_col_stats<ValT><<<nparts, 512, smem, st>>>(idx, v, nnz, g, partial);
+    k_reduce_rows<double><<<grid_for(2 * g, 256, num_sms), 256, 0, st>>>(partial, nparts, 2 * g, out, 0);
+  } else {
+    cudaMemsetAsync(out, 0, sizeof(double) * 2 * g, st);
+    k_col_stats_global<ValT><<<grid_for(nnz, 256, num_sms), 256, 0, st>>>(idx, v, nnz, g, out);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_col_stats(int dtype, const int32_t* idx, const void* val, int64_t nnz,
+                             int32_t g, double* partial, int nparts, double* out,
+                             cudaStream_t st, int num_sms) {
+  switch (dtype) {
+    case 0: return col_stats_t<float>(idx, val, nnz, g, partial, nparts, out, st, num_sms);
+    case 1: return col_stats_t<__nv_bfloat16>(idx, val, nnz, g, partial, nparts, out, st, num_sms);
+    default: return col_stats_t<__half>(idx, val, nnz, g, partial, nparts, out, st, num_sms);
+  }
+}
+
+template <typename InT>
+static cudaError_t transform_in(int out_dtype, const int32_t* idx, const void* in, void* out,
+                                int64_t nnz, int mode, const double* mu, const double* inv_std,
+                                const double* cshift, double clip, cudaStream_t st, int num_sms) {
+  const InT* src = static_cast<const InT*>(in);
+  int grid = grid_for(nnz, 256, num_sms);
+  switch (out_dtype) {
+    case 0: k_transform_values<InT, float><<<grid, 256, 0, st>>>(idx, src, (float*)out, nnz, mode, mu, inv_std, cshift, clip); break;
+    case 1: k_transform_values<InT, __nv_bfloat16><<<grid, 256, 0, st>>>(idx, src, (__nv_bfloat16*)out, nnz, mode, mu, inv_std, cshift, clip); break;
+    default: k_transform_values<InT, __half><<<grid, 256, 0, st>>>(idx, src, (__half*)out, nnz, mode, mu, inv_std, cshift, clip); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transform_values(int in_dtype, int out_dtype, const int32_t* idx, const void* in,
+                                    void* out, int64_t nnz, int mode, const double* mu,
+                                    const double* inv_std, const double* cshift, double clip,
+                                    cudaStream_t st, int num_sms) {
+  if (nnz == 0) return cudaSuccess;
+  switch (in_dtype) {
+    case 0: return transform_in<float>(out_dtype, idx, in, out, nnz, mode, mu, inv_std, cshift, clip, st, num_sms);
+    case 1: return transform_in<__nv_bfloat16>(out_dtype, idx, in, out, nnz, mode, mu, inv_std, cshift, clip, st, num_sms);
+    default: return transform_in<__half>(out_dtype, idx, in, out, nnz, mode, mu, inv_std, cshift, clip, st, num_sms);
+  }
+}
+
+template <int C, typename ValT>
+static cudaError_t fwd_c(const int64_t* indptr, const int32_t* idx, const void* val, int64_t n,
+                         const float* V, int ldv, const float* mc, float* Y, int ldy,
+                         cudaStream_t st, int num_sms) {
+  int grid = grid_for(n * 32, 256, num_sms, 8);
+  k_spmm_fwd<C, ValT><<<grid, 256, 0, st>>>(indptr, idx, static_cast<const ValT*>(val), n, V, ldv,
+                                            mc, Y, ldy);
+  return cudaGetLastError();
+}
+
+template <typename ValT>
+static cudaError_t fwd_t(int ld, const int64_t* indptr, const int32_t* idx, const void* val,
+                         int64_t n, const float* V, int ldv, const float* mc, float* Y, int ldy,
+                         cudaStream_t st, int num_sms) {
+  switch (ld) {
+    case 32: return fwd_c<1, ValT>(indptr, idx, val, n, V, ldv, mc, Y, ldy, st, num_sms);
+    case 64: return fwd_c<2, ValT>(indptr, idx, val, n, V, ldv, mc, Y, ldy, st, num_sms);
+    case 96: return fwd_c<3, ValT>(indptr, idx, val, n, V, ldv, mc, Y, ldy, st, num_sms);
+    default: return fwd_c<4, ValT>(indptr, idx, val, n, V, ldv, mc, Y, ldy, st, num_sms);
+  }
+}
+
+cudaError_t launch_spmm_fwd(int dtype, int ld, const int64_t* indptr, const int32_t* idx,
+                            const void* val, int64_t n, const float* V, const float* mc,
+                            float* Y, cudaStream_t st, int num_sms) {
+  if (n == 0) return cudaSuccess;
+  switch (dtype) {
+    case 0: return fwd_t<float>(ld, indptr, idx, val, n, V, ld, mc, Y, ld, st, num_sms);
+    case 1: return fwd_t<__nv_bfloat16>(ld, indptr, idx, val, n, V, ld, mc, Y, ld, st, num_sms);
+    default: return fwd_t<__half>(ld, indptr, idx, val, n, V, ld, mc, Y, ld, st, num_sms);
+  }
+}
+
+cudaError_t launch_row_block_ptr(const int64_t* indptr, const int32_t* idx, int64_t n, int nb,
+                                 int gb, int32_t* rbp, cudaStream_t st, int num_sms) {
+  if (n == 0) return cudaSuccess;
+  k_row_block_ptr<<<grid_for(n * 32, 256, num_sms, 8), 256, 0, st>>>(indptr, idx, n, nb, gb, rbp);
+  return cudaGetLastError();
+}
+
+template <int C, typename ValT>
+static cudaError_t spmm_t_c(const int64_t* indptr, const int32_t* idx, const void* val, int64_t n,
+                            int32_t g, const int32_t* rbp, int nb, int nchunks,
+                            int64_t rows_per_chunk, const float* Q, int ldq, float* part,
+                            cudaStream_t st) {
+  constexpr int GB = kTransposeGeneBlock;
+  size_t smem = (size_t)GB * 32 * C * sizeof(float);
+  auto kern = k_spmm_t<C, ValT, GB>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 grid(nchunks, nb);
+  kern<<<grid, 512, smem, st>>>(indptr, idx, static_cast<const ValT*>(val), n, g, rbp, nb,
+                                rows_per_chunk, Q, ldq, part);
+  return cudaGetLastError();
+}
+
+template <typename ValT>
+static cudaError_t spmm_t_t(int ld, const int64_t* indptr, const int32_t* idx, const void* val,
+                            int64_t n, int32_t g, const int32_t* rbp, int nb, int nchunks,
+                            int64_t rpc, const float* Q, float* part, cudaStream_t st) {
+  switch (ld) {
+    case 32: return spmm_t_c<1, ValT>(indptr, idx, val, n, g, rbp, nb, nchunks, rpc, Q, ld, part, st);
+    case 64: return spmm_t_c<2, ValT>(indptr, idx, val, n, g, rbp, nb, nchunks, rpc, Q, ld, part, st);
+    case 96: return spmm_t_c<3, ValT>(indptr, idx, val, n, g, rbp, nb, nchunks, rpc, Q, ld, part, st);
+    default: return spmm_t_c<4, ValT>(indptr, idx, val, n, g, rbp, nb, nchunks, rpc, Q, ld, part, st);
+  }
+}
+
+cudaError_t launch_spmm_t(int dtype, int ld, const int64_t* indptr, const int32_t* idx,
+                          const void* val, int64_t n, int32_t g, const int32_t* rbp, int nb,
+                          int nchunks, int64_t rows_per_chunk, const float* Q, float* part,
+                          cudaStream_t st) {
+  switch (dtype) {
+    case 0: return spmm_t_t<float>(ld, indptr, idx, val, n, g, rbp, nb, nchunks, rows_per_chunk, Q, part, st);
+    case 1: return spmm_t_t<__nv_bfloat16>(ld, indptr, idx, val, n, g, rbp, nb, nchunks, rows_per_chunk, Q, part, st);
+    default: return spmm_t_t<__half>(ld, indptr, idx, val, n, g, rbp, nb, nchunks, rows_per_chunk, Q, part, st);
+  }
+}
+
+cudaError_t launch_reduce_rows_f32(const float* part, int nparts, int64_t len, double* out,
+                                   int accumulate, cudaStream_t st, int num_sms) {
+  k_reduce_rows<float><<<grid_for(len, 256, num_sms), 256, 0, st>>>(part, nparts, len, out, accumulate);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_rows_f64(const double* part, int nparts, int64_t len, double* out,
+                                   int accumulate, cudaStream_t st, int num_sms) {
+  k_reduce_rows<double><<<grid_for(len, 256, num_sms), 256, 0, st>>>(part, nparts, len, out, accumulate);
+  return cudaGetLastError();
+}
+
+}  // namespace scx

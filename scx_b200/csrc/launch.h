@@ -1,0 +1,111 @@
+// Host-side launcher declarations shared by the kernel translation units and
+// the plan orchestration (scxpca.cu).  All launchers enqueue on `st` and
+// return the launch status; none synchronises.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace scx {
+
+constexpr size_t kStatsSmemMax = 200 * 1024;  // per-block FP64 gene accumulators
+constexpr int kTransposeGeneBlock = 256;       // genes per block, CUDA-core transposed product
+
+// ---- sparse side (kernels_sparse.cu) ----
+cudaError_t launch_col_stats(int dtype, const int32_t* idx, const void* val, int64_t nnz,
+                             int32_t g, double* partial, int nparts, double* out,
+                             cudaStream_t st, int num_sms);
+cudaError_t launch_transform_values(int in_dtype, int out_dtype, const int32_t* idx,
+                                    const void* in, void* out, int64_t nnz, int mode,
+                                    const double* mu, const double* inv_std,
+                                    const double* cshift, double clip, cudaStream_t st,
+                                    int num_sms);
+cudaError_t launch_spmm_fwd(int dtype, int ld, const int64_t* indptr, const int32_t* idx,
+                            const void* val, int64_t n, const float* V, const float* mc,
+                            float* Y, cudaStream_t st, int num_sms);
+cudaError_t launch_row_block_ptr(const int64_t* indptr, const int32_t* idx, int64_t n, int nb,
+                                 int gb, int32_t* rbp, cudaStream_t st, int num_sms);
+cudaError_t launch_spmm_t(int dtype, int ld, const int64_t* indptr, const int32_t* idx,
+                          const void* val, int64_t n, int32_t g, const int32_t* rbp, int nb,
+                          int nchunks, int64_t rows_per_chunk, const float* Q, float* part,
+                          cudaStream_t st);
+cudaError_t launch_reduce_rows_f32(const float* part, int nparts, int64_t len, double* out,
+                                   int accumulate, cudaStream_t st, int num_sms);
+cudaError_t launch_reduce_rows_f64(const double* part, int nparts, int64_t len, double* out,
+                                   int accumulate, cudaStream_t st, int num_sms);
+
+// ---- CSR validation (kernels_csr.cu) ----
+// flags[0]: bad indptr (non-monotone / out of range), flags[1]: column index
+// out of range, flags[2]: a row not sorted strictly ascending (duplicates or
+// disorder), flags[3]: non-finite value.
+cudaError_t launch_validate_csr(int dtype, const int64_t* indptr, const int32_t* idx,
+                                const void* val, int64_t n, int64_t g, int64_t nnz,
+                                int32_t* flags, cudaStream_t st, int num_sms);
+// Sort every row by gene in place (values follow), one warp per row.
+cudaError_t launch_sort_rows(int dtype, const int64_t* indptr, int32_t* idx, void* val,
+                             int64_t n, cudaStream_t st, int num_sms);
+
+// ---- dense side (kernels_dense.cu) ----
+// Gram partials of a tall row-major matrix A (n x ld, first k columns used):
+// part[b] = [A_b^T A_b (ld x ld), colsum(A_b) (ld)] in FP64.
+cudaError_t launch_gram_f32(const float* A, int64_t n, int ld, double* part, int nparts,
+                            cudaStream_t st);
+cudaError_t launch_gram_f64(const double* A, int64_t n, int ld, double* part, int nparts,
+                            cudaStream_t st);
+// Cholesky G = R^T R of the leading k x k block (single block).  Writes R and
+// R^{-1} (ld x ld, zero outside the leading upper triangle; R^{-1} pad
+// diagonal = 0), plus R^{-1} as float.  status[0] += 1 on a shifted
+// factorisation (shift_on_fail) or is set to -(j+1) on a failed pivot j.
+cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shift_on_fail,
+                            double* R, double* Rinv, float* Rinv_f, int* status, cudaStream_t st);
+// Tall apply: Out[i, :] = In[i, :] * M (ld x ld float, upper-triangular or full).
+cudaError_t launch_apply_right_f32(const float* In, int64_t n, int ld, const float* M,
+                                   float* Out, cudaStream_t st, int num_sms);
+// Gene-side ops (n_vars x ld, FP64):
+//   Z = (W - mu s^T) M        (mu may be null)
+cudaError_t launch_center_apply(const double* W, int64_t g, int ld, const double* mu,
+                                const double* s, const double* M, double* Z, cudaStream_t st);
+//   A = A * M  in place (FP64)
+cudaError_t launch_apply_right_f64(double* A, int64_t g, int ld, const double* M,
+                                   cudaStream_t st);
+//   Vf = (float)A ; mc = A^T mu (float, from the rounded Vf) ; mu may be null
+cudaError_t launch_round_v(const double* A, int64_t g, int ld, const double* mu, float* Vf,
+                           float* mc, cudaStream_t st);
+//   mc = Vf^T mu for a float V (mu may be null -> zeros)
+cudaError_t launch_mean_prefactor(const float* Vf, int64_t g, int ld, const double* mu,
+                                  float* mc, cudaStream_t st);
+// Symmetric eigendecomposition (parallel cyclic Jacobi, single block) of the
+// leading k x k block of C (ld x ld FP64).  evals descending, evecs columns.
+cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, double* evecs,
+                              int* sweeps, cudaStream_t st);
+// Rayleigh-Ritz finish: sigma = sqrt(max(evals,0)); components[c][j] =
+// (B E)[j][c] / sigma_c (c < nc); M_emb = Rinv2 * E[:, :nc] * diag(sigma)
+// (ld x nc, float).
+cudaError_t launch_ritz_finish(const double* B, int64_t g, int ld, int k, int nc,
+                               const double* evals, const double* evecs, const double* Rinv2,
+                               double* sigma, float* components, float* M_emb,
+                               cudaStream_t st);
+// Embeddings U (n x nc row-major) = Q (n x ld) * M_emb (ld x nc).
+cudaError_t launch_embed(const float* Q, int64_t n, int ld, int k, const float* M_emb, int nc,
+                         float* U, cudaStream_t st, int num_sms);
+// Seeded Gaussian n_rows x n_cols column-major into out (ld_out = n_rows) or,
+// when ld_pad > 0, into a gene-major padded buffer out[i * ld_pad + j].
+cudaError_t launch_gaussian(uint64_t seed, int64_t n_rows, int64_t n_cols, float* out,
+                            int ld_pad, cudaStream_t st, int num_sms);
+// Copy a column-major n_rows x n_cols float matrix into a row-major padded one.
+cudaError_t launch_colmajor_to_padded(const float* in, int64_t n_rows, int64_t n_cols, int ld,
+                                      float* out, cudaStream_t st, int num_sms);
+
+// ---- synthetic generator (synth.cu) ----
+cudaError_t launch_synth_count(uint64_t seed, int64_t n, int64_t g, double loc, double disp,
+                               const float* mu_g, int64_t* row_nnz, float* rowsum,
+                               cudaStream_t st, int num_sms);
+cudaError_t launch_synth_fill(uint64_t seed, int64_t n, int64_t g, double loc, double disp,
+                              const float* mu_g, const int64_t* indptr, const float* rowsum,
+                              int32_t* idx, float* val, cudaStream_t st, int num_sms);
+cudaError_t launch_synth_gene_means(uint64_t seed, int64_t g, double loc, float* mu_g,
+                                    cudaStream_t st);
+cudaError_t launch_exclusive_scan_i64(const int64_t* in, int64_t n, int64_t* out,
+                                      cudaStream_t st);
+
+}  // namespace scx

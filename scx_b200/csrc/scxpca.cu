@@ -1,0 +1,828 @@
+// Host orchestration and C ABI of the randomized PCA (libscxpca.so).
+//
+// A plan owns (or borrows) the device CSR, its per-gene statistics and every
+// work buffer; running it enqueues the whole power loop and Rayleigh-Ritz
+// step on one stream with no host synchronisation until the end.
+//
+// Power loop (same step order as run_power_loop,
+// scx-gpu/src/pca_operator.rs:100-119):
+//   Y = (X - mu) Omega ; qr(Y) ; [ Z = (X - mu)^T Q ; qr(Z) ; Y = (X - mu) Z ;
+//   qr(Y) ] x q ; B = (X - mu)^T Q
+// qr(Y) is a Cholesky QR whose Gram Y^T Y is accumulated in FP64 from the
+// stored FP32 Y; inside the loop Q = Y R^{-1} stays implicit
+// (Z = (X^T Y - mu (1^T Y)^T) R^{-1}), and the last Q is formed explicitly
+// and re-orthonormalised (second Cholesky pass folded into B and the
+// embeddings) before the final projection.  qr(Z) is CholeskyQR2 in FP64.
+// The SVD of B is an FP64 Jacobi eigendecomposition of B^T B on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/scxpca.h"
+#include "common.cuh"
+#include "launch.h"
+
+using namespace scx;
+
+namespace {
+
+struct Failure {
+  int32_t code;
+  std::string msg;
+};
+
+[[noreturn]] void fail(int32_t code, const std::string& msg) { throw Failure{code, msg}; }
+
+void ck(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();
+  int32_t code = (e == cudaErrorMemoryAllocation) ? SCXPCA_OUT_OF_MEMORY : SCXPCA_CUDA_ERROR;
+  fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(expr) ck((expr), #expr)
+
+void write_err(char* err, size_t len, const std::string& msg) {
+  if (!err || len == 0) return;
+  size_t n = std::min(len - 1, msg.size());
+  memcpy(err, msg.data(), n);
+  err[n] = '\0';
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+      fail(SCXPCA_CUDA_ERROR, "no CUDA device is available");
+    if (dev < 0 || dev >= count)
+      fail(SCXPCA_INVALID_ARGUMENT, "device_ordinal " + std::to_string(dev) + " out of range (" +
+                                        std::to_string(count) + " devices)");
+    CK(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  void alloc(size_t b) {
+    if (b <= bytes && p) return;
+    release();
+    if (b == 0) b = 16;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      fail(SCXPCA_OUT_OF_MEMORY, "device allocation of " + std::to_string(b) + " bytes failed: " +
+                                     cudaGetErrorString(e));
+    }
+    bytes = b;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+size_t dtype_size(int dt) { return dt == SCXPCA_F32 ? 4 : 2; }
+
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+struct scxpca_plan {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  scxpca_params params{};
+  int64_t n = 0, g = 0, nnz = 0, k = 0, ld = 0, nc = 0;
+  int in_dtype = 0, dtype = 0;  // input and compute value types
+  bool centered = true;
+  bool scaled = false;
+  double clip = 0.0;
+
+  const int64_t* indptr = nullptr;
+  const int32_t* idx = nullptr;
+  const void* val = nullptr;
+  DevBuf b_indptr, b_idx, b_val, b_stage;
+
+  // statistics
+  int stats_parts = 0;
+  DevBuf stats_part, stats_out, d_mu, d_inv_std, d_cshift;
+  std::vector<double> mean_x, std_x, col_sum, col_sq;  // working-matrix sums
+  double total_var = 0.0;
+  bool total_var_recomputed = false;
+
+  // transposed product
+  int nb = 0, nchunks = 0;
+  int64_t rows_per_chunk = 0;
+  DevBuf rbp, wpart;
+
+  // dense work
+  int gram_parts = 0, gram_parts_small = 0;
+  DevBuf Y, W, Z, V, mc, gpart, G, R, Rinv, Rinv_f, R2inv, eye, evals, evecs, sigma, comps,
+      M_emb, U, status, omega_stage;
+  size_t device_bytes = 0;
+
+  double tau = 1e-8;
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// validation of arguments (scx-accel/src/pca/cpu.rs:979-997; gpu_pca.rs:433-446)
+// ---------------------------------------------------------------------------
+void validate_params(const scxpca_csr* x, const scxpca_params* p) {
+  if (!x || !p) fail(SCXPCA_INVALID_ARGUMENT, "null csr or params");
+  if (x->n_obs < 0 || x->n_vars < 0 || x->nnz < 0)
+    fail(SCXPCA_INVALID_ARGUMENT, "negative matrix dimension");
+  if (p->n_components <= 0) fail(SCXPCA_INVALID_ARGUMENT, "n_components must be > 0");
+  if (x->n_obs == 0 || x->n_vars == 0) fail(SCXPCA_INVALID_ARGUMENT, "matrix must be non-empty");
+  int64_t mn = std::min(x->n_obs, x->n_vars);
+  if (p->n_components > mn)
+    fail(SCXPCA_INVALID_ARGUMENT, "n_components (" + std::to_string(p->n_components) +
+                                      ") exceeds matrix rank bound min(n_obs, n_vars) = " +
+                                      std::to_string(mn));
+  if (p->n_oversamples < 0 || p->n_power_iterations < 0)
+    fail(SCXPCA_INVALID_ARGUMENT, "n_oversamples and n_power_iterations must be >= 0");
+  if (x->n_vars > INT32_MAX) fail(SCXPCA_INVALID_ARGUMENT, "n_vars exceeds int32 index range");
+  if (x->values_dtype < 0 || x->values_dtype > 2) fail(SCXPCA_INVALID_ARGUMENT, "bad values_dtype");
+  if (p->math_mode < 0 || p->math_mode > 2) fail(SCXPCA_INVALID_ARGUMENT, "bad math_mode");
+  if (p->qr_method < 0 || p->qr_method > 1) fail(SCXPCA_INVALID_ARGUMENT, "bad qr_method");
+  if (x->nnz > 0 && (!x->indices || !x->values)) fail(SCXPCA_INVALID_ARGUMENT, "null CSR arrays");
+  if (!x->indptr) fail(SCXPCA_INVALID_ARGUMENT, "null indptr");
+  if (!std::isfinite(p->clip_max)) fail(SCXPCA_INVALID_ARGUMENT, "clip_max must be finite");
+  int64_t k = std::min({p->n_components + p->n_oversamples, x->n_vars, x->n_obs});
+  if (k > kMaxK)
+    fail(SCXPCA_UNSUPPORTED, "sketch width k = min(n_components + n_oversamples, n_vars, n_obs) = " +
+                                 std::to_string(k) + " exceeds the supported maximum " +
+                                 std::to_string(kMaxK));
+}
+
+void stats_pass(scxpca_plan* pl, const void* val, int dtype, std::vector<double>& sums,
+                std::vector<double>& sq) {
+  CK(launch_col_stats(dtype, pl->idx, val, pl->nnz, (int32_t)pl->g, pl->stats_part.as<double>(),
+                      pl->stats_parts, pl->stats_out.as<double>(), pl->stream, pl->num_sms));
+  std::vector<double> host(2 * pl->g);
+  CK(cudaMemcpyAsync(host.data(), pl->stats_out.p, sizeof(double) * 2 * pl->g,
+                     cudaMemcpyDeviceToHost, pl->stream));
+  CK(cudaStreamSynchronize(pl->stream));
+  sums.assign(host.begin(), host.begin() + pl->g);
+  sq.assign(host.begin() + pl->g, host.end());
+}
+
+void upload(DevBuf& buf, const std::vector<double>& v, cudaStream_t st) {
+  buf.alloc(sizeof(double) * v.size());
+  CK(cudaMemcpyAsync(buf.p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, st));
+}
+
+// Closed-form total variance with the cancellation guard
+// (scx-sparse/src/csr.rs:868-880, moments.rs:288-308, scx-accel cpu.rs:1066-1171).
+void compute_total_variance(scxpca_plan* pl) {
+  const double n = (double)pl->n;
+  const double denom = std::max(n - 1.0, 1.0);
+  double sumsq = 0.0, meansq = 0.0;
+  for (int64_t j = 0; j < pl->g; ++j) sumsq += pl->col_sq[j];
+  if (!pl->centered) {
+    pl->total_var = sumsq / denom;
+    return;
+  }
+  double total = 0.0;
+  std::vector<double> mu(pl->g);
+  for (int64_t j = 0; j < pl->g; ++j) {
+    mu[j] = pl->col_sum[j] / n;
+    total += pl->col_sq[j] - n * mu[j] * mu[j];
+    meansq += mu[j] * mu[j];
+  }
+  pl->total_var = total / denom;
+  if (sumsq <= 0.0) return;                          // degenerate: exact zero
+  if (!(sumsq - meansq * n <= 1e-7 * sumsq)) return;  // usable
+  // Cancelled: stable recompute sum (x - mu)^2 over stored entries plus
+  // implicit zeros (n - nnz_j) mu_j^2, on the device.
+  DevBuf dmu, shifted;
+  upload(dmu, mu, pl->stream);
+  shifted.alloc(sizeof(float) * std::max<int64_t>(pl->nnz, 1));
+  // (x - mu) in FP32 is exact enough for a variance that the FP64 closed form lost.
+  std::vector<double> zero(pl->g, 0.0), one(pl->g, 1.0);
+  DevBuf dz, d1;
+  upload(dz, zero, pl->stream);
+  upload(d1, one, pl->stream);
+  CK(launch_transform_values(pl->dtype, 0, pl->idx, pl->val, shifted.p, pl->nnz, 1, dmu.as<double>(),
+                             d1.as<double>(), dz.as<double>(), 0.0, pl->stream, pl->num_sms));
+  std::vector<double> s1, s2;
+  stats_pass(pl, shifted.p, 0, s1, s2);
+  // nnz per gene from sum x and sum (x - mu): nnz_j = (sum x - sum(x - mu)) / mu_j
+  double t = 0.0;
+  for (int64_t j = 0; j < pl->g; ++j) {
+    double nnz_j = (mu[j] != 0.0) ? std::round((pl->col_sum[j] - s1[j]) / mu[j]) : 0.0;
+    double zeros = std::max(n - nnz_j, 0.0);
+    t += s2[j] + zeros * mu[j] * mu[j];
+  }
+  pl->total_var = t / denom;
+  pl->total_var_recomputed = true;
+}
+
+scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
+  validate_params(x, p);
+  auto pl = new scxpca_plan();
+  try {
+    pl->device = p->device_ordinal;
+    CK(cudaDeviceGetAttribute(&pl->num_sms, cudaDevAttrMultiProcessorCount, pl->device));
+    pl->params = *p;
+    pl->n = x->n_obs;
+    pl->g = x->n_vars;
+    pl->nnz = x->nnz;
+    pl->k = std::min({p->n_components + p->n_oversamples, x->n_vars, x->n_obs});
+    pl->ld = padded_k(pl->k);
+    pl->nc = p->n_components;
+    pl->in_dtype = x->values_dtype;
+    pl->dtype = p->math_mode == SCXPCA_MATH_STRICT_FP32 ? SCXPCA_F32
+                : p->math_mode == SCXPCA_MATH_MIXED_BF16 ? SCXPCA_BF16
+                                                         : SCXPCA_F16;
+    pl->centered = p->zero_center != 0;
+    pl->scaled = p->scale != 0;
+    pl->clip = p->clip_max > 0 ? p->clip_max : 0.0;
+    if (p->stream) {
+      pl->stream = static_cast<cudaStream_t>(p->stream);
+    } else {
+      CK(cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking));
+      pl->own_stream = true;
+    }
+    cudaStream_t st = pl->stream;
+    const int64_t n = pl->n, g = pl->g, nnz = pl->nnz, ld = pl->ld;
+
+    // ---- pre-flight (gpu_pca.rs:450-462): resident CSR + work buffers ----
+    {
+      size_t need = (size_t)(n + 1) * 8 + (size_t)nnz * 4 + (size_t)nnz * dtype_size(pl->dtype) * 2 +
+                    (size_t)n * ld * 4 + (size_t)n * pl->nc * 4 + (size_t)n * 36 +
+                    (size_t)g * ld * 4 * 80;
+      size_t fr = 0, tot = 0;
+      CK(cudaMemGetInfo(&fr, &tot));
+      double with_headroom = (double)need * 1.1;
+      if (with_headroom > (double)fr)
+        fail(SCXPCA_OUT_OF_MEMORY, "GPU PCA requires ~" + std::to_string((size_t)with_headroom >> 20) +
+                                       " MB but only " + std::to_string(fr >> 20) +
+                                       " MB free on device");
+    }
+
+    // ---- resident CSR ----
+    const bool dev_in = x->memory == SCXPCA_MEM_DEVICE;
+    if (dev_in) {
+      pl->indptr = x->indptr;
+      pl->idx = x->indices;
+    } else {
+      pl->b_indptr.alloc(sizeof(int64_t) * (n + 1));
+      pl->b_idx.alloc(sizeof(int32_t) * std::max<int64_t>(nnz, 1));
+      CK(cudaMemcpyAsync(pl->b_indptr.p, x->indptr, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
+      if (nnz) CK(cudaMemcpyAsync(pl->b_idx.p, x->indices, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
+      pl->indptr = pl->b_indptr.as<int64_t>();
+      pl->idx = pl->b_idx.as<int32_t>();
+    }
+    const void* vin = x->values;
+    if (!dev_in && nnz) {
+      pl->b_stage.alloc(dtype_size(pl->in_dtype) * nnz);
+      CK(cudaMemcpyAsync(pl->b_stage.p, x->values, dtype_size(pl->in_dtype) * nnz,
+                         cudaMemcpyHostToDevice, st));
+      vin = pl->b_stage.p;
+    }
+
+    // ---- validation ----
+    {
+      DevBuf flags;
+      flags.alloc(16);
+      CK(cudaMemsetAsync(flags.p, 0, 16, st));
+      CK(launch_validate_csr(pl->in_dtype, pl->indptr, pl->idx, vin, n, g, nnz, flags.as<int32_t>(),
+                             st, pl->num_sms));
+      int32_t hf[4];
+      CK(cudaMemcpyAsync(hf, flags.p, 16, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (hf[0]) fail(SCXPCA_INVALID_CSR, "invalid CSR: indptr is not monotone within [0, nnz]");
+      if (hf[1]) fail(SCXPCA_INVALID_CSR, "invalid CSR: column index out of range [0, n_vars)");
+      if (hf[3]) fail(SCXPCA_INVALID_CSR, "invalid CSR: non-finite value");
+      if (hf[2]) {
+        // unsorted (or duplicated) rows: sort an owned copy by gene
+        if (dev_in) {
+          pl->b_idx.alloc(sizeof(int32_t) * nnz);
+          CK(cudaMemcpyAsync(pl->b_idx.p, pl->idx, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, st));
+          pl->idx = pl->b_idx.as<int32_t>();
+          pl->b_stage.alloc(dtype_size(pl->in_dtype) * nnz);
+          CK(cudaMemcpyAsync(pl->b_stage.p, vin, dtype_size(pl->in_dtype) * nnz, cudaMemcpyDeviceToDevice, st));
+          vin = pl->b_stage.p;
+        }
+        CK(launch_sort_rows(pl->in_dtype, pl->indptr, pl->b_idx.as<int32_t>(), pl->b_stage.p, n, st,
+                            pl->num_sms));
+      }
+    }
+
+    // ---- statistics of the input ----
+    pl->stats_parts = 2 * pl->num_sms;
+    pl->stats_part.alloc(sizeof(double) * 2 * g * pl->stats_parts);
+    pl->stats_out.alloc(sizeof(double) * 2 * g);
+    std::vector<double> sx, sxx;
+    stats_pass(pl, vin, pl->in_dtype, sx, sxx);
+    pl->mean_x.resize(g);
+    for (int64_t j = 0; j < g; ++j) pl->mean_x[j] = sx[j] / (double)n;
+
+    // ---- working values ----
+    const bool borrow = !pl->scaled && pl->in_dtype == pl->dtype;
+    if (borrow) {
+      pl->val = vin;
+      if (!dev_in || vin != x->values) {
+        // vin is our staging buffer: keep it
+        pl->b_val.p = pl->b_stage.p;
+        pl->b_val.bytes = pl->b_stage.bytes;
+        pl->b_stage.p = nullptr;
+        pl->b_stage.bytes = 0;
+        pl->val = pl->b_val.p;
+      }
+      pl->col_sum = sx;
+      pl->col_sq = sxx;
+    } else {
+      pl->b_val.alloc(dtype_size(pl->dtype) * std::max<int64_t>(nnz, 1));
+      int mode = 0;
+      std::vector<double> mu(g, 0.0), inv_std(g, 1.0), cshift(g, 0.0);
+      if (pl->scaled) {
+        pl->std_x.resize(g);
+        for (int64_t j = 0; j < g; ++j) {
+          double m = pl->mean_x[j];
+          double var = (sxx[j] - (double)n * m * m) / std::max<double>((double)n - 1.0, 1.0);
+          double sd = std::sqrt(std::max(var, 0.0));
+          if (sd == 0.0) sd = 1.0;
+          pl->std_x[j] = sd;
+          mu[j] = m;
+          inv_std[j] = 1.0 / sd;
+          if (pl->centered) {
+            double c = -m / sd;
+            if (pl->clip > 0) c = std::min(std::max(c, -pl->clip), pl->clip);
+            cshift[j] = c;
+          }
+        }
+        mode = pl->centered ? 1 : 2;
+      }
+      upload(pl->d_mu, mu, st);
+      upload(pl->d_inv_std, inv_std, st);
+      upload(pl->d_cshift, cshift, st);
+      CK(launch_transform_values(pl->in_dtype, pl->dtype, pl->idx, vin, pl->b_val.p, nnz, mode,
+                                 pl->d_mu.as<double>(), pl->d_inv_std.as<double>(),
+                                 pl->d_cshift.as<double>(), pl->clip, st, pl->num_sms));
+      pl->val = pl->b_val.p;
+      stats_pass(pl, pl->val, pl->dtype, pl->col_sum, pl->col_sq);
+      pl->b_stage.release();
+    }
+    {
+      std::vector<double> mu_w(g, 0.0);
+      if (pl->centered)
+        for (int64_t j = 0; j < g; ++j) mu_w[j] = pl->col_sum[j] / (double)n;
+      upload(pl->d_mu, mu_w, st);
+    }
+    compute_total_variance(pl);
+
+    // ---- transposed-product tables ----
+    pl->nb = (int)((g + kTransposeGeneBlock - 1) / kTransposeGeneBlock);
+    pl->nchunks = std::max(1, (2 * pl->num_sms + pl->nb - 1) / pl->nb);
+    pl->nchunks = (int)std::min<int64_t>(pl->nchunks, n);
+    pl->rows_per_chunk = (n + pl->nchunks - 1) / pl->nchunks;
+    pl->rbp.alloc(sizeof(int32_t) * n * (pl->nb + 1));
+    CK(launch_row_block_ptr(pl->indptr, pl->idx, n, pl->nb, kTransposeGeneBlock, pl->rbp.as<int32_t>(),
+                            st, pl->num_sms));
+    pl->wpart.alloc(sizeof(float) * (size_t)pl->nchunks * g * ld);
+
+    // ---- dense work buffers ----
+    pl->gram_parts = 2 * pl->num_sms;
+    pl->gram_parts_small = (int)std::max<int64_t>(1, std::min<int64_t>(2 * pl->num_sms, (g + 31) / 32));
+    pl->Y.alloc(sizeof(float) * n * ld);
+    pl->W.alloc(sizeof(double) * g * ld);
+    pl->Z.alloc(sizeof(double) * g * ld);
+    pl->V.alloc(sizeof(float) * g * ld);
+    pl->mc.alloc(sizeof(float) * ld);
+    pl->gpart.alloc(sizeof(double) * pl->gram_parts * (ld * ld + ld));
+    pl->G.alloc(sizeof(double) * (ld * ld + ld));
+    pl->R.alloc(sizeof(double) * ld * ld);
+    pl->Rinv.alloc(sizeof(double) * ld * ld);
+    pl->Rinv_f.alloc(sizeof(float) * ld * ld);
+    pl->R2inv.alloc(sizeof(double) * ld * ld);
+    pl->evals.alloc(sizeof(double) * ld);
+    pl->evecs.alloc(sizeof(double) * 2 * ld * ld);
+    pl->sigma.alloc(sizeof(double) * ld);
+    pl->comps.alloc(sizeof(float) * pl->nc * g);
+    pl->M_emb.alloc(sizeof(float) * ld * pl->nc);
+    pl->status.alloc(sizeof(int) * 4);
+    {
+      std::vector<double> eye(ld * ld, 0.0);
+      for (int64_t i = 0; i < ld; ++i) eye[i * ld + i] = 1.0;
+      upload(pl->eye, eye, st);
+    }
+    CK(cudaStreamSynchronize(st));
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    pl->device_bytes = pl->b_indptr.bytes + pl->b_idx.bytes + pl->b_val.bytes + pl->stats_part.bytes +
+                       pl->rbp.bytes + pl->wpart.bytes + pl->Y.bytes + pl->gpart.bytes +
+                       pl->W.bytes + pl->Z.bytes + pl->V.bytes;
+    return pl;
+  } catch (...) {
+    if (pl->own_stream && pl->stream) cudaStreamDestroy(pl->stream);
+    delete pl;
+    throw;
+  }
+}
+
+// Tall Gram + Cholesky (FP64) of the plan's Y buffer.
+void tall_chol(scxpca_plan* pl, const float* A, int64_t rows, double* Rinv, float* Rinv_f,
+               int shift) {
+  cudaStream_t st = pl->stream;
+  const int ld = (int)pl->ld;
+  const int parts = (int)std::max<int64_t>(1, std::min<int64_t>(pl->gram_parts, (rows + 31) / 32));
+  CK(launch_gram_f32(A, rows, ld, pl->gpart.as<double>(), parts, st));
+  CK(launch_reduce_rows_f64(pl->gpart.as<double>(), parts, (int64_t)ld * ld + ld, pl->G.as<double>(), 0,
+                            st, pl->num_sms));
+  CK(launch_cholesky(pl->G.as<double>(), (int)pl->k, ld, pl->tau, shift, pl->R.as<double>(), Rinv,
+                     Rinv_f, pl->status.as<int>(), st));
+}
+
+// CholeskyQR2 of a gene-side FP64 matrix in place.
+void small_qr(scxpca_plan* pl, double* A, int shift) {
+  cudaStream_t st = pl->stream;
+  const int ld = (int)pl->ld;
+  for (int pass = 0; pass < 2; ++pass) {
+    CK(launch_gram_f64(A, pl->g, ld, pl->gpart.as<double>(), pl->gram_parts_small, st));
+    CK(launch_reduce_rows_f64(pl->gpart.as<double>(), pl->gram_parts_small, (int64_t)ld * ld + ld,
+                              pl->G.as<double>(), 0, st, pl->num_sms));
+    CK(launch_cholesky(pl->G.as<double>(), (int)pl->k, ld, pl->tau, shift, pl->R.as<double>(),
+                       pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), pl->status.as<int>(), st));
+    CK(launch_apply_right_f64(A, pl->g, ld, pl->Rinv.as<double>(), st));
+  }
+}
+
+// W = X^T A (raw, uncentred), FP64, for a tall float A (n x ld).
+void rmatmat_raw(scxpca_plan* pl, const float* A) {
+  cudaStream_t st = pl->stream;
+  CK(launch_spmm_t(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, (int32_t)pl->g,
+                   pl->rbp.as<int32_t>(), pl->nb, pl->nchunks, pl->rows_per_chunk, A,
+                   pl->wpart.as<float>(), st));
+  CK(launch_reduce_rows_f32(pl->wpart.as<float>(), pl->nchunks, pl->g * pl->ld, pl->W.as<double>(), 0,
+                            st, pl->num_sms));
+}
+
+void forward(scxpca_plan* pl) {
+  CK(launch_spmm_fwd(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, pl->V.as<float>(),
+                     pl->centered ? pl->mc.as<float>() : nullptr, pl->Y.as<float>(), pl->stream,
+                     pl->num_sms));
+}
+
+void load_omega(scxpca_plan* pl, const scxpca_params* p) {
+  cudaStream_t st = pl->stream;
+  const int64_t g = pl->g, k = pl->k, ld = pl->ld;
+  CK(cudaMemsetAsync(pl->V.p, 0, sizeof(float) * g * ld, st));
+  if (p->omega) {
+    const float* src = p->omega;
+    if (p->omega_memory != SCXPCA_MEM_DEVICE) {
+      pl->omega_stage.alloc(sizeof(float) * g * k);
+      CK(cudaMemcpyAsync(pl->omega_stage.p, p->omega, sizeof(float) * g * k, cudaMemcpyHostToDevice, st));
+      src = pl->omega_stage.as<float>();
+    }
+    CK(launch_colmajor_to_padded(src, g, k, (int)ld, pl->V.as<float>(), st, pl->num_sms));
+  } else {
+    CK(launch_gaussian(p->seed, g, k, pl->V.as<float>(), (int)ld, st, pl->num_sms));
+  }
+  CK(launch_mean_prefactor(pl->V.as<float>(), g, (int)ld, pl->centered ? pl->d_mu.as<double>() : nullptr,
+                           pl->mc.as<float>(), st));
+}
+
+void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
+  if (!out) fail(SCXPCA_INVALID_ARGUMENT, "null result");
+  if (!out->embeddings) fail(SCXPCA_INVALID_ARGUMENT, "null embeddings output");
+  scxpca_params p = pl->params;
+  if (over) {
+    p.seed = over->seed;
+    p.omega = over->omega;
+    p.omega_memory = over->omega_memory;
+    p.n_power_iterations = over->n_power_iterations;
+    if (p.n_power_iterations < 0) fail(SCXPCA_INVALID_ARGUMENT, "n_power_iterations must be >= 0");
+  }
+  cudaStream_t st = pl->stream;
+  const int ld = (int)pl->ld;
+  const int shift = p.qr_method == SCXPCA_QR_HOUSEHOLDER ? 1 : 0;
+  const double* mu = pl->centered ? pl->d_mu.as<double>() : nullptr;
+  double* sY = pl->G.as<double>() + (size_t)ld * ld;  // column sums follow the Gram
+
+  CK(cudaMemsetAsync(pl->status.p, 0, sizeof(int) * 4, st));
+  load_omega(pl, &p);
+  // Y = (X - mu) Omega ; qr(Y)
+  forward(pl);
+  tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift);
+  for (int64_t it = 0; it < p.n_power_iterations; ++it) {
+    // Z = (X - mu)^T Q = (X^T Y - mu (1^T Y)) R^{-1}
+    rmatmat_raw(pl, pl->Y.as<float>());
+    CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->Rinv.as<double>(),
+                           pl->Z.as<double>(), st));
+    small_qr(pl, pl->Z.as<double>(), shift);
+    CK(launch_round_v(pl->Z.as<double>(), pl->g, ld, mu, pl->V.as<float>(), pl->mc.as<float>(), st));
+    forward(pl);
+    tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift);
+  }
+  // Explicit Q = Y R^{-1}, re-orthonormalised by a second FP64 Cholesky pass.
+  CK(launch_apply_right_f32(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(), st,
+                            pl->num_sms));
+  tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift);
+  // B = (X - mu)^T Q R2^{-1}
+  rmatmat_raw(pl, pl->Y.as<float>());
+  CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->R2inv.as<double>(),
+                         pl->Z.as<double>(), st));
+  // SVD of B through the FP64 eigendecomposition of B^T B.
+  CK(launch_gram_f64(pl->Z.as<double>(), pl->g, ld, pl->gpart.as<double>(), pl->gram_parts_small, st));
+  CK(launch_reduce_rows_f64(pl->gpart.as<double>(), pl->gram_parts_small, (int64_t)ld * ld + ld,
+                            pl->G.as<double>(), 0, st, pl->num_sms));
+  CK(launch_jacobi_eig(pl->G.as<double>(), (int)pl->k, ld, pl->evals.as<double>(), pl->evecs.as<double>(),
+                       pl->status.as<int>() + 2, st));
+  CK(launch_ritz_finish(pl->Z.as<double>(), pl->g, ld, (int)pl->k, (int)pl->nc, pl->evals.as<double>(),
+                        pl->evecs.as<double>(), pl->R2inv.as<double>(), pl->sigma.as<double>(),
+                        pl->comps.as<float>(), pl->M_emb.as<float>(), st));
+  // Embeddings U = Q R2^{-1} E Sigma (first n_components).
+  float* U = out->embeddings;
+  const bool host_out = out->embeddings_memory != SCXPCA_MEM_DEVICE;
+  if (host_out) {
+    pl->U.alloc(sizeof(float) * pl->n * pl->nc);
+    U = pl->U.as<float>();
+  }
+  CK(launch_embed(pl->Y.as<float>(), pl->n, ld, (int)pl->k, pl->M_emb.as<float>(), (int)pl->nc, U, st,
+                  pl->num_sms));
+  if (host_out)
+    CK(cudaMemcpyAsync(out->embeddings, U, sizeof(float) * pl->n * pl->nc, cudaMemcpyDeviceToHost, st));
+
+  int hstatus[4];
+  std::vector<double> sigma(pl->k);
+  CK(cudaMemcpyAsync(hstatus, pl->status.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(sigma.data(), pl->sigma.p, sizeof(double) * pl->k, cudaMemcpyDeviceToHost, st));
+  if (out->components)
+    CK(cudaMemcpyAsync(out->components, pl->comps.p, sizeof(float) * pl->nc * pl->g,
+                       cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (hstatus[0] < 0)
+    fail(SCXPCA_NOT_SPD, "CholeskyQR2 failed: non-SPD; retry with qr_method='householder'");
+
+  const double denom = std::max<double>((double)pl->n - 1.0, 1.0);
+  for (int64_t c = 0; c < pl->nc; ++c) {
+    double ve = sigma[c] * sigma[c] / denom;
+    if (out->variance_explained) out->variance_explained[c] = ve;
+    if (out->variance_ratio) out->variance_ratio[c] = pl->total_var > 0.0 ? ve / pl->total_var : 0.0;
+    if (out->singular_values) out->singular_values[c] = sigma[c];
+  }
+  if (out->mean) {
+    for (int64_t j = 0; j < pl->g; ++j) out->mean[j] = pl->mean_x[j];
+  }
+  if (out->std) {
+    for (int64_t j = 0; j < pl->g; ++j) out->std[j] = pl->scaled ? pl->std_x[j] : 1.0;
+  }
+  out->resident_csr = 1;
+  out->total_var_recomputed = pl->total_var_recomputed ? 1 : 0;
+  out->shifted_cholesky = hstatus[0] > 0 ? hstatus[0] : 0;
+  out->total_var = pl->total_var;
+}
+
+template <typename F>
+int32_t guarded(char* err, size_t err_len, F&& f) {
+  try {
+    f();
+    write_err(err, err_len, "");
+    return SCXPCA_OK;
+  } catch (const Failure& e) {
+    write_err(err, err_len, e.msg);
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    write_err(err, err_len, "host allocation failed");
+    return SCXPCA_OUT_OF_MEMORY;
+  } catch (...) {
+    write_err(err, err_len, "unexpected internal error");
+    return SCXPCA_CUDA_ERROR;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* scxpca_status_string(int32_t s) {
+  switch (s) {
+    case SCXPCA_OK: return "ok";
+    case SCXPCA_INVALID_ARGUMENT: return "invalid argument";
+    case SCXPCA_OUT_OF_MEMORY: return "out of memory";
+    case SCXPCA_NOT_SPD: return "not SPD";
+    case SCXPCA_INVALID_CSR: return "invalid CSR";
+    case SCXPCA_CUDA_ERROR: return "CUDA error";
+    case SCXPCA_TIMEOUT: return "timeout";
+    case SCXPCA_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+int32_t scxpca_abi_version(void) { return SCXPCA_ABI_VERSION; }
+
+int32_t scxpca_plan_create(const scxpca_csr* x, const scxpca_params* params, scxpca_plan** plan,
+                           char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!plan) fail(SCXPCA_INVALID_ARGUMENT, "null plan output");
+    *plan = nullptr;
+    if (!params) fail(SCXPCA_INVALID_ARGUMENT, "null params");
+    validate_params(x, params);
+    DeviceGuard dg(params->device_ordinal);
+    *plan = create_plan(x, params);
+  });
+}
+
+void scxpca_plan_destroy(scxpca_plan* plan) {
+  if (!plan) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(plan->device);
+  cudaStreamSynchronize(plan->stream);
+  bool own = plan->own_stream;
+  cudaStream_t st = plan->stream;
+  delete plan;
+  if (own) cudaStreamDestroy(st);
+  if (prev >= 0) cudaSetDevice(prev);
+}
+
+int32_t scxpca_plan_run(scxpca_plan* plan, const scxpca_params* params, scxpca_result* out,
+                        char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!plan) fail(SCXPCA_INVALID_ARGUMENT, "null plan");
+    DeviceGuard dg(plan->device);
+    run_plan(plan, params, out);
+  });
+}
+
+int32_t scxpca_plan_info(const scxpca_plan* plan, int64_t* k, int64_t* ld, int64_t* device_bytes) {
+  if (!plan) return SCXPCA_INVALID_ARGUMENT;
+  if (k) *k = plan->k;
+  if (ld) *ld = plan->ld;
+  if (device_bytes) *device_bytes = (int64_t)plan->device_bytes;
+  return SCXPCA_OK;
+}
+
+int32_t scxpca_randomized(const scxpca_csr* x, const scxpca_params* params, scxpca_result* out,
+                          char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!params) fail(SCXPCA_INVALID_ARGUMENT, "null params");
+    if (!out || !out->embeddings) fail(SCXPCA_INVALID_ARGUMENT, "null embeddings output");
+    validate_params(x, params);
+    DeviceGuard dg(params->device_ordinal);
+    scxpca_plan* pl = create_plan(x, params);
+    try {
+      run_plan(pl, nullptr, out);
+    } catch (...) {
+      scxpca_plan_destroy(pl);
+      throw;
+    }
+    scxpca_plan_destroy(pl);
+  });
+}
+
+int32_t scxpca_plan_col_stats(scxpca_plan* plan, double* col_sums, double* col_sum_sq, char* err,
+                              size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!plan) fail(SCXPCA_INVALID_ARGUMENT, "null plan");
+    DeviceGuard dg(plan->device);
+    std::vector<double> s, q;
+    stats_pass(plan, plan->val, plan->dtype, s, q);
+    if (col_sums) memcpy(col_sums, s.data(), sizeof(double) * plan->g);
+    if (col_sum_sq) memcpy(col_sum_sq, q.data(), sizeof(double) * plan->g);
+  });
+}
+
+int32_t scxpca_plan_matmat(scxpca_plan* plan, const float* v, int64_t ld_v, float* y, int64_t ld_y,
+                           char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!plan || !v || !y) fail(SCXPCA_INVALID_ARGUMENT, "null argument");
+    if (ld_v < plan->k || ld_y < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "leading dimension < k");
+    DeviceGuard dg(plan->device);
+    cudaStream_t st = plan->stream;
+    const int64_t ld = plan->ld;
+    CK(cudaMemsetAsync(plan->V.p, 0, sizeof(float) * plan->g * ld, st));
+    CK(cudaMemcpy2DAsync(plan->V.p, sizeof(float) * ld, v, sizeof(float) * ld_v, sizeof(float) * plan->k,
+                         plan->g, cudaMemcpyDeviceToDevice, st));
+    CK(launch_mean_prefactor(plan->V.as<float>(), plan->g, (int)ld,
+                             plan->centered ? plan->d_mu.as<double>() : nullptr, plan->mc.as<float>(), st));
+    forward(plan);
+    CK(cudaMemcpy2DAsync(y, sizeof(float) * ld_y, plan->Y.p, sizeof(float) * ld, sizeof(float) * plan->k,
+                         plan->n, cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t scxpca_plan_rmatmat(scxpca_plan* plan, const float* q, int64_t ld_q, double* z, int64_t ld_z,
+                            char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!plan || !q || !z) fail(SCXPCA_INVALID_ARGUMENT, "null argument");
+    if (ld_q < plan->k || ld_z < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "leading dimension < k");
+    DeviceGuard dg(plan->device);
+    cudaStream_t st = plan->stream;
+    const int64_t ld = plan->ld;
+    CK(cudaMemsetAsync(plan->Y.p, 0, sizeof(float) * plan->n * ld, st));
+    CK(cudaMemcpy2DAsync(plan->Y.p, sizeof(float) * ld, q, sizeof(float) * ld_q, sizeof(float) * plan->k,
+                         plan->n, cudaMemcpyDeviceToDevice, st));
+    const int parts = (int)std::max<int64_t>(1, std::min<int64_t>(plan->gram_parts, (plan->n + 31) / 32));
+    CK(launch_gram_f32(plan->Y.as<float>(), plan->n, (int)ld, plan->gpart.as<double>(), parts, st));
+    CK(launch_reduce_rows_f64(plan->gpart.as<double>(), parts, ld * ld + ld, plan->G.as<double>(), 0, st,
+                              plan->num_sms));
+    rmatmat_raw(plan, plan->Y.as<float>());
+    CK(launch_center_apply(plan->W.as<double>(), plan->g, (int)ld,
+                           plan->centered ? plan->d_mu.as<double>() : nullptr,
+                           plan->G.as<double>() + ld * ld, plan->eye.as<double>(), plan->Z.as<double>(), st));
+    CK(cudaMemcpy2DAsync(z, sizeof(double) * ld_z, plan->Z.p, sizeof(double) * ld, sizeof(double) * plan->k,
+                         plan->g, cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t scxpca_plan_qr(scxpca_plan* plan, float* a, int64_t m, int64_t ld_a, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!plan || !a) fail(SCXPCA_INVALID_ARGUMENT, "null argument");
+    if (ld_a < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "leading dimension < k");
+    if (m < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "CholeskyQR2 requires m >= k");
+    DeviceGuard dg(plan->device);
+    cudaStream_t st = plan->stream;
+    const int64_t ld = plan->ld;
+    const int shift = plan->params.qr_method == SCXPCA_QR_HOUSEHOLDER ? 1 : 0;
+    DevBuf tmp;
+    tmp.alloc(sizeof(float) * m * ld);
+    CK(cudaMemsetAsync(tmp.p, 0, sizeof(float) * m * ld, st));
+    CK(cudaMemcpy2DAsync(tmp.p, sizeof(float) * ld, a, sizeof(float) * ld_a, sizeof(float) * plan->k, m,
+                         cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(plan->status.p, 0, sizeof(int) * 4, st));
+    for (int pass = 0; pass < 2; ++pass) {
+      tall_chol(plan, tmp.as<float>(), m, plan->Rinv.as<double>(), plan->Rinv_f.as<float>(), shift);
+      CK(launch_apply_right_f32(tmp.as<float>(), m, (int)ld, plan->Rinv_f.as<float>(), tmp.as<float>(), st,
+                                plan->num_sms));
+    }
+    int hs[4];
+    CK(cudaMemcpyAsync(hs, plan->status.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpy2DAsync(a, sizeof(float) * ld_a, tmp.p, sizeof(float) * ld, sizeof(float) * plan->k, m,
+                         cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    if (hs[0] < 0) fail(SCXPCA_NOT_SPD, "CholeskyQR2 failed: non-SPD; retry with qr_method='householder'");
+  });
+}
+
+int32_t scxpca_gaussian(int32_t device_ordinal, uint64_t seed, int64_t n_rows, int64_t n_cols,
+                        float* out, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!out || n_rows < 0 || n_cols < 0) fail(SCXPCA_INVALID_ARGUMENT, "bad gaussian arguments");
+    DeviceGuard dg(device_ordinal);
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal));
+    CK(launch_gaussian(seed, n_rows, n_cols, out, 0, nullptr, sms));
+    CK(cudaStreamSynchronize(nullptr));
+  });
+}
+
+int32_t scxpca_synth_nb_csr(int32_t device_ordinal, uint64_t seed, int64_t n_obs, int64_t n_vars,
+                            double loc, double dispersion, int64_t* indptr, int32_t* indices,
+                            float* values, int64_t* nnz_out, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_obs <= 0 || n_vars <= 0 || !indptr || !nnz_out)
+      fail(SCXPCA_INVALID_ARGUMENT, "bad synth arguments");
+    if (!(dispersion > 0.0 && dispersion <= 1.0))
+      fail(SCXPCA_INVALID_ARGUMENT, "dispersion must be in (0, 1]");
+    DeviceGuard dg(device_ordinal);
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal));
+    cudaStream_t st = nullptr;
+    DevBuf mu, row_nnz, rowsum;
+    mu.alloc(sizeof(float) * n_vars);
+    row_nnz.alloc(sizeof(int64_t) * n_obs);
+    rowsum.alloc(sizeof(float) * n_obs);
+    CK(launch_synth_gene_means(seed, n_vars, loc, mu.as<float>(), st));
+    CK(launch_synth_count(seed, n_obs, n_vars, loc, dispersion, mu.as<float>(), row_nnz.as<int64_t>(),
+                          rowsum.as<float>(), st, sms));
+    CK(launch_exclusive_scan_i64(row_nnz.as<int64_t>(), n_obs, indptr, st));
+    CK(cudaMemcpyAsync(nnz_out, indptr + n_obs, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (indices && values) {
+      CK(launch_synth_fill(seed, n_obs, n_vars, loc, dispersion, mu.as<float>(), indptr,
+                           rowsum.as<float>(), indices, values, st, sms));
+      CK(cudaStreamSynchronize(st));
+    }
+  });
+}
+
+}  // extern "C"
