@@ -1,0 +1,452 @@
+#!/usr/bin/env python
+"""Benchmark: 50-PC randomized PCA of a 1,000,000 x 2,000 sparse CSR on B200.
+
+Workload (seeded synthetic stand-in for a census-scale log-normalised HVG
+matrix): negative-binomial counts, ~10 % density (~2.1e8 nonzeros),
+log1p(1e4 * count / rowsum) values, n_comps=50, n_oversamples=10,
+4 power iterations, implicit centring plus per-gene unit-variance scaling
+clipped at 10.  One step = one complete PCA (plan run) on the resident matrix.
+
+Headline ``value``: ms per PCA in BF16-mixed precision (values streamed as
+BF16, FP32 accumulation, FP64 Gram/Cholesky/SVD); the strict FP32 path is
+timed on the same workload alongside (``fp32``) with the singular-value
+agreement between the two.  ``e2e``: the same PCA through the one-shot C ABI
+call with host (pinned) CSR buffers, upload and embedding download included.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (the path has no collective), one process
+per GPU under torchrun; the step time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+N_OBS = 1_000_000
+N_VARS = 2_000
+LOC = -3.0
+DISPERSION = 0.3
+SEED = 0
+N_COMPS = 50
+N_OVERSAMPLES = 10
+N_POWER = 4
+CLIP = 10.0
+METRIC = "1M x 2k-gene rPCA (50 PCs) ms per PCA, BF16-mixed (FP32 path alongside)"
+FALLBACK_HBM_GBS = 6650.0
+
+# DRAM bytes per stored nonzero for the dominant kernel, from the ncu capture
+# summarised in profiles/ (dram__bytes_read.sum + dram__bytes_write.sum of one
+# launch divided by that launch's nonzeros); None until captured.
+NCU_TRAFFIC_BYTES_PER_NNZ = {"transpose": None, "forward": None}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n-obs", type=int, default=N_OBS)
+    ap.add_argument("--mode", choices=["mixed_bf16", "mixed_f16", "strict_fp32"], default="mixed_bf16")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 comparison leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-rows", type=int, default=50_000)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# process group (replicas) helpers
+# ---------------------------------------------------------------------------
+
+def dist_setup(backend: str):
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return 0, 1, 0
+    from datetime import timedelta
+
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=timedelta(seconds=300))
+    return dist.get_rank(), world, int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def max_over_ranks(x: float, device=None) -> float:
+    """Max of a scalar over all ranks (identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(device=None):
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        if device is not None:
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(self.NAMES, parts[3:7]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes
+# ---------------------------------------------------------------------------
+
+def bytes_of_a(nnz: int, n: int, s_v: int) -> int:
+    return nnz * (s_v + 4) + 8 * (n + 1)
+
+
+def kernel_bytes(stage: str, nnz: int, n: int, g: int, k: int, s_v: int) -> int:
+    """Algorithmic bytes of one launch: the matrix once, the tall operand once."""
+    a = bytes_of_a(nnz, n, s_v)
+    if stage == "forward":     # read A and V, write Y (n x k FP32)
+        return a + 4 * g * k + 4 * n * k
+    if stage == "transpose":   # read A and Q (n x k FP32), write Z (g x k)
+        return a + 4 * n * k + 4 * g * k
+    raise ValueError(stage)
+
+
+def pca_bytes(nnz: int, n: int, k: int, c: int, q: int, s_v: int) -> int:
+    """Executed-pass algorithmic bytes of one PCA on the resident matrix.
+
+    (q+1) forward products (read A, write Y) + (q+1) transposed products (read
+    A and Q) + (q+2) tall Gram reads + the explicit Q formation (read + write)
+    + the embeddings (read Q, write n x c).  Statistics and the value transform
+    run once at plan creation and are not part of a step.
+    """
+    a = bytes_of_a(nnz, n, s_v)
+    tall = 4 * n * k
+    return ((q + 1) * (a + tall) + (q + 1) * (a + tall) + (q + 2) * tall + 2 * tall
+            + tall + 4 * n * c)
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the multithreaded C++ restatement of the reference's CPU path
+# ---------------------------------------------------------------------------
+
+def cpu_baseline(indptr, indices, values, n_full: int, rows: int, threads: int):
+    import numpy as np
+
+    from oracle import build_cpu, rpca
+
+    rows = min(rows, len(indptr) - 1)
+    ip = np.ascontiguousarray(indptr[: rows + 1], dtype=np.int64)
+    nnz = int(ip[-1])
+    ix = np.ascontiguousarray(indices[:nnz])
+    vv = np.ascontiguousarray(values[:nnz], dtype=np.float32)
+    k = N_COMPS + N_OVERSAMPLES
+    om = rpca.gaussian_omega(N_VARS, k, SEED)
+    build_cpu.load()
+    t0 = time.perf_counter()
+    build_cpu.run(ip, ix, vv, (rows, N_VARS), N_COMPS, k, N_POWER, om, zero_center=True,
+                  scale=True, clip_max=CLIP, threads=threads)
+    dt = time.perf_counter() - t0
+    return dt * 1e3 * (n_full / rows), nnz, dt
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+
+def base_config(n_obs, nnz, mode, world):
+    return {
+        "workload": f"randomized PCA of a {n_obs:,} x {N_VARS:,} NB-synthetic CSR "
+                    f"(50 PCs, oversample 10, 4 power iterations, centred + unit-variance "
+                    f"scaled, clip 10)",
+        "n_obs": n_obs, "n_vars": N_VARS, "nnz": nnz,
+        "density": round(nnz / (n_obs * N_VARS), 4),
+        "n_components": N_COMPS, "n_oversamples": N_OVERSAMPLES,
+        "n_power_iterations": N_POWER, "values": mode, "qr_method": "cholesky",
+        "generator": f"NB: mu_g~LogNormal({LOC},1.5), s_c~LogNormal(0,0.5), dispersion 0.3, seed {SEED}",
+        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "l2": "inputs larger than L2 (CSR >> 126 MB); no flush needed",
+    }
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from scx_b200 import accel
+
+    rank, world, local = dist_setup("nccl")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n_obs = args.n_obs
+    ip, ix, vv = accel.synth_nb_csr_device(n_obs, N_VARS, seed=SEED, loc=LOC,
+                                           dispersion=DISPERSION, device=local)
+    nnz = int(ix.numel())
+    stream = torch.cuda.Stream(device=dev)
+    s_v = 4 if args.mode == "strict_fp32" else 2
+
+    def make_plan(mode):
+        return accel.Plan(ip, ix, vv, (n_obs, N_VARS), n_components=N_COMPS,
+                          n_oversamples=N_OVERSAMPLES, n_power_iterations=N_POWER,
+                          zero_center=True, scale=True, clip_max=CLIP, seed=SEED,
+                          qr_method="cholesky", math_mode=mode, device=local,
+                          stream=stream.cuda_stream)
+
+    def timed(plan, steps, warmup, sample_clocks):
+        emb = torch.empty((n_obs, N_COMPS), dtype=torch.float32, device=dev)
+        res = None
+        for _ in range(warmup):
+            res = plan.run(embeddings_out=emb)
+        plan.set_profiling(True)
+        barrier(dev)
+        torch.cuda.synchronize(dev)
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps):
+            res = plan.run(embeddings_out=emb)
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+        clocks = sampler.stop() if sampler else None
+        barrier(dev)
+        ms = start.elapsed_time(end) / steps
+        return ms, res, plan.profile(), clocks
+
+    plan = make_plan(args.mode)
+    k = plan.k
+    ms, res, prof, clocks = timed(plan, args.steps, args.warmup, True)
+    ms_max = max_over_ranks(ms, dev)
+    plan.close()
+
+    out = {
+        "metric": METRIC, "value": None, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": {"mixed_bf16": "bf16", "mixed_f16": "f16", "strict_fp32": "f32"}[args.mode],
+        "data": "synthetic (seeded negative-binomial CSR generated on device)",
+        "config": base_config(n_obs, nnz, args.mode, world),
+    }
+    out["ms_per_step"] = round(ms_max, 4)
+    out["value"] = round(ms_max / world, 4)
+
+    # roofline of the dominant kernel, from the live stage timing of the timed region
+    peak, peak_kind = measured_hbm_peak()
+    stages = prof["stages"]
+    dom = max(("forward", "transpose"), key=lambda s: stages[s]["device_ms"])
+    launch_ms = stages[dom]["device_ms"] / max(stages[dom]["launches"], 1)
+    kb = kernel_bytes(dom, nnz, n_obs, N_VARS, k, s_v)
+    achieved = kb / (launch_ms * 1e-3) / 1e9
+    traffic = NCU_TRAFFIC_BYTES_PER_NNZ.get(dom)
+    out["roofline"] = {
+        "bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+        "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+        "traffic": int(traffic * nnz) if traffic else None,
+        "algorithmic_bytes_per_launch": kb, "launch_ms": round(launch_ms, 4),
+    }
+    total_ms = sum(v["device_ms"] for v in stages.values())
+    out["stage_share"] = {s: round(v["device_ms"] / total_ms, 4) for s, v in stages.items()
+                          if v["launches"]}
+    pb = pca_bytes(nnz, n_obs, k, N_COMPS, N_POWER, s_v)
+    out["pca_hbm"] = {"algorithmic_bytes": pb, "gbs": round(pb / (ms_max * 1e-3) / 1e9, 1),
+                      "frac": round(pb / (ms_max * 1e-3) / 1e9 / peak, 4)}
+    out["gpu_launches"] = int(prof["kernel_launches"])
+    out["clocks"] = clocks
+    sv_main = np.asarray(res.singular_values)
+
+    if not args.no_fp32 and args.mode != "strict_fp32":
+        p32 = make_plan("strict_fp32")
+        ms32, res32, prof32, _ = timed(p32, max(2, args.steps // 2), 1, False)
+        ms32 = max_over_ranks(ms32, dev)
+        p32.close()
+        sv32 = np.asarray(res32.singular_values)
+        out["fp32"] = {"ms": round(ms32, 4), "speedup_mixed_vs_fp32": round(ms32 / ms_max, 3),
+                       "sigma_max_rel_diff_mixed_vs_fp32":
+                           float(np.max(np.abs(sv_main - sv32) / sv32))}
+
+    if not args.no_e2e:
+        # host (pinned) CSR through the one-shot C ABI call
+        h_ip = ip.cpu().pin_memory()
+        h_ix = ix.cpu().pin_memory()
+        h_vv = vv.cpu().pin_memory()
+        h_emb = torch.empty((n_obs, N_COMPS), dtype=torch.float32).pin_memory()
+        a_ip, a_ix, a_vv, a_emb = h_ip.numpy(), h_ix.numpy(), h_vv.numpy(), h_emb.numpy()
+
+        def one():
+            return accel.randomized_pca(a_ip, a_ix, a_vv, (n_obs, N_VARS), n_components=N_COMPS,
+                                        n_oversamples=N_OVERSAMPLES, n_power_iterations=N_POWER,
+                                        zero_center=True, scale=True, clip_max=CLIP, seed=SEED,
+                                        qr_method="cholesky", math_mode=args.mode, device=local,
+                                        embeddings_out=a_emb)
+
+        one()
+        e2e_steps = max(1, min(3, args.steps))
+        barrier(dev)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            one()
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+        e2e_ms = max_over_ranks(e2e_ms, dev)
+        h2d = a_ip.nbytes + a_ix.nbytes + a_vv.nbytes
+        d2h = a_emb.nbytes + N_COMPS * N_VARS * 4 + N_COMPS * 8 * 3 + N_VARS * 8 * 2
+        out["e2e"] = {"value": round(e2e_ms / world, 3), "unit": "ms", "h2d_bytes_per_step": h2d,
+                      "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                      "path": "scxpca_randomized (host pinned CSR -> host embeddings)"}
+        host_csr = (a_ip, a_ix, a_vv)
+    else:
+        host_csr = (ip.cpu().numpy(), ix.cpu().numpy(), vv.cpu().numpy())
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cpu_ms, sample_nnz, sample_s = cpu_baseline(*host_csr, n_obs, args.cpu_sample_rows, threads)
+        out["cpu_baseline"] = {
+            "value": round(cpu_ms, 1), "unit": "ms", "cores": threads, "kind": "port",
+            "sample": f"first {min(args.cpu_sample_rows, n_obs):,} rows ({sample_nnz:,} nnz) of the "
+                      f"same matrix, FP64 C++ restatement of the reference CPU randomized PCA, "
+                      f"{sample_s:.2f} s, scaled by rows to {n_obs:,}",
+        }
+
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    _finish_dist()
+
+
+def _finish_dist():
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """Reference arm: the reference's CPU randomized PCA (its C++ restatement,
+    the Rust reference being unbuildable here) on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+
+    from scx_b200.synth import synth_nb_csr
+
+    rows = min(args.cpu_sample_rows, args.n_obs)
+    ip, ix, vv = synth_nb_csr(rows, N_VARS, seed=SEED, loc=LOC, dispersion=DISPERSION)
+    threads = os.cpu_count() or 1
+    times = []
+    for i in range(args.warmup + args.steps):
+        ms, nnz, dt = cpu_baseline(ip, ix, vv, args.n_obs, rows, threads)
+        if i >= args.warmup:
+            times.append(ms)
+    value = float(np.mean(times))
+    nnz_full_est = int(nnz * args.n_obs / rows)
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "ms", "impl": "reference",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(value, 1), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded negative-binomial CSR, host generator)",
+        "config": base_config(args.n_obs, nnz_full_est, "f32 input, f64 compute", 1),
+        "cpu_baseline": {"value": round(value, 1), "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": f"{rows:,} rows ({nnz:,} nnz) per step, scaled by rows to "
+                                   f"{args.n_obs:,}; reference is Rust (unbuildable here), "
+                                   "timed via its FP64 C++ restatement"},
+        "e2e": {"value": round(value, 1), "unit": "ms", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

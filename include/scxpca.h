@@ -189,6 +189,35 @@ int32_t scxpca_plan_rmatmat(scxpca_plan* plan, const float* q, int64_t ld_q, dou
 int32_t scxpca_plan_qr(scxpca_plan* plan, float* a, int64_t m, int64_t ld_a,
                        char* err, size_t err_len);
 
+/* Opt-in per-stage device timing (the counterpart of SCX_GPU_PROFILE,
+ * scx-gpu/src/profile.rs:1-60, and the SpMM timing hook of
+ * cusparse.rs:501-528).  When enabled, plan_run brackets each stage's kernels
+ * with CUDA events on the plan's stream and accumulates per-stage launch
+ * counts and device milliseconds.  kernel_launches counts every kernel the
+ * library launched on the plan since the last reset, profiling on or off. */
+enum {
+  SCXPCA_STAGE_PREPARE = 0,   /* validation, statistics, value transform */
+  SCXPCA_STAGE_FORWARD = 1,   /* Y = (X - mu) V */
+  SCXPCA_STAGE_TRANSPOSE = 2, /* partial X^T Q */
+  SCXPCA_STAGE_REDUCE = 3,    /* fixed-order reduction of the partials */
+  SCXPCA_STAGE_GRAM = 4,      /* tall Gram Y^T Y (FP64) */
+  SCXPCA_STAGE_APPLY = 5,     /* tall Q = Y R^{-1} */
+  SCXPCA_STAGE_SMALL = 6,     /* Cholesky, gene-side QR, Jacobi, Ritz */
+  SCXPCA_STAGE_EMBED = 7,     /* embeddings */
+  SCXPCA_NUM_STAGES = 8
+};
+
+typedef struct {
+  int64_t launches[SCXPCA_NUM_STAGES]; /* bracketed stage executions */
+  double device_ms[SCXPCA_NUM_STAGES];
+  int64_t kernel_launches;             /* all kernels launched since reset */
+  int64_t runs;                        /* plan_run calls since reset */
+} scxpca_profile;
+
+/* Enable (1) or disable (0) stage timing; any call resets the counters. */
+int32_t scxpca_plan_set_profiling(scxpca_plan* plan, int32_t enable);
+int32_t scxpca_plan_get_profile(const scxpca_plan* plan, scxpca_profile* out);
+
 /* Per-gene statistics of the plan's working matrix: column sums and sums of
  * squares in FP64, host outputs (n_vars each).  Replaces
  * col_means_and_sum_sq_prefetched (scx-format-io/src/prefetch.rs:616-650) and

@@ -41,9 +41,13 @@ EXPORTED = (
     "scxpca_plan_rmatmat",
     "scxpca_plan_qr",
     "scxpca_plan_col_stats",
+    "scxpca_plan_set_profiling",
+    "scxpca_plan_get_profile",
     "scxpca_gaussian",
     "scxpca_synth_nb_csr",
 )
+
+STAGES = ("prepare", "forward", "transpose", "reduce", "gram", "apply", "small", "embed")
 
 
 class ScxLibraryError(RuntimeError):
@@ -100,6 +104,15 @@ class Result(C.Structure):
     ]
 
 
+class Profile(C.Structure):
+    _fields_ = [
+        ("launches", C.c_int64 * len(STAGES)),
+        ("device_ms", C.c_double * len(STAGES)),
+        ("kernel_launches", C.c_int64),
+        ("runs", C.c_int64),
+    ]
+
+
 _lib = None
 
 
@@ -131,6 +144,8 @@ def load() -> C.CDLL:
         "scxpca_plan_rmatmat": (C.c_int32, [P, P, C.c_int64, P, C.c_int64, *E]),
         "scxpca_plan_qr": (C.c_int32, [P, P, C.c_int64, C.c_int64, *E]),
         "scxpca_plan_col_stats": (C.c_int32, [P, P, P, *E]),
+        "scxpca_plan_set_profiling": (C.c_int32, [P, C.c_int32]),
+        "scxpca_plan_get_profile": (C.c_int32, [P, C.POINTER(Profile)]),
         "scxpca_gaussian": (C.c_int32, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, P, *E]),
         "scxpca_synth_nb_csr": (C.c_int32, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, C.c_double,
                                             C.c_double, P, P, P, C.POINTER(C.c_int64), *E]),

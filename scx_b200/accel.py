@@ -198,11 +198,14 @@ def randomized_pca(indptr, indices, values, shape, n_components: int = 50,
                    zero_center: bool = True, scale: bool = False, clip_max: float | None = None,
                    seed: int = 0, omega=None, qr_method: str = "householder",
                    math_mode: str = "strict_fp32", spmm_policy: str = "default",
-                   device: int = 0, device_embeddings: bool = False) -> PcaResult:
+                   device: int = 0, device_embeddings: bool = False,
+                   embeddings_out=None) -> PcaResult:
     """One-shot randomized PCA of a CSR matrix (host numpy or CUDA torch arrays).
 
     Same contract as ``scx_gpu::gpu_randomized_pca`` (scx-gpu/src/gpu_pca.rs:706-763)
     with an optional explicit ``omega`` (n_vars x k) and per-gene scaling.
+    ``embeddings_out`` may be a preallocated (n_obs, n_components) float32
+    buffer: a numpy array (e.g. pinned host memory) or a CUDA torch tensor.
     """
     lib = _lib.load()
     csr, keep, mem, dev = _prepare_csr(indptr, indices, values, shape)
@@ -216,7 +219,14 @@ def randomized_pca(indptr, indices, values, shape, n_components: int = 50,
     p.omega = optr or None
     p.omega_memory = omem
     nc = int(n_components)
-    res, bufs = _alloc_outputs(n_obs, n_vars, max(nc, 0), device_embeddings, device)
+    if embeddings_out is not None:
+        device_embeddings = _is_torch(embeddings_out) and embeddings_out.is_cuda
+        res, bufs = _alloc_outputs(0, n_vars, max(nc, 0), False, device)
+        res.embeddings = _ptr(embeddings_out)
+        res.embeddings_memory = _lib.MEM_DEVICE if device_embeddings else _lib.MEM_HOST
+        bufs = (embeddings_out,) + tuple(bufs[1:])
+    else:
+        res, bufs = _alloc_outputs(n_obs, n_vars, max(nc, 0), device_embeddings, device)
     err = _lib.errbuf()
     st = lib.scxpca_randomized(C.byref(csr), C.byref(p), C.byref(res), err, len(err))
     _lib.check(st, err)
@@ -235,7 +245,9 @@ class Plan:
                  n_oversamples: int = 10, n_power_iterations: int = 2, zero_center: bool = True,
                  scale: bool = False, clip_max: float | None = None, seed: int = 0,
                  qr_method: str = "householder", math_mode: str = "strict_fp32",
-                 spmm_policy: str = "default", device: int = 0):
+                 spmm_policy: str = "default", device: int = 0, stream: int | None = None):
+        """``stream`` is a raw ``cudaStream_t`` handle (e.g. ``torch.cuda.Stream().cuda_stream``)
+        every kernel of this plan is ordered on; None lets the plan own a stream."""
         self._lib = _lib.load()
         csr, keep, mem, dev = _prepare_csr(indptr, indices, values, shape)
         if dev is not None:
@@ -247,6 +259,8 @@ class Plan:
         self.scale = scale
         self._params = _params(n_components, n_oversamples, n_power_iterations, zero_center,
                                scale, clip_max, seed, qr_method, math_mode, spmm_policy, device)
+        if stream:
+            self._params.stream = int(stream)
         self._keep = keep if mem == _lib.MEM_DEVICE else None  # borrowed device CSR must live
         handle = C.c_void_p()
         err = _lib.errbuf()
@@ -259,6 +273,21 @@ class Plan:
         nbytes = C.c_int64()
         self._lib.scxpca_plan_info(self._h, C.byref(k), C.byref(ld), C.byref(nbytes))
         self.k, self.ld, self.device_bytes = int(k.value), int(ld.value), int(nbytes.value)
+
+    def set_profiling(self, enable: bool = True) -> None:
+        """Enable per-stage CUDA-event timing (resets the counters)."""
+        self._lib.scxpca_plan_set_profiling(self._h, 1 if enable else 0)
+
+    def profile(self) -> dict:
+        """Per-stage launches and device ms accumulated since set_profiling()."""
+        pr = _lib.Profile()
+        self._lib.scxpca_plan_get_profile(self._h, C.byref(pr))
+        return {
+            "stages": {name: {"launches": int(pr.launches[i]), "device_ms": float(pr.device_ms[i])}
+                       for i, name in enumerate(_lib.STAGES)},
+            "kernel_launches": int(pr.kernel_launches),
+            "runs": int(pr.runs),
+        }
 
     def close(self):
         if getattr(self, "_h", None):

@@ -37,6 +37,7 @@ cudaError_t launch_validate_csr(int dtype, const int64_t* indptr, const int32_t*
                                 const void* val, int64_t n, int64_t g, int64_t nnz,
                                 int32_t* flags, cudaStream_t st, int num_sms) {
   int grid = grid_for(n * 32 + 32, 256, num_sms, 8);
+  note_launches(1);
   switch (dtype) {
     case 0: k_validate_csr<float><<<grid, 256, 0, st>>>(indptr, idx, (const float*)val, n, g, nnz, flags); break;
     case 1: k_validate_csr<__nv_bfloat16><<<grid, 256, 0, st>>>(indptr, idx, (const __nv_bfloat16*)val, n, g, nnz, flags); break;
@@ -117,6 +118,7 @@ cudaError_t launch_sort_rows(int dtype, const int64_t* indptr, int32_t* idx, voi
                              cudaStream_t st, int num_sms) {
   if (n == 0) return cudaSuccess;
   int grid = grid_for(n, 1, num_sms, 8);
+  note_launches(1);
   switch (dtype) {
     case 0: k_sort_rows<float><<<grid, 256, 0, st>>>(indptr, idx, (float*)val, n); break;
     case 1: k_sort_rows<__nv_bfloat16><<<grid, 256, 0, st>>>(indptr, idx, (__nv_bfloat16*)val, n); break;

@@ -68,6 +68,7 @@ __global__ void __launch_bounds__(256) k_gram(const T* __restrict__ A, int64_t n
 
 template <typename T>
 static cudaError_t gram_t(const T* A, int64_t n, int ld, double* part, int nparts, cudaStream_t st) {
+  note_launches(1);
   switch (ld) {
     case 32: k_gram<T, 32><<<nparts, 256, 0, st>>>(A, n, part); break;
     case 64: k_gram<T, 64><<<nparts, 256, 0, st>>>(A, n, part); break;
@@ -176,6 +177,7 @@ cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shif
   size_t smem = (size_t)k * k * sizeof(double);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(k_cholesky, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  note_launches(1);
   k_cholesky<<<1, 256, smem, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
   return cudaGetLastError();
 }
@@ -220,6 +222,7 @@ cudaError_t launch_apply_right_f32(const float* In, int64_t n, int ld, const flo
   if (n == 0) return cudaSuccess;
   size_t smem = (size_t)ld * ld * sizeof(float);
   int grid = grid_for(n * 32, 256, num_sms, 4);
+  note_launches(1);
   switch (ld) {
     case 32: k_apply_right_f32<1><<<grid, 256, smem, st>>>(In, n, M, Out); break;
     case 64: k_apply_right_f32<2><<<grid, 256, smem, st>>>(In, n, M, Out); break;
@@ -268,6 +271,7 @@ cudaError_t launch_center_apply(const double* W, int64_t g, int ld, const double
   cudaFuncSetAttribute(k_center_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int rpb = 256 / ld;
   int grid = (int)std::min<int64_t>((g + rpb - 1) / rpb, 1184);
+  note_launches(1);
   k_center_apply<<<grid, 256, smem, st>>>(W, g, ld, mu, s, M, Z);
   return cudaGetLastError();
 }
@@ -301,12 +305,14 @@ __global__ void k_mean_prefactor(const float* __restrict__ Vf, int64_t g, int ld
 
 cudaError_t launch_mean_prefactor(const float* Vf, int64_t g, int ld, const double* mu, float* mc,
                                   cudaStream_t st) {
+  note_launches(1);
   k_mean_prefactor<<<ld, 256, 0, st>>>(Vf, g, ld, mu, mc);
   return cudaGetLastError();
 }
 
 cudaError_t launch_round_v(const double* A, int64_t g, int ld, const double* mu, float* Vf,
                            float* mc, cudaStream_t st) {
+  note_launches(1);
   k_round_v<<<(int)std::min<int64_t>((g * ld + 255) / 256, 1184), 256, 0, st>>>(A, g, ld, Vf);
   return launch_mean_prefactor(Vf, g, ld, mu, mc, st);
 }
@@ -443,6 +449,7 @@ cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, dou
     smem = one;
   }
   cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  note_launches(1);
   k_jacobi<<<1, 256, smem, st>>>(C, k, ld, evals, evecs, eglob, sweeps);
   return cudaGetLastError();
 }
@@ -488,6 +495,7 @@ cudaError_t launch_ritz_finish(const double* B, int64_t g, int ld, int k, int nc
   size_t smem = (size_t)(ld * nc + nc) * sizeof(double);
   cudaFuncSetAttribute(k_ritz_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int grid = (int)std::min<int64_t>(g, 2048);
+  note_launches(1);
   k_ritz_finish<<<grid, 128, smem, st>>>(B, g, ld, k, nc, evals, evecs, Rinv2, sigma, components,
                                          M_emb);
   return cudaGetLastError();
@@ -544,6 +552,7 @@ cudaError_t launch_embed(const float* Q, int64_t n, int ld, int k, const float* 
   int ncp = (nc + 31) / 32 * 32;
   size_t smem = (size_t)ld * ncp * sizeof(float);
   int grid = grid_for(n * 32, 256, num_sms, 4);
+  note_launches(1);
   switch (ld) {
     case 32: k_embed<1><<<grid, 256, smem, st>>>(Q, n, k, M_emb, nc, U); break;
     case 64:
@@ -603,6 +612,7 @@ cudaError_t launch_gaussian(uint64_t seed, int64_t n_rows, int64_t n_cols, float
                             cudaStream_t st, int num_sms) {
   int64_t total = n_rows * n_cols;
   if (total == 0) return cudaSuccess;
+  note_launches(1);
   k_gaussian<<<grid_for(total, 256, num_sms), 256, 0, st>>>(seed, n_rows, n_cols, out, ld_pad);
   return cudaGetLastError();
 }
@@ -619,6 +629,7 @@ __global__ void k_colmajor_to_padded(const float* __restrict__ in, int64_t n_row
 cudaError_t launch_colmajor_to_padded(const float* in, int64_t n_rows, int64_t n_cols, int ld,
                                       float* out, cudaStream_t st, int num_sms) {
   if (n_rows == 0) return cudaSuccess;
+  note_launches(1);
   k_colmajor_to_padded<<<grid_for(n_rows * ld, 256, num_sms), 256, 0, st>>>(in, n_rows, n_cols, ld, out);
   return cudaGetLastError();
 }

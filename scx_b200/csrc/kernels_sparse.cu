@@ -259,9 +259,11 @@ static cudaError_t col_stats_t(const int32_t* idx, const void* val, int64_t nnz,
       cudaFuncSetAttribute(k_col_stats<ValT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_col_stats<ValT><<<nparts, 512, smem, st>>>(idx, v, nnz, g, partial);
     k_reduce_rows<double><<<grid_for(2 * g, 256, num_sms), 256, 0, st>>>(partial, nparts, 2 * g, out, 0);
+    note_launches(2);
   } else {
     cudaMemsetAsync(out, 0, sizeof(double) * 2 * g, st);
     k_col_stats_global<ValT><<<grid_for(nnz, 256, num_sms), 256, 0, st>>>(idx, v, nnz, g, out);
+    note_launches(1);
   }
   return cudaGetLastError();
 }
@@ -282,6 +284,7 @@ static cudaError_t transform_in(int out_dtype, const int32_t* idx, const void* i
                                 const double* cshift, double clip, cudaStream_t st, int num_sms) {
   const InT* src = static_cast<const InT*>(in);
   int grid = grid_for(nnz, 256, num_sms);
+  note_launches(1);
   switch (out_dtype) {
     case 0: k_transform_values<InT, float><<<grid, 256, 0, st>>>(idx, src, (float*)out, nnz, mode, mu, inv_std, cshift, clip); break;
     case 1: k_transform_values<InT, __nv_bfloat16><<<grid, 256, 0, st>>>(idx, src, (__nv_bfloat16*)out, nnz, mode, mu, inv_std, cshift, clip); break;
@@ -307,6 +310,7 @@ static cudaError_t fwd_c(const int64_t* indptr, const int32_t* idx, const void* 
                          const float* V, int ldv, const float* mc, float* Y, int ldy,
                          cudaStream_t st, int num_sms) {
   int grid = grid_for(n * 32, 256, num_sms, 8);
+  note_launches(1);
   k_spmm_fwd<C, ValT><<<grid, 256, 0, st>>>(indptr, idx, static_cast<const ValT*>(val), n, V, ldv,
                                             mc, Y, ldy);
   return cudaGetLastError();
@@ -338,6 +342,7 @@ cudaError_t launch_spmm_fwd(int dtype, int ld, const int64_t* indptr, const int3
 cudaError_t launch_row_block_ptr(const int64_t* indptr, const int32_t* idx, int64_t n, int nb,
                                  int gb, int32_t* rbp, cudaStream_t st, int num_sms) {
   if (n == 0) return cudaSuccess;
+  note_launches(1);
   k_row_block_ptr<<<grid_for(n * 32, 256, num_sms, 8), 256, 0, st>>>(indptr, idx, n, nb, gb, rbp);
   return cudaGetLastError();
 }
@@ -352,6 +357,7 @@ static cudaError_t spmm_t_c(const int64_t* indptr, const int32_t* idx, const voi
   auto kern = k_spmm_t<C, ValT, GB>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid(nchunks, nb);
+  note_launches(1);
   kern<<<grid, 512, smem, st>>>(indptr, idx, static_cast<const ValT*>(val), n, g, rbp, nb,
                                 rows_per_chunk, Q, ldq, part);
   return cudaGetLastError();
@@ -382,12 +388,14 @@ cudaError_t launch_spmm_t(int dtype, int ld, const int64_t* indptr, const int32_
 
 cudaError_t launch_reduce_rows_f32(const float* part, int nparts, int64_t len, double* out,
                                    int accumulate, cudaStream_t st, int num_sms) {
+  note_launches(1);
   k_reduce_rows<float><<<grid_for(len, 256, num_sms), 256, 0, st>>>(part, nparts, len, out, accumulate);
   return cudaGetLastError();
 }
 
 cudaError_t launch_reduce_rows_f64(const double* part, int nparts, int64_t len, double* out,
                                    int accumulate, cudaStream_t st, int num_sms) {
+  note_launches(1);
   k_reduce_rows<double><<<grid_for(len, 256, num_sms), 256, 0, st>>>(part, nparts, len, out, accumulate);
   return cudaGetLastError();
 }

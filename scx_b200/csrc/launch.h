@@ -8,6 +8,11 @@
 
 namespace scx {
 
+// Process-wide count of kernels launched by this library (every launcher
+// adds the number of kernels it enqueued).
+void note_launches(int n);
+int64_t launches_total();
+
 constexpr size_t kStatsSmemMax = 200 * 1024;  // per-block FP64 gene accumulators
 constexpr int kTransposeGeneBlock = 256;       // genes per block, CUDA-core transposed product
 

@@ -15,6 +15,7 @@
 // embeddings) before the final projection.  qr(Z) is CholeskyQR2 in FP64.
 // The SVD of B is an FP64 Jacobi eigendecomposition of B^T B on the device.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,6 +27,12 @@
 #include "launch.h"
 
 using namespace scx;
+
+namespace scx {
+static std::atomic<int64_t> g_launches{0};
+void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+int64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace scx
 
 namespace {
 
@@ -145,6 +152,17 @@ struct scxpca_plan {
   size_t device_bytes = 0;
 
   double tau = 1e-8;
+
+  // opt-in stage timing
+  bool profiling = false;
+  std::vector<cudaEvent_t> events;
+  std::vector<std::pair<int, int>> marks;  // (stage, index of the begin event)
+  int events_used = 0;
+  scxpca_profile prof{};
+
+  ~scxpca_plan() {
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+  }
 };
 
 namespace {
@@ -446,17 +464,55 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
   }
 }
 
+// ---- stage timing: events bracket each stage on the plan's stream ----
+int stage_begin(scxpca_plan* pl) {
+  if (!pl->profiling) return -1;
+  if (pl->events_used + 2 > (int)pl->events.size()) {
+    for (int i = 0; i < 64; ++i) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      pl->events.push_back(e);
+    }
+  }
+  int i = pl->events_used;
+  pl->events_used += 2;
+  CK(cudaEventRecord(pl->events[i], pl->stream));
+  return i;
+}
+
+void stage_end(scxpca_plan* pl, int stage, int i) {
+  if (i < 0) return;
+  CK(cudaEventRecord(pl->events[i + 1], pl->stream));
+  pl->marks.emplace_back(stage, i);
+}
+
+// Fold the recorded stage intervals into the profile (stream already synced).
+void collect_stages(scxpca_plan* pl) {
+  for (auto& m : pl->marks) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, pl->events[m.second], pl->events[m.second + 1]));
+    pl->prof.device_ms[m.first] += ms;
+    pl->prof.launches[m.first] += 1;
+  }
+  pl->marks.clear();
+  pl->events_used = 0;
+}
+
 // Tall Gram + Cholesky (FP64) of the plan's Y buffer.
 void tall_chol(scxpca_plan* pl, const float* A, int64_t rows, double* Rinv, float* Rinv_f,
                int shift) {
   cudaStream_t st = pl->stream;
   const int ld = (int)pl->ld;
   const int parts = (int)std::max<int64_t>(1, std::min<int64_t>(pl->gram_parts, (rows + 31) / 32));
+  int s = stage_begin(pl);
   CK(launch_gram_f32(A, rows, ld, pl->gpart.as<double>(), parts, st));
   CK(launch_reduce_rows_f64(pl->gpart.as<double>(), parts, (int64_t)ld * ld + ld, pl->G.as<double>(), 0,
                             st, pl->num_sms));
+  stage_end(pl, SCXPCA_STAGE_GRAM, s);
+  s = stage_begin(pl);
   CK(launch_cholesky(pl->G.as<double>(), (int)pl->k, ld, pl->tau, shift, pl->R.as<double>(), Rinv,
                      Rinv_f, pl->status.as<int>(), st));
+  stage_end(pl, SCXPCA_STAGE_SMALL, s);
 }
 
 // CholeskyQR2 of a gene-side FP64 matrix in place.
@@ -476,17 +532,23 @@ void small_qr(scxpca_plan* pl, double* A, int shift) {
 // W = X^T A (raw, uncentred), FP64, for a tall float A (n x ld).
 void rmatmat_raw(scxpca_plan* pl, const float* A) {
   cudaStream_t st = pl->stream;
+  int s = stage_begin(pl);
   CK(launch_spmm_t(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, (int32_t)pl->g,
                    pl->rbp.as<int32_t>(), pl->nb, pl->nchunks, pl->rows_per_chunk, A,
                    pl->wpart.as<float>(), st));
+  stage_end(pl, SCXPCA_STAGE_TRANSPOSE, s);
+  s = stage_begin(pl);
   CK(launch_reduce_rows_f32(pl->wpart.as<float>(), pl->nchunks, pl->g * pl->ld, pl->W.as<double>(), 0,
                             st, pl->num_sms));
+  stage_end(pl, SCXPCA_STAGE_REDUCE, s);
 }
 
 void forward(scxpca_plan* pl) {
+  int s = stage_begin(pl);
   CK(launch_spmm_fwd(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, pl->V.as<float>(),
                      pl->centered ? pl->mc.as<float>() : nullptr, pl->Y.as<float>(), pl->stream,
                      pl->num_sms));
+  stage_end(pl, SCXPCA_STAGE_FORWARD, s);
 }
 
 void load_omega(scxpca_plan* pl, const scxpca_params* p) {
@@ -525,27 +587,35 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   const double* mu = pl->centered ? pl->d_mu.as<double>() : nullptr;
   double* sY = pl->G.as<double>() + (size_t)ld * ld;  // column sums follow the Gram
 
+  const int64_t launches0 = launches_total();
   CK(cudaMemsetAsync(pl->status.p, 0, sizeof(int) * 4, st));
+  int s = stage_begin(pl);
   load_omega(pl, &p);
+  stage_end(pl, SCXPCA_STAGE_SMALL, s);
   // Y = (X - mu) Omega ; qr(Y)
   forward(pl);
   tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift);
   for (int64_t it = 0; it < p.n_power_iterations; ++it) {
     // Z = (X - mu)^T Q = (X^T Y - mu (1^T Y)) R^{-1}
     rmatmat_raw(pl, pl->Y.as<float>());
+    s = stage_begin(pl);
     CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->Rinv.as<double>(),
                            pl->Z.as<double>(), st));
     small_qr(pl, pl->Z.as<double>(), shift);
     CK(launch_round_v(pl->Z.as<double>(), pl->g, ld, mu, pl->V.as<float>(), pl->mc.as<float>(), st));
+    stage_end(pl, SCXPCA_STAGE_SMALL, s);
     forward(pl);
     tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift);
   }
   // Explicit Q = Y R^{-1}, re-orthonormalised by a second FP64 Cholesky pass.
+  s = stage_begin(pl);
   CK(launch_apply_right_f32(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(), st,
                             pl->num_sms));
+  stage_end(pl, SCXPCA_STAGE_APPLY, s);
   tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift);
   // B = (X - mu)^T Q R2^{-1}
   rmatmat_raw(pl, pl->Y.as<float>());
+  s = stage_begin(pl);
   CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->R2inv.as<double>(),
                          pl->Z.as<double>(), st));
   // SVD of B through the FP64 eigendecomposition of B^T B.
@@ -557,6 +627,7 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   CK(launch_ritz_finish(pl->Z.as<double>(), pl->g, ld, (int)pl->k, (int)pl->nc, pl->evals.as<double>(),
                         pl->evecs.as<double>(), pl->R2inv.as<double>(), pl->sigma.as<double>(),
                         pl->comps.as<float>(), pl->M_emb.as<float>(), st));
+  stage_end(pl, SCXPCA_STAGE_SMALL, s);
   // Embeddings U = Q R2^{-1} E Sigma (first n_components).
   float* U = out->embeddings;
   const bool host_out = out->embeddings_memory != SCXPCA_MEM_DEVICE;
@@ -564,8 +635,12 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
     pl->U.alloc(sizeof(float) * pl->n * pl->nc);
     U = pl->U.as<float>();
   }
+  s = stage_begin(pl);
   CK(launch_embed(pl->Y.as<float>(), pl->n, ld, (int)pl->k, pl->M_emb.as<float>(), (int)pl->nc, U, st,
                   pl->num_sms));
+  stage_end(pl, SCXPCA_STAGE_EMBED, s);
+  pl->prof.kernel_launches += launches_total() - launches0;
+  pl->prof.runs += 1;
   if (host_out)
     CK(cudaMemcpyAsync(out->embeddings, U, sizeof(float) * pl->n * pl->nc, cudaMemcpyDeviceToHost, st));
 
@@ -577,6 +652,7 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
     CK(cudaMemcpyAsync(out->components, pl->comps.p, sizeof(float) * pl->nc * pl->g,
                        cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  collect_stages(pl);
   if (hstatus[0] < 0)
     fail(SCXPCA_NOT_SPD, "CholeskyQR2 failed: non-SPD; retry with qr_method='householder'");
 
@@ -669,6 +745,21 @@ int32_t scxpca_plan_run(scxpca_plan* plan, const scxpca_params* params, scxpca_r
     DeviceGuard dg(plan->device);
     run_plan(plan, params, out);
   });
+}
+
+int32_t scxpca_plan_set_profiling(scxpca_plan* plan, int32_t enable) {
+  if (!plan) return SCXPCA_INVALID_ARGUMENT;
+  plan->profiling = enable != 0;
+  plan->prof = scxpca_profile{};
+  plan->marks.clear();
+  plan->events_used = 0;
+  return SCXPCA_OK;
+}
+
+int32_t scxpca_plan_get_profile(const scxpca_plan* plan, scxpca_profile* out) {
+  if (!plan || !out) return SCXPCA_INVALID_ARGUMENT;
+  *out = plan->prof;
+  return SCXPCA_OK;
 }
 
 int32_t scxpca_plan_info(const scxpca_plan* plan, int64_t* k, int64_t* ld, int64_t* device_bytes) {

@@ -178,6 +178,7 @@ __global__ void k_fill(uint64_t seed, int64_t n, int64_t g, float shape,
 
 cudaError_t launch_synth_gene_means(uint64_t seed, int64_t g, double loc, float* mu_g,
                                     cudaStream_t st) {
+  note_launches(1);
   k_gene_means<<<(int)((g + 255) / 256), 256, 0, st>>>(seed, g, (float)loc, mu_g);
   return cudaGetLastError();
 }
@@ -186,6 +187,7 @@ cudaError_t launch_synth_count(uint64_t seed, int64_t n, int64_t g, double loc, 
                                const float* mu_g, int64_t* row_nnz, float* rowsum,
                                cudaStream_t st, int num_sms) {
   (void)loc;
+  note_launches(1);
   k_count<<<grid_for(n * 32, 256, num_sms, 8), 256, 0, st>>>(seed, n, g, (float)(1.0 / disp), mu_g,
                                                             row_nnz, rowsum);
   return cudaGetLastError();
@@ -195,6 +197,7 @@ cudaError_t launch_synth_fill(uint64_t seed, int64_t n, int64_t g, double loc, d
                               const float* mu_g, const int64_t* indptr, const float* rowsum,
                               int32_t* idx, float* val, cudaStream_t st, int num_sms) {
   (void)loc;
+  note_launches(1);
   k_fill<<<grid_for(n * 32, 256, num_sms, 8), 256, 0, st>>>(seed, n, g, (float)(1.0 / disp), mu_g,
                                                            indptr, rowsum, idx, val);
   return cudaGetLastError();
