@@ -1,0 +1,834 @@
+// Tensor-core SpMM for the mixed-precision path (BF16/FP16 values, FP32
+// accumulation in TMEM), sm_100a.
+//
+// Sparse format ("tile-chunk packed"), built once per plan:
+//   rows are grouped in tiles of 128 cells, genes in chunks of 64; the stored
+//   entries of tile t and chunk c form one segment, ordered by row then gene,
+//   padded with zero words to a multiple of 4 entries (16 bytes) so that every
+//   segment can be fetched with bulk copies.  Each entry is one 32-bit word:
+//       bits  0..15  value (bf16 or f16 bits)
+//       bits 16..29  byte offset of (row within the tile, gene within the
+//                    chunk) in the 128 x 64 swizzled tile (sw128_offset)
+//   meta[t * n_chunks + c] (16 bytes) = {segment start, q[0..2], q[3]}: q[w] is
+//   the number of entries in rows < 32 (w + 1), so densify warp w handles
+//   entries [q[w-1], q[w]) and q[3] is the segment's real entry count.
+//   4 bytes per stored entry instead of 6 (bf16 value + int32 index).
+//
+// Both products densify a segment into a 128 x 64 16-bit shared-memory tile
+// (128-byte swizzle, see tc.cuh) and run tcgen05.mma on it:
+//   forward    Y(128 cells x 2ld) += A(cells x 64 genes, K-major) [Vhi|Vlo]
+//   transposed Z(128 genes x 2ld) += A^T(genes x cells, MN-major) [Qhi|Qlo]
+// The dense operand enters as two 16-bit planes side by side, hi = round(x)
+// and lo = round(x - hi), so one N = 2 ld MMA multiplies both and the
+// epilogue adds the two halves: about 16 mantissa bits on the dense operand,
+// the matrix values being the only operand rounded to 16 bits.
+//
+// Warp roles (23 warps): warps 0-15 densify in four groups of four that take
+// stages in turn (each warp zeroes its 32 rows, scatters its quarter from the
+// staging ring, fences, arrives); warps 16-19 drain TMEM (one lane quarter
+// each); warp 20 issues the MMAs from one thread; warp 21 loads the dense
+// operand by TMA; warp 22 bulk-copies segment metadata (per tile) and entry
+// pieces (up to kCap entries) into shared-memory rings, many segments ahead.
+// All waits are bounded (tc.cuh).
+#include <algorithm>
+
+#include "common.cuh"
+#include "launch.h"
+#include "tc.cuh"
+
+namespace scx {
+
+using namespace tc;
+
+namespace {
+
+constexpr int TM = 128;          // cells per tile
+constexpr int CW = 64;           // genes per chunk
+constexpr int kCap = 1024;       // entries per staging slot (4 KB)
+constexpr int kGroups = 4;       // densify groups of four warps, one stage each in turn
+constexpr int kThreads = 736;    // 23 warps
+constexpr int kMaxChunks = 128;  // genes <= 8192
+constexpr int W_EPI = 4 * kGroups, W_MMA = W_EPI + 4, W_DENSE = W_MMA + 1, W_SPARSE = W_MMA + 2;
+
+struct SegMeta {
+  int64_t start;
+  uint16_t q[4];
+};
+static_assert(sizeof(SegMeta) == 16, "segment metadata is one 16-byte record");
+
+__host__ __device__ constexpr int fwd_stages(int LD) { return LD == 64 ? 4 : 3; }
+__host__ __device__ constexpr int fwd_slots(int LD) { return LD == 64 ? 16 : 12; }
+__host__ __device__ constexpr int rmat_stages(int LD) { return LD == 64 ? 3 : 2; }
+__host__ __device__ constexpr int rmat_slots(int LD) { return LD == 64 ? 12 : 6; }
+
+__host__ __device__ __forceinline__ int padded4(int x) { return (x + 3) & ~3; }
+__host__ __device__ __forceinline__ int n_pieces(int real) { return (padded4(real) + kCap - 1) / kCap; }
+
+// ---------------------------------------------------------------------------
+// format build
+// ---------------------------------------------------------------------------
+__global__ void k_tile_count(const int64_t* __restrict__ indptr, const int32_t* __restrict__ idx,
+                             int64_t n, int64_t n_tiles, int nc, int64_t* __restrict__ counts) {
+  extern __shared__ int cnt[];
+  for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) cnt[c] = 0;
+    __syncthreads();
+    const int64_t r0 = t * TM, r1 = min(n, r0 + TM);
+    for (int64_t p = indptr[r0] + threadIdx.x; p < indptr[r1]; p += blockDim.x)
+      atomicAdd(&cnt[__ldg(idx + p) >> 6], 1);
+    __syncthreads();
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) counts[t * nc + c] = padded4(cnt[c]);
+    __syncthreads();
+  }
+}
+
+__global__ void k_tile_fill(const int64_t* __restrict__ indptr, const int32_t* __restrict__ idx,
+                            const uint16_t* __restrict__ val, int64_t n, int64_t n_tiles, int nc,
+                            const int64_t* __restrict__ seg, uint32_t* __restrict__ ent,
+                            SegMeta* __restrict__ meta) {
+  extern __shared__ int sm[];
+  int* colpre = sm;            // [TM][nc]: entries of chunk c in rows before r
+  int* rowpre = sm + TM * nc;  // [TM][nc]: entries of row r in chunks before c
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    for (int i = threadIdx.x; i < TM * nc; i += blockDim.x) colpre[i] = 0;
+    __syncthreads();
+    const int64_t r0 = t * TM;
+    const int rows = (int)min((int64_t)TM, n - r0);
+    for (int r = warp; r < rows; r += nw)
+      for (int64_t p = indptr[r0 + r] + lane; p < indptr[r0 + r + 1]; p += 32)
+        atomicAdd(&colpre[r * nc + (__ldg(idx + p) >> 6)], 1);
+    __syncthreads();
+    for (int r = threadIdx.x; r < TM; r += blockDim.x) {
+      int run = 0;
+      for (int c = 0; c < nc; ++c) {
+        rowpre[r * nc + c] = run;
+        run += colpre[r * nc + c];
+      }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+      SegMeta m;
+      m.start = seg[t * nc + c];
+      int run = 0;
+      for (int r = 0; r < TM; ++r) {
+        const int v = colpre[r * nc + c];
+        colpre[r * nc + c] = run;
+        run += v;
+        if (r == 31 || r == 63 || r == 95) m.q[r >> 5] = (uint16_t)run;
+      }
+      m.q[3] = (uint16_t)run;
+      meta[t * nc + c] = m;
+    }
+    __syncthreads();
+    for (int r = warp; r < rows; r += nw) {
+      const int64_t s = indptr[r0 + r];
+      for (int64_t p = s + lane; p < indptr[r0 + r + 1]; p += 32) {
+        const int32_t j = __ldg(idx + p);
+        const int c = j >> 6;
+        const int64_t dst = seg[t * nc + c] + colpre[r * nc + c] + ((p - s) - rowpre[r * nc + c]);
+        ent[dst] = (uint32_t)val[p] | (sw128_offset((uint32_t)r, (uint32_t)(j & 63)) << 16);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// shared pieces of the two product kernels
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
+  return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
+}
+
+__device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
+  uint32_t v;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ void sts_u16(uint32_t addr, uint32_t v) {
+  asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"((unsigned short)v) : "memory");
+}
+__device__ __forceinline__ void sts_zero16(uint32_t addr) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(addr), "r"(0u) : "memory");
+}
+
+// Two floats as a pair of 16-bit values (fmt 1 = bf16, 0 = f16), low word first.
+__device__ __forceinline__ uint32_t pack16x2(float a, float b, int fmt) {
+  if (fmt) {
+    __nv_bfloat162 p = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&p);
+  }
+  __half2 p = __floats2half2_rn(a, b);
+  return *reinterpret_cast<uint32_t*>(&p);
+}
+__device__ __forceinline__ float unpack16(uint32_t bits, int fmt) {
+  if (fmt) return __bfloat162float(__ushort_as_bfloat16((unsigned short)bits));
+  return __half2float(__ushort_as_half((unsigned short)bits));
+}
+
+// Zero rows 32q .. 32q+31 of a 128 x 64 16-bit swizzled tile, lane = row.
+// Iteration i writes physical chunk i ^ (row % 8): the 32 lanes of one store
+// cover all eight 16-byte bank groups, so every store is conflict-free.
+__device__ __forceinline__ void zero_rows(uint32_t tile, int quarter, int lane) {
+  const uint32_t row = 32u * quarter + lane;
+  const uint32_t base = tile + (row >> 3) * 1024u + (row & 7u) * 128u;
+#pragma unroll
+  for (uint32_t i = 0; i < 8; ++i) sts_zero16(base + ((i ^ (row & 7u)) << 4));
+}
+
+__device__ __forceinline__ void scatter_one(uint32_t tile, uint32_t w) { sts_u16(tile + (w >> 16), w & 0xFFFFu); }
+
+// Staging ring shared by the sparse loader and the densify warps.
+struct Ring {
+  uint32_t base;    // shared address of slot 0
+  uint64_t* full;   // [nslot], 1 arrival + tx bytes
+  uint64_t* empty;  // [nslot], one arrival per densify warp of the consuming group
+  int nslot;
+};
+
+// Densify warp (quarter q): scatter the quarter's entries of one segment into
+// `tile` (already zeroed), consuming the segment's pieces from the ring.
+__device__ __forceinline__ bool densify_segment(uint32_t tile, const SegMeta& m, const Ring& ring,
+                                                uint32_t& pc, int q, int lane, volatile int* abort_flag,
+                                                int* err, int code) {
+  const int plen = padded4(m.q[3]);
+  const int lo = q ? (int)m.q[q - 1] : 0;
+  const int hi = (int)m.q[q];
+  for (int p0 = 0; p0 < plen; p0 += kCap, ++pc) {
+    const int slot = (int)(pc % (uint32_t)ring.nslot);
+    if (!warp_wait(&ring.full[slot], (pc / ring.nslot) & 1u, abort_flag, err, code)) return false;
+    const uint32_t b = ring.base + (uint32_t)slot * (kCap * 4u) - (uint32_t)p0 * 4u;
+    const int e = min(hi, p0 + kCap);
+    int p = max(lo, p0) + lane;
+    for (; p + 96 < e; p += 128) {
+      const uint32_t w0 = lds_u32(b + 4u * p), w1 = lds_u32(b + 4u * (p + 32));
+      const uint32_t w2 = lds_u32(b + 4u * (p + 64)), w3 = lds_u32(b + 4u * (p + 96));
+      scatter_one(tile, w0);
+      scatter_one(tile, w1);
+      scatter_one(tile, w2);
+      scatter_one(tile, w3);
+    }
+    for (; p < e; p += 32) scatter_one(tile, lds_u32(b + 4u * p));
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&ring.empty[slot]);
+  }
+  return true;
+}
+
+// Sparse loader: bulk-copy one segment into the ring, piece by piece.
+__device__ __forceinline__ bool load_segment(const uint32_t* __restrict__ ent, const SegMeta& m,
+                                             const Ring& ring, uint32_t* ring_ptr, uint32_t& pc,
+                                             volatile int* abort_flag, int* err, int code) {
+  const int plen = padded4(m.q[3]);
+  for (int p0 = 0; p0 < plen; p0 += kCap, ++pc) {
+    const int slot = (int)(pc % (uint32_t)ring.nslot);
+    if (!mbar_wait(&ring.empty[slot], ((pc / ring.nslot) & 1u) ^ 1u, abort_flag, err, code)) return false;
+    const uint32_t bytes = (uint32_t)min(kCap, plen - p0) * 4u;
+    mbar_arrive_expect_tx(&ring.full[slot], bytes);
+    bulk_load(ring_ptr + (size_t)slot * kCap, ent + m.start + p0, bytes, &ring.full[slot]);
+  }
+  return true;
+}
+
+// Sparse loader: metadata of tile t (nc records) into meta ring slot mi & 1.
+__device__ __forceinline__ bool load_meta(const SegMeta* __restrict__ meta, int64_t t, int nc,
+                                          SegMeta* mring, uint64_t* mfull, uint64_t* mempty, uint32_t mi,
+                                          volatile int* abort_flag, int* err, int code) {
+  const int ms = mi & 1u;
+  if (!mbar_wait(&mempty[ms], ((mi >> 1) & 1u) ^ 1u, abort_flag, err, code)) return false;
+  const uint32_t bytes = (uint32_t)nc * 16u;
+  mbar_arrive_expect_tx(&mfull[ms], bytes);
+  bulk_load(mring + (size_t)ms * kMaxChunks, meta + t * nc, bytes, &mfull[ms]);
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// forward: Y[tile rows, :LD] = A_tile (Vhi + Vlo) - mc   (persistent over tiles)
+// ---------------------------------------------------------------------------
+template <int LD>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_fwd_tc(const uint32_t* __restrict__ ent, const SegMeta* __restrict__ meta, int64_t n_tiles, int nc,
+             int64_t n, const __grid_constant__ CUtensorMap vmap_hi, const __grid_constant__ CUtensorMap vmap_lo,
+             const float* __restrict__ mc, float* __restrict__ Y, uint16_t* __restrict__ Yhi,
+             uint16_t* __restrict__ Ylo, int fmt, int* err) {
+  constexpr int N2 = 2 * LD;                // [hi | lo] columns
+  constexpr int S = fwd_stages(LD);
+  constexpr int NSLOT = fwd_slots(LD);
+  constexpr int A_BYTES = TM * CW * 2;      // 16 KB
+  constexpr int B_PLANE = CW * LD * 2;      // 64 genes x LD, one 16-bit plane
+  constexpr int B_BYTES = 2 * B_PLANE;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = align1024(smem_raw);
+  uint8_t* As = smem;
+  uint8_t* Bs = As + S * A_BYTES;
+  uint32_t* ring_ptr = reinterpret_cast<uint32_t*>(Bs + S * B_BYTES);
+  SegMeta* mring = reinterpret_cast<SegMeta*>(ring_ptr + NSLOT * kCap);  // [2][kMaxChunks]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(mring + 2 * kMaxChunks);
+  uint64_t* full = bars;
+  uint64_t* empty = full + S;
+  uint64_t* acc_full = empty + S;
+  uint64_t* acc_empty = acc_full + 2;
+  uint64_t* sfull = acc_empty + 2;
+  uint64_t* sempty = sfull + NSLOT;
+  uint64_t* mfull = sempty + NSLOT;
+  uint64_t* mempty = mfull + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mempty + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const Ring ring{smem_u32(ring_ptr), sfull, sempty, NSLOT};
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 129);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], 128);
+      mbar_init(&mfull[a], 1);
+      mbar_init(&mempty[a], 4 * kGroups);
+    }
+    for (int s = 0; s < NSLOT; ++s) {
+      mbar_init(&sfull[s], 1);
+      mbar_init(&sempty[s], 4);
+    }
+    *abort_flag = 0;
+    mbar_fence_init();
+  }
+  if (warp == W_MMA) {
+    tmem_alloc(tmem_slot, 2 * N2);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < W_EPI) {
+    // ---- densify: group (warp / 4) takes stages it % kGroups == group ----
+    const int group = warp >> 2, q = warp & 3;
+    uint32_t it = 0, pc = 0, ti = 0;
+    for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++ti) {
+      if (!warp_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 11)) goto done;
+      const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
+      for (int c = 0; c < nc; ++c, ++it) {
+        const SegMeta m = mt[c];
+        if ((int)(it % kGroups) != group) {
+          pc += n_pieces(m.q[3]);
+          continue;
+        }
+        const int s = it % S;
+        if (!warp_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 12)) goto done;
+        const uint32_t tile = smem_u32(As + s * A_BYTES);
+        zero_rows(tile, q, lane);
+        __syncwarp();
+        if (!densify_segment(tile, m, ring, pc, q, lane, abort_flag, err, 13)) goto done;
+        fence_proxy_async_smem();
+        mbar_arrive(&full[s]);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&mempty[ti & 1u]);
+    }
+  } else if (warp < W_MMA) {
+    // ---- epilogue: TMEM -> hi + lo halves -> Y (FP32) and its hi/lo 16-bit planes ----
+    const int q = warp & 3;
+    const uint32_t row = 32u * q + lane;
+    uint32_t k = 0;
+    for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++k) {
+      const uint32_t a = k & 1u, ph = (k >> 1) & 1u;
+      if (!warp_wait(&acc_full[a], ph, abort_flag, err, 14)) goto done;
+      tc_fence_after();
+      const uint32_t tbase = tmem + ((32u * q) << 16) + a * N2;
+      const int64_t grow = t * TM + row;
+#pragma unroll 1
+      for (int cb = 0; cb < LD / 16; ++cb) {
+        uint32_t h[16], l[16];
+        tmem_ld16(tbase + cb * 16, h);
+        tmem_ld16(tbase + LD + cb * 16, l);
+        tmem_wait_ld();
+        if (grow < n) {
+          float o[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            o[i] = __uint_as_float(h[i]) + __uint_as_float(l[i]) - __ldg(mc + cb * 16 + i);
+          float4* yr = reinterpret_cast<float4*>(Y + grow * LD + cb * 16);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) yr[i] = make_float4(o[4 * i], o[4 * i + 1], o[4 * i + 2], o[4 * i + 3]);
+          uint32_t ph16[8], pl16[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            ph16[i] = pack16x2(o[2 * i], o[2 * i + 1], fmt);
+            pl16[i] = pack16x2(o[2 * i] - unpack16(ph16[i] & 0xFFFFu, fmt),
+                               o[2 * i + 1] - unpack16(ph16[i] >> 16, fmt), fmt);
+          }
+          uint4* hr = reinterpret_cast<uint4*>(Yhi + grow * LD + cb * 16);
+          uint4* lr = reinterpret_cast<uint4*>(Ylo + grow * LD + cb * 16);
+          hr[0] = make_uint4(ph16[0], ph16[1], ph16[2], ph16[3]);
+          hr[1] = make_uint4(ph16[4], ph16[5], ph16[6], ph16[7]);
+          lr[0] = make_uint4(pl16[0], pl16[1], pl16[2], pl16[3]);
+          lr[1] = make_uint4(pl16[4], pl16[5], pl16[6], pl16[7]);
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acc_empty[a]);
+    }
+  } else if (warp == W_MMA) {
+    // ---- MMA issuer ----
+    if (lane == 0) {
+      const uint32_t idesc = idesc_f16(128, N2, fmt, 0, 1);
+      uint32_t it = 0, k = 0;
+      for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++k) {
+        const uint32_t a = k & 1u, ph = (k >> 1) & 1u;
+        if (!mbar_wait(&acc_empty[a], ph ^ 1u, abort_flag, err, 15)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + a * N2;
+        bool ok = true;
+        for (int c = 0; c < nc; ++c, ++it) {
+          const int s = it % S;
+          if (!mbar_wait(&full[s], (it / S) & 1u, abort_flag, err, 16)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a_base = smem_u32(As + s * A_BYTES);
+          const uint32_t b_base = smem_u32(Bs + s * B_BYTES);
+#pragma unroll
+          for (int kk = 0; kk < CW / 16; ++kk)
+            umma_f16(d, sdesc_sw128(a_base + kk * 32, 16, 1024), sdesc_sw128(b_base + kk * 2048, CW * 128, 1024),
+                     idesc, (c | kk) != 0);
+          umma_commit(&empty[s]);
+        }
+        if (!ok) break;
+        umma_commit(&acc_full[a]);
+      }
+    }
+    __syncwarp();
+  } else if (warp == W_DENSE) {
+    // ---- dense loader: [Vhi | Vlo] chunk into the B stage ----
+    if (lane == 0) {
+      uint32_t it = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+        for (int c = 0; c < nc; ++c, ++it) {
+          const int s = it % S;
+          if (!mbar_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 19)) {
+            ok = false;
+            break;
+          }
+          uint8_t* b = Bs + s * B_BYTES;
+          mbar_arrive_expect_tx(&full[s], B_BYTES);
+#pragma unroll
+          for (int h = 0; h < LD / 64; ++h) {
+            tma_load_2d(b + h * (CW * 128), &vmap_hi, &full[s], 64 * h, CW * c);
+            tma_load_2d(b + B_PLANE + h * (CW * 128), &vmap_lo, &full[s], 64 * h, CW * c);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---- sparse loader: tile metadata and entry pieces, ahead of the stages ----
+    if (lane == 0) {
+      uint32_t pc = 0, ti = 0;
+      int64_t t = blockIdx.x;
+      if (t < n_tiles && !load_meta(meta, t, nc, mring, mfull, mempty, 0, abort_flag, err, 17)) goto loader_out;
+      for (; t < n_tiles; t += gridDim.x, ++ti) {
+        const int64_t tn = t + gridDim.x;
+        if (tn < n_tiles && !load_meta(meta, tn, nc, mring, mfull, mempty, ti + 1, abort_flag, err, 17))
+          break;
+        if (!mbar_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 18)) break;
+        const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
+        bool ok = true;
+        for (int c = 0; c < nc && ok; ++c) ok = load_segment(ent, mt[c], ring, ring_ptr, pc, abort_flag, err, 20);
+        if (!ok) break;
+      }
+    }
+  loader_out:
+    __syncwarp();
+  }
+done:
+  // After an abort, give MMAs and copies already issued time to land
+  // (microseconds of work) before the block frees TMEM and shared memory.
+  if (*abort_flag) __nanosleep(500000);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == W_MMA) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 2 * N2);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// transposed: part[row group][genes of this CTA, :LD] = sum over its tiles of
+// A_tile^T (Qhi_tile + Qlo_tile).  grid = G gene groups x R row groups; one
+// CTA per SM (the accumulators fill TMEM).
+// ---------------------------------------------------------------------------
+template <int LD>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_rmat_tc(const uint32_t* __restrict__ ent, const SegMeta* __restrict__ meta, int64_t n_tiles, int nc,
+              int64_t g, int n_gene_groups, const __grid_constant__ CUtensorMap qmap_hi,
+              const __grid_constant__ CUtensorMap qmap_lo, float* __restrict__ part, int fmt, int* err) {
+  constexpr int N2 = 2 * LD;
+  constexpr int S = rmat_stages(LD);
+  constexpr int NSLOT = rmat_slots(LD);
+  constexpr int SUB = TM * CW * 2;       // one 64-gene sub-tile, 16 KB
+  constexpr int A_BYTES = 2 * SUB;       // 128 genes
+  constexpr int Q_PLANE = TM * LD * 2;   // 128 cells x LD
+  constexpr int Q_BYTES = 2 * Q_PLANE;   // [hi | lo]
+  constexpr int SPG = 512 / N2;          // 128-gene super-chunks per CTA (TMEM columns)
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = align1024(smem_raw);
+  uint8_t* As = smem;
+  uint8_t* Qs = As + S * A_BYTES;  // [2 buffers][hi, lo]
+  uint32_t* ring_ptr = reinterpret_cast<uint32_t*>(Qs + 2 * Q_BYTES);
+  SegMeta* mring = reinterpret_cast<SegMeta*>(ring_ptr + NSLOT * kCap);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(mring + 2 * kMaxChunks);
+  uint64_t* full = bars;
+  uint64_t* empty = full + S;
+  uint64_t* qfull = empty + S;
+  uint64_t* qempty = qfull + 2;
+  uint64_t* sfull = qempty + 2;
+  uint64_t* sempty = sfull + NSLOT;
+  uint64_t* mfull = sempty + NSLOT;
+  uint64_t* mempty = mfull + 2;
+  uint64_t* done_bar = mempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done_bar + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const Ring ring{smem_u32(ring_ptr), sfull, sempty, NSLOT};
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gg = blockIdx.x % n_gene_groups;
+  const int rg = blockIdx.x / n_gene_groups;
+  const int R = gridDim.x / n_gene_groups;
+  const int64_t t0 = (int64_t)rg * n_tiles / R, t1 = (int64_t)(rg + 1) * n_tiles / R;
+  const int n_super = (nc + 1) / 2;
+  const int sc0 = gg * SPG, sc1 = min(n_super, sc0 + SPG);
+  const int nsc = max(0, sc1 - sc0);
+  const bool have_work = (t1 > t0) && nsc > 0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 128);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&qfull[b], 1);
+      mbar_init(&qempty[b], 1);
+      mbar_init(&mfull[b], 1);
+      mbar_init(&mempty[b], 4 * kGroups);
+    }
+    for (int s = 0; s < NSLOT; ++s) {
+      mbar_init(&sfull[s], 1);
+      mbar_init(&sempty[s], 4);
+    }
+    mbar_init(done_bar, 1);
+    *abort_flag = 0;
+    mbar_fence_init();
+  }
+  if (warp == W_MMA) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < W_EPI) {
+    // ---- densify: group (warp / 4) takes super-chunk stages it % kGroups == group ----
+    const int group = warp >> 2, q = warp & 3;
+    uint32_t it = 0, pc = 0, ti = 0;
+    if (have_work)
+      for (int64_t t = t0; t < t1; ++t, ++ti) {
+        if (!warp_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 21)) goto done;
+        const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
+        for (int sc = sc0; sc < sc1; ++sc, ++it) {
+          const SegMeta m0 = mt[2 * sc];
+          const bool two = 2 * sc + 1 < nc;
+          const SegMeta m1 = two ? mt[2 * sc + 1] : m0;
+          if ((int)(it % kGroups) != group) {
+            pc += n_pieces(m0.q[3]) + (two ? n_pieces(m1.q[3]) : 0);
+            continue;
+          }
+          const int s = it % S;
+          if (!warp_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 22)) goto done;
+          const uint32_t tile = smem_u32(As + s * A_BYTES);
+          zero_rows(tile, q, lane);
+          zero_rows(tile + SUB, q, lane);
+          __syncwarp();
+          if (!densify_segment(tile, m0, ring, pc, q, lane, abort_flag, err, 23)) goto done;
+          if (two && !densify_segment(tile + SUB, m1, ring, pc, q, lane, abort_flag, err, 23)) goto done;
+          fence_proxy_async_smem();
+          mbar_arrive(&full[s]);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&mempty[ti & 1u]);
+      }
+  } else if (warp < W_MMA) {
+    // ---- epilogue: accumulators (hi + lo halves) -> partials ----
+    const int q = warp & 3;
+    const uint32_t row = 32u * q + lane;
+    if (have_work && !warp_wait(done_bar, 0, abort_flag, err, 24)) goto done;
+    tc_fence_after();
+    for (int j = 0; j < nsc; ++j) {
+      const int64_t gene = (int64_t)(sc0 + j) * 128 + row;
+      const uint32_t tbase = tmem + ((32u * q) << 16) + j * N2;
+#pragma unroll 1
+      for (int cb = 0; cb < LD / 16; ++cb) {
+        uint32_t h[16], l[16];
+        if (have_work) {
+          tmem_ld16(tbase + cb * 16, h);
+          tmem_ld16(tbase + LD + cb * 16, l);
+          tmem_wait_ld();
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) h[i] = l[i] = 0u;
+        }
+        if (gene < g) {
+          float4* out = reinterpret_cast<float4*>(part + ((int64_t)rg * g + gene) * LD + cb * 16);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            out[i] = make_float4(__uint_as_float(h[4 * i]) + __uint_as_float(l[4 * i]),
+                                 __uint_as_float(h[4 * i + 1]) + __uint_as_float(l[4 * i + 1]),
+                                 __uint_as_float(h[4 * i + 2]) + __uint_as_float(l[4 * i + 2]),
+                                 __uint_as_float(h[4 * i + 3]) + __uint_as_float(l[4 * i + 3]));
+        }
+      }
+    }
+  } else if (warp == W_MMA) {
+    // ---- MMA issuer ----
+    if (lane == 0 && have_work) {
+      const uint32_t idesc = idesc_f16(128, N2, fmt, 1, 1);
+      uint32_t it = 0, ti = 0;
+      bool ok = true;
+      for (int64_t t = t0; t < t1 && ok; ++t, ++ti) {
+        const uint32_t b = ti & 1u;
+        if (!mbar_wait(&qfull[b], (ti >> 1) & 1u, abort_flag, err, 25)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t qh = smem_u32(Qs + b * Q_BYTES);
+        for (int sc = sc0; sc < sc1; ++sc, ++it) {
+          const int s = it % S;
+          if (!mbar_wait(&full[s], (it / S) & 1u, abort_flag, err, 26)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a_base = smem_u32(As + s * A_BYTES);
+          const uint32_t d = tmem + (sc - sc0) * N2;
+#pragma unroll
+          for (int kk = 0; kk < TM / 16; ++kk)
+            umma_f16(d, sdesc_sw128(a_base + kk * 2048, SUB, 1024), sdesc_sw128(qh + kk * 2048, TM * 128, 1024),
+                     idesc, (ti | kk) != 0);
+          umma_commit(&empty[s]);
+        }
+        if (!ok) break;
+        umma_commit(&qempty[b]);
+      }
+      if (ok) umma_commit(done_bar);
+    }
+    __syncwarp();
+  } else if (warp == W_DENSE) {
+    // ---- dense loader: [Qhi | Qlo] tiles, double-buffered per row tile ----
+    if (lane == 0 && have_work) {
+      uint32_t ti = 0;
+      for (int64_t t = t0; t < t1; ++t, ++ti) {
+        const uint32_t b = ti & 1u;
+        if (!mbar_wait(&qempty[b], ((ti >> 1) & 1u) ^ 1u, abort_flag, err, 28)) break;
+        uint8_t* qb = Qs + b * Q_BYTES;
+        mbar_arrive_expect_tx(&qfull[b], Q_BYTES);
+#pragma unroll
+        for (int h = 0; h < LD / 64; ++h) {
+          tma_load_2d(qb + h * (TM * 128), &qmap_hi, &qfull[b], 64 * h, (int)(t * TM));
+          tma_load_2d(qb + Q_PLANE + h * (TM * 128), &qmap_lo, &qfull[b], 64 * h, (int)(t * TM));
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---- sparse loader: tile metadata and entry pieces of this gene group ----
+    if (lane == 0 && have_work) {
+      uint32_t pc = 0, ti = 0;
+      int64_t t = t0;
+      if (!load_meta(meta, t, nc, mring, mfull, mempty, 0, abort_flag, err, 27)) goto loader_out;
+      for (; t < t1; ++t, ++ti) {
+        if (t + 1 < t1 && !load_meta(meta, t + 1, nc, mring, mfull, mempty, ti + 1, abort_flag, err, 27)) break;
+        if (!mbar_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 29)) break;
+        const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
+        bool ok = true;
+        for (int sc = sc0; sc < sc1 && ok; ++sc) {
+          ok = load_segment(ent, mt[2 * sc], ring, ring_ptr, pc, abort_flag, err, 30);
+          if (ok && 2 * sc + 1 < nc) ok = load_segment(ent, mt[2 * sc + 1], ring, ring_ptr, pc, abort_flag, err, 30);
+        }
+        if (!ok) break;
+      }
+    }
+  loader_out:
+    __syncwarp();
+  }
+done:
+  if (*abort_flag) __nanosleep(500000);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == W_MMA) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// hi = round16(x), lo = round16(x - hi) (fmt 1 = bf16, 0 = f16); lo may be null.
+__global__ void k_split16(float* __restrict__ in, int64_t count, uint16_t* __restrict__ hi,
+                          uint16_t* __restrict__ lo, int fmt, int write_back) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float x = in[i];
+    float h;
+    if (fmt) {
+      const __nv_bfloat16 b = __float2bfloat16_rn(x);
+      hi[i] = __bfloat16_as_ushort(b);
+      h = __bfloat162float(b);
+      if (lo) lo[i] = __bfloat16_as_ushort(__float2bfloat16_rn(x - h));
+    } else {
+      const __half b = __float2half_rn(x);
+      hi[i] = __half_as_ushort(b);
+      h = __half2float(b);
+      if (lo) lo[i] = __half_as_ushort(__float2half_rn(x - h));
+    }
+    if (write_back) in[i] = h;
+  }
+}
+
+size_t smem_tail() { return 2 * kMaxChunks * sizeof(SegMeta) + 64 * sizeof(uint64_t) + 64; }
+size_t fwd_smem(int LD) {
+  return 1024 + (size_t)fwd_stages(LD) * (TM * CW * 2 + 2 * CW * LD * 2) + (size_t)fwd_slots(LD) * kCap * 4 +
+         smem_tail();
+}
+size_t rmat_smem(int LD) {
+  return 1024 + (size_t)rmat_stages(LD) * (2 * TM * CW * 2) + 4 * (size_t)TM * LD * 2 +
+         (size_t)rmat_slots(LD) * kCap * 4 + smem_tail();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+size_t tile_meta_bytes(int64_t n, int nc) { return (size_t)((n + TM - 1) / TM) * nc * sizeof(SegMeta); }
+
+cudaError_t tile_format_count(const int64_t* indptr, const int32_t* idx, int64_t n, int nc,
+                              int64_t* counts, cudaStream_t st, int num_sms) {
+  const int64_t n_tiles = (n + TM - 1) / TM;
+  note_launches(1);
+  k_tile_count<<<grid_for(n_tiles, 1, num_sms, 8), 256, nc * sizeof(int), st>>>(indptr, idx, n, n_tiles,
+                                                                               nc, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t tile_format_fill(const int64_t* indptr, const int32_t* idx, const void* val16, int64_t n,
+                             int nc, const int64_t* seg, uint32_t* ent, void* meta, cudaStream_t st,
+                             int num_sms) {
+  const int64_t n_tiles = (n + TM - 1) / TM;
+  size_t smem = (size_t)2 * TM * nc * sizeof(int);
+  cudaFuncSetAttribute(k_tile_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  note_launches(1);
+  k_tile_fill<<<grid_for(n_tiles, 1, num_sms, 2), 512, smem, st>>>(
+      indptr, idx, static_cast<const uint16_t*>(val16), n, n_tiles, nc, seg, ent,
+      static_cast<SegMeta*>(meta));
+  return cudaGetLastError();
+}
+
+// The driver entry point is resolved through the runtime, so the library
+// does not link libcuda directly (it still loads on hosts without a driver).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// Row-major 16-bit matrix [rows][cols] (fmt 1 = bf16, 0 = f16) as a TMA map
+// with 64 x box_rows boxes, 128-byte swizzle; out-of-range rows read as zero.
+int make_tmap16(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, int box_rows, int fmt) {
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1u, 1u};
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return -1;
+  CUresult r = enc(map, fmt ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                   const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (int)r;
+}
+
+cudaError_t launch_fwd_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc,
+                          const CUtensorMap* vhi, const CUtensorMap* vlo, const float* mc, float* Y,
+                          uint16_t* Yhi, uint16_t* Ylo, int fmt, int* err, cudaStream_t st, int num_sms) {
+  const int64_t n_tiles = (n + TM - 1) / TM;
+  const int grid = (int)std::min<int64_t>(n_tiles, (int64_t)num_sms);
+  const SegMeta* m = static_cast<const SegMeta*>(meta);
+  note_launches(1);
+  if (ld == 64) {
+    size_t smem = fwd_smem(64);
+    cudaFuncSetAttribute(k_fwd_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fwd_tc<64><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, n, *vhi, *vlo, mc, Y, Yhi, Ylo, fmt, err);
+  } else {
+    size_t smem = fwd_smem(128);
+    cudaFuncSetAttribute(k_fwd_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fwd_tc<128><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, n, *vhi, *vlo, mc, Y, Yhi, Ylo, fmt, err);
+  }
+  return cudaGetLastError();
+}
+
+int rmat_tc_groups(int ld, int nc, int num_sms, int* gene_groups) {
+  const int spg = 256 / ld;  // 512 TMEM columns / (2 ld) per super-chunk
+  const int n_super = (nc + 1) / 2;
+  const int G = (n_super + spg - 1) / spg;
+  *gene_groups = G;
+  return std::max(1, num_sms / G);  // row groups
+}
+
+cudaError_t launch_rmat_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc, int64_t g,
+                           int gene_groups, int row_groups, const CUtensorMap* qhi, const CUtensorMap* qlo,
+                           float* part, int fmt, int* err, cudaStream_t st) {
+  const int64_t n_tiles = (n + TM - 1) / TM;
+  const int grid = gene_groups * row_groups;
+  const SegMeta* m = static_cast<const SegMeta*>(meta);
+  note_launches(1);
+  if (ld == 64) {
+    size_t smem = rmat_smem(64);
+    cudaFuncSetAttribute(k_rmat_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_rmat_tc<64><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, g, gene_groups, *qhi, *qlo, part, fmt, err);
+  } else {
+    size_t smem = rmat_smem(128);
+    cudaFuncSetAttribute(k_rmat_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_rmat_tc<128><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, g, gene_groups, *qhi, *qlo, part, fmt, err);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_split16(float* in, int64_t count, uint16_t* hi, uint16_t* lo, int fmt, int write_back,
+                           cudaStream_t st, int num_sms) {
+  note_launches(1);
+  k_split16<<<grid_for(count, 256, num_sms), 256, 0, st>>>(in, count, hi, lo, fmt, write_back);
+  return cudaGetLastError();
+}
+
+size_t fwd_tc_smem_bytes(int ld) { return fwd_smem(ld); }
+size_t rmat_tc_smem_bytes(int ld) { return rmat_smem(ld); }
+
+}  // namespace scx

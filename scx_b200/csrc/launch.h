@@ -3,6 +3,7 @@
 // return the launch status; none synchronises.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -100,6 +101,36 @@ cudaError_t launch_gaussian(uint64_t seed, int64_t n_rows, int64_t n_cols, float
 // Copy a column-major n_rows x n_cols float matrix into a row-major padded one.
 cudaError_t launch_colmajor_to_padded(const float* in, int64_t n_rows, int64_t n_cols, int ld,
                                       float* out, cudaStream_t st, int num_sms);
+
+// ---- tensor-core path (kernels_tc.cu) ----
+// Tile-chunk packed format: counts[t * nc + c] entries per (128-row tile,
+// 64-gene chunk); seg = exclusive scan of counts; ent/qoff filled from a
+// sorted, duplicate-free CSR whose values are 16-bit (bf16/f16 bits).
+// counts are padded to multiples of 4 entries; meta holds one 16-byte record
+// per segment (tile_meta_bytes).
+size_t tile_meta_bytes(int64_t n, int nc);
+cudaError_t tile_format_count(const int64_t* indptr, const int32_t* idx, int64_t n, int nc,
+                              int64_t* counts, cudaStream_t st, int num_sms);
+cudaError_t tile_format_fill(const int64_t* indptr, const int32_t* idx, const void* val16, int64_t n,
+                             int nc, const int64_t* seg, uint32_t* ent, void* meta, cudaStream_t st,
+                             int num_sms);
+// TMA map of a row-major [rows][cols] 16-bit matrix (fmt 1 = bf16, 0 = f16);
+// returns the CUresult.
+int make_tmap16(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, int box_rows, int fmt);
+// Y (n x ld, FP32) = A (Vhi + Vlo) - mc, plus the hi/lo 16-bit planes of Y.
+cudaError_t launch_fwd_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc,
+                          const CUtensorMap* vhi, const CUtensorMap* vlo, const float* mc, float* Y,
+                          uint16_t* Yhi, uint16_t* Ylo, int fmt, int* err, cudaStream_t st, int num_sms);
+// Partials part[row_group][g][ld] of A^T (Qhi + Qlo); returns row groups.
+int rmat_tc_groups(int ld, int nc, int num_sms, int* gene_groups);
+cudaError_t launch_rmat_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc, int64_t g,
+                           int gene_groups, int row_groups, const CUtensorMap* qhi, const CUtensorMap* qlo,
+                           float* part, int fmt, int* err, cudaStream_t st);
+size_t fwd_tc_smem_bytes(int ld);
+size_t rmat_tc_smem_bytes(int ld);
+// hi = round16(x), lo = round16(x - hi); lo may be null; write_back: x = hi.
+cudaError_t launch_split16(float* in, int64_t count, uint16_t* hi, uint16_t* lo, int fmt, int write_back,
+                           cudaStream_t st, int num_sms);
 
 // ---- synthetic generator (synth.cu) ----
 cudaError_t launch_synth_count(uint64_t seed, int64_t n, int64_t g, double loc, double disp,

@@ -153,6 +153,14 @@ struct scxpca_plan {
 
   double tau = 1e-8;
 
+  // tensor-core path (16-bit values): tile-chunk packed matrix, 16-bit dense
+  // operands and their TMA maps
+  bool use_tc = false;
+  int fmt16 = 1;  // 1 = bf16, 0 = f16
+  int n_chunks = 0, tc_gene_groups = 0, tc_row_groups = 0;
+  DevBuf tf_meta, tf_ent, V16, V16lo, Y16, Q16lo, tc_part, tc_err;
+  CUtensorMap vmap{}, vmap_lo{}, qmap_hi{}, qmap_lo{};
+
   // opt-in stage timing
   bool profiling = false;
   std::vector<cudaEvent_t> events;
@@ -287,13 +295,14 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
       pl->own_stream = true;
     }
     cudaStream_t st = pl->stream;
-    const int64_t n = pl->n, g = pl->g, nnz = pl->nnz, ld = pl->ld;
+    const int64_t n = pl->n, g = pl->g, nnz = pl->nnz;
 
     // ---- pre-flight (gpu_pca.rs:450-462): resident CSR + work buffers ----
     {
+      const int64_t ldp = (pl->k + 63) / 64 * 64;
       size_t need = (size_t)(n + 1) * 8 + (size_t)nnz * 4 + (size_t)nnz * dtype_size(pl->dtype) * 2 +
-                    (size_t)n * ld * 4 + (size_t)n * pl->nc * 4 + (size_t)n * 36 +
-                    (size_t)g * ld * 4 * 80;
+                    (size_t)nnz * 4 + (size_t)n * ldp * 8 + (size_t)n * pl->nc * 4 + (size_t)n * 36 +
+                    (size_t)g * ldp * 4 * 400;
       size_t fr = 0, tot = 0;
       CK(cudaMemGetInfo(&fr, &tot));
       double with_headroom = (double)need * 1.1;
@@ -337,6 +346,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
       if (hf[0]) fail(SCXPCA_INVALID_CSR, "invalid CSR: indptr is not monotone within [0, nnz]");
       if (hf[1]) fail(SCXPCA_INVALID_CSR, "invalid CSR: column index out of range [0, n_vars)");
       if (hf[3]) fail(SCXPCA_INVALID_CSR, "invalid CSR: non-finite value");
+      bool duplicates = false;
       if (hf[2]) {
         // unsorted (or duplicated) rows: sort an owned copy by gene
         if (dev_in) {
@@ -349,8 +359,23 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
         }
         CK(launch_sort_rows(pl->in_dtype, pl->indptr, pl->b_idx.as<int32_t>(), pl->b_stage.p, n, st,
                             pl->num_sms));
+        // after sorting, any remaining "not strictly ascending" pair is a duplicate
+        CK(cudaMemsetAsync(flags.p, 0, 16, st));
+        CK(launch_validate_csr(pl->in_dtype, pl->indptr, pl->idx, vin, n, g, nnz, flags.as<int32_t>(),
+                               st, pl->num_sms));
+        CK(cudaMemcpyAsync(hf, flags.p, 16, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        duplicates = hf[2] != 0;
       }
+      // Tensor cores for 16-bit values on sorted, duplicate-free rows with at
+      // most 128 gene chunks (8,192 genes); SCXPCA_TC=0 forces the CUDA cores.
+      const char* env = getenv("SCXPCA_TC");
+      const bool tc_allowed = !(env && env[0] == '0');
+      pl->use_tc = tc_allowed && pl->dtype != SCXPCA_F32 && !duplicates && g <= 64 * 128;
+      if (pl->use_tc) pl->ld = (pl->k + 63) / 64 * 64;
+      pl->fmt16 = pl->dtype == SCXPCA_BF16 ? 1 : 0;
     }
+    const int64_t ld = pl->ld;
 
     // ---- statistics of the input ----
     pl->stats_parts = 2 * pl->num_sms;
@@ -414,6 +439,42 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
       upload(pl->d_mu, mu_w, st);
     }
     compute_total_variance(pl);
+
+    // ---- tensor-core path: tile-chunk packed matrix, 16-bit operands, TMA maps ----
+    if (pl->use_tc) {
+      const int64_t n_tiles = (n + 127) / 128;
+      pl->n_chunks = (int)((g + 63) / 64);
+      const int64_t nseg = n_tiles * pl->n_chunks;
+      DevBuf counts, seg;
+      counts.alloc(sizeof(int64_t) * nseg);
+      seg.alloc(sizeof(int64_t) * (nseg + 1));
+      CK(tile_format_count(pl->indptr, pl->idx, n, pl->n_chunks, counts.as<int64_t>(), st, pl->num_sms));
+      CK(launch_exclusive_scan_i64(counts.as<int64_t>(), nseg, seg.as<int64_t>(), st));
+      int64_t padded_nnz = 0;
+      CK(cudaMemcpyAsync(&padded_nnz, seg.as<int64_t>() + nseg, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      pl->tf_ent.alloc(sizeof(uint32_t) * std::max<int64_t>(padded_nnz, 4));
+      CK(cudaMemsetAsync(pl->tf_ent.p, 0, sizeof(uint32_t) * std::max<int64_t>(padded_nnz, 4), st));
+      pl->tf_meta.alloc(tile_meta_bytes(n, pl->n_chunks));
+      CK(tile_format_fill(pl->indptr, pl->idx, pl->val, n, pl->n_chunks, seg.as<int64_t>(),
+                          pl->tf_ent.as<uint32_t>(), pl->tf_meta.p, st, pl->num_sms));
+      pl->V16.alloc(sizeof(uint16_t) * g * ld);
+      pl->V16lo.alloc(sizeof(uint16_t) * g * ld);
+      pl->Y16.alloc(sizeof(uint16_t) * n * ld);
+      pl->Q16lo.alloc(sizeof(uint16_t) * n * ld);
+      pl->tc_err.alloc(sizeof(int) * 4);
+      CK(cudaMemsetAsync(pl->tc_err.p, 0, sizeof(int) * 4, st));
+      pl->tc_row_groups = rmat_tc_groups((int)ld, pl->n_chunks, pl->num_sms, &pl->tc_gene_groups);
+      pl->tc_part.alloc(sizeof(float) * (size_t)pl->tc_row_groups * g * ld);
+      int r1 = make_tmap16(&pl->vmap, pl->V16.p, g, ld, 64, pl->fmt16);
+      int r4 = make_tmap16(&pl->vmap_lo, pl->V16lo.p, g, ld, 64, pl->fmt16);
+      int r2 = make_tmap16(&pl->qmap_hi, pl->Y16.p, n, ld, 128, pl->fmt16);
+      int r3 = make_tmap16(&pl->qmap_lo, pl->Q16lo.p, n, ld, 128, pl->fmt16);
+      if (r1 || r2 || r3 || r4)
+        fail(SCXPCA_CUDA_ERROR, "cuTensorMapEncodeTiled failed (" + std::to_string(r1) + ", " +
+                                    std::to_string(r2) + ", " + std::to_string(r3) + ", " +
+                                    std::to_string(r4) + ")");
+    }
 
     // ---- transposed-product tables ----
     pl->nb = (int)((g + kTransposeGeneBlock - 1) / kTransposeGeneBlock);
@@ -530,8 +591,29 @@ void small_qr(scxpca_plan* pl, double* A, int shift) {
 }
 
 // W = X^T A (raw, uncentred), FP64, for a tall float A (n x ld).
-void rmatmat_raw(scxpca_plan* pl, const float* A) {
+// W = X^T A (raw, uncentred) into pl->W (FP64).  On the tensor-core path the
+// tall operand enters as two 16-bit planes Y16 (hi) and Q16lo (lo): `split`
+// != 0 first splits the FP32 A into them; otherwise they already hold the
+// forward product's planes of A.
+void rmatmat_raw(scxpca_plan* pl, float* A, int split) {
   cudaStream_t st = pl->stream;
+  if (pl->use_tc) {
+    int s = stage_begin(pl);
+    if (split)
+      CK(launch_split16(A, pl->n * pl->ld, pl->Y16.as<uint16_t>(), pl->Q16lo.as<uint16_t>(), pl->fmt16, 0,
+                        st, pl->num_sms));
+    stage_end(pl, SCXPCA_STAGE_APPLY, s);
+    s = stage_begin(pl);
+    CK(launch_rmat_tc((int)pl->ld, pl->tf_ent.as<uint32_t>(), pl->tf_meta.p, pl->n, pl->n_chunks, pl->g,
+                      pl->tc_gene_groups, pl->tc_row_groups, &pl->qmap_hi, &pl->qmap_lo,
+                      pl->tc_part.as<float>(), pl->fmt16, pl->tc_err.as<int>(), st));
+    stage_end(pl, SCXPCA_STAGE_TRANSPOSE, s);
+    s = stage_begin(pl);
+    CK(launch_reduce_rows_f32(pl->tc_part.as<float>(), pl->tc_row_groups, pl->g * pl->ld,
+                              pl->W.as<double>(), 0, st, pl->num_sms));
+    stage_end(pl, SCXPCA_STAGE_REDUCE, s);
+    return;
+  }
   int s = stage_begin(pl);
   CK(launch_spmm_t(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, (int32_t)pl->g,
                    pl->rbp.as<int32_t>(), pl->nb, pl->nchunks, pl->rows_per_chunk, A,
@@ -543,12 +625,38 @@ void rmatmat_raw(scxpca_plan* pl, const float* A) {
   stage_end(pl, SCXPCA_STAGE_REDUCE, s);
 }
 
+// Y = (X - mu) V.  On the tensor-core path V enters as hi/lo 16-bit planes and
+// the product also leaves the hi/lo planes of Y for the transposed product.
 void forward(scxpca_plan* pl) {
+  cudaStream_t st = pl->stream;
+  if (pl->use_tc) {
+    int s = stage_begin(pl);
+    CK(launch_split16(pl->V.as<float>(), pl->g * pl->ld, pl->V16.as<uint16_t>(), pl->V16lo.as<uint16_t>(),
+                      pl->fmt16, 0, st, pl->num_sms));
+    stage_end(pl, SCXPCA_STAGE_SMALL, s);
+    s = stage_begin(pl);
+    CK(launch_fwd_tc((int)pl->ld, pl->tf_ent.as<uint32_t>(), pl->tf_meta.p, pl->n, pl->n_chunks, &pl->vmap,
+                     &pl->vmap_lo, pl->mc.as<float>(), pl->Y.as<float>(), pl->Y16.as<uint16_t>(),
+                     pl->Q16lo.as<uint16_t>(), pl->fmt16, pl->tc_err.as<int>(), st, pl->num_sms));
+    stage_end(pl, SCXPCA_STAGE_FORWARD, s);
+    return;
+  }
   int s = stage_begin(pl);
   CK(launch_spmm_fwd(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, pl->V.as<float>(),
-                     pl->centered ? pl->mc.as<float>() : nullptr, pl->Y.as<float>(), pl->stream,
-                     pl->num_sms));
+                     pl->centered ? pl->mc.as<float>() : nullptr, pl->Y.as<float>(), st, pl->num_sms));
   stage_end(pl, SCXPCA_STAGE_FORWARD, s);
+}
+
+// Raise the error a tensor-core kernel recorded (a bounded wait that ran out).
+void check_tc_error(scxpca_plan* pl) {
+  if (!pl->use_tc) return;
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, pl->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, pl->stream));
+  CK(cudaStreamSynchronize(pl->stream));
+  if (e != 0) {
+    CK(cudaMemsetAsync(pl->tc_err.p, 0, sizeof(int), pl->stream));
+    fail(SCXPCA_TIMEOUT, "tensor-core pipeline wait timed out (site " + std::to_string(e) + ")");
+  }
 }
 
 void load_omega(scxpca_plan* pl, const scxpca_params* p) {
@@ -597,7 +705,7 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift);
   for (int64_t it = 0; it < p.n_power_iterations; ++it) {
     // Z = (X - mu)^T Q = (X^T Y - mu (1^T Y)) R^{-1}
-    rmatmat_raw(pl, pl->Y.as<float>());
+    rmatmat_raw(pl, pl->Y.as<float>(), 0);
     s = stage_begin(pl);
     CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->Rinv.as<double>(),
                            pl->Z.as<double>(), st));
@@ -614,7 +722,7 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   stage_end(pl, SCXPCA_STAGE_APPLY, s);
   tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift);
   // B = (X - mu)^T Q R2^{-1}
-  rmatmat_raw(pl, pl->Y.as<float>());
+  rmatmat_raw(pl, pl->Y.as<float>(), 1);
   s = stage_begin(pl);
   CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->R2inv.as<double>(),
                          pl->Z.as<double>(), st));
@@ -653,6 +761,7 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
                        cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   collect_stages(pl);
+  check_tc_error(pl);
   if (hstatus[0] < 0)
     fail(SCXPCA_NOT_SPD, "CholeskyQR2 failed: non-SPD; retry with qr_method='householder'");
 
@@ -817,6 +926,7 @@ int32_t scxpca_plan_matmat(scxpca_plan* plan, const float* v, int64_t ld_v, floa
     CK(cudaMemcpy2DAsync(y, sizeof(float) * ld_y, plan->Y.p, sizeof(float) * ld, sizeof(float) * plan->k,
                          plan->n, cudaMemcpyDeviceToDevice, st));
     CK(cudaStreamSynchronize(st));
+    check_tc_error(plan);
   });
 }
 
@@ -835,13 +945,14 @@ int32_t scxpca_plan_rmatmat(scxpca_plan* plan, const float* q, int64_t ld_q, dou
     CK(launch_gram_f32(plan->Y.as<float>(), plan->n, (int)ld, plan->gpart.as<double>(), parts, st));
     CK(launch_reduce_rows_f64(plan->gpart.as<double>(), parts, ld * ld + ld, plan->G.as<double>(), 0, st,
                               plan->num_sms));
-    rmatmat_raw(plan, plan->Y.as<float>());
+    rmatmat_raw(plan, plan->Y.as<float>(), 1);
     CK(launch_center_apply(plan->W.as<double>(), plan->g, (int)ld,
                            plan->centered ? plan->d_mu.as<double>() : nullptr,
                            plan->G.as<double>() + ld * ld, plan->eye.as<double>(), plan->Z.as<double>(), st));
     CK(cudaMemcpy2DAsync(z, sizeof(double) * ld_z, plan->Z.p, sizeof(double) * ld, sizeof(double) * plan->k,
                          plan->g, cudaMemcpyDeviceToDevice, st));
     CK(cudaStreamSynchronize(st));
+    check_tc_error(plan);
   });
 }
 
