@@ -94,54 +94,54 @@ cudaError_t launch_gram_f64(const double* A, int64_t n, int ld, double* part, in
 // With shift_on_fail the factorisation restarts once on G + s I,
 // s = 10 tau max_j G_jj, which always succeeds on finite input.
 // ---------------------------------------------------------------------------
-__global__ void k_cholesky(const double* __restrict__ G, int k, int ld, double tau,
-                           int shift_on_fail, double* __restrict__ R, double* __restrict__ Rinv,
-                           float* __restrict__ Rinv_f, int* __restrict__ status) {
-  extern __shared__ double A[];  // [k][k]
-  __shared__ int fail;
-  __shared__ double maxdiag;
-  const int tid = threadIdx.x, nt = blockDim.x;
+// One barrier per elimination step: every thread reads the pivot d_j itself,
+// the trailing update uses the unscaled row j (A_ac -= A_ja A_jc / d_j), and
+// the scaled row j of R goes straight to global memory.  R^{-1} is then
+// formed in place row by row from the bottom (row i needs only rows > i),
+// one warp per column dot product.
+__global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G, int k, int ld, double tau,
+                                                   int shift_on_fail, double* __restrict__ R,
+                                                   double* __restrict__ Rinv, float* __restrict__ Rinv_f,
+                                                   int* __restrict__ status) {
+  extern __shared__ double A[];  // [k][k], then tmp[k]
+  double* tmp = A + k * k;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  double maxdiag = 0.0;
+  for (int j = 0; j < k; ++j) maxdiag = fmax(maxdiag, G[j * ld + j]);
   double shift = 0.0;
+  int fail = -1;
   for (int attempt = 0; attempt < 2; ++attempt) {
+    for (int t = tid; t < ld * ld; t += nt) R[t] = 0.0;
     for (int t = tid; t < k * k; t += nt) {
-      int r = t / k, c = t % k;
-      double v = G[r * ld + c];
-      if (r == c) v += shift;
-      A[t] = v;
-    }
-    if (tid == 0) {
-      fail = -1;
-      double m = 0.0;
-      for (int j = 0; j < k; ++j) m = fmax(m, G[j * ld + j]);
-      maxdiag = m;
+      const int r = t / k, c = t % k;
+      A[t] = G[r * ld + c] + (r == c ? shift : 0.0);
     }
     __syncthreads();
+    fail = -1;
     for (int j = 0; j < k; ++j) {
-      if (tid == 0) {
-        double d = A[j * k + j];
-        double d0 = G[j * ld + j] + shift;
-        bool ok = isfinite(d) && d > 0.0 && (attempt == 1 || d > tau * d0);
-        if (!ok) fail = j; else A[j * k + j] = sqrt(d);
+      const double d = A[j * k + j];
+      const double d0 = G[j * ld + j] + shift;
+      if (!(isfinite(d) && d > 0.0 && (attempt == 1 || d > tau * d0))) {
+        fail = j;  // every thread sees the same pivot: uniform exit
+        break;
       }
-      __syncthreads();
-      if (fail >= 0) break;
-      const double r = A[j * k + j];
-      for (int c = j + 1 + tid; c < k; c += nt) A[j * k + c] /= r;
-      __syncthreads();
-      const int m = k - j - 1;  // trailing block size
+      const double rinv = rsqrt(d), dinv = 1.0 / d;
+      for (int c = j + tid; c < k; c += nt) R[j * ld + c] = A[j * k + c] * rinv;
+      const int m = k - j - 1;
       for (int t = tid; t < m * m; t += nt) {
-        int a = j + 1 + t / m, c = j + 1 + t % m;
-        if (c >= a) A[a * k + c] -= A[j * k + a] * A[j * k + c];
+        const int a = j + 1 + t / m, c = j + 1 + t % m;
+        if (c >= a) A[a * k + c] -= A[j * k + a] * A[j * k + c] * dinv;
       }
       __syncthreads();
     }
     if (fail < 0) break;
+    __syncthreads();
     if (!shift_on_fail || attempt == 1) {
       if (tid == 0) status[0] = -(fail + 1);
       // Leave well-defined (identity) factors so downstream kernels stay finite.
       for (int t = tid; t < ld * ld; t += nt) {
-        int r = t / ld, c = t % ld;
-        double v = (r == c && r < k) ? 1.0 : 0.0;
+        const int r = t / ld, c = t % ld;
+        const double v = (r == c && r < k) ? 1.0 : 0.0;
         R[t] = v;
         Rinv[t] = v;
         Rinv_f[t] = (float)v;
@@ -150,90 +150,114 @@ __global__ void k_cholesky(const double* __restrict__ G, int k, int ld, double t
     }
     if (tid == 0) status[0] += 1;
     shift = 10.0 * tau * fmax(maxdiag, 1e-300);
+  }
+  __syncthreads();
+  // A <- R (upper; lower part ignored), then invert in place from the bottom row up.
+  for (int t = tid; t < k * k; t += nt) A[t] = R[(t / k) * ld + (t % k)];
+  __syncthreads();
+  for (int i = k - 1; i >= 0; --i) {
+    for (int c = i + tid; c < k; c += nt) tmp[c] = A[i * k + c];
+    __syncthreads();
+    for (int c = i + warp; c < k; c += nw) {
+      double s = 0.0;
+      for (int l = i + 1 + lane; l <= c; l += 32) s += tmp[l] * A[l * k + c];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) A[i * k + c] = ((i == c ? 1.0 : 0.0) - s) / tmp[i];
+    }
     __syncthreads();
   }
-  // R (upper) to global, zero elsewhere.
   for (int t = tid; t < ld * ld; t += nt) {
-    int r = t / ld, c = t % ld;
-    R[t] = (r < k && c < k && c >= r) ? A[r * k + c] : 0.0;
-  }
-  // R^{-1}: thread per column, back substitution (upper triangular).
-  for (int c = tid; c < ld; c += nt) {
-    for (int i = ld - 1; i >= 0; --i) {
-      double v = 0.0;
-      if (c < k && i <= c) {
-        v = (i == c) ? 1.0 : 0.0;
-        for (int l = i + 1; l <= c; ++l) v -= A[i * k + l] * Rinv[l * ld + c];
-        v /= A[i * k + i];
-      }
-      Rinv[i * ld + c] = v;
-      Rinv_f[i * ld + c] = (float)v;
-    }
+    const int r = t / ld, c = t % ld;
+    const double v = (r < k && c < k && c >= r) ? A[r * k + c] : 0.0;
+    Rinv[t] = v;
+    Rinv_f[t] = (float)v;
   }
 }
 
 cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shift_on_fail,
                             double* R, double* Rinv, float* Rinv_f, int* status, cudaStream_t st) {
-  size_t smem = (size_t)k * k * sizeof(double);
+  size_t smem = (size_t)(k * k + k) * sizeof(double);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(k_cholesky, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   note_launches(1);
-  k_cholesky<<<1, 256, smem, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
+  k_cholesky<<<1, 1024, smem, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-// Tall apply Out = In * M (float, ld x ld M in shared memory), warp per row.
-// In-place use (Out == In) is safe: a warp holds its whole row first.
+// Tall x small: Out[i, :cnt] = In[i, :K] * M (K x cnt), one thread per row.
+// M (zero-padded to OUTB columns) sits in shared memory and every thread of a
+// warp reads the same M entries (broadcast); the row and its OUTB outputs stay
+// in registers, so there are four FMAs per shared load.  A thread reads its
+// whole row before writing, so Out may alias In.
 // ---------------------------------------------------------------------------
-template <int C>
-__global__ void __launch_bounds__(256) k_apply_right_f32(const float* In, int64_t n,
-                                                         const float* __restrict__ M, float* Out) {
-  constexpr int LD = 32 * C;
-  extern __shared__ float Ms[];  // [LD][LD]
-  for (int t = threadIdx.x; t < LD * LD; t += blockDim.x) Ms[t] = M[t];
+template <int OUTB>
+__global__ void __launch_bounds__(128) k_tall_mm(const float* In, int64_t n, int K, int ldi,
+                                                 const float* __restrict__ M, int ldm, int cnt,
+                                                 float* Out, int ldo) {
+  extern __shared__ float Ms[];  // [K][OUTB]
+  for (int t = threadIdx.x; t < K * OUTB; t += blockDim.x) {
+    const int l = t / OUTB, o = t % OUTB;
+    Ms[t] = o < cnt ? M[l * ldm + o] : 0.f;
+  }
   __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t row = warp; row < n; row += nwarps) {
-    float in[C], out[C];
+  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < n;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    float acc[OUTB];
 #pragma unroll
-    for (int c = 0; c < C; ++c) {
-      in[c] = In[row * LD + lane + 32 * c];
-      out[c] = 0.f;
-    }
+    for (int o = 0; o < OUTB; ++o) acc[o] = 0.f;
+    const float4* in4 = reinterpret_cast<const float4*>(In + row * ldi);
+    for (int l = 0; l < K; l += 4) {
+      const float4 x = in4[l >> 2];
+      const float xs[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-    for (int cc = 0; cc < C; ++cc) {
-      for (int t = 0; t < 32; ++t) {
-        const float v = __shfl_sync(0xffffffffu, in[cc], t);
-        const float* mr = Ms + (cc * 32 + t) * LD + lane;
+      for (int u = 0; u < 4; ++u) {
+        const float4* mr = reinterpret_cast<const float4*>(Ms + (l + u) * OUTB);
 #pragma unroll
-        for (int c = 0; c < C; ++c) out[c] = fmaf(v, mr[32 * c], out[c]);
+        for (int o = 0; o < OUTB / 4; ++o) {
+          const float4 m = mr[o];
+          acc[4 * o + 0] = fmaf(xs[u], m.x, acc[4 * o + 0]);
+          acc[4 * o + 1] = fmaf(xs[u], m.y, acc[4 * o + 1]);
+          acc[4 * o + 2] = fmaf(xs[u], m.z, acc[4 * o + 2]);
+          acc[4 * o + 3] = fmaf(xs[u], m.w, acc[4 * o + 3]);
+        }
       }
     }
+    float* out = Out + row * ldo;
+    if ((cnt & 3) == 0 && (ldo & 3) == 0) {
 #pragma unroll
-    for (int c = 0; c < C; ++c) Out[row * LD + lane + 32 * c] = out[c];
+      for (int o = 0; o < OUTB / 4; ++o)
+        if (4 * o < cnt)
+          reinterpret_cast<float4*>(out)[o] =
+              make_float4(acc[4 * o], acc[4 * o + 1], acc[4 * o + 2], acc[4 * o + 3]);
+    } else {
+#pragma unroll
+      for (int o = 0; o < OUTB; ++o)
+        if (o < cnt) out[o] = acc[o];
+    }
   }
+}
+
+static cudaError_t tall_mm(const float* In, int64_t n, int K, int ldi, const float* M, int ldm, int cnt,
+                           float* Out, int ldo, cudaStream_t st, int num_sms) {
+  if (n == 0) return cudaSuccess;
+  const int outb = cnt <= 64 ? 64 : 128;
+  const size_t smem = (size_t)K * outb * sizeof(float);
+  const int grid = grid_for(n, 128, num_sms, 8);
+  note_launches(1);
+  if (outb == 64) {
+    cudaFuncSetAttribute(k_tall_mm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_tall_mm<64><<<grid, 128, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo);
+  } else {
+    cudaFuncSetAttribute(k_tall_mm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_tall_mm<128><<<grid, 128, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo);
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_apply_right_f32(const float* In, int64_t n, int ld, const float* M, float* Out,
                                    cudaStream_t st, int num_sms) {
-  if (n == 0) return cudaSuccess;
-  size_t smem = (size_t)ld * ld * sizeof(float);
-  int grid = grid_for(n * 32, 256, num_sms, 4);
-  note_launches(1);
-  switch (ld) {
-    case 32: k_apply_right_f32<1><<<grid, 256, smem, st>>>(In, n, M, Out); break;
-    case 64: k_apply_right_f32<2><<<grid, 256, smem, st>>>(In, n, M, Out); break;
-    case 96:
-      cudaFuncSetAttribute(k_apply_right_f32<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_apply_right_f32<3><<<grid, 256, smem, st>>>(In, n, M, Out); break;
-    default:
-      cudaFuncSetAttribute(k_apply_right_f32<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_apply_right_f32<4><<<grid, 256, smem, st>>>(In, n, M, Out); break;
-  }
-  return cudaGetLastError();
+  return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, st, num_sms);
 }
 
 // ---------------------------------------------------------------------------
@@ -342,32 +366,12 @@ __global__ void k_jacobi(const double* __restrict__ C, int k, int ld, double* __
   __syncthreads();
   const int npair = kk / 2;
   int sweep = 0;
+  (void)red;
   for (; sweep < 40; ++sweep) {
-    // convergence test
-    double off = 0.0, tot = 0.0;
-    for (int t = tid; t < kk * kk; t += nt) {
-      int r = t / kk, c = t % kk;
-      double v = A[t] * A[t];
-      tot += v;
-      if (r != c) off += v;
-    }
-    red[tid] = off;
+    // Converged when a whole sweep performs no rotation: every off-diagonal
+    // entry is below 1e-15 of the geometric mean of its two diagonal entries.
+    if (tid == 0) done = 1;
     __syncthreads();
-    for (int s = nt / 2; s > 0; s >>= 1) {
-      if (tid < s) red[tid] += red[tid + s];
-      __syncthreads();
-    }
-    double off_all = red[0];
-    __syncthreads();
-    red[tid] = tot;
-    __syncthreads();
-    for (int s = nt / 2; s > 0; s >>= 1) {
-      if (tid < s) red[tid] += red[tid + s];
-      __syncthreads();
-    }
-    if (tid == 0) done = (off_all <= 1e-30 * red[0]) || red[0] == 0.0;
-    __syncthreads();
-    if (done) break;
     for (int round = 0; round < kk - 1; ++round) {
       for (int i = tid; i < npair; i += nt) {
         int a, b;
@@ -378,11 +382,12 @@ __global__ void k_jacobi(const double* __restrict__ C, int k, int ld, double* __
         if (q < k) {
           double apq = A[p * kk + q];
           double app = A[p * kk + p], aqq = A[q * kk + q];
-          if (fabs(apq) > 1e-300 && fabs(apq) > 1e-18 * sqrt(fabs(app * aqq))) {
+          if (fabs(apq) > 1e-300 && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq))) {
             double theta = (aqq - app) / (2.0 * apq);
             double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
             c = 1.0 / sqrt(t * t + 1.0);
             s = t * c;
+            done = 0;
           }
         }
         pp[i] = p; qq[i] = q; cs[i] = c; sn[i] = s;
@@ -414,6 +419,8 @@ __global__ void k_jacobi(const double* __restrict__ C, int k, int ld, double* __
       }
       __syncthreads();
     }
+    if (done) break;
+    __syncthreads();
   }
   // sort eigenvalues descending: rank of each by counting (ties by index)
   for (int i = tid; i < k; i += nt) {
@@ -501,71 +508,11 @@ cudaError_t launch_ritz_finish(const double* B, int64_t g, int ld, int k, int nc
   return cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------
-// Embeddings U = Q M_emb, warp per row; lane owns outputs lane + 32 t.
-// ---------------------------------------------------------------------------
-template <int C>
-__global__ void __launch_bounds__(256) k_embed(const float* __restrict__ Q, int64_t n, int k,
-                                               const float* __restrict__ M, int nc,
-                                               float* __restrict__ U) {
-  constexpr int LD = 32 * C;
-  extern __shared__ float Ms[];  // [LD][ncp], ncp = nc rounded to 32
-  const int ncp = (nc + 31) / 32 * 32;
-  for (int t = threadIdx.x; t < LD * ncp; t += blockDim.x) {
-    int l = t / ncp, c = t % ncp;
-    Ms[t] = (c < nc) ? M[l * nc + c] : 0.f;
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int T = ncp / 32;
-  for (int64_t row = warp; row < n; row += nwarps) {
-    float q[C];
-#pragma unroll
-    for (int c = 0; c < C; ++c) q[c] = Q[row * LD + lane + 32 * c];
-    float out[kMaxK / 32];
-#pragma unroll
-    for (int t = 0; t < kMaxK / 32; ++t) out[t] = 0.f;
-#pragma unroll
-    for (int cc = 0; cc < C; ++cc) {
-      for (int s = 0; s < 32; ++s) {
-        const int l = cc * 32 + s;
-        if (l >= k) break;
-        const float v = __shfl_sync(0xffffffffu, q[cc], s);
-#pragma unroll
-        for (int t = 0; t < kMaxK / 32; ++t)
-          if (t < T) out[t] = fmaf(v, Ms[l * ncp + lane + 32 * t], out[t]);
-      }
-    }
-#pragma unroll
-    for (int t = 0; t < kMaxK / 32; ++t) {
-      int c = lane + 32 * t;
-      if (t < T && c < nc) U[row * nc + c] = out[t];
-    }
-  }
-}
-
+// Embeddings U = Q M_emb (n x nc row-major).
 cudaError_t launch_embed(const float* Q, int64_t n, int ld, int k, const float* M_emb, int nc,
                          float* U, cudaStream_t st, int num_sms) {
-  if (n == 0) return cudaSuccess;
-  int ncp = (nc + 31) / 32 * 32;
-  size_t smem = (size_t)ld * ncp * sizeof(float);
-  int grid = grid_for(n * 32, 256, num_sms, 4);
-  note_launches(1);
-  switch (ld) {
-    case 32: k_embed<1><<<grid, 256, smem, st>>>(Q, n, k, M_emb, nc, U); break;
-    case 64:
-      cudaFuncSetAttribute(k_embed<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_embed<2><<<grid, 256, smem, st>>>(Q, n, k, M_emb, nc, U); break;
-    case 96:
-      cudaFuncSetAttribute(k_embed<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_embed<3><<<grid, 256, smem, st>>>(Q, n, k, M_emb, nc, U); break;
-    default:
-      cudaFuncSetAttribute(k_embed<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_embed<4><<<grid, 256, smem, st>>>(Q, n, k, M_emb, nc, U); break;
-  }
-  return cudaGetLastError();
+  (void)k;  // rows k..ld-1 of M_emb are zero
+  return tall_mm(Q, n, ld, ld, M_emb, nc, nc, U, nc, st, num_sms);
 }
 
 // ---------------------------------------------------------------------------

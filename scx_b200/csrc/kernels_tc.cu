@@ -45,10 +45,10 @@ namespace {
 constexpr int TM = 128;          // cells per tile
 constexpr int CW = 64;           // genes per chunk
 constexpr int kCap = 1024;       // entries per staging slot (4 KB)
-constexpr int kGroups = 4;       // densify groups of four warps, one stage each in turn
+constexpr int kMaxGroups = 4;    // densify groups of four warps
 constexpr int kThreads = 736;    // 23 warps
 constexpr int kMaxChunks = 128;  // genes <= 8192
-constexpr int W_EPI = 4 * kGroups, W_MMA = W_EPI + 4, W_DENSE = W_MMA + 1, W_SPARSE = W_MMA + 2;
+constexpr int W_EPI = 4 * kMaxGroups, W_MMA = W_EPI + 4, W_DENSE = W_MMA + 1, W_SPARSE = W_MMA + 2;
 
 struct SegMeta {
   int64_t start;
@@ -56,10 +56,20 @@ struct SegMeta {
 };
 static_assert(sizeof(SegMeta) == 16, "segment metadata is one 16-byte record");
 
-__host__ __device__ constexpr int fwd_stages(int LD) { return LD == 64 ? 4 : 3; }
-__host__ __device__ constexpr int fwd_slots(int LD) { return LD == 64 ? 16 : 12; }
+// Pipeline shapes.  Densify group g takes the stages it with it % G == g, so
+// stage buffer it % S is only ever used by one group (S is a multiple of G)
+// and every group has a private staging ring: each waiter then runs at most
+// one barrier phase ahead of the phase it waits for, which is what a parity
+// wait can distinguish.
+__host__ __device__ constexpr int fwd_stages(int LD) { return LD == 64 ? 4 : 2; }
+__host__ __device__ constexpr int fwd_groups(int LD) { return LD == 64 ? 4 : 2; }
+__host__ __device__ constexpr int fwd_slots(int LD) { return LD == 64 ? 16 : 8; }  // all groups
 __host__ __device__ constexpr int rmat_stages(int LD) { return LD == 64 ? 3 : 2; }
-__host__ __device__ constexpr int rmat_slots(int LD) { return LD == 64 ? 12 : 6; }
+__host__ __device__ constexpr int rmat_groups(int LD) { return LD == 64 ? 3 : 2; }
+__host__ __device__ constexpr int rmat_slots(int LD) { return LD == 64 ? 9 : 4; }
+static_assert(fwd_stages(64) % fwd_groups(64) == 0 && fwd_stages(128) % fwd_groups(128) == 0, "");
+static_assert(rmat_stages(64) % rmat_groups(64) == 0 && rmat_stages(128) % rmat_groups(128) == 0, "");
+static_assert(fwd_slots(64) % fwd_groups(64) == 0 && rmat_slots(64) % rmat_groups(64) == 0, "");
 
 __host__ __device__ __forceinline__ int padded4(int x) { return (x + 3) & ~3; }
 __host__ __device__ __forceinline__ int n_pieces(int real) { return (padded4(real) + kCap - 1) / kCap; }
@@ -179,13 +189,20 @@ __device__ __forceinline__ void zero_rows(uint32_t tile, int quarter, int lane) 
 
 __device__ __forceinline__ void scatter_one(uint32_t tile, uint32_t w) { sts_u16(tile + (w >> 16), w & 0xFFFFu); }
 
-// Staging ring shared by the sparse loader and the densify warps.
+// Private staging ring of one densify group, filled by the sparse loader.
 struct Ring {
   uint32_t base;    // shared address of slot 0
+  uint32_t* ptr;    // the same, as a generic pointer (bulk-copy destination)
   uint64_t* full;   // [nslot], 1 arrival + tx bytes
-  uint64_t* empty;  // [nslot], one arrival per densify warp of the consuming group
+  uint64_t* empty;  // [nslot], one arrival per densify warp of the group
   int nslot;
 };
+
+__device__ __forceinline__ Ring group_ring(uint32_t* ring_ptr, uint64_t* sfull, uint64_t* sempty, int g,
+                                           int nsg) {
+  uint32_t* p = ring_ptr + (size_t)g * nsg * kCap;
+  return Ring{smem_u32(p), p, sfull + g * nsg, sempty + g * nsg, nsg};
+}
 
 // Densify warp (quarter q): scatter the quarter's entries of one segment into
 // `tile` (already zeroed), consuming the segment's pieces from the ring.
@@ -218,15 +235,15 @@ __device__ __forceinline__ bool densify_segment(uint32_t tile, const SegMeta& m,
 
 // Sparse loader: bulk-copy one segment into the ring, piece by piece.
 __device__ __forceinline__ bool load_segment(const uint32_t* __restrict__ ent, const SegMeta& m,
-                                             const Ring& ring, uint32_t* ring_ptr, uint32_t& pc,
-                                             volatile int* abort_flag, int* err, int code) {
+                                             const Ring& ring, uint32_t& pc, volatile int* abort_flag, int* err,
+                                             int code) {
   const int plen = padded4(m.q[3]);
   for (int p0 = 0; p0 < plen; p0 += kCap, ++pc) {
     const int slot = (int)(pc % (uint32_t)ring.nslot);
     if (!mbar_wait(&ring.empty[slot], ((pc / ring.nslot) & 1u) ^ 1u, abort_flag, err, code)) return false;
     const uint32_t bytes = (uint32_t)min(kCap, plen - p0) * 4u;
     mbar_arrive_expect_tx(&ring.full[slot], bytes);
-    bulk_load(ring_ptr + (size_t)slot * kCap, ent + m.start + p0, bytes, &ring.full[slot]);
+    bulk_load(ring.ptr + (size_t)slot * kCap, ent + m.start + p0, bytes, &ring.full[slot]);
   }
   return true;
 }
@@ -254,7 +271,9 @@ __global__ void __launch_bounds__(kThreads, 1)
              uint16_t* __restrict__ Ylo, int fmt, int* err) {
   constexpr int N2 = 2 * LD;                // [hi | lo] columns
   constexpr int S = fwd_stages(LD);
+  constexpr int G = fwd_groups(LD);
   constexpr int NSLOT = fwd_slots(LD);
+  constexpr int NSG = NSLOT / G;            // staging slots per group
   constexpr int A_BYTES = TM * CW * 2;      // 16 KB
   constexpr int B_PLANE = CW * LD * 2;      // 64 genes x LD, one 16-bit plane
   constexpr int B_BYTES = 2 * B_PLANE;
@@ -275,7 +294,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* mempty = mfull + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mempty + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  const Ring ring{smem_u32(ring_ptr), sfull, sempty, NSLOT};
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -287,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&acc_full[a], 1);
       mbar_init(&acc_empty[a], 128);
       mbar_init(&mfull[a], 1);
-      mbar_init(&mempty[a], 4 * kGroups);
+      mbar_init(&mempty[a], 4 * G);
     }
     for (int s = 0; s < NSLOT; ++s) {
       mbar_init(&sfull[s], 1);
@@ -306,18 +324,17 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp < W_EPI) {
-    // ---- densify: group (warp / 4) takes stages it % kGroups == group ----
+    // ---- densify: group (warp / 4) takes stages it % G == group ----
     const int group = warp >> 2, q = warp & 3;
+    if (group >= G) goto done;  // spare warps of a narrower configuration
+    const Ring ring = group_ring(ring_ptr, sfull, sempty, group, NSG);
     uint32_t it = 0, pc = 0, ti = 0;
     for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++ti) {
       if (!warp_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 11)) goto done;
       const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
       for (int c = 0; c < nc; ++c, ++it) {
+        if ((int)(it % G) != group) continue;
         const SegMeta m = mt[c];
-        if ((int)(it % kGroups) != group) {
-          pc += n_pieces(m.q[3]);
-          continue;
-        }
         const int s = it % S;
         if (!warp_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 12)) goto done;
         const uint32_t tile = smem_u32(As + s * A_BYTES);
@@ -430,7 +447,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else {
     // ---- sparse loader: tile metadata and entry pieces, ahead of the stages ----
     if (lane == 0) {
-      uint32_t pc = 0, ti = 0;
+      uint32_t pcg[kMaxGroups] = {0, 0, 0, 0};  // per-group piece counters
+      uint32_t it = 0, ti = 0;
       int64_t t = blockIdx.x;
       if (t < n_tiles && !load_meta(meta, t, nc, mring, mfull, mempty, 0, abort_flag, err, 17)) goto loader_out;
       for (; t < n_tiles; t += gridDim.x, ++ti) {
@@ -440,7 +458,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!mbar_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 18)) break;
         const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
         bool ok = true;
-        for (int c = 0; c < nc && ok; ++c) ok = load_segment(ent, mt[c], ring, ring_ptr, pc, abort_flag, err, 20);
+        for (int c = 0; c < nc && ok; ++c, ++it) {
+          const int g = (int)(it % G);
+          ok = load_segment(ent, mt[c], group_ring(ring_ptr, sfull, sempty, g, NSG), pcg[g], abort_flag, err, 20);
+        }
         if (!ok) break;
       }
     }
@@ -471,7 +492,9 @@ __global__ void __launch_bounds__(kThreads, 1)
               const __grid_constant__ CUtensorMap qmap_lo, float* __restrict__ part, int fmt, int* err) {
   constexpr int N2 = 2 * LD;
   constexpr int S = rmat_stages(LD);
+  constexpr int G = rmat_groups(LD);
   constexpr int NSLOT = rmat_slots(LD);
+  constexpr int NSG = NSLOT / G;
   constexpr int SUB = TM * CW * 2;       // one 64-gene sub-tile, 16 KB
   constexpr int A_BYTES = 2 * SUB;       // 128 genes
   constexpr int Q_PLANE = TM * LD * 2;   // 128 cells x LD
@@ -495,7 +518,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* done_bar = mempty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done_bar + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  const Ring ring{smem_u32(ring_ptr), sfull, sempty, NSLOT};
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gg = blockIdx.x % n_gene_groups;
@@ -516,7 +538,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&qfull[b], 1);
       mbar_init(&qempty[b], 1);
       mbar_init(&mfull[b], 1);
-      mbar_init(&mempty[b], 4 * kGroups);
+      mbar_init(&mempty[b], 4 * G);
     }
     for (int s = 0; s < NSLOT; ++s) {
       mbar_init(&sfull[s], 1);
@@ -536,21 +558,20 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp < W_EPI) {
-    // ---- densify: group (warp / 4) takes super-chunk stages it % kGroups == group ----
+    // ---- densify: group (warp / 4) takes super-chunk stages it % G == group ----
     const int group = warp >> 2, q = warp & 3;
+    if (group >= G) goto done;  // spare warps of a narrower configuration
+    const Ring ring = group_ring(ring_ptr, sfull, sempty, group, NSG);
     uint32_t it = 0, pc = 0, ti = 0;
     if (have_work)
       for (int64_t t = t0; t < t1; ++t, ++ti) {
         if (!warp_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 21)) goto done;
         const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
         for (int sc = sc0; sc < sc1; ++sc, ++it) {
+          if ((int)(it % G) != group) continue;
           const SegMeta m0 = mt[2 * sc];
           const bool two = 2 * sc + 1 < nc;
           const SegMeta m1 = two ? mt[2 * sc + 1] : m0;
-          if ((int)(it % kGroups) != group) {
-            pc += n_pieces(m0.q[3]) + (two ? n_pieces(m1.q[3]) : 0);
-            continue;
-          }
           const int s = it % S;
           if (!warp_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 22)) goto done;
           const uint32_t tile = smem_u32(As + s * A_BYTES);
@@ -651,7 +672,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else {
     // ---- sparse loader: tile metadata and entry pieces of this gene group ----
     if (lane == 0 && have_work) {
-      uint32_t pc = 0, ti = 0;
+      uint32_t pcg[kMaxGroups] = {0, 0, 0, 0};  // per-group piece counters
+      uint32_t it = 0, ti = 0;
       int64_t t = t0;
       if (!load_meta(meta, t, nc, mring, mfull, mempty, 0, abort_flag, err, 27)) goto loader_out;
       for (; t < t1; ++t, ++ti) {
@@ -659,9 +681,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!mbar_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 29)) break;
         const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
         bool ok = true;
-        for (int sc = sc0; sc < sc1 && ok; ++sc) {
-          ok = load_segment(ent, mt[2 * sc], ring, ring_ptr, pc, abort_flag, err, 30);
-          if (ok && 2 * sc + 1 < nc) ok = load_segment(ent, mt[2 * sc + 1], ring, ring_ptr, pc, abort_flag, err, 30);
+        for (int sc = sc0; sc < sc1 && ok; ++sc, ++it) {
+          const int gq = (int)(it % G);
+          const Ring ring = group_ring(ring_ptr, sfull, sempty, gq, NSG);
+          ok = load_segment(ent, mt[2 * sc], ring, pcg[gq], abort_flag, err, 30);
+          if (ok && 2 * sc + 1 < nc) ok = load_segment(ent, mt[2 * sc + 1], ring, pcg[gq], abort_flag, err, 30);
         }
         if (!ok) break;
       }
@@ -676,6 +700,149 @@ done:
   if (warp == W_MMA) {
     tc_fence_after();
     tmem_dealloc(tmem, 512);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tall Gram on tensor cores (ld = 64): for the rows of this CTA,
+//   D  = [h|l]^T [h|l]   (128 x 128, FP32 in TMEM)  -> G = hh + hl + lh + ll
+//   Ds = [h|l]^T 1       (128 x 64)                 -> column sums of h + l
+// from the hi/lo 16-bit planes of Y (TMA, 4-stage ring).  One MMA per 16 rows
+// for each; the per-CTA partial is written in FP64 as [G (64 x 64), colsum
+// (64)], the layout the fixed-order reduction expects.
+// ---------------------------------------------------------------------------
+constexpr int kGramStages = 4;
+
+__global__ void __launch_bounds__(128, 1)
+    k_gram_tc(int64_t n_tiles, const __grid_constant__ CUtensorMap qmap_hi, const __grid_constant__ CUtensorMap qmap_lo,
+              double* __restrict__ part, int fmt, int* err) {
+  constexpr int LD = 64;
+  constexpr int PLANE = TM * LD * 2;  // 16 KB
+  constexpr int TILE = 2 * PLANE;     // [h | l]
+  constexpr int S = kGramStages;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = align1024(smem_raw);
+  uint8_t* tiles = smem;
+  uint8_t* ones = tiles + S * TILE;  // 128 rows x 64 ones, 16 KB
+  float* pbuf = reinterpret_cast<float*>(ones + PLANE);  // [128][64] partial sums for the epilogue
+  uint64_t* bars = reinterpret_cast<uint64_t*>(pbuf + TM * LD);
+  uint64_t* full = bars;
+  uint64_t* empty = full + S;
+  uint64_t* done_bar = empty + S;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done_bar + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t t0 = (int64_t)blockIdx.x * n_tiles / gridDim.x;
+  const int64_t t1 = (int64_t)(blockIdx.x + 1) * n_tiles / gridDim.x;
+  const uint16_t one16 = fmt ? (uint16_t)0x3F80u : (uint16_t)0x3C00u;
+  {
+    const uint32_t w = (uint32_t)one16 | ((uint32_t)one16 << 16);
+    uint32_t* o = reinterpret_cast<uint32_t*>(ones);
+    for (int i = threadIdx.x; i < PLANE / 4; i += blockDim.x) o[i] = w;  // all ones: swizzle-invariant
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done_bar, 1);
+    *abort_flag = 0;
+    mbar_fence_init();
+  }
+  fence_proxy_async_smem();
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, 256);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const bool have_work = t1 > t0;
+
+  if (threadIdx.x == 0 && have_work) {
+    // loader
+    uint32_t it = 0;
+    for (int64_t t = t0; t < t1; ++t, ++it) {
+      const int s = it % S;
+      if (!mbar_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 41)) break;
+      uint8_t* tile = tiles + s * TILE;
+      mbar_arrive_expect_tx(&full[s], TILE);
+      tma_load_2d(tile, &qmap_hi, &full[s], 0, (int)(t * TM));
+      tma_load_2d(tile + PLANE, &qmap_lo, &full[s], 0, (int)(t * TM));
+    }
+  } else if (threadIdx.x == 32 && have_work) {
+    // MMA issuer
+    const uint32_t idesc_g = idesc_f16(128, 128, fmt, 1, 1);
+    const uint32_t idesc_s = idesc_f16(128, 64, fmt, 1, 1);
+    const uint32_t ones_base = smem_u32(ones);
+    uint32_t it = 0;
+    bool ok = true;
+    for (int64_t t = t0; t < t1; ++t, ++it) {
+      const int s = it % S;
+      if (!mbar_wait(&full[s], (it / S) & 1u, abort_flag, err, 42)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t base = smem_u32(tiles + s * TILE);
+#pragma unroll
+      for (int kk = 0; kk < TM / 16; ++kk) {
+        const uint64_t d = sdesc_sw128(base + kk * 2048, PLANE, 1024);
+        umma_f16(tmem, d, d, idesc_g, (it | kk) != 0);
+        umma_f16(tmem + 128, d, sdesc_sw128(ones_base + kk * 2048, PLANE, 1024), idesc_s, (it | kk) != 0);
+      }
+      umma_commit(&empty[s]);
+    }
+    if (ok) umma_commit(done_bar);
+  }
+  __syncwarp();
+  // epilogue: all four warps (TMEM lane quarter = warp)
+  const uint32_t row = 32u * warp + lane;
+  float srow = 0.f;
+  if (have_work) {
+    if (!warp_wait(done_bar, 0, abort_flag, err, 43)) goto done;
+    tc_fence_after();
+    const uint32_t tb = tmem + ((32u * warp) << 16);
+#pragma unroll 1
+    for (int cb = 0; cb < 4; ++cb) {
+      uint32_t a[16], b[16];
+      tmem_ld16(tb + cb * 16, a);
+      tmem_ld16(tb + 64 + cb * 16, b);
+      tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) pbuf[row * LD + cb * 16 + i] = __uint_as_float(a[i]) + __uint_as_float(b[i]);
+    }
+    uint32_t c16[16];
+    tmem_ld16(tb + 128, c16);
+    tmem_wait_ld();
+    srow = __uint_as_float(c16[0]);
+  } else {
+    for (int j = 0; j < LD; ++j) pbuf[row * LD + j] = 0.f;
+  }
+  __syncthreads();
+  {
+    double* out = part + (int64_t)blockIdx.x * (LD * LD + LD);
+    // row < 64 holds h-rows, row >= 64 the l-rows of the same column index
+    for (int t = threadIdx.x; t < LD * LD; t += blockDim.x) {
+      const int i = t / LD, j = t % LD;
+      out[t] = (double)pbuf[i * LD + j] + (double)pbuf[(i + LD) * LD + j];
+    }
+    pbuf[row * LD] = srow;  // column sums of [h | l], one per row of Ds
+  }
+  __syncthreads();
+  if (threadIdx.x < LD) {
+    double* out = part + (int64_t)blockIdx.x * (LD * LD + LD);
+    out[LD * LD + threadIdx.x] = (double)pbuf[threadIdx.x * LD] + (double)pbuf[(threadIdx.x + LD) * LD];
+  }
+done:
+  if (*abort_flag) __nanosleep(500000);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 256);
   }
 }
 
@@ -826,6 +993,17 @@ cudaError_t launch_split16(float* in, int64_t count, uint16_t* hi, uint16_t* lo,
   note_launches(1);
   k_split16<<<grid_for(count, 256, num_sms), 256, 0, st>>>(in, count, hi, lo, fmt, write_back);
   return cudaGetLastError();
+}
+
+int launch_gram_tc(int64_t n, const CUtensorMap* qhi, const CUtensorMap* qlo, double* part, int fmt, int* err,
+                   cudaStream_t st, int num_sms) {
+  const int64_t n_tiles = (n + TM - 1) / TM;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, num_sms));
+  const size_t smem = 1024 + (size_t)kGramStages * 2 * TM * 64 * 2 + TM * 64 * 2 + TM * 64 * 4 + 256;
+  cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  note_launches(1);
+  k_gram_tc<<<grid, 128, smem, st>>>(n_tiles, *qhi, *qlo, part, fmt, err);
+  return cudaGetLastError() == cudaSuccess ? grid : -1;
 }
 
 size_t fwd_tc_smem_bytes(int ld) { return fwd_smem(ld); }

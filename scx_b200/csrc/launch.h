@@ -126,6 +126,10 @@ int rmat_tc_groups(int ld, int nc, int num_sms, int* gene_groups);
 cudaError_t launch_rmat_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc, int64_t g,
                            int gene_groups, int row_groups, const CUtensorMap* qhi, const CUtensorMap* qlo,
                            float* part, int fmt, int* err, cudaStream_t st);
+// Gram partials [G (64 x 64), colsum (64)] of (hi + lo) on tensor cores, ld 64;
+// returns the number of partials written, or -1 on a launch error.
+int launch_gram_tc(int64_t n, const CUtensorMap* qhi, const CUtensorMap* qlo, double* part, int fmt, int* err,
+                   cudaStream_t st, int num_sms);
 size_t fwd_tc_smem_bytes(int ld);
 size_t rmat_tc_smem_bytes(int ld);
 // hi = round16(x), lo = round16(x - hi); lo may be null; write_back: x = hi.

@@ -559,13 +559,20 @@ void collect_stages(scxpca_plan* pl) {
   pl->events_used = 0;
 }
 
-// Tall Gram + Cholesky (FP64) of the plan's Y buffer.
+// Tall Gram + Cholesky (FP64) of a tall matrix A.  With `planes` (tensor-core
+// path, ld 64) the Gram is taken on tensor cores from the hi/lo 16-bit planes
+// of A held in Y16/Q16lo; otherwise from the FP32 A with FP64 FMAs.
 void tall_chol(scxpca_plan* pl, const float* A, int64_t rows, double* Rinv, float* Rinv_f,
-               int shift) {
+               int shift, bool planes = false) {
   cudaStream_t st = pl->stream;
   const int ld = (int)pl->ld;
-  const int parts = (int)std::max<int64_t>(1, std::min<int64_t>(pl->gram_parts, (rows + 31) / 32));
+  int parts = (int)std::max<int64_t>(1, std::min<int64_t>(pl->gram_parts, (rows + 31) / 32));
   int s = stage_begin(pl);
+  if (planes && pl->use_tc && ld == 64) {
+    parts = launch_gram_tc(rows, &pl->qmap_hi, &pl->qmap_lo, pl->gpart.as<double>(), pl->fmt16,
+                           pl->tc_err.as<int>(), st, pl->num_sms);
+    if (parts < 0) CK(cudaGetLastError());
+  } else
   CK(launch_gram_f32(A, rows, ld, pl->gpart.as<double>(), parts, st));
   CK(launch_reduce_rows_f64(pl->gpart.as<double>(), parts, (int64_t)ld * ld + ld, pl->G.as<double>(), 0,
                             st, pl->num_sms));
@@ -702,7 +709,7 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   stage_end(pl, SCXPCA_STAGE_SMALL, s);
   // Y = (X - mu) Omega ; qr(Y)
   forward(pl);
-  tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift);
+  tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
   for (int64_t it = 0; it < p.n_power_iterations; ++it) {
     // Z = (X - mu)^T Q = (X^T Y - mu (1^T Y)) R^{-1}
     rmatmat_raw(pl, pl->Y.as<float>(), 0);
@@ -713,16 +720,19 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
     CK(launch_round_v(pl->Z.as<double>(), pl->g, ld, mu, pl->V.as<float>(), pl->mc.as<float>(), st));
     stage_end(pl, SCXPCA_STAGE_SMALL, s);
     forward(pl);
-    tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift);
+    tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
   }
   // Explicit Q = Y R^{-1}, re-orthonormalised by a second FP64 Cholesky pass.
   s = stage_begin(pl);
   CK(launch_apply_right_f32(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(), st,
                             pl->num_sms));
+  if (pl->use_tc)  // hi/lo planes of Q for the tensor-core Gram and transposed product
+    CK(launch_split16(pl->Y.as<float>(), pl->n * pl->ld, pl->Y16.as<uint16_t>(), pl->Q16lo.as<uint16_t>(),
+                      pl->fmt16, 0, st, pl->num_sms));
   stage_end(pl, SCXPCA_STAGE_APPLY, s);
-  tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift);
+  tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
   // B = (X - mu)^T Q R2^{-1}
-  rmatmat_raw(pl, pl->Y.as<float>(), 1);
+  rmatmat_raw(pl, pl->Y.as<float>(), 0);
   s = stage_begin(pl);
   CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->R2inv.as<double>(),
                          pl->Z.as<double>(), st));
