@@ -94,43 +94,63 @@ cudaError_t launch_gram_f64(const double* A, int64_t n, int ld, double* part, in
 // With shift_on_fail the factorisation restarts once on G + s I,
 // s = 10 tau max_j G_jj, which always succeeds on finite input.
 // ---------------------------------------------------------------------------
-// One barrier per elimination step: every thread reads the pivot d_j itself,
-// the trailing update uses the unscaled row j (A_ac -= A_ja A_jc / d_j), and
-// the scaled row j of R goes straight to global memory.  R^{-1} is then
-// formed in place row by row from the bottom (row i needs only rows > i),
-// one warp per column dot product.
+// Layout: A (the working copy of G) is k x S row-major in shared memory with
+// an odd stride S, so a warp reading one column (32 rows) touches 32 distinct
+// banks.  The elimination only touches the upper triangle, so R is stored
+// transposed in the strict lower triangle (A[c][j] = R_jc, c > j) with its
+// diagonal in rd[].  One barrier per elimination step: warp ty updates rows
+// a = j+1+ty+32u of the trailing block, lanes striding over the columns
+// c >= a, from the unscaled row j (A_ac -= A_ja A_jc / d_j), and the scaled
+// row j of R goes to column j below the diagonal.  R^{-1} is then formed one column per
+// warp by column-oriented back substitution: lane i keeps the running
+// right-hand side of rows i, i+32, ...; step l takes x_l from its owner lane
+// by a shuffle and updates the rows above it, so a step costs one shuffle.
 __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G, int k, int ld, double tau,
                                                    int shift_on_fail, double* __restrict__ R,
                                                    double* __restrict__ Rinv, float* __restrict__ Rinv_f,
                                                    int* __restrict__ status) {
-  extern __shared__ double A[];  // [k][k], then tmp[k]
-  double* tmp = A + k * k;
+  extern __shared__ double sm[];
+  const int S = k | 1;
+  double* A = sm;           // [k][S]
+  double* dg = A + k * S;   // [k] diagonal of G
+  double* rd = dg + k;      // [k] R_jj
+  double* dinv = rd + k;    // [k] 1 / R_jj
+  __shared__ double maxdiag_s;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-  double maxdiag = 0.0;
-  for (int j = 0; j < k; ++j) maxdiag = fmax(maxdiag, G[j * ld + j]);
+  const int tx = lane, ty = warp;
+  for (int j = tid; j < k; j += nt) dg[j] = G[(int64_t)j * ld + j];
+  __syncthreads();
+  if (warp == 0) {
+    double m = 0.0;
+    for (int j = lane; j < k; j += 32) m = fmax(m, dg[j]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) maxdiag_s = m;
+  }
   double shift = 0.0;
   int fail = -1;
   for (int attempt = 0; attempt < 2; ++attempt) {
-    for (int t = tid; t < ld * ld; t += nt) R[t] = 0.0;
-    for (int t = tid; t < k * k; t += nt) {
-      const int r = t / k, c = t % k;
-      A[t] = G[r * ld + c] + (r == c ? shift : 0.0);
+    for (int t = tid; t < k * S; t += nt) {
+      const int r = t / S, c = t - r * S;
+      A[t] = c < k ? G[(int64_t)r * ld + c] + (r == c ? shift : 0.0) : 0.0;
     }
     __syncthreads();
     fail = -1;
     for (int j = 0; j < k; ++j) {
-      const double d = A[j * k + j];
-      const double d0 = G[j * ld + j] + shift;
+      const double d = A[j * S + j];
+      const double d0 = dg[j] + shift;
       if (!(isfinite(d) && d > 0.0 && (attempt == 1 || d > tau * d0))) {
         fail = j;  // every thread sees the same pivot: uniform exit
         break;
       }
-      const double rinv = rsqrt(d), dinv = 1.0 / d;
-      for (int c = j + tid; c < k; c += nt) R[j * ld + c] = A[j * k + c] * rinv;
-      const int m = k - j - 1;
-      for (int t = tid; t < m * m; t += nt) {
-        const int a = j + 1 + t / m, c = j + 1 + t % m;
-        if (c >= a) A[a * k + c] -= A[j * k + a] * A[j * k + c] * dinv;
+      const double rinv = rsqrt(d), di = 1.0 / d;
+      if (tid == 0) {
+        rd[j] = d * rinv;
+        dinv[j] = 1.0 / (d * rinv);
+      }
+      for (int c = j + 1 + tid; c < k; c += nt) A[c * S + j] = A[j * S + c] * rinv;
+      for (int a = j + 1 + ty; a < k; a += nw) {
+        const double f = A[j * S + a] * di;
+        for (int c = a + tx; c < k; c += 32) A[a * S + c] -= f * A[j * S + c];
       }
       __syncthreads();
     }
@@ -149,34 +169,58 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
       return;
     }
     if (tid == 0) status[0] += 1;
-    shift = 10.0 * tau * fmax(maxdiag, 1e-300);
+    shift = 10.0 * tau * fmax(maxdiag_s, 1e-300);
   }
-  __syncthreads();
-  // A <- R (upper; lower part ignored), then invert in place from the bottom row up.
-  for (int t = tid; t < k * k; t += nt) A[t] = R[(t / k) * ld + (t % k)];
-  __syncthreads();
-  for (int i = k - 1; i >= 0; --i) {
-    for (int c = i + tid; c < k; c += nt) tmp[c] = A[i * k + c];
-    __syncthreads();
-    for (int c = i + warp; c < k; c += nw) {
-      double s = 0.0;
-      for (int l = i + 1 + lane; l <= c; l += 32) s += tmp[l] * A[l * k + c];
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) A[i * k + c] = ((i == c ? 1.0 : 0.0) - s) / tmp[i];
-    }
-    __syncthreads();
-  }
+  // R to global (zero outside the leading upper triangle).
   for (int t = tid; t < ld * ld; t += nt) {
     const int r = t / ld, c = t % ld;
-    const double v = (r < k && c < k && c >= r) ? A[r * k + c] : 0.0;
-    Rinv[t] = v;
-    Rinv_f[t] = (float)v;
+    R[t] = (r < k && c < k && c >= r) ? (c == r ? rd[r] : A[c * S + r]) : 0.0;
+  }
+  // R^{-1}, column c per warp: solve R x = e_c from the bottom.
+  constexpr int U = kMaxK / 32;
+  for (int c = warp; c < k; c += nw) {
+    double acc[U], x[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      acc[u] = (lane + 32 * u == c) ? 1.0 : 0.0;
+      x[u] = 0.0;
+    }
+    for (int l = c; l >= 0; --l) {
+      const int ul = l >> 5;
+      double v = acc[0];
+#pragma unroll
+      for (int u = 1; u < U; ++u)
+        if (ul == u) v = acc[u];
+      const double xl = __shfl_sync(0xffffffffu, v, l & 31) * dinv[l];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int i = lane + 32 * u;
+        if (ul == u && lane == (l & 31)) x[u] = xl;
+        if (i < l) acc[u] -= A[l * S + i] * xl;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = lane + 32 * u;
+      if (i < ld) {
+        const double v = (i <= c) ? x[u] : 0.0;
+        Rinv[(int64_t)i * ld + c] = v;
+        Rinv_f[(int64_t)i * ld + c] = (float)v;
+      }
+    }
+  }
+  // columns k..ld-1 of R^{-1} are zero
+  for (int t = tid; t < ld * (ld - k); t += nt) {
+    const int r = t / (ld - k), c = k + t % (ld - k);
+    Rinv[(int64_t)r * ld + c] = 0.0;
+    Rinv_f[(int64_t)r * ld + c] = 0.f;
   }
 }
 
 cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shift_on_fail,
                             double* R, double* Rinv, float* Rinv_f, int* status, cudaStream_t st) {
-  size_t smem = (size_t)(k * k + k) * sizeof(double);
+  const int S = k | 1;
+  size_t smem = (size_t)(k * S + 3 * k) * sizeof(double);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(k_cholesky, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   note_launches(1);
@@ -185,79 +229,145 @@ cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shif
 }
 
 // ---------------------------------------------------------------------------
-// Tall x small: Out[i, :cnt] = In[i, :K] * M (K x cnt), one thread per row.
-// M (zero-padded to OUTB columns) sits in shared memory and every thread of a
-// warp reads the same M entries (broadcast); the row and its OUTB outputs stay
-// in registers, so there are four FMAs per shared load.  A thread reads its
-// whole row before writing, so Out may alias In.
+// Tall x small: Out[i, :cnt] = In[i, :K] * M (K x cnt), 64-row tiles.
+// M (zero-padded to OUTB columns) and the tile sit in shared memory; thread
+// (ty, tx) of the 16 x 16 grid computes rows 4 ty .. 4 ty + 3 at columns
+// 4 tx + 64 h + (0..3): per four k-steps it reads four float4 of its rows
+// (two distinct addresses per warp: broadcast) and 4 OUTB/64 float4 of M for
+// 16 OUTB/64 FMAs each.  A block stages its rows before writing any of them,
+// so Out may alias In.  Optionally writes the hi/lo 16-bit planes of Out
+// (hi = round16(x), lo = round16(x - hi); fmt 1 = bf16, 0 = f16) in the same
+// pass.
 // ---------------------------------------------------------------------------
+constexpr int kTallRows = 64;
+
+__device__ __forceinline__ void split16(float x, int fmt, uint16_t& h, uint16_t& l) {
+  if (fmt) {
+    const __nv_bfloat16 b = __float2bfloat16_rn(x);
+    h = __bfloat16_as_ushort(b);
+    l = __bfloat16_as_ushort(__float2bfloat16_rn(x - __bfloat162float(b)));
+  } else {
+    const __half b = __float2half_rn(x);
+    h = __half_as_ushort(b);
+    l = __half_as_ushort(__float2half_rn(x - __half2float(b)));
+  }
+}
+
 template <int OUTB>
-__global__ void __launch_bounds__(128) k_tall_mm(const float* In, int64_t n, int K, int ldi,
-                                                 const float* __restrict__ M, int ldm, int cnt,
-                                                 float* Out, int ldo) {
-  extern __shared__ float Ms[];  // [K][OUTB]
+__global__ void __launch_bounds__(256) k_tall_mm(const float* In, int64_t n, int K, int ldi,
+                                                 const float* __restrict__ M, int ldm, int cnt, float* Out,
+                                                 int ldo, uint16_t* __restrict__ hi, uint16_t* __restrict__ lo,
+                                                 int fmt) {
+  constexpr int H = OUTB / 64;
+  extern __shared__ __align__(16) float sm_f[];
+  const int KP = K + 4;
+  float* Ms = sm_f;             // [K][OUTB]
+  float* Ts = sm_f + K * OUTB;  // [kTallRows][KP]
   for (int t = threadIdx.x; t < K * OUTB; t += blockDim.x) {
     const int l = t / OUTB, o = t % OUTB;
     Ms[t] = o < cnt ? M[l * ldm + o] : 0.f;
   }
-  __syncthreads();
-  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < n;
-       row += (int64_t)gridDim.x * blockDim.x) {
-    float acc[OUTB];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int k4 = K >> 2;
+  const bool vec_out = ((cnt & 3) == 0) && ((ldo & 3) == 0);
+  const int64_t n_tiles = (n + kTallRows - 1) / kTallRows;
+  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int64_t r0 = tile * kTallRows;
+    __syncthreads();  // the previous tile is consumed (and M is staged)
+    for (int t = threadIdx.x; t < kTallRows * k4; t += blockDim.x) {
+      const int r = t / k4, c4 = t - r * k4;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (r0 + r < n) v = reinterpret_cast<const float4*>(In + (r0 + r) * ldi)[c4];
+      *reinterpret_cast<float4*>(Ts + r * KP + 4 * c4) = v;
+    }
+    __syncthreads();
+    float acc[4][4 * H];
 #pragma unroll
-    for (int o = 0; o < OUTB; ++o) acc[o] = 0.f;
-    const float4* in4 = reinterpret_cast<const float4*>(In + row * ldi);
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int o = 0; o < 4 * H; ++o) acc[i][o] = 0.f;
     for (int l = 0; l < K; l += 4) {
-      const float4 x = in4[l >> 2];
-      const float xs[4] = {x.x, x.y, x.z, x.w};
+      float4 a[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = *reinterpret_cast<const float4*>(Ts + (4 * ty + i) * KP + l);
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const float4* mr = reinterpret_cast<const float4*>(Ms + (l + u) * OUTB);
 #pragma unroll
-        for (int o = 0; o < OUTB / 4; ++o) {
-          const float4 m = mr[o];
-          acc[4 * o + 0] = fmaf(xs[u], m.x, acc[4 * o + 0]);
-          acc[4 * o + 1] = fmaf(xs[u], m.y, acc[4 * o + 1]);
-          acc[4 * o + 2] = fmaf(xs[u], m.z, acc[4 * o + 2]);
-          acc[4 * o + 3] = fmaf(xs[u], m.w, acc[4 * o + 3]);
+        for (int h = 0; h < H; ++h) {
+          const float4 m = *reinterpret_cast<const float4*>(Ms + (l + u) * OUTB + 64 * h + 4 * tx);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float x = u == 0 ? a[i].x : u == 1 ? a[i].y : u == 2 ? a[i].z : a[i].w;
+            acc[i][4 * h + 0] = fmaf(x, m.x, acc[i][4 * h + 0]);
+            acc[i][4 * h + 1] = fmaf(x, m.y, acc[i][4 * h + 1]);
+            acc[i][4 * h + 2] = fmaf(x, m.z, acc[i][4 * h + 2]);
+            acc[i][4 * h + 3] = fmaf(x, m.w, acc[i][4 * h + 3]);
+          }
         }
       }
     }
-    float* out = Out + row * ldo;
-    if ((cnt & 3) == 0 && (ldo & 3) == 0) {
 #pragma unroll
-      for (int o = 0; o < OUTB / 4; ++o)
-        if (4 * o < cnt)
-          reinterpret_cast<float4*>(out)[o] =
-              make_float4(acc[4 * o], acc[4 * o + 1], acc[4 * o + 2], acc[4 * o + 3]);
-    } else {
+    for (int i = 0; i < 4; ++i) {
+      const int64_t row = r0 + 4 * ty + i;
+      if (row >= n) continue;
 #pragma unroll
-      for (int o = 0; o < OUTB; ++o)
-        if (o < cnt) out[o] = acc[o];
+      for (int h = 0; h < H; ++h) {
+        const int col = 64 * h + 4 * tx;
+        if (col >= cnt) continue;
+        float* out = Out + row * ldo + col;
+        const float* v = &acc[i][4 * h];
+        if (vec_out) {
+          *reinterpret_cast<float4*>(out) = make_float4(v[0], v[1], v[2], v[3]);
+          if (hi) {
+            uint16_t hh[4], ll[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) split16(v[j], fmt, hh[j], ll[j]);
+            *reinterpret_cast<uint2*>(hi + row * ldo + col) =
+                make_uint2(hh[0] | ((uint32_t)hh[1] << 16), hh[2] | ((uint32_t)hh[3] << 16));
+            *reinterpret_cast<uint2*>(lo + row * ldo + col) =
+                make_uint2(ll[0] | ((uint32_t)ll[1] << 16), ll[2] | ((uint32_t)ll[3] << 16));
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (col + j < cnt) {
+              out[j] = v[j];
+              if (hi) split16(v[j], fmt, hi[row * ldo + col + j], lo[row * ldo + col + j]);
+            }
+        }
+      }
     }
   }
 }
 
 static cudaError_t tall_mm(const float* In, int64_t n, int K, int ldi, const float* M, int ldm, int cnt,
-                           float* Out, int ldo, cudaStream_t st, int num_sms) {
+                           float* Out, int ldo, uint16_t* hi, uint16_t* lo, int fmt, cudaStream_t st,
+                           int num_sms) {
   if (n == 0) return cudaSuccess;
+  if ((K & 3) || (ldi & 3)) return cudaErrorInvalidValue;
   const int outb = cnt <= 64 ? 64 : 128;
-  const size_t smem = (size_t)K * outb * sizeof(float);
-  const int grid = grid_for(n, 128, num_sms, 8);
+  const size_t smem = ((size_t)K * outb + (size_t)kTallRows * (K + 4)) * sizeof(float);
+  const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024) / smem));
+  const int grid = grid_for(n, kTallRows, num_sms, per_sm);
   note_launches(1);
   if (outb == 64) {
     cudaFuncSetAttribute(k_tall_mm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_tall_mm<64><<<grid, 128, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo);
+    k_tall_mm<64><<<grid, 256, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo, hi, lo, fmt);
   } else {
     cudaFuncSetAttribute(k_tall_mm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_tall_mm<128><<<grid, 128, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo);
+    k_tall_mm<128><<<grid, 256, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo, hi, lo, fmt);
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_apply_right_f32(const float* In, int64_t n, int ld, const float* M, float* Out,
                                    cudaStream_t st, int num_sms) {
-  return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, st, num_sms);
+  return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, nullptr, nullptr, 0, st, num_sms);
+}
+
+cudaError_t launch_apply_right_split(const float* In, int64_t n, int ld, const float* M, float* Out,
+                                     uint16_t* hi, uint16_t* lo, int fmt, cudaStream_t st, int num_sms) {
+  return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, hi, lo, fmt, st, num_sms);
 }
 
 // ---------------------------------------------------------------------------
@@ -294,7 +404,7 @@ cudaError_t launch_center_apply(const double* W, int64_t g, int ld, const double
   size_t smem = (size_t)(ld * ld + 256) * sizeof(double);
   cudaFuncSetAttribute(k_center_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int rpb = 256 / ld;
-  int grid = (int)std::min<int64_t>((g + rpb - 1) / rpb, 1184);
+  int grid = (int)std::min<int64_t>((g + rpb - 1) / rpb, 160);  // M is staged once per block
   note_launches(1);
   k_center_apply<<<grid, 256, smem, st>>>(W, g, ld, mu, s, M, Z);
   return cudaGetLastError();
@@ -343,98 +453,105 @@ cudaError_t launch_round_v(const double* A, int64_t g, int ld, const double* mu,
 
 // ---------------------------------------------------------------------------
 // Parallel cyclic Jacobi (round-robin pairing) for the symmetric k x k block
-// of C.  Each round rotates kk/2 disjoint pairs: angles first, then column
-// rotations of A and E, then row rotations of A.  Stops when the off-diagonal
-// mass falls below (1e-15)^2 of the total or after 40 sweeps.
+// of C, one warp per rotation pair.  A round computes the kk/2 angles of
+// disjoint pairs from the round's starting A, rotates columns p, q of A and E
+// (phase 1, each warp its own two columns: no other warp touches them), then
+// rows p, q of A (phase 2): two barriers per round.  Matrices are row-major in
+// shared memory with an odd stride so column walks are free of bank
+// conflicts; E moves to global scratch when both do not fit.  Stops after a
+// sweep with no rotation (every off-diagonal entry below 1e-15 of the
+// geometric mean of its two diagonal entries) or after 40 sweeps.
 // ---------------------------------------------------------------------------
-__global__ void k_jacobi(const double* __restrict__ C, int k, int ld, double* __restrict__ evals,
-                         double* __restrict__ evecs, double* __restrict__ Eglob, int* sweeps_out) {
+__global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, int k, int ld,
+                                                 double* __restrict__ evals, double* __restrict__ evecs,
+                                                 double* __restrict__ Eglob, int* sweeps_out) {
   extern __shared__ double sm[];
   const int kk = (k + 1) & ~1;  // even number of players; index k (if odd) is a dummy
-  double* A = sm;               // [kk][kk]
-  double* E = (Eglob != nullptr) ? Eglob : sm + kk * kk;
+  const int S = kk + 1;
+  double* A = sm;  // [kk][S]
+  double* E = (Eglob != nullptr) ? Eglob : sm + kk * S;
   __shared__ double cs[kMaxK / 2], sn[kMaxK / 2];
-  __shared__ int pp[kMaxK / 2], qq[kMaxK / 2];
-  __shared__ double red[256];
   __shared__ int done;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int t = tid; t < kk * kk; t += nt) {
-    int r = t / kk, c = t % kk;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  for (int t = tid; t < kk * S; t += nt) {
+    const int r = t / S, c = t - r * S;
     A[t] = (r < k && c < k) ? C[r * ld + c] : 0.0;
     E[t] = (r == c) ? 1.0 : 0.0;
   }
+  if (tid == 0) done = 1;
   __syncthreads();
-  const int npair = kk / 2;
+  const int npair = kk / 2, m = kk - 1;
   int sweep = 0;
-  (void)red;
   for (; sweep < 40; ++sweep) {
-    // Converged when a whole sweep performs no rotation: every off-diagonal
-    // entry is below 1e-15 of the geometric mean of its two diagonal entries.
-    if (tid == 0) done = 1;
-    __syncthreads();
-    for (int round = 0; round < kk - 1; ++round) {
-      for (int i = tid; i < npair; i += nt) {
+    for (int round = 0; round < m; ++round) {
+      for (int i = warp; i < npair; i += nw) {
         int a, b;
-        if (i == 0) { a = round; b = kk - 1; }
-        else { a = (round + i) % (kk - 1); b = (round - i + (kk - 1)) % (kk - 1); }
-        int p = min(a, b), q = max(a, b);
+        if (i == 0) { a = round; b = m; }
+        else { a = (round + i) % m; b = (round - i + m) % m; }
+        const int p = min(a, b), q = max(a, b);
         double c = 1.0, s = 0.0;
         if (q < k) {
-          double apq = A[p * kk + q];
-          double app = A[p * kk + p], aqq = A[q * kk + q];
+          const double apq = A[p * S + q], app = A[p * S + p], aqq = A[q * S + q];
           if (fabs(apq) > 1e-300 && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq))) {
-            double theta = (aqq - app) / (2.0 * apq);
-            double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            const double theta = (aqq - app) / (2.0 * apq);
+            const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
             c = 1.0 / sqrt(t * t + 1.0);
             s = t * c;
-            done = 0;
           }
         }
-        pp[i] = p; qq[i] = q; cs[i] = c; sn[i] = s;
+        if (lane == 0) {
+          cs[i] = c;
+          sn[i] = s;
+        }
+        if (s != 0.0) {  // warp-uniform
+          __syncwarp();  // the angle reads above precede every write below
+          for (int r = lane; r < kk; r += 32) {
+            const double xp = A[r * S + p], xq = A[r * S + q];
+            A[r * S + p] = c * xp - s * xq;
+            A[r * S + q] = s * xp + c * xq;
+            const double ep = E[r * S + p], eq = E[r * S + q];
+            E[r * S + p] = c * ep - s * eq;
+            E[r * S + q] = s * ep + c * eq;
+          }
+          if (lane == 0) done = 0;
+        }
       }
       __syncthreads();
-      // columns of A and E: (x_p, x_q) <- (c x_p - s x_q, s x_p + c x_q)
-      for (int t = tid; t < npair * kk; t += nt) {
-        int i = t / kk, r = t % kk;
-        double c = cs[i], s = sn[i];
+      for (int i = warp; i < npair; i += nw) {
+        const double s = sn[i];
         if (s == 0.0) continue;
-        int p = pp[i], q = qq[i];
-        double xp = A[r * kk + p], xq = A[r * kk + q];
-        A[r * kk + p] = c * xp - s * xq;
-        A[r * kk + q] = s * xp + c * xq;
-        double ep = E[r * kk + p], eq = E[r * kk + q];
-        E[r * kk + p] = c * ep - s * eq;
-        E[r * kk + q] = s * ep + c * eq;
-      }
-      __syncthreads();
-      // rows of A
-      for (int t = tid; t < npair * kk; t += nt) {
-        int i = t / kk, col = t % kk;
-        double c = cs[i], s = sn[i];
-        if (s == 0.0) continue;
-        int p = pp[i], q = qq[i];
-        double xp = A[p * kk + col], xq = A[q * kk + col];
-        A[p * kk + col] = c * xp - s * xq;
-        A[q * kk + col] = s * xp + c * xq;
+        const double c = cs[i];
+        int a, b;
+        if (i == 0) { a = round; b = m; }
+        else { a = (round + i) % m; b = (round - i + m) % m; }
+        const int p = min(a, b), q = max(a, b);
+        for (int col = lane; col < kk; col += 32) {
+          const double xp = A[p * S + col], xq = A[q * S + col];
+          A[p * S + col] = c * xp - s * xq;
+          A[q * S + col] = s * xp + c * xq;
+        }
       }
       __syncthreads();
     }
-    if (done) break;
+    const int converged = done;
+    __syncthreads();  // every thread has read the flag before it is reset
+    if (converged) break;
+    if (tid == 0) done = 1;
     __syncthreads();
   }
   // sort eigenvalues descending: rank of each by counting (ties by index)
   for (int i = tid; i < k; i += nt) {
-    double v = A[i * kk + i];
+    const double v = A[i * S + i];
     int rank = 0;
     for (int j = 0; j < k; ++j) {
-      double w = A[j * kk + j];
+      const double w = A[j * S + j];
       if (w > v || (w == v && j < i)) ++rank;
     }
     evals[rank] = v;
-    for (int r = 0; r < ld; ++r) evecs[r * ld + rank] = (r < k) ? E[r * kk + i] : 0.0;
+    for (int r = 0; r < ld; ++r) evecs[r * ld + rank] = (r < k) ? E[r * S + i] : 0.0;
   }
   for (int t = tid; t < ld * ld; t += nt) {
-    int c = t % ld;
+    const int c = t % ld;
     if (c >= k) evecs[t] = 0.0;
   }
   if (tid == 0 && sweeps_out) *sweeps_out = sweep;
@@ -442,22 +559,20 @@ __global__ void k_jacobi(const double* __restrict__ C, int k, int ld, double* __
 
 cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, double* evecs,
                               int* sweeps, cudaStream_t st) {
-  int kk = (k + 1) & ~1;
-  size_t both = (size_t)2 * kk * kk * sizeof(double);
-  size_t one = (size_t)kk * kk * sizeof(double);
-  // E lives in shared memory when both matrices fit, else in the tail of evecs'
-  // allocation is not available, so use a dedicated global scratch: evecs itself
-  // cannot be reused (it is written at the end), so the caller's evecs buffer is
-  // followed by kk*kk doubles of scratch (the plan allocates 2 * ld * ld).
+  const int kk = (k + 1) & ~1;
+  const size_t one = (size_t)kk * (kk + 1) * sizeof(double);
+  // E lives in shared memory when both matrices fit, else in the scratch that
+  // follows evecs (the plan allocates 2 * ld * ld doubles there).
   double* eglob = nullptr;
-  size_t smem = both;
-  if (both > 200 * 1024) {
+  size_t smem = 2 * one;
+  if (smem > 200 * 1024) {
     eglob = evecs + (size_t)ld * ld;
     smem = one;
   }
   cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int warps = std::min(32, std::max(1, kk / 2));
   note_launches(1);
-  k_jacobi<<<1, 256, smem, st>>>(C, k, ld, evals, evecs, eglob, sweeps);
+  k_jacobi<<<1, 32 * warps, smem, st>>>(C, k, ld, evals, evecs, eglob, sweeps);
   return cudaGetLastError();
 }
 
@@ -465,28 +580,30 @@ cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, dou
 // Rayleigh-Ritz finish (single kernel, one block per gene row for the
 // components plus block 0 building M_emb).
 // ---------------------------------------------------------------------------
-__global__ void k_ritz_finish(const double* __restrict__ B, int64_t g, int ld, int k, int nc,
-                              const double* __restrict__ evals, const double* __restrict__ E,
-                              const double* __restrict__ Rinv2, double* __restrict__ sigma,
-                              float* __restrict__ comps, float* __restrict__ M_emb) {
+__global__ void __launch_bounds__(128) k_ritz_finish(const double* __restrict__ B, int64_t g, int ld, int k,
+                                                     int nc, const double* __restrict__ evals,
+                                                     const double* __restrict__ E,
+                                                     const double* __restrict__ Rinv2, double* __restrict__ sigma,
+                                                     float* __restrict__ comps, float* __restrict__ M_emb) {
   extern __shared__ double sm[];
   double* Es = sm;             // [ld][nc]
   double* sg = sm + ld * nc;   // [nc]
   for (int t = threadIdx.x; t < ld * nc; t += blockDim.x) {
-    int l = t / nc, c = t % nc;
+    const int l = t / nc, c = t - l * nc;
     Es[t] = E[l * ld + c];
   }
   for (int c = threadIdx.x; c < nc; c += blockDim.x) sg[c] = sqrt(fmax(evals[c], 0.0));
   __syncthreads();
-  if (blockIdx.x == 0) {
+  if (blockIdx.x == 0)
     for (int c = threadIdx.x; c < k; c += blockDim.x) sigma[c] = sqrt(fmax(evals[c], 0.0));
-    for (int t = threadIdx.x; t < ld * nc; t += blockDim.x) {
-      int l = t / nc, c = t % nc;
+  // M_emb row l (one row per block in turn) = Rinv2[l, :] E[:, :nc] diag(sigma)
+  for (int l = blockIdx.x; l < ld; l += gridDim.x)
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
       double acc = 0.0;
       for (int m = 0; m < ld; ++m) acc = fma(Rinv2[l * ld + m], Es[m * nc + c], acc);
-      M_emb[t] = (float)(acc * sg[c]);
+      M_emb[l * nc + c] = (float)(acc * sg[c]);
     }
-  }
+  // components[c][j] = (B E)[j][c] / sigma_c
   for (int64_t j = blockIdx.x; j < g; j += gridDim.x) {
     for (int c = threadIdx.x; c < nc; c += blockDim.x) {
       double acc = 0.0;
@@ -501,7 +618,8 @@ cudaError_t launch_ritz_finish(const double* B, int64_t g, int ld, int k, int nc
                                double* sigma, float* components, float* M_emb, cudaStream_t st) {
   size_t smem = (size_t)(ld * nc + nc) * sizeof(double);
   cudaFuncSetAttribute(k_ritz_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int grid = (int)std::min<int64_t>(g, 2048);
+  // Few blocks: each stages E once and then takes a run of genes.
+  const int grid = (int)std::max<int64_t>(std::min<int64_t>(g, 296), std::min<int64_t>(ld, 296));
   note_launches(1);
   k_ritz_finish<<<grid, 128, smem, st>>>(B, g, ld, k, nc, evals, evecs, Rinv2, sigma, components,
                                          M_emb);
@@ -512,7 +630,7 @@ cudaError_t launch_ritz_finish(const double* B, int64_t g, int ld, int k, int nc
 cudaError_t launch_embed(const float* Q, int64_t n, int ld, int k, const float* M_emb, int nc,
                          float* U, cudaStream_t st, int num_sms) {
   (void)k;  // rows k..ld-1 of M_emb are zero
-  return tall_mm(Q, n, ld, ld, M_emb, nc, nc, U, nc, st, num_sms);
+  return tall_mm(Q, n, ld, ld, M_emb, nc, nc, U, nc, nullptr, nullptr, 0, st, num_sms);
 }
 
 // ---------------------------------------------------------------------------

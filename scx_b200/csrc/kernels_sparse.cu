@@ -51,15 +51,41 @@ __global__ void k_col_stats_global(const int32_t* __restrict__ idx, const ValT* 
   }
 }
 
-// out[i] = sum_{b < nparts} part[b * len + i], summed in b order (deterministic).
+// out[i] (+)= sum_{b < nparts} part[b * len + i] in FP64.  A block takes 32
+// consecutive outputs (one per lane, coalesced); warp w sums the partials
+// b = w, w + 8, ... with four loads in flight, and warp 0 adds the eight warp
+// sums in warp order: a fixed order, so the result is deterministic.
 template <typename T>
-__global__ void k_reduce_rows(const T* __restrict__ part, int nparts, int64_t len,
-                              double* __restrict__ out, int accumulate) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    double acc = accumulate ? out[i] : 0.0;
-    for (int b = 0; b < nparts; ++b) acc += (double)part[(int64_t)b * len + i];
-    out[i] = acc;
+__global__ void __launch_bounds__(256) k_reduce_rows(const T* __restrict__ part, int nparts, int64_t len,
+                                                     double* __restrict__ out, int accumulate) {
+  __shared__ double red[8][33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int64_t base = (int64_t)blockIdx.x * 32; base < len; base += (int64_t)gridDim.x * 32) {
+    const int64_t i = base + lane;
+    double acc = 0.0;
+    if (i < len) {
+      int b = w;
+      for (; b + 24 < nparts; b += 32) {
+        const double v0 = (double)part[(int64_t)b * len + i];
+        const double v1 = (double)part[(int64_t)(b + 8) * len + i];
+        const double v2 = (double)part[(int64_t)(b + 16) * len + i];
+        const double v3 = (double)part[(int64_t)(b + 24) * len + i];
+        acc += v0;
+        acc += v1;
+        acc += v2;
+        acc += v3;
+      }
+      for (; b < nparts; b += 8) acc += (double)part[(int64_t)b * len + i];
+    }
+    red[w][lane] = acc;
+    __syncthreads();
+    if (w == 0 && i < len) {
+      double s = accumulate ? out[i] : 0.0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) s += red[u][lane];
+      out[i] = s;
+    }
+    __syncthreads();
   }
 }
 
@@ -389,14 +415,14 @@ cudaError_t launch_spmm_t(int dtype, int ld, const int64_t* indptr, const int32_
 cudaError_t launch_reduce_rows_f32(const float* part, int nparts, int64_t len, double* out,
                                    int accumulate, cudaStream_t st, int num_sms) {
   note_launches(1);
-  k_reduce_rows<float><<<grid_for(len, 256, num_sms), 256, 0, st>>>(part, nparts, len, out, accumulate);
+  k_reduce_rows<float><<<grid_for(len, 32, num_sms), 256, 0, st>>>(part, nparts, len, out, accumulate);
   return cudaGetLastError();
 }
 
 cudaError_t launch_reduce_rows_f64(const double* part, int nparts, int64_t len, double* out,
                                    int accumulate, cudaStream_t st, int num_sms) {
   note_launches(1);
-  k_reduce_rows<double><<<grid_for(len, 256, num_sms), 256, 0, st>>>(part, nparts, len, out, accumulate);
+  k_reduce_rows<double><<<grid_for(len, 32, num_sms), 256, 0, st>>>(part, nparts, len, out, accumulate);
   return cudaGetLastError();
 }
 

@@ -67,6 +67,10 @@ cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shif
 // Tall apply: Out[i, :] = In[i, :] * M (ld x ld float, upper-triangular or full).
 cudaError_t launch_apply_right_f32(const float* In, int64_t n, int ld, const float* M,
                                    float* Out, cudaStream_t st, int num_sms);
+// Same, also writing the hi/lo 16-bit planes of Out (row stride ld; fmt 1 =
+// bf16, 0 = f16).
+cudaError_t launch_apply_right_split(const float* In, int64_t n, int ld, const float* M, float* Out,
+                                     uint16_t* hi, uint16_t* lo, int fmt, cudaStream_t st, int num_sms);
 // Gene-side ops (n_vars x ld, FP64):
 //   Z = (W - mu s^T) M        (mu may be null)
 cudaError_t launch_center_apply(const double* W, int64_t g, int ld, const double* mu,

@@ -501,7 +501,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
     pl->Rinv_f.alloc(sizeof(float) * ld * ld);
     pl->R2inv.alloc(sizeof(double) * ld * ld);
     pl->evals.alloc(sizeof(double) * ld);
-    pl->evecs.alloc(sizeof(double) * 2 * ld * ld);
+    pl->evecs.alloc(sizeof(double) * (ld * ld + ld * (ld + 1)));  // + eigensolver scratch
     pl->sigma.alloc(sizeof(double) * ld);
     pl->comps.alloc(sizeof(float) * pl->nc * g);
     pl->M_emb.alloc(sizeof(float) * ld * pl->nc);
@@ -724,11 +724,12 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   }
   // Explicit Q = Y R^{-1}, re-orthonormalised by a second FP64 Cholesky pass.
   s = stage_begin(pl);
-  CK(launch_apply_right_f32(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(), st,
-                            pl->num_sms));
-  if (pl->use_tc)  // hi/lo planes of Q for the tensor-core Gram and transposed product
-    CK(launch_split16(pl->Y.as<float>(), pl->n * pl->ld, pl->Y16.as<uint16_t>(), pl->Q16lo.as<uint16_t>(),
-                      pl->fmt16, 0, st, pl->num_sms));
+  if (pl->use_tc)  // with the hi/lo planes of Q for the tensor-core Gram and transposed product
+    CK(launch_apply_right_split(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(),
+                                pl->Y16.as<uint16_t>(), pl->Q16lo.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
+  else
+    CK(launch_apply_right_f32(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(), st,
+                              pl->num_sms));
   stage_end(pl, SCXPCA_STAGE_APPLY, s);
   tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
   // B = (X - mu)^T Q R2^{-1}
