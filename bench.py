@@ -313,6 +313,7 @@ def run_ours(args):
         "config": base_config(n_obs, nnz, args.mode, world),
     }
     out["ms_per_step"] = round(ms_max, 4)
+    out["eig_sweeps"] = int(res.eig_sweeps)
     out["value"] = round(ms_max / world, 4)
 
     # roofline of the dominant kernel, from the live stage timing of the timed region

@@ -125,6 +125,8 @@ typedef struct {
   int32_t total_var_recomputed; /* out: 1 when the cancellation guard fired */
   int32_t shifted_cholesky;     /* out: number of shifted Gram factorisations */
   double total_var;             /* out: total variance used for the ratios */
+  int32_t eig_sweeps;           /* out: Jacobi sweeps of the k x k eigensolver */
+  int32_t reserved1;
 } scxpca_result;
 
 typedef struct scxpca_plan scxpca_plan;

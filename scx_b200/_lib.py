@@ -101,6 +101,8 @@ class Result(C.Structure):
         ("total_var_recomputed", C.c_int32),
         ("shifted_cholesky", C.c_int32),
         ("total_var", C.c_double),
+        ("eig_sweeps", C.c_int32),
+        ("reserved1", C.c_int32),
     ]
 
 

@@ -46,6 +46,7 @@ class PcaResult:
     total_var: float = 0.0
     total_var_recomputed: bool = False
     shifted_cholesky: int = 0
+    eig_sweeps: int = 0
     resident_csr: bool = True
     k: int = 0
     extra: dict = field(default_factory=dict)
@@ -186,7 +187,8 @@ def _finish(res, bufs, n_obs, n_vars, nc, zero_center, scale, k):
         singular_values=sv, mean=mean if zero_center or scale else None,
         std=std if scale else None, n_components=nc, n_obs=n_obs, n_vars=n_vars,
         total_var=float(res.total_var), total_var_recomputed=bool(res.total_var_recomputed),
-        shifted_cholesky=int(res.shifted_cholesky), resident_csr=bool(res.resident_csr), k=k)
+        shifted_cholesky=int(res.shifted_cholesky), resident_csr=bool(res.resident_csr), k=k,
+        eig_sweeps=int(res.eig_sweeps))
 
 
 # ---------------------------------------------------------------------------

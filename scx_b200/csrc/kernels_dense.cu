@@ -88,78 +88,141 @@ cudaError_t launch_gram_f64(const double* A, int64_t n, int ld, double* part, in
 }
 
 // ---------------------------------------------------------------------------
-// Cholesky of the leading k x k block of G (ld x ld), right-looking, one
-// block.  A pivot j fails when its Schur complement d_j <= tau * G_jj (the
-// column is numerically dependent on the previous ones) or is not finite.
-// With shift_on_fail the factorisation restarts once on G + s I,
-// s = 10 tau max_j G_jj, which always succeeds on finite input.
+// Cholesky of the leading k x k block of G (ld x ld) and the inverse of its
+// factor, one block of 1024 threads.  A pivot j fails when its Schur
+// complement d_j <= tau * G_jj (the column is numerically dependent on the
+// previous ones) or is not finite.  With shift_on_fail the factorisation
+// restarts once on G + s I, s = 10 tau max_j G_jj, which always succeeds on
+// finite input.
+//
+// Symmetric Gaussian elimination of the augmented matrix [A | I]: step j
+// subtracts (A_ja / d_j) times row j from every row a > j, which turns A's
+// upper triangle into D L^T and the identity into X = L^{-1} (unit lower
+// triangular), where A = L D L^T.  Then R = D^{1/2} L^T and
+// R^{-1} = X^T D^{-1/2}: R_jc = A_jc / sqrt(d_j), R^{-1}_ca = X_ac / sqrt(d_a).
+// Every matrix entry lives in a register of its owner, thread (ty, tx) owning
+// rows ty + 32u and columns tx + 32v; one register holds A_ac above the
+// diagonal (c >= a) or X_ac below it.  Per step the owners of row j + 1
+// publish it (double-buffered rows in shared memory) and the owner of the
+// next diagonal entry computes the next pivot's reciprocals, so a step is
+// one barrier plus a short dependent chain.
 // ---------------------------------------------------------------------------
-// Layout: A (the working copy of G) is k x S row-major in shared memory with
-// an odd stride S, so a warp reading one column (32 rows) touches 32 distinct
-// banks.  The elimination only touches the upper triangle, so R is stored
-// transposed in the strict lower triangle (A[c][j] = R_jc, c > j) with its
-// diagonal in rd[].  One barrier per elimination step: warp ty updates rows
-// a = j+1+ty+32u of the trailing block, lanes striding over the columns
-// c >= a, from the unscaled row j (A_ac -= A_ja A_jc / d_j), and the scaled
-// row j of R goes to column j below the diagonal.  R^{-1} is then formed one column per
-// warp by column-oriented back substitution: lane i keeps the running
-// right-hand side of rows i, i+32, ...; step l takes x_l from its owner lane
-// by a shuffle and updates the rows above it, so a step costs one shuffle.
+template <int U>
 __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G, int k, int ld, double tau,
                                                    int shift_on_fail, double* __restrict__ R,
                                                    double* __restrict__ Rinv, float* __restrict__ Rinv_f,
                                                    int* __restrict__ status) {
-  extern __shared__ double sm[];
-  const int S = k | 1;
-  double* A = sm;           // [k][S]
-  double* dg = A + k * S;   // [k] diagonal of G
-  double* rd = dg + k;      // [k] R_jj
-  double* dinv = rd + k;    // [k] 1 / R_jj
+  __shared__ double rowA[2][kMaxK], rowX[2][kMaxK];
+  __shared__ double pv_rinv[kMaxK], pv_di[kMaxK], dg[kMaxK];
+  __shared__ int pv_ok[kMaxK];
   __shared__ double maxdiag_s;
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-  const int tx = lane, ty = warp;
-  for (int j = tid; j < k; j += nt) dg[j] = G[(int64_t)j * ld + j];
+  __shared__ int fail_s;
+  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  for (int j = tid; j < k; j += 1024) dg[j] = G[(int64_t)j * ld + j];
+  for (int t = tid; t < ld * ld; t += 1024) {
+    R[t] = 0.0;
+    Rinv[t] = 0.0;
+    Rinv_f[t] = 0.f;
+  }
   __syncthreads();
-  if (warp == 0) {
+  if (ty == 0) {
     double m = 0.0;
-    for (int j = lane; j < k; j += 32) m = fmax(m, dg[j]);
+    for (int j = tx; j < k; j += 32) m = fmax(m, dg[j]);
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) maxdiag_s = m;
+    if (tx == 0) maxdiag_s = m;
   }
   double shift = 0.0;
   int fail = -1;
+  double val[U][U];
   for (int attempt = 0; attempt < 2; ++attempt) {
-    for (int t = tid; t < k * S; t += nt) {
-      const int r = t / S, c = t - r * S;
-      A[t] = c < k ? G[(int64_t)r * ld + c] + (r == c ? shift : 0.0) : 0.0;
+    // Pivot j from its updated diagonal entry d (called by the entry's owner).
+    auto pivot = [&](int j, double d) {
+      const bool ok = isfinite(d) && d > 0.0 && (attempt == 1 || d > tau * (dg[j] + shift));
+      pv_ok[j] = ok ? 1 : 0;
+      if (ok) {
+        const double rinv = rsqrt(d);
+        pv_rinv[j] = rinv;
+        pv_di[j] = rinv * rinv;
+      }
+    };
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int v = 0; v < U; ++v) {
+        const int a = ty + 32 * u, c = tx + 32 * v;
+        double x = 0.0;
+        if (a < k && c < k) {
+          if (c >= a) x = G[(int64_t)a * ld + c] + (a == c ? shift : 0.0);
+        }
+        val[u][v] = x;  // X starts as the identity; its unit diagonal is implicit
+      }
+    if (ty == 0) {
+#pragma unroll
+      for (int v = 0; v < U; ++v) {
+        const int c = tx + 32 * v;
+        if (c < k) {
+          rowA[0][c] = val[0][v];
+          rowX[0][c] = c == 0 ? 1.0 : 0.0;
+        }
+      }
+    }
+    if (tid == 0) {
+      fail_s = -1;
+      pivot(0, val[0][0]);
     }
     __syncthreads();
-    fail = -1;
     for (int j = 0; j < k; ++j) {
-      const double d = A[j * S + j];
-      const double d0 = dg[j] + shift;
-      if (!(isfinite(d) && d > 0.0 && (attempt == 1 || d > tau * d0))) {
-        fail = j;  // every thread sees the same pivot: uniform exit
+      if (!pv_ok[j]) {  // every thread reads the same flag: uniform exit
+        if (tid == 0) fail_s = j;
         break;
       }
-      const double rinv = rsqrt(d), di = 1.0 / d;
-      if (tid == 0) {
-        rd[j] = d * rinv;
-        dinv[j] = 1.0 / (d * rinv);
-      }
-      for (int c = j + 1 + tid; c < k; c += nt) A[c * S + j] = A[j * S + c] * rinv;
-      for (int a = j + 1 + ty; a < k; a += nw) {
-        const double f = A[j * S + a] * di;
-        for (int c = a + tx; c < k; c += 32) A[a * S + c] -= f * A[j * S + c];
+      const int b = j & 1;
+      const double di = pv_di[j], rj = pv_rinv[j];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int a = ty + 32 * u;
+        if (a == j) {  // row j is final: R_jc = A_jc / sqrt(d_j)
+#pragma unroll
+          for (int v = 0; v < U; ++v) {
+            const int c = tx + 32 * v;
+            if (c >= j && c < k) R[(int64_t)j * ld + c] = val[u][v] * rj;
+          }
+        }
+        if (a > j && a < k) {
+          const double m = rowA[b][a] * di;
+#pragma unroll
+          for (int v = 0; v < U; ++v) {
+            const int c = tx + 32 * v;
+            if (c < k) {
+              if (c >= a) val[u][v] -= m * rowA[b][c];
+              else if (c <= j) val[u][v] -= m * rowX[b][c];
+            }
+          }
+          if (a == j + 1) {  // publish row j + 1 for the next step
+#pragma unroll
+            for (int v = 0; v < U; ++v) {
+              const int c = tx + 32 * v;
+              if (c < k) {
+                if (c >= a) rowA[b ^ 1][c] = val[u][v];
+                if (c < a) rowX[b ^ 1][c] = val[u][v];
+                if (c == a) {
+                  rowX[b ^ 1][c] = 1.0;
+                  pivot(a, val[u][v]);
+                }
+              }
+            }
+          }
+        }
       }
       __syncthreads();
     }
-    if (fail < 0) break;
     __syncthreads();
+    fail = fail_s;
+    if (fail < 0) break;
     if (!shift_on_fail || attempt == 1) {
       if (tid == 0) status[0] = -(fail + 1);
       // Leave well-defined (identity) factors so downstream kernels stay finite.
-      for (int t = tid; t < ld * ld; t += nt) {
+      for (int t = tid; t < ld * ld; t += 1024) {
         const int r = t / ld, c = t % ld;
         const double v = (r == c && r < k) ? 1.0 : 0.0;
         R[t] = v;
@@ -170,76 +233,47 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
     }
     if (tid == 0) status[0] += 1;
     shift = 10.0 * tau * fmax(maxdiag_s, 1e-300);
+    __syncthreads();
   }
-  // R to global (zero outside the leading upper triangle).
-  for (int t = tid; t < ld * ld; t += nt) {
-    const int r = t / ld, c = t % ld;
-    R[t] = (r < k && c < k && c >= r) ? (c == r ? rd[r] : A[c * S + r]) : 0.0;
-  }
-  // R^{-1}, column c per warp: solve R x = e_c from the bottom.
-  constexpr int U = kMaxK / 32;
-  for (int c = warp; c < k; c += nw) {
-    double acc[U], x[U];
+  // R^{-1}_ca = X_ac / sqrt(d_a), c <= a.
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      acc[u] = (lane + 32 * u == c) ? 1.0 : 0.0;
-      x[u] = 0.0;
-    }
-    for (int l = c; l >= 0; --l) {
-      const int ul = l >> 5;
-      double v = acc[0];
+  for (int u = 0; u < U; ++u)
 #pragma unroll
-      for (int u = 1; u < U; ++u)
-        if (ul == u) v = acc[u];
-      const double xl = __shfl_sync(0xffffffffu, v, l & 31) * dinv[l];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int i = lane + 32 * u;
-        if (ul == u && lane == (l & 31)) x[u] = xl;
-        if (i < l) acc[u] -= A[l * S + i] * xl;
+    for (int v = 0; v < U; ++v) {
+      const int a = ty + 32 * u, c = tx + 32 * v;
+      if (a < k && c <= a) {
+        const double x = (c == a ? 1.0 : val[u][v]) * pv_rinv[a];
+        Rinv[(int64_t)c * ld + a] = x;
+        Rinv_f[(int64_t)c * ld + a] = (float)x;
       }
     }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int i = lane + 32 * u;
-      if (i < ld) {
-        const double v = (i <= c) ? x[u] : 0.0;
-        Rinv[(int64_t)i * ld + c] = v;
-        Rinv_f[(int64_t)i * ld + c] = (float)v;
-      }
-    }
-  }
-  // columns k..ld-1 of R^{-1} are zero
-  for (int t = tid; t < ld * (ld - k); t += nt) {
-    const int r = t / (ld - k), c = k + t % (ld - k);
-    Rinv[(int64_t)r * ld + c] = 0.0;
-    Rinv_f[(int64_t)r * ld + c] = 0.f;
-  }
 }
 
 cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shift_on_fail,
                             double* R, double* Rinv, float* Rinv_f, int* status, cudaStream_t st) {
-  const int S = k | 1;
-  size_t smem = (size_t)(k * S + 3 * k) * sizeof(double);
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_cholesky, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (k > kMaxK) return cudaErrorInvalidValue;
   note_launches(1);
-  k_cholesky<<<1, 1024, smem, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
+  if (k <= 64)
+    k_cholesky<2><<<1, 1024, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
+  else
+    k_cholesky<4><<<1, 1024, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-// Tall x small: Out[i, :cnt] = In[i, :K] * M (K x cnt), 64-row tiles.
-// M (zero-padded to OUTB columns) and the tile sit in shared memory; thread
-// (ty, tx) of the 16 x 16 grid computes rows 4 ty .. 4 ty + 3 at columns
-// 4 tx + 64 h + (0..3): per four k-steps it reads four float4 of its rows
-// (two distinct addresses per warp: broadcast) and 4 OUTB/64 float4 of M for
-// 16 OUTB/64 FMAs each.  A block stages its rows before writing any of them,
-// so Out may alias In.  Optionally writes the hi/lo 16-bit planes of Out
-// (hi = round16(x), lo = round16(x - hi); fmt 1 = bf16, 0 = f16) in the same
-// pass.
+// Tall x small: Out[i, :cnt] = In[i, :K] * M (K x cnt), 128-row tiles.
+// M (zero-padded to OUTB columns) sits in shared memory; row tiles are
+// double-buffered in shared memory by cp.async (16-byte copies, rows padded
+// by 4 floats), so the next tile streams in while this one is multiplied.
+// Thread (ty, tx) of the 16 x 16 grid computes rows ty + 16 i (i < 8) at
+// columns 64 h + 4 tx + (0..3): per four k-steps it reads eight float4 of
+// its rows (two distinct addresses per warp: broadcast) and 4 OUTB/64
+// float4 of M, for 128 OUTB/64 FMAs.  A block loads a tile before it writes
+// any of its rows, and only ever writes its own tiles, so Out may alias In.
+// Optionally writes the hi/lo 16-bit planes of Out (hi = round16(x),
+// lo = round16(x - hi); fmt 1 = bf16, 0 = f16) in the same pass.
 // ---------------------------------------------------------------------------
-constexpr int kTallRows = 64;
+constexpr int kTallRows = 128;
 
 __device__ __forceinline__ void split16(float x, int fmt, uint16_t& h, uint16_t& l) {
   if (fmt) {
@@ -253,16 +287,27 @@ __device__ __forceinline__ void split16(float x, int fmt, uint16_t& h, uint16_t&
   }
 }
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 template <int OUTB>
-__global__ void __launch_bounds__(256) k_tall_mm(const float* In, int64_t n, int K, int ldi,
-                                                 const float* __restrict__ M, int ldm, int cnt, float* Out,
-                                                 int ldo, uint16_t* __restrict__ hi, uint16_t* __restrict__ lo,
-                                                 int fmt) {
+__global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, int K, int ldi,
+                                                    const float* __restrict__ M, int ldm, int cnt, float* Out,
+                                                    int ldo, uint16_t* __restrict__ hi,
+                                                    uint16_t* __restrict__ lo, int fmt) {
   constexpr int H = OUTB / 64;
+  constexpr int RPT = kTallRows / 16;  // rows per thread
   extern __shared__ __align__(16) float sm_f[];
   const int KP = K + 4;
-  float* Ms = sm_f;             // [K][OUTB]
-  float* Ts = sm_f + K * OUTB;  // [kTallRows][KP]
+  float* Ms = sm_f;  // [K][OUTB]
+  float* T0 = sm_f + K * OUTB;
+  float* T1 = T0 + kTallRows * KP;
   for (int t = threadIdx.x; t < K * OUTB; t += blockDim.x) {
     const int l = t / OUTB, o = t % OUTB;
     Ms[t] = o < cnt ? M[l * ldm + o] : 0.f;
@@ -271,32 +316,43 @@ __global__ void __launch_bounds__(256) k_tall_mm(const float* In, int64_t n, int
   const int k4 = K >> 2;
   const bool vec_out = ((cnt & 3) == 0) && ((ldo & 3) == 0);
   const int64_t n_tiles = (n + kTallRows - 1) / kTallRows;
-  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+
+  auto issue = [&](int64_t tile, float* T) {
     const int64_t r0 = tile * kTallRows;
-    __syncthreads();  // the previous tile is consumed (and M is staged)
     for (int t = threadIdx.x; t < kTallRows * k4; t += blockDim.x) {
       const int r = t / k4, c4 = t - r * k4;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (r0 + r < n) v = reinterpret_cast<const float4*>(In + (r0 + r) * ldi)[c4];
-      *reinterpret_cast<float4*>(Ts + r * KP + 4 * c4) = v;
+      float* dst = T + r * KP + 4 * c4;
+      if (r0 + r < n) cp_async16(dst, In + (r0 + r) * ldi + 4 * c4);
+      else *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
     }
+  };
+
+  int64_t tile = blockIdx.x;
+  if (tile < n_tiles) issue(tile, T0);
+  cp_async_commit();
+  for (int it = 0; tile < n_tiles; tile += gridDim.x, ++it) {
+    float* T = (it & 1) ? T1 : T0;
+    const int64_t next = tile + gridDim.x;
+    if (next < n_tiles) issue(next, (it & 1) ? T0 : T1);
+    cp_async_commit();
+    cp_async_wait1();  // this tile's copies are done (the next tile's may still run)
     __syncthreads();
-    float acc[4][4 * H];
+    float acc[RPT][4 * H];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < RPT; ++i)
 #pragma unroll
       for (int o = 0; o < 4 * H; ++o) acc[i][o] = 0.f;
     for (int l = 0; l < K; l += 4) {
-      float4 a[4];
+      float4 a[RPT];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = *reinterpret_cast<const float4*>(Ts + (4 * ty + i) * KP + l);
+      for (int i = 0; i < RPT; ++i) a[i] = *reinterpret_cast<const float4*>(T + (ty + 16 * i) * KP + l);
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
 #pragma unroll
         for (int h = 0; h < H; ++h) {
           const float4 m = *reinterpret_cast<const float4*>(Ms + (l + u) * OUTB + 64 * h + 4 * tx);
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
+          for (int i = 0; i < RPT; ++i) {
             const float x = u == 0 ? a[i].x : u == 1 ? a[i].y : u == 2 ? a[i].z : a[i].w;
             acc[i][4 * h + 0] = fmaf(x, m.x, acc[i][4 * h + 0]);
             acc[i][4 * h + 1] = fmaf(x, m.y, acc[i][4 * h + 1]);
@@ -306,9 +362,10 @@ __global__ void __launch_bounds__(256) k_tall_mm(const float* In, int64_t n, int
         }
       }
     }
+    const int64_t r0 = tile * kTallRows;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int64_t row = r0 + 4 * ty + i;
+    for (int i = 0; i < RPT; ++i) {
+      const int64_t row = r0 + ty + 16 * i;
       if (row >= n) continue;
 #pragma unroll
       for (int h = 0; h < H; ++h) {
@@ -337,7 +394,9 @@ __global__ void __launch_bounds__(256) k_tall_mm(const float* In, int64_t n, int
         }
       }
     }
+    __syncthreads();  // every thread is done with T before it is refilled
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 static cudaError_t tall_mm(const float* In, int64_t n, int K, int ldi, const float* M, int ldm, int cnt,
@@ -346,8 +405,8 @@ static cudaError_t tall_mm(const float* In, int64_t n, int K, int ldi, const flo
   if (n == 0) return cudaSuccess;
   if ((K & 3) || (ldi & 3)) return cudaErrorInvalidValue;
   const int outb = cnt <= 64 ? 64 : 128;
-  const size_t smem = ((size_t)K * outb + (size_t)kTallRows * (K + 4)) * sizeof(float);
-  const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024) / smem));
+  const size_t smem = ((size_t)K * outb + 2 * (size_t)kTallRows * (K + 4)) * sizeof(float);
+  const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(2, (220 * 1024) / smem));
   const int grid = grid_for(n, kTallRows, num_sms, per_sm);
   note_launches(1);
   if (outb == 64) {
@@ -453,14 +512,18 @@ cudaError_t launch_round_v(const double* A, int64_t g, int ld, const double* mu,
 
 // ---------------------------------------------------------------------------
 // Parallel cyclic Jacobi (round-robin pairing) for the symmetric k x k block
-// of C, one warp per rotation pair.  A round computes the kk/2 angles of
-// disjoint pairs from the round's starting A, rotates columns p, q of A and E
-// (phase 1, each warp its own two columns: no other warp touches them), then
-// rows p, q of A (phase 2): two barriers per round.  Matrices are row-major in
-// shared memory with an odd stride so column walks are free of bank
-// conflicts; E moves to global scratch when both do not fit.  Stops after a
-// sweep with no rotation (every off-diagonal entry below 1e-15 of the
-// geometric mean of its two diagonal entries) or after 40 sweeps.
+// of C.  A round rotates kk/2 disjoint pairs in three barrier-separated
+// phases: (0) one lane per pair computes the angle from the round's starting
+// A (the pairing of every round is tabulated once); (1) one warp per pair
+// rotates columns p, q of A and E (no other pair touches them); (2) one warp
+// per pair rotates rows p, q of A and sets the rotated 2 x 2 block to its
+// exact diagonal form (rounding would otherwise leave residues of order
+// eps * max(app, aqq) that keep the criterion below, relative to
+// sqrt(app aqq), from ever being met).  Matrices are row-major in shared
+// memory with an odd stride so column walks are free of bank conflicts; E
+// moves to global scratch when both do not fit.  Stops after a sweep with no
+// rotation (every off-diagonal entry below 1e-15 of the geometric mean of its
+// two diagonal entries) or after 40 sweeps.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, int k, int ld,
                                                  double* __restrict__ evals, double* __restrict__ evecs,
@@ -468,9 +531,11 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, i
   extern __shared__ double sm[];
   const int kk = (k + 1) & ~1;  // even number of players; index k (if odd) is a dummy
   const int S = kk + 1;
+  const int npair = kk / 2, m = kk - 1;
   double* A = sm;  // [kk][S]
-  double* E = (Eglob != nullptr) ? Eglob : sm + kk * S;
-  __shared__ double cs[kMaxK / 2], sn[kMaxK / 2];
+  uint16_t* sched = reinterpret_cast<uint16_t*>(sm + kk * S);  // [m][npair]: p | q << 8
+  double* E = (Eglob != nullptr) ? Eglob : sm + kk * S + (m * npair + 3) / 4;
+  __shared__ double cs[kMaxK / 2], sn[kMaxK / 2], dpp[kMaxK / 2], dqq[kMaxK / 2];
   __shared__ int done;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   for (int t = tid; t < kk * S; t += nt) {
@@ -478,57 +543,74 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, i
     A[t] = (r < k && c < k) ? C[r * ld + c] : 0.0;
     E[t] = (r == c) ? 1.0 : 0.0;
   }
+  for (int t = tid; t < m * npair; t += nt) {
+    const int round = t / npair, i = t - round * npair;
+    int a, b;
+    if (i == 0) { a = round; b = m; }
+    else { a = (round + i) % m; b = (round - i + m) % m; }
+    sched[t] = (uint16_t)(min(a, b) | (max(a, b) << 8));
+  }
   if (tid == 0) done = 1;
   __syncthreads();
-  const int npair = kk / 2, m = kk - 1;
   int sweep = 0;
   for (; sweep < 40; ++sweep) {
     for (int round = 0; round < m; ++round) {
-      for (int i = warp; i < npair; i += nw) {
-        int a, b;
-        if (i == 0) { a = round; b = m; }
-        else { a = (round + i) % m; b = (round - i + m) % m; }
-        const int p = min(a, b), q = max(a, b);
-        double c = 1.0, s = 0.0;
+      const uint16_t* pr = sched + round * npair;
+      // phase 0: angles, one lane per pair
+      for (int i = tid; i < npair; i += nt) {
+        const int p = pr[i] & 0xff, q = pr[i] >> 8;
+        double c = 1.0, s = 0.0, npp = 0.0, nqq = 0.0;
         if (q < k) {
           const double apq = A[p * S + q], app = A[p * S + p], aqq = A[q * S + q];
           if (fabs(apq) > 1e-300 && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq))) {
             const double theta = (aqq - app) / (2.0 * apq);
             const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-            c = 1.0 / sqrt(t * t + 1.0);
+            c = rsqrt(t * t + 1.0);
             s = t * c;
+            npp = app - t * apq;  // the rotated 2 x 2 block is diag(npp, nqq)
+            nqq = aqq + t * apq;
+            done = 0;
           }
         }
-        if (lane == 0) {
-          cs[i] = c;
-          sn[i] = s;
-        }
-        if (s != 0.0) {  // warp-uniform
-          __syncwarp();  // the angle reads above precede every write below
-          for (int r = lane; r < kk; r += 32) {
-            const double xp = A[r * S + p], xq = A[r * S + q];
-            A[r * S + p] = c * xp - s * xq;
-            A[r * S + q] = s * xp + c * xq;
-            const double ep = E[r * S + p], eq = E[r * S + q];
-            E[r * S + p] = c * ep - s * eq;
-            E[r * S + q] = s * ep + c * eq;
-          }
-          if (lane == 0) done = 0;
-        }
+        cs[i] = c;
+        sn[i] = s;
+        dpp[i] = npp;
+        dqq[i] = nqq;
       }
       __syncthreads();
+      // phase 1: columns p, q of A and E
       for (int i = warp; i < npair; i += nw) {
         const double s = sn[i];
         if (s == 0.0) continue;
         const double c = cs[i];
-        int a, b;
-        if (i == 0) { a = round; b = m; }
-        else { a = (round + i) % m; b = (round - i + m) % m; }
-        const int p = min(a, b), q = max(a, b);
+        const int p = pr[i] & 0xff, q = pr[i] >> 8;
+        for (int r = lane; r < kk; r += 32) {
+          const double xp = A[r * S + p], xq = A[r * S + q];
+          A[r * S + p] = c * xp - s * xq;
+          A[r * S + q] = s * xp + c * xq;
+          const double ep = E[r * S + p], eq = E[r * S + q];
+          E[r * S + p] = c * ep - s * eq;
+          E[r * S + q] = s * ep + c * eq;
+        }
+      }
+      __syncthreads();
+      // phase 2: rows p, q of A, then the exact 2 x 2 block
+      for (int i = warp; i < npair; i += nw) {
+        const double s = sn[i];
+        if (s == 0.0) continue;
+        const double c = cs[i];
+        const int p = pr[i] & 0xff, q = pr[i] >> 8;
         for (int col = lane; col < kk; col += 32) {
           const double xp = A[p * S + col], xq = A[q * S + col];
           A[p * S + col] = c * xp - s * xq;
           A[q * S + col] = s * xp + c * xq;
+        }
+        __syncwarp();
+        if (lane == 0) {
+          A[p * S + p] = dpp[i];
+          A[q * S + q] = dqq[i];
+          A[p * S + q] = 0.0;
+          A[q * S + p] = 0.0;
         }
       }
       __syncthreads();
@@ -561,13 +643,14 @@ cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, dou
                               int* sweeps, cudaStream_t st) {
   const int kk = (k + 1) & ~1;
   const size_t one = (size_t)kk * (kk + 1) * sizeof(double);
+  const size_t sched = ((size_t)(kk - 1) * (kk / 2) + 3) / 4 * sizeof(double);
   // E lives in shared memory when both matrices fit, else in the scratch that
-  // follows evecs (the plan allocates 2 * ld * ld doubles there).
+  // follows evecs (the plan allocates ld * ld + ld * (ld + 1) doubles there).
   double* eglob = nullptr;
-  size_t smem = 2 * one;
+  size_t smem = 2 * one + sched;
   if (smem > 200 * 1024) {
     eglob = evecs + (size_t)ld * ld;
-    smem = one;
+    smem = one + sched;
   }
   cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int warps = std::min(32, std::max(1, kk / 2));

@@ -792,6 +792,7 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   out->resident_csr = 1;
   out->total_var_recomputed = pl->total_var_recomputed ? 1 : 0;
   out->shifted_cholesky = hstatus[0] > 0 ? hstatus[0] : 0;
+  out->eig_sweeps = hstatus[2];
   out->total_var = pl->total_var;
 }
 
