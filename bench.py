@@ -47,10 +47,12 @@ CLIP = 10.0
 METRIC = "1M x 2k-gene rPCA (50 PCs) ms per PCA, BF16-mixed (FP32 path alongside)"
 FALLBACK_HBM_GBS = 6650.0
 
-# DRAM bytes per stored nonzero for the dominant kernel, from the ncu capture
-# summarised in profiles/ (dram__bytes_read.sum + dram__bytes_write.sum of one
-# launch divided by that launch's nonzeros); None until captured.
-NCU_TRAFFIC_BYTES_PER_NNZ = {"transpose": None, "forward": None}
+# DRAM bytes per stored nonzero of the two product kernels, from one ncu
+# capture at 250,000 x 2,000 (profiles/spmm_tc_250k_full.txt:
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch / its 57,193,010
+# nonzeros).  Traffic grows in proportion to the nonzeros at fixed density, so
+# the figure scales to the bench workload.
+NCU_TRAFFIC_BYTES_PER_NNZ = {"transpose": 5.223, "forward": 5.657}
 
 
 def parse():
