@@ -227,6 +227,35 @@ int32_t scxpca_plan_get_profile(const scxpca_plan* plan, scxpca_profile* out);
 int32_t scxpca_plan_col_stats(scxpca_plan* plan, double* col_sums, double* col_sum_sq,
                               char* err, size_t err_len);
 
+/* Per-gene column statistics that allocate no device memory.  This entry point
+ * has no counterpart in the reference.  It is for callers that cannot let a
+ * library call cudaMalloc: processes whose device memory is owned by a caching
+ * pool (a PyTorch or RMM allocator that has reserved the device or enforces a
+ * budget), and pipelines where cudaMalloc/cudaFree would add device-wide
+ * synchronisation between their streams.
+ *
+ * `x` must be a device CSR (memory = DEVICE) on `device_ordinal`;
+ * `out_stats` is caller-allocated device memory of 2 * n_vars doubles,
+ * written as [sum x (n_vars) | sum x^2 (n_vars)] in FP64 (the same sums as
+ * scxpca_plan_col_stats on an unscaled plan of the same matrix).  The CSR is
+ * validated first (SCXPCA_INVALID_CSR as for plan creation; unsorted rows are
+ * accepted).  `stream` may be NULL (the legacy default stream); the call waits
+ * for it before returning.
+ *
+ * Scratch: one static device array of SCXPCA_NOALLOC_SCRATCH_BYTES (8 MiB)
+ * that every GPU which loads the library holds until the process exits, so
+ * n_vars is limited to SCXPCA_NOALLOC_MAX_VARS; larger matrices get
+ * SCXPCA_INVALID_ARGUMENT.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  All calls share the array and it keeps the last call's
+ * contents: two calls whose kernels overlapped on the GPU would race on it, so
+ * the library takes a process-wide lock around each call and synchronises the
+ * stream before releasing it. */
+#define SCXPCA_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define SCXPCA_NOALLOC_MAX_VARS 12800
+int32_t scxpca_col_stats_noalloc(int32_t device_ordinal, const scxpca_csr* x, double* out_stats,
+                                 void* stream, char* err, size_t err_len);
+
 /* Seeded N(0,1) test matrix, n_rows x n_cols column-major float32, into device
  * memory `out` on `device_ordinal`.  Replaces random_gaussian_gpu
  * (scx-gpu/src/curand.rs:76-157); the stream is Philox4x32-10 + Box-Muller,

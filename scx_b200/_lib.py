@@ -28,6 +28,10 @@ QR_HOUSEHOLDER, QR_CHOLESKY = 0, 1
 MATH_STRICT_FP32, MATH_MIXED_BF16, MATH_MIXED_F16 = 0, 1, 2
 SPMM_DEFAULT, SPMM_DETERMINISTIC = 0, 1
 
+# Static scratch of scxpca_col_stats_noalloc and the widest matrix it takes.
+NOALLOC_SCRATCH_BYTES = 8 << 20
+NOALLOC_MAX_VARS = 12800
+
 # Every symbol include/scxpca.h declares.
 EXPORTED = (
     "scxpca_status_string",
@@ -41,6 +45,7 @@ EXPORTED = (
     "scxpca_plan_rmatmat",
     "scxpca_plan_qr",
     "scxpca_plan_col_stats",
+    "scxpca_col_stats_noalloc",
     "scxpca_plan_set_profiling",
     "scxpca_plan_get_profile",
     "scxpca_gaussian",
@@ -146,6 +151,7 @@ def load() -> C.CDLL:
         "scxpca_plan_rmatmat": (C.c_int32, [P, P, C.c_int64, P, C.c_int64, *E]),
         "scxpca_plan_qr": (C.c_int32, [P, P, C.c_int64, C.c_int64, *E]),
         "scxpca_plan_col_stats": (C.c_int32, [P, P, P, *E]),
+        "scxpca_col_stats_noalloc": (C.c_int32, [C.c_int32, C.POINTER(Csr), P, P, *E]),
         "scxpca_plan_set_profiling": (C.c_int32, [P, C.c_int32]),
         "scxpca_plan_get_profile": (C.c_int32, [P, C.POINTER(Profile)]),
         "scxpca_gaussian": (C.c_int32, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, P, *E]),
