@@ -4,8 +4,8 @@
 // Sparse format ("tile-chunk packed"), built once per plan:
 //   rows are grouped in tiles of 128 cells, genes in chunks of 64; the stored
 //   entries of tile t and chunk c form one segment, ordered by row then gene,
-//   padded with zero words to a multiple of 4 entries (16 bytes) so that every
-//   segment can be fetched with bulk copies.  Each entry is one 32-bit word:
+//   padded with zero words to a multiple of 4 entries (16 bytes), so every
+//   segment starts on a 16-byte boundary.  Each entry is one 32-bit word:
 //       bits  0..15  value (bf16 or f16 bits)
 //       bits 16..29  byte offset of (row within the tile, gene within the
 //                    chunk) in the 128 x 64 swizzled tile (sw128_offset)
@@ -23,12 +23,17 @@
 // epilogue adds the two halves: about 16 mantissa bits on the dense operand,
 // the matrix values being the only operand rounded to 16 bits.
 //
-// Warp roles (23 warps): warps 0-15 densify in four groups of four that take
-// stages in turn (each warp zeroes its 32 rows, scatters its quarter from the
-// staging ring, fences, arrives); warps 16-19 drain TMEM (one lane quarter
-// each); warp 20 issues the MMAs from one thread; warp 21 loads the dense
-// operand by TMA; warp 22 bulk-copies segment metadata (per tile) and entry
-// pieces (up to kCap entries) into shared-memory rings, many segments ahead.
+// Warp roles (23 warps): warps 0-15 densify in four groups of four; group g
+// takes every fourth stage (its own A buffers: two in the forward kernel, one
+// in the transposed kernel, whose stages are twice as large).  Each densify warp reads its
+// quarter of a segment straight from global memory with 16-byte loads (the
+// tile's entries were prefetched into L2 a tile ahead), keeping the loads of
+// its group's next segment in flight in registers while the current one is
+// scattered, so many warps -- not one issuing thread -- keep the entry stream
+// moving.  Warps 16-19 drain TMEM (one lane quarter each); warp 20 issues the
+// MMAs from one thread; warp 21 loads the dense operand by TMA into its own
+// ring (forward) or per row tile (transposed); warp 22 copies segment
+// metadata per tile and prefetches the entries of the tile after into L2.
 // All waits are bounded (tc.cuh).
 #include <algorithm>
 
@@ -44,11 +49,10 @@ namespace {
 
 constexpr int TM = 128;          // cells per tile
 constexpr int CW = 64;           // genes per chunk
-constexpr int kCap = 1024;       // entries per staging slot (4 KB)
-constexpr int kMaxGroups = 4;    // densify groups of four warps
+constexpr int kGroups = 4;       // densify groups of four warps
 constexpr int kThreads = 736;    // 23 warps
 constexpr int kMaxChunks = 128;  // genes <= 8192
-constexpr int W_EPI = 4 * kMaxGroups, W_MMA = W_EPI + 4, W_DENSE = W_MMA + 1, W_SPARSE = W_MMA + 2;
+constexpr int W_EPI = 4 * kGroups, W_MMA = W_EPI + 4, W_DENSE = W_MMA + 1, W_META = W_MMA + 2;
 
 struct SegMeta {
   int64_t start;
@@ -56,23 +60,22 @@ struct SegMeta {
 };
 static_assert(sizeof(SegMeta) == 16, "segment metadata is one 16-byte record");
 
-// Pipeline shapes.  Densify group g takes the stages it with it % G == g, so
-// stage buffer it % S is only ever used by one group (S is a multiple of G)
-// and every group has a private staging ring: each waiter then runs at most
-// one barrier phase ahead of the phase it waits for, which is what a parity
-// wait can distinguish.
-__host__ __device__ constexpr int fwd_stages(int LD) { return LD == 64 ? 4 : 2; }
-__host__ __device__ constexpr int fwd_groups(int LD) { return LD == 64 ? 4 : 2; }
-__host__ __device__ constexpr int fwd_slots(int LD) { return LD == 64 ? 16 : 8; }  // all groups
-__host__ __device__ constexpr int rmat_stages(int LD) { return LD == 64 ? 3 : 2; }
-__host__ __device__ constexpr int rmat_groups(int LD) { return LD == 64 ? 3 : 2; }
-__host__ __device__ constexpr int rmat_slots(int LD) { return LD == 64 ? 9 : 4; }
-static_assert(fwd_stages(64) % fwd_groups(64) == 0 && fwd_stages(128) % fwd_groups(128) == 0, "");
-static_assert(rmat_stages(64) % rmat_groups(64) == 0 && rmat_stages(128) % rmat_groups(128) == 0, "");
-static_assert(fwd_slots(64) % fwd_groups(64) == 0 && rmat_slots(64) % rmat_groups(64) == 0, "");
+// Pipeline shapes.  Densify group g takes the stages it with it % G == g.  In
+// the forward kernel it owns A stage buffers g and g + G (S == 2 G), so it
+// densifies its next segment while the MMAs read the previous one; in the
+// transposed kernel it owns buffer g (S == G).  Either way each waiter runs at
+// most one barrier phase ahead of the phase it waits for, which is what a
+// parity wait can distinguish.  The forward kernel's dense operand has its
+// own ring of fwd_bslots(LD) chunk buffers, filled ahead of the MMAs.
+__host__ __device__ constexpr int fwd_stages(int LD) { return 2 * kGroups; }
+__host__ __device__ constexpr int fwd_bslots(int LD) { return LD == 64 ? 4 : 2; }
+__host__ __device__ constexpr int rmat_stages(int LD) { return LD == 64 ? 4 : 2; }
+// 16-byte entry words a densify lane keeps in flight per segment quarter
+// (x 128 entries per warp); a larger quarter loads the rest on demand.
+constexpr int kFwdRegs = 4;
+constexpr int kRmatRegs = 3;
 
 __host__ __device__ __forceinline__ int padded4(int x) { return (x + 3) & ~3; }
-__host__ __device__ __forceinline__ int n_pieces(int real) { return (padded4(real) + kCap - 1) / kCap; }
 
 // ---------------------------------------------------------------------------
 // format build
@@ -144,6 +147,7 @@ __global__ void k_tile_fill(const int64_t* __restrict__ indptr, const int32_t* _
   }
 }
 
+
 // ---------------------------------------------------------------------------
 // shared pieces of the two product kernels
 // ---------------------------------------------------------------------------
@@ -151,16 +155,19 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
   return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
 }
 
-__device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
-  uint32_t v;
-  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
-  return v;
-}
 __device__ __forceinline__ void sts_u16(uint32_t addr, uint32_t v) {
   asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"((unsigned short)v) : "memory");
 }
 __device__ __forceinline__ void sts_zero16(uint32_t addr) {
   asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(addr), "r"(0u) : "memory");
+}
+// 16 bytes of entries, read-only path (the packed matrix never changes during a launch).
+__device__ __forceinline__ uint4 ldg_entries(const uint32_t* p) {
+  uint4 v;
+  asm volatile("ld.global.nc.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
 }
 
 // Two floats as a pair of 16-bit values (fmt 1 = bf16, 0 = f16), low word first.
@@ -189,66 +196,55 @@ __device__ __forceinline__ void zero_rows(uint32_t tile, int quarter, int lane) 
 
 __device__ __forceinline__ void scatter_one(uint32_t tile, uint32_t w) { sts_u16(tile + (w >> 16), w & 0xFFFFu); }
 
-// Private staging ring of one densify group, filled by the sparse loader.
-struct Ring {
-  uint32_t base;    // shared address of slot 0
-  uint32_t* ptr;    // the same, as a generic pointer (bulk-copy destination)
-  uint64_t* full;   // [nslot], 1 arrival + tx bytes
-  uint64_t* empty;  // [nslot], one arrival per densify warp of the group
-  int nslot;
+// Entries [lo, hi) of quarter q of segment m (indices into the entry array).
+struct Span {
+  int64_t lo, hi;
 };
-
-__device__ __forceinline__ Ring group_ring(uint32_t* ring_ptr, uint64_t* sfull, uint64_t* sempty, int g,
-                                           int nsg) {
-  uint32_t* p = ring_ptr + (size_t)g * nsg * kCap;
-  return Ring{smem_u32(p), p, sfull + g * nsg, sempty + g * nsg, nsg};
+__device__ __forceinline__ Span quarter_span(const SegMeta& m, int q) {
+  return Span{m.start + (q ? (int64_t)m.q[q - 1] : 0), m.start + (int64_t)m.q[q]};
 }
 
-// Densify warp (quarter q): scatter the quarter's entries of one segment into
-// `tile` (already zeroed), consuming the segment's pieces from the ring.
-__device__ __forceinline__ bool densify_segment(uint32_t tile, const SegMeta& m, const Ring& ring,
-                                                uint32_t& pc, int q, int lane, volatile int* abort_flag,
-                                                int* err, int code) {
-  const int plen = padded4(m.q[3]);
-  const int lo = q ? (int)m.q[q - 1] : 0;
-  const int hi = (int)m.q[q];
-  for (int p0 = 0; p0 < plen; p0 += kCap, ++pc) {
-    const int slot = (int)(pc % (uint32_t)ring.nslot);
-    if (!warp_wait(&ring.full[slot], (pc / ring.nslot) & 1u, abort_flag, err, code)) return false;
-    const uint32_t b = ring.base + (uint32_t)slot * (kCap * 4u) - (uint32_t)p0 * 4u;
-    const int e = min(hi, p0 + kCap);
-    int p = max(lo, p0) + lane;
-    for (; p + 96 < e; p += 128) {
-      const uint32_t w0 = lds_u32(b + 4u * p), w1 = lds_u32(b + 4u * (p + 32));
-      const uint32_t w2 = lds_u32(b + 4u * (p + 64)), w3 = lds_u32(b + 4u * (p + 96));
-      scatter_one(tile, w0);
-      scatter_one(tile, w1);
-      scatter_one(tile, w2);
-      scatter_one(tile, w3);
-    }
-    for (; p < e; p += 32) scatter_one(tile, lds_u32(b + 4u * p));
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&ring.empty[slot]);
+// Issue the first R 16-byte loads of a span (its start rounded down to a
+// 16-byte boundary; segments start on one and are padded to one, so a load
+// never leaves its segment).  Lane L holds words 4 (L + 32 r) .. + 3.
+template <int R>
+__device__ __forceinline__ void span_load(const uint32_t* __restrict__ ent, Span sp, int lane, uint4 (&w)[R]) {
+  const int64_t a0 = sp.lo & ~int64_t(3);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t e = a0 + 4 * (lane + 32 * r);
+    w[r] = e < sp.hi ? ldg_entries(ent + e) : make_uint4(0u, 0u, 0u, 0u);
   }
-  return true;
 }
 
-// Sparse loader: bulk-copy one segment into the ring, piece by piece.
-__device__ __forceinline__ bool load_segment(const uint32_t* __restrict__ ent, const SegMeta& m,
-                                             const Ring& ring, uint32_t& pc, volatile int* abort_flag, int* err,
-                                             int code) {
-  const int plen = padded4(m.q[3]);
-  for (int p0 = 0; p0 < plen; p0 += kCap, ++pc) {
-    const int slot = (int)(pc % (uint32_t)ring.nslot);
-    if (!mbar_wait(&ring.empty[slot], ((pc / ring.nslot) & 1u) ^ 1u, abort_flag, err, code)) return false;
-    const uint32_t bytes = (uint32_t)min(kCap, plen - p0) * 4u;
-    mbar_arrive_expect_tx(&ring.full[slot], bytes);
-    bulk_load(ring.ptr + (size_t)slot * kCap, ent + m.start + p0, bytes, &ring.full[slot]);
-  }
-  return true;
+__device__ __forceinline__ void scatter4(uint32_t tile, const uint4& w, int64_t e, Span sp) {
+  if (e >= sp.lo && e < sp.hi) scatter_one(tile, w.x);
+  if (e + 1 >= sp.lo && e + 1 < sp.hi) scatter_one(tile, w.y);
+  if (e + 2 >= sp.lo && e + 2 < sp.hi) scatter_one(tile, w.z);
+  if (e + 3 >= sp.lo && e + 3 < sp.hi) scatter_one(tile, w.w);
 }
 
-// Sparse loader: metadata of tile t (nc records) into meta ring slot mi & 1.
+// Scatter a span into `tile` (already zeroed): the R words in flight first,
+// then whatever lies beyond them, loaded here.
+template <int R>
+__device__ __forceinline__ void span_scatter(uint32_t tile, const uint32_t* __restrict__ ent, Span sp, int lane,
+                                             const uint4 (&w)[R]) {
+  const int64_t a0 = sp.lo & ~int64_t(3);
+#pragma unroll
+  for (int r = 0; r < R; ++r) scatter4(tile, w[r], a0 + 4 * (lane + 32 * r), sp);
+  for (int64_t e = a0 + 4 * (lane + 32 * R); e < sp.hi; e += 128) scatter4(tile, ldg_entries(ent + e), e, sp);
+}
+
+// Meta loader: L2 prefetch of the entries of segments [c0, c1) of one tile
+// (metadata `mt`), so the densify warps' loads a tile later find them in L2.
+__device__ __forceinline__ void prefetch_segments(const uint32_t* __restrict__ ent, const SegMeta* mt, int c0,
+                                                  int c1) {
+  const int64_t b = mt[c0].start;
+  const int64_t e = mt[c1 - 1].start + padded4(mt[c1 - 1].q[3]);
+  for (int64_t p = b; p < e; p += 8192) bulk_prefetch_l2(ent + p, (uint32_t)(min((int64_t)8192, e - p) * 4));
+}
+
+// Meta loader: metadata of tile t (nc records) into meta ring slot mi & 1.
 __device__ __forceinline__ bool load_meta(const SegMeta* __restrict__ meta, int64_t t, int nc,
                                           SegMeta* mring, uint64_t* mfull, uint64_t* mempty, uint32_t mi,
                                           volatile int* abort_flag, int* err, int code) {
@@ -270,27 +266,26 @@ __global__ void __launch_bounds__(kThreads, 1)
              const float* __restrict__ mc, float* __restrict__ Y, uint16_t* __restrict__ Yhi,
              uint16_t* __restrict__ Ylo, int fmt, int* err) {
   constexpr int N2 = 2 * LD;                // [hi | lo] columns
-  constexpr int S = fwd_stages(LD);
-  constexpr int G = fwd_groups(LD);
-  constexpr int NSLOT = fwd_slots(LD);
-  constexpr int NSG = NSLOT / G;            // staging slots per group
+  constexpr int S = fwd_stages(LD);         // A stages, two per densify group
+  constexpr int G = kGroups;
+  constexpr int NB = fwd_bslots(LD);        // dense-operand ring
   constexpr int A_BYTES = TM * CW * 2;      // 16 KB
   constexpr int B_PLANE = CW * LD * 2;      // 64 genes x LD, one 16-bit plane
   constexpr int B_BYTES = 2 * B_PLANE;
+  static_assert(S == 2 * G, "two A stages per densify group");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = align1024(smem_raw);
   uint8_t* As = smem;
   uint8_t* Bs = As + S * A_BYTES;
-  uint32_t* ring_ptr = reinterpret_cast<uint32_t*>(Bs + S * B_BYTES);
-  SegMeta* mring = reinterpret_cast<SegMeta*>(ring_ptr + NSLOT * kCap);  // [2][kMaxChunks]
+  SegMeta* mring = reinterpret_cast<SegMeta*>(Bs + NB * B_BYTES);  // [2][kMaxChunks]
   uint64_t* bars = reinterpret_cast<uint64_t*>(mring + 2 * kMaxChunks);
-  uint64_t* full = bars;
-  uint64_t* empty = full + S;
-  uint64_t* acc_full = empty + S;
+  uint64_t* full = bars;            // [S]  A stage densified (4 warp arrivals)
+  uint64_t* empty = full + S;       // [S]  A stage consumed (MMA commit)
+  uint64_t* bfull = empty + S;      // [NB] dense chunk landed (TMA)
+  uint64_t* bempty = bfull + NB;    // [NB] dense chunk consumed (MMA commit)
+  uint64_t* acc_full = bempty + NB;
   uint64_t* acc_empty = acc_full + 2;
-  uint64_t* sfull = acc_empty + 2;
-  uint64_t* sempty = sfull + NSLOT;
-  uint64_t* mfull = sempty + NSLOT;
+  uint64_t* mfull = acc_empty + 2;
   uint64_t* mempty = mfull + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mempty + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
@@ -298,18 +293,18 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
-      mbar_init(&full[s], 129);
+      mbar_init(&full[s], 4);  // one arrival per warp of the stage's densify group
       mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < NB; ++b) {
+      mbar_init(&bfull[b], 1);
+      mbar_init(&bempty[b], 1);
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&acc_full[a], 1);
-      mbar_init(&acc_empty[a], 128);
+      mbar_init(&acc_empty[a], 4);  // one arrival per epilogue warp
       mbar_init(&mfull[a], 1);
-      mbar_init(&mempty[a], 4 * G);
-    }
-    for (int s = 0; s < NSLOT; ++s) {
-      mbar_init(&sfull[s], 1);
-      mbar_init(&sempty[s], 4);
+      mbar_init(&mempty[a], 4 * kGroups);
     }
     *abort_flag = 0;
     mbar_fence_init();
@@ -326,23 +321,37 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp < W_EPI) {
     // ---- densify: group (warp / 4) takes stages it % G == group ----
     const int group = warp >> 2, q = warp & 3;
-    if (group >= G) goto done;  // spare warps of a narrower configuration
-    const Ring ring = group_ring(ring_ptr, sfull, sempty, group, NSG);
-    uint32_t it = 0, pc = 0, ti = 0;
+    uint32_t it = 0, ti = 0;
+    uint4 w[kFwdRegs];
+    Span pre{-1, -1};  // span whose loads are in flight in w
     for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++ti) {
       if (!warp_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 11)) goto done;
       const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
       for (int c = 0; c < nc; ++c, ++it) {
         if ((int)(it % G) != group) continue;
-        const SegMeta m = mt[c];
+        const Span sp = quarter_span(mt[c], q);
+        if (sp.lo != pre.lo || sp.hi != pre.hi) span_load<kFwdRegs>(ent, sp, lane, w);
         const int s = it % S;
         if (!warp_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 12)) goto done;
         const uint32_t tile = smem_u32(As + s * A_BYTES);
         zero_rows(tile, q, lane);
         __syncwarp();
-        if (!densify_segment(tile, m, ring, pc, q, lane, abort_flag, err, 13)) goto done;
+        span_scatter<kFwdRegs>(tile, ent, sp, lane, w);
+        // put the group's next segment in flight: chunk c + G of this tile, or
+        // of the next tile once its metadata is in
+        pre = Span{-1, -1};
+        const int cn = c + G;
+        if (cn < nc) {
+          pre = quarter_span(mt[cn], q);
+        } else if (cn - nc < nc && t + gridDim.x < n_tiles) {
+          if (!warp_wait(&mfull[(ti + 1) & 1u], ((ti + 1) >> 1) & 1u, abort_flag, err, 11)) goto done;
+          pre = quarter_span(mring[((ti + 1) & 1u) * kMaxChunks + (cn - nc)], q);
+        }
+        if (pre.lo >= 0) span_load<kFwdRegs>(ent, pre, lane, w);
+        // every lane's shared stores -> async proxy, then one arrival per warp
         fence_proxy_async_smem();
-        mbar_arrive(&full[s]);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&full[s]);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&mempty[ti & 1u]);
@@ -388,7 +397,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       }
       tc_fence_before();
-      mbar_arrive(&acc_empty[a]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[a]);
     }
   } else if (warp == W_MMA) {
     // ---- MMA issuer ----
@@ -402,19 +412,21 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t d = tmem + a * N2;
         bool ok = true;
         for (int c = 0; c < nc; ++c, ++it) {
-          const int s = it % S;
-          if (!mbar_wait(&full[s], (it / S) & 1u, abort_flag, err, 16)) {
+          const int s = it % S, b = it % NB;
+          if (!mbar_wait(&bfull[b], (it / NB) & 1u, abort_flag, err, 16) ||
+              !mbar_wait(&full[s], (it / S) & 1u, abort_flag, err, 16)) {
             ok = false;
             break;
           }
           tc_fence_after();
           const uint32_t a_base = smem_u32(As + s * A_BYTES);
-          const uint32_t b_base = smem_u32(Bs + s * B_BYTES);
+          const uint32_t b_base = smem_u32(Bs + b * B_BYTES);
 #pragma unroll
           for (int kk = 0; kk < CW / 16; ++kk)
             umma_f16(d, sdesc_sw128(a_base + kk * 32, 16, 1024), sdesc_sw128(b_base + kk * 2048, CW * 128, 1024),
                      idesc, (c | kk) != 0);
           umma_commit(&empty[s]);
+          umma_commit(&bempty[b]);
         }
         if (!ok) break;
         umma_commit(&acc_full[a]);
@@ -422,50 +434,38 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncwarp();
   } else if (warp == W_DENSE) {
-    // ---- dense loader: [Vhi | Vlo] chunk into the B stage ----
+    // ---- dense loader: [Vhi | Vlo] chunks into the B ring, up to NB ahead ----
     if (lane == 0) {
       uint32_t it = 0;
       bool ok = true;
       for (int64_t t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
         for (int c = 0; c < nc; ++c, ++it) {
-          const int s = it % S;
-          if (!mbar_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 19)) {
+          const int b = it % NB;
+          if (!mbar_wait(&bempty[b], ((it / NB) & 1u) ^ 1u, abort_flag, err, 19)) {
             ok = false;
             break;
           }
-          uint8_t* b = Bs + s * B_BYTES;
-          mbar_arrive_expect_tx(&full[s], B_BYTES);
+          uint8_t* bb = Bs + b * B_BYTES;
+          mbar_arrive_expect_tx(&bfull[b], B_BYTES);
 #pragma unroll
           for (int h = 0; h < LD / 64; ++h) {
-            tma_load_2d(b + h * (CW * 128), &vmap_hi, &full[s], 64 * h, CW * c);
-            tma_load_2d(b + B_PLANE + h * (CW * 128), &vmap_lo, &full[s], 64 * h, CW * c);
+            tma_load_2d(bb + h * (CW * 128), &vmap_hi, &bfull[b], 64 * h, CW * c);
+            tma_load_2d(bb + B_PLANE + h * (CW * 128), &vmap_lo, &bfull[b], 64 * h, CW * c);
           }
         }
       }
     }
     __syncwarp();
-  } else {
-    // ---- sparse loader: tile metadata and entry pieces, ahead of the stages ----
+  } else if (warp == W_META) {
+    // ---- meta loader: tile metadata, and the tile's entries into L2 ----
     if (lane == 0) {
-      uint32_t pcg[kMaxGroups] = {0, 0, 0, 0};  // per-group piece counters
-      uint32_t it = 0, ti = 0;
-      int64_t t = blockIdx.x;
-      if (t < n_tiles && !load_meta(meta, t, nc, mring, mfull, mempty, 0, abort_flag, err, 17)) goto loader_out;
-      for (; t < n_tiles; t += gridDim.x, ++ti) {
-        const int64_t tn = t + gridDim.x;
-        if (tn < n_tiles && !load_meta(meta, tn, nc, mring, mfull, mempty, ti + 1, abort_flag, err, 17))
-          break;
+      uint32_t ti = 0;
+      for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++ti) {
+        if (!load_meta(meta, t, nc, mring, mfull, mempty, ti, abort_flag, err, 17)) break;
         if (!mbar_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 18)) break;
-        const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
-        bool ok = true;
-        for (int c = 0; c < nc && ok; ++c, ++it) {
-          const int g = (int)(it % G);
-          ok = load_segment(ent, mt[c], group_ring(ring_ptr, sfull, sempty, g, NSG), pcg[g], abort_flag, err, 20);
-        }
-        if (!ok) break;
+        prefetch_segments(ent, mring + (ti & 1u) * kMaxChunks, 0, nc);
       }
     }
-  loader_out:
     __syncwarp();
   }
 done:
@@ -491,10 +491,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               int64_t g, int n_gene_groups, const __grid_constant__ CUtensorMap qmap_hi,
               const __grid_constant__ CUtensorMap qmap_lo, float* __restrict__ part, int fmt, int* err) {
   constexpr int N2 = 2 * LD;
-  constexpr int S = rmat_stages(LD);
-  constexpr int G = rmat_groups(LD);
-  constexpr int NSLOT = rmat_slots(LD);
-  constexpr int NSG = NSLOT / G;
+  constexpr int S = rmat_stages(LD);     // A stages == active densify groups
   constexpr int SUB = TM * CW * 2;       // one 64-gene sub-tile, 16 KB
   constexpr int A_BYTES = 2 * SUB;       // 128 genes
   constexpr int Q_PLANE = TM * LD * 2;   // 128 cells x LD
@@ -504,16 +501,13 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint8_t* smem = align1024(smem_raw);
   uint8_t* As = smem;
   uint8_t* Qs = As + S * A_BYTES;  // [2 buffers][hi, lo]
-  uint32_t* ring_ptr = reinterpret_cast<uint32_t*>(Qs + 2 * Q_BYTES);
-  SegMeta* mring = reinterpret_cast<SegMeta*>(ring_ptr + NSLOT * kCap);
+  SegMeta* mring = reinterpret_cast<SegMeta*>(Qs + 2 * Q_BYTES);
   uint64_t* bars = reinterpret_cast<uint64_t*>(mring + 2 * kMaxChunks);
   uint64_t* full = bars;
   uint64_t* empty = full + S;
   uint64_t* qfull = empty + S;
   uint64_t* qempty = qfull + 2;
-  uint64_t* sfull = qempty + 2;
-  uint64_t* sempty = sfull + NSLOT;
-  uint64_t* mfull = sempty + NSLOT;
+  uint64_t* mfull = qempty + 2;
   uint64_t* mempty = mfull + 2;
   uint64_t* done_bar = mempty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done_bar + 1);
@@ -531,18 +525,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
-      mbar_init(&full[s], 128);
+      mbar_init(&full[s], 4);  // one arrival per warp of the stage's densify group
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&qfull[b], 1);
       mbar_init(&qempty[b], 1);
       mbar_init(&mfull[b], 1);
-      mbar_init(&mempty[b], 4 * G);
-    }
-    for (int s = 0; s < NSLOT; ++s) {
-      mbar_init(&sfull[s], 1);
-      mbar_init(&sempty[s], 4);
+      mbar_init(&mempty[b], 4 * S);
     }
     mbar_init(done_bar, 1);
     *abort_flag = 0;
@@ -558,30 +548,53 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp < W_EPI) {
-    // ---- densify: group (warp / 4) takes super-chunk stages it % G == group ----
+    // ---- densify: group (warp / 4) takes super-chunk stages it % S == group ----
     const int group = warp >> 2, q = warp & 3;
-    if (group >= G) goto done;  // spare warps of a narrower configuration
-    const Ring ring = group_ring(ring_ptr, sfull, sempty, group, NSG);
-    uint32_t it = 0, pc = 0, ti = 0;
+    if (group >= S) goto done;  // spare warps of a narrower configuration
+    uint32_t it = 0, ti = 0;
+    uint4 w0[kRmatRegs], w1[kRmatRegs];
+    Span pre0{-1, -1}, pre1{-1, -1};  // spans whose loads are in flight in w0 / w1
     if (have_work)
       for (int64_t t = t0; t < t1; ++t, ++ti) {
         if (!warp_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 21)) goto done;
         const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
         for (int sc = sc0; sc < sc1; ++sc, ++it) {
-          if ((int)(it % G) != group) continue;
-          const SegMeta m0 = mt[2 * sc];
+          if ((int)(it % S) != group) continue;
           const bool two = 2 * sc + 1 < nc;
-          const SegMeta m1 = two ? mt[2 * sc + 1] : m0;
+          const Span s0 = quarter_span(mt[2 * sc], q);
+          const Span s1 = two ? quarter_span(mt[2 * sc + 1], q) : Span{s0.hi, s0.hi};
+          if (s0.lo != pre0.lo || s0.hi != pre0.hi) span_load<kRmatRegs>(ent, s0, lane, w0);
+          if (s1.lo != pre1.lo || s1.hi != pre1.hi) span_load<kRmatRegs>(ent, s1, lane, w1);
           const int s = it % S;
           if (!warp_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 22)) goto done;
           const uint32_t tile = smem_u32(As + s * A_BYTES);
           zero_rows(tile, q, lane);
           zero_rows(tile + SUB, q, lane);
           __syncwarp();
-          if (!densify_segment(tile, m0, ring, pc, q, lane, abort_flag, err, 23)) goto done;
-          if (two && !densify_segment(tile + SUB, m1, ring, pc, q, lane, abort_flag, err, 23)) goto done;
+          span_scatter<kRmatRegs>(tile, ent, s0, lane, w0);
+          span_scatter<kRmatRegs>(tile + SUB, ent, s1, lane, w1);
+          // the group's next stage: super-chunk sc + S of this tile, or of the next
+          pre0 = pre1 = Span{-1, -1};
+          const int scn = sc + S;
+          const SegMeta* mn = nullptr;
+          int scx = 0;
+          if (scn < sc1) {
+            mn = mt;
+            scx = scn;
+          } else if (scn - nsc < sc1 && t + 1 < t1) {
+            if (!warp_wait(&mfull[(ti + 1) & 1u], ((ti + 1) >> 1) & 1u, abort_flag, err, 21)) goto done;
+            mn = mring + ((ti + 1) & 1u) * kMaxChunks;
+            scx = scn - nsc;
+          }
+          if (mn) {
+            pre0 = quarter_span(mn[2 * scx], q);
+            pre1 = 2 * scx + 1 < nc ? quarter_span(mn[2 * scx + 1], q) : Span{pre0.hi, pre0.hi};
+            span_load<kRmatRegs>(ent, pre0, lane, w0);
+            span_load<kRmatRegs>(ent, pre1, lane, w1);
+          }
           fence_proxy_async_smem();
-          mbar_arrive(&full[s]);
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&full[s]);
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&mempty[ti & 1u]);
@@ -669,28 +682,16 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
     __syncwarp();
-  } else {
-    // ---- sparse loader: tile metadata and entry pieces of this gene group ----
+  } else if (warp == W_META) {
+    // ---- meta loader: tile metadata, and this gene group's entries of the tile into L2 ----
     if (lane == 0 && have_work) {
-      uint32_t pcg[kMaxGroups] = {0, 0, 0, 0};  // per-group piece counters
-      uint32_t it = 0, ti = 0;
-      int64_t t = t0;
-      if (!load_meta(meta, t, nc, mring, mfull, mempty, 0, abort_flag, err, 27)) goto loader_out;
-      for (; t < t1; ++t, ++ti) {
-        if (t + 1 < t1 && !load_meta(meta, t + 1, nc, mring, mfull, mempty, ti + 1, abort_flag, err, 27)) break;
+      uint32_t ti = 0;
+      for (int64_t t = t0; t < t1; ++t, ++ti) {
+        if (!load_meta(meta, t, nc, mring, mfull, mempty, ti, abort_flag, err, 27)) break;
         if (!mbar_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 29)) break;
-        const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
-        bool ok = true;
-        for (int sc = sc0; sc < sc1 && ok; ++sc, ++it) {
-          const int gq = (int)(it % G);
-          const Ring ring = group_ring(ring_ptr, sfull, sempty, gq, NSG);
-          ok = load_segment(ent, mt[2 * sc], ring, pcg[gq], abort_flag, err, 30);
-          if (ok && 2 * sc + 1 < nc) ok = load_segment(ent, mt[2 * sc + 1], ring, pcg[gq], abort_flag, err, 30);
-        }
-        if (!ok) break;
+        prefetch_segments(ent, mring + (ti & 1u) * kMaxChunks, 2 * sc0, min(nc, 2 * sc1));
       }
     }
-  loader_out:
     __syncwarp();
   }
 done:
@@ -870,12 +871,10 @@ __global__ void k_split16(float* __restrict__ in, int64_t count, uint16_t* __res
 
 size_t smem_tail() { return 2 * kMaxChunks * sizeof(SegMeta) + 64 * sizeof(uint64_t) + 64; }
 size_t fwd_smem(int LD) {
-  return 1024 + (size_t)fwd_stages(LD) * (TM * CW * 2 + 2 * CW * LD * 2) + (size_t)fwd_slots(LD) * kCap * 4 +
-         smem_tail();
+  return 1024 + (size_t)fwd_stages(LD) * (TM * CW * 2) + (size_t)fwd_bslots(LD) * (2 * CW * LD * 2) + smem_tail();
 }
 size_t rmat_smem(int LD) {
-  return 1024 + (size_t)rmat_stages(LD) * (2 * TM * CW * 2) + 4 * (size_t)TM * LD * 2 +
-         (size_t)rmat_slots(LD) * kCap * 4 + smem_tail();
+  return 1024 + (size_t)rmat_stages(LD) * (2 * TM * CW * 2) + 4 * (size_t)TM * LD * 2 + smem_tail();
 }
 
 }  // namespace

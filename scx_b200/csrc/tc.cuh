@@ -118,6 +118,12 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
+// Bring [src, src + bytes) into L2 ahead of use (16-byte aligned address, size
+// a multiple of 16); no completion tracking, the later bulk copy finds it there.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 // 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple
 // of 16), completing `bytes` of transaction count on `bar`.
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
