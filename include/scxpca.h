@@ -165,6 +165,37 @@ int32_t scxpca_plan_run(scxpca_plan* plan, const scxpca_params* params,
 
 void scxpca_plan_destroy(scxpca_plan* plan);
 
+/* Resident plan of the affine map X~ = (X - 1 center^T) diag(scale) with
+ * explicit per-gene vectors (n_vars doubles each, host or device per
+ * `vectors_memory`; NULL center = no centring, NULL scale = 1).  The PCA is
+ * of X~ itself: no column means are re-subtracted.  With center = column
+ * means and scale = 1 / std this is the matrix that zero_center + scale
+ * (without clipping) describe.  params->scale must be 0 and clip_max <= 0;
+ * params->zero_center is ignored.  Scale entries must be non-zero.  Extends
+ * try_build_resident_csr (scx-gpu/src/gpu_pca_resident.rs:87-179) with the
+ * differentiable inputs of scxpca_plan_backward; the reference has no
+ * gradient path. */
+int32_t scxpca_plan_create_affine(const scxpca_csr* x, const scxpca_params* params,
+                                  const double* center, const double* scale, int32_t vectors_memory,
+                                  scxpca_plan** plan, char* err, size_t err_len);
+
+/* Backward pass of the scores S = X~ V (the embeddings of the plan's last
+ * run, V the top n_components right singular vectors) for a loss L(S):
+ * given dL/dS, writes dL/dx for every stored value x of the CSR (in the
+ * CSR's entry order), dL/dcenter and dL/dscale (n_vars each; either may be
+ * NULL).  The gradient is the adjoint of the truncated SVD: the part of each
+ * singular-vector derivative inside the sketch subspace comes from the
+ * run's Ritz pairs, the part outside it from `solve_iterations` conjugate-
+ * gradient steps (each one product with X~^T X~, recomputed rather than
+ * stored).  All pointers are device memory on the plan's device: scores and
+ * grad_scores n_obs x n_components row-major float32, grad_values nnz float32.
+ * Must follow scxpca_plan_run with no other call on the plan in between; not
+ * available with clip_max > 0 or when the plan had to re-sort the CSR rows.
+ * No reference counterpart (the reference PCA is not differentiable). */
+int32_t scxpca_plan_backward(scxpca_plan* plan, const float* scores, const float* grad_scores,
+                             int32_t solve_iterations, float* grad_values, double* grad_center,
+                             double* grad_scale, char* err, size_t err_len);
+
 /* Plan geometry: k (sketch width), ld (padded row stride of the tall
  * buffers), bytes of device memory the plan holds. */
 int32_t scxpca_plan_info(const scxpca_plan* plan, int64_t* k, int64_t* ld,

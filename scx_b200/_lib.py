@@ -40,6 +40,8 @@ EXPORTED = (
     "scxpca_plan_create",
     "scxpca_plan_run",
     "scxpca_plan_destroy",
+    "scxpca_plan_create_affine",
+    "scxpca_plan_backward",
     "scxpca_plan_info",
     "scxpca_plan_matmat",
     "scxpca_plan_rmatmat",
@@ -145,6 +147,9 @@ def load() -> C.CDLL:
         "scxpca_plan_create": (C.c_int32, [C.POINTER(Csr), C.POINTER(Params), C.POINTER(P), *E]),
         "scxpca_plan_run": (C.c_int32, [P, C.POINTER(Params), C.POINTER(Result), *E]),
         "scxpca_plan_destroy": (None, [P]),
+        "scxpca_plan_create_affine": (C.c_int32, [C.POINTER(Csr), C.POINTER(Params), P, P, C.c_int32,
+                                                  C.POINTER(P), *E]),
+        "scxpca_plan_backward": (C.c_int32, [P, P, P, C.c_int32, P, P, P, *E]),
         "scxpca_plan_info": (C.c_int32, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                          C.POINTER(C.c_int64)]),
         "scxpca_plan_matmat": (C.c_int32, [P, P, C.c_int64, P, C.c_int64, *E]),

@@ -129,6 +129,22 @@ def _prepare_omega(omega, n_vars: int, k: int):
     return _ptr(om), _lib.MEM_HOST, om
 
 
+def _prepare_gene_vector(v, n_vars: int, name: str):
+    """A per-gene float64 vector -> (pointer, memory, keepalive); None -> (0, host, None)."""
+    if v is None:
+        return 0, _lib.MEM_HOST, None
+    if _is_torch(v) and v.is_cuda:
+        import torch
+        t = v.detach().to(torch.float64).contiguous()
+        if t.numel() != n_vars:
+            raise ValueError(f"{name} must have n_vars = {n_vars} entries")
+        return _ptr(t), _lib.MEM_DEVICE, t
+    a = np.ascontiguousarray(np.asarray(v.detach().cpu() if _is_torch(v) else v, dtype=np.float64))
+    if a.shape != (n_vars,):
+        raise ValueError(f"{name} must have n_vars = {n_vars} entries")
+    return _ptr(a), _lib.MEM_HOST, a
+
+
 def _params(n_components, n_oversamples, n_power_iterations, zero_center, scale, clip_max, seed,
             qr_method, math_mode, spmm_policy, device):
     if qr_method not in _QR:
@@ -247,9 +263,15 @@ class Plan:
                  n_oversamples: int = 10, n_power_iterations: int = 2, zero_center: bool = True,
                  scale: bool = False, clip_max: float | None = None, seed: int = 0,
                  qr_method: str = "householder", math_mode: str = "strict_fp32",
-                 spmm_policy: str = "default", device: int = 0, stream: int | None = None):
+                 spmm_policy: str = "default", device: int = 0, stream: int | None = None,
+                 center=None, gene_scale=None):
         """``stream`` is a raw ``cudaStream_t`` handle (e.g. ``torch.cuda.Stream().cuda_stream``)
-        every kernel of this plan is ordered on; None lets the plan own a stream."""
+        every kernel of this plan is ordered on; None lets the plan own a stream.
+
+        ``center`` / ``gene_scale`` (n_vars float64, numpy or CUDA torch) make the
+        plan's matrix the affine map (X - 1 center^T) diag(gene_scale), with no
+        column means re-subtracted (scxpca_plan_create_affine); ``zero_center``,
+        ``scale`` and ``clip_max`` are then ignored."""
         self._lib = _lib.load()
         csr, keep, mem, dev = _prepare_csr(indptr, indices, values, shape)
         if dev is not None:
@@ -264,10 +286,25 @@ class Plan:
         if stream:
             self._params.stream = int(stream)
         self._keep = keep if mem == _lib.MEM_DEVICE else None  # borrowed device CSR must live
+        self.nnz = int(csr.nnz)
         handle = C.c_void_p()
         err = _lib.errbuf()
-        st = self._lib.scxpca_plan_create(C.byref(csr), C.byref(self._params), C.byref(handle),
-                                          err, len(err))
+        if center is not None or gene_scale is not None:
+            self._params.scale = 0
+            self._params.clip_max = 0.0
+            cptr, cmem, ckeep = _prepare_gene_vector(center, self.shape[1], "center")
+            sptr, smem, skeep = _prepare_gene_vector(gene_scale, self.shape[1], "gene_scale")
+            if cptr and sptr and cmem != smem:
+                raise ValueError("center and gene_scale must both be host or both be device arrays")
+            vmem = cmem if cptr else smem
+            self.zero_center = center is not None
+            self.scale = gene_scale is not None
+            st = self._lib.scxpca_plan_create_affine(C.byref(csr), C.byref(self._params), cptr or None,
+                                                     sptr or None, vmem, C.byref(handle), err, len(err))
+            del ckeep, skeep
+        else:
+            st = self._lib.scxpca_plan_create(C.byref(csr), C.byref(self._params), C.byref(handle),
+                                              err, len(err))
         _lib.check(st, err)
         self._h = handle
         k = C.c_int64()
@@ -361,6 +398,27 @@ class Plan:
         st = self._lib.scxpca_plan_qr(self._h, _ptr(a), a.shape[0], a.stride(0), err, len(err))
         _lib.check(st, err)
         return a
+
+    def backward(self, scores, grad_scores, solve_iterations: int = 8):
+        """Gradients of a loss of the last run's scores (scxpca_plan_backward).
+
+        ``scores`` and ``grad_scores`` are CUDA float32 (n_obs, n_components)
+        tensors; returns (grad_values (nnz,) float32, grad_center (n_vars,)
+        float64, grad_scale (n_vars,) float64), all CUDA tensors."""
+        import torch
+        dev = scores.device
+        s = scores.to(torch.float32).contiguous()
+        gs = grad_scores.to(device=dev, dtype=torch.float32).contiguous()
+        if tuple(s.shape) != (self.shape[0], self.n_components) or s.shape != gs.shape:
+            raise ValueError(f"scores and grad_scores must be ({self.shape[0]}, {self.n_components})")
+        gv = torch.empty(max(self.nnz, 1), dtype=torch.float32, device=dev)
+        gc = torch.empty(self.shape[1], dtype=torch.float64, device=dev)
+        gsc = torch.empty(self.shape[1], dtype=torch.float64, device=dev)
+        err = _lib.errbuf()
+        st = self._lib.scxpca_plan_backward(self._h, _ptr(s), _ptr(gs), int(solve_iterations), _ptr(gv),
+                                            _ptr(gc), _ptr(gsc), err, len(err))
+        _lib.check(st, err)
+        return gv[: self.nnz], gc, gsc
 
     def col_stats(self):
         n_vars = self.shape[1]

@@ -30,6 +30,7 @@ SOURCES = [
     "kernels_dense.cu",
     "kernels_csr.cu",
     "synth.cu",
+    "kernels_adjoint.cu",
     "noalloc.cu",
 ]
 EXTRA_SOURCES_OPTIONAL = ["kernels_tc.cu"]

@@ -140,6 +140,43 @@ size_t rmat_tc_smem_bytes(int ld);
 cudaError_t launch_split16(float* in, int64_t count, uint16_t* hi, uint16_t* lo, int fmt, int write_back,
                            cudaStream_t st, int num_sms);
 
+// ---- truncated-SVD adjoint (kernels_adjoint.cu) ----
+// Column sums (FP64) of a tall float matrix A (n x ld, first ncols columns)
+// into out[ld]; part holds nparts x ld partials.
+cudaError_t launch_colsum_f32(const float* A, int64_t n, int ld, int ncols, double* part, int nparts,
+                              double* out, cudaStream_t st, int num_sms);
+// T (ld x ld) = A^T B over g rows, first ka x kb block (FP64).
+cudaError_t launch_atb(const double* A, const double* B, int64_t g, int ld, int ka, int kb, double* T,
+                       cudaStream_t st);
+// M = E diag(1 / sqrt(evals)) over the first k columns.
+cudaError_t launch_ritz_scale(const double* E, const double* evals, int k, int ld, double* M, cudaStream_t st);
+// Phi[j][i] = T[j][i] / (evals[i] - evals[j]), j < k, i < c, j != i.
+cudaError_t launch_phi(const double* T, const double* evals, int k, int c, int ld, double* Phi, cudaStream_t st);
+// Out = X + beta Y on the first c columns (g x ld).
+cudaError_t launch_axpy_cols(const double* X, const double* Y, double beta, int64_t g, int ld, int c, double* Out,
+                             cudaStream_t st);
+// out[i] = column i of X . column i of Y, i < c.
+cudaError_t launch_coldot(const double* X, const double* Y, int64_t g, int ld, int c, double* out, cudaStream_t st);
+// Conjugate-gradient pieces for (lambda_i I - X~^T X~) on the complement of the sketch subspace.
+cudaError_t launch_cg_ap(const double* P, const double* W, const double* Proj, const double* evals, int64_t g,
+                         int ld, int c, double* Ap, cudaStream_t st);
+cudaError_t launch_cg_step(double* X, double* R, const double* P, const double* Ap, const double* rr,
+                           const double* pAp, int64_t g, int ld, int c, cudaStream_t st);
+cudaError_t launch_cg_dir(double* P, const double* R, double* rr, const double* rr_new, int64_t g, int ld, int c,
+                          cudaStream_t st);
+// colD[j] = sum_i sF[i] V[j][i] + sS[i] A[j][i].
+cudaError_t launch_col_d(const double* V, const double* A, const double* sF, const double* sS, int64_t g, int ld,
+                         int c, double* colD, cudaStream_t st);
+// Gradients of the per-gene centre and scale (either output may be null).
+cudaError_t launch_grad_vectors(const double* colD, const double* sumDP, const double* center, const double* scale,
+                                int64_t g, double* grad_center, double* grad_scale, cudaStream_t st);
+// SDDMM of the gradient at the stored entries (column slice of cs <= 64
+// columns); part[nchunks][g] receives per-gene sums of d * x~.
+cudaError_t launch_sddmm(int dtype, const int64_t* indptr, const int32_t* idx, const void* val, int64_t n, int32_t g,
+                         const int32_t* rbp, int nb, int nchunks, int64_t rows_per_chunk, const float* G, int ldg,
+                         const float* Y, int ldy, const float* S, int lds, const double* V, const double* A, int ldv,
+                         int cs, const double* scale, int accumulate, float* grad, double* part, cudaStream_t st);
+
 // ---- synthetic generator (synth.cu) ----
 cudaError_t launch_synth_count(uint64_t seed, int64_t n, int64_t g, double loc, double disp,
                                const float* mu_g, int64_t* row_nnz, float* rowsum,

@@ -161,6 +161,16 @@ struct scxpca_plan {
   DevBuf tf_meta, tf_ent, V16, V16lo, Y16, Q16lo, tc_part, tc_err;
   CUtensorMap vmap{}, vmap_lo{}, qmap_hi{}, qmap_lo{};
 
+  // differentiation: raw per-gene centre c and scale s of X~ = (X - 1 c^T) diag(s)
+  // (device, n_vars each), whether the last run's Ritz state (B in Z, E, evals)
+  // is intact, and the backward pass's work buffers
+  DevBuf d_center_raw, d_scale_raw;
+  bool affine = false;
+  bool rows_resorted = false;
+  bool run_valid = false;
+  DevBuf bw_Vk, bw_H, bw_A, bw_X, bw_R, bw_P, bw_Ap, bw_Proj, bw_T, bw_M, bw_vec, bw_colD, bw_sumDP, bw_part,
+      bw_cpart;
+
   // opt-in stage timing
   bool profiling = false;
   std::vector<cudaEvent_t> events;
@@ -268,7 +278,26 @@ void compute_total_variance(scxpca_plan* pl) {
   pl->total_var_recomputed = true;
 }
 
-scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
+// Explicit centre / scale vectors of an affine plan (either may be null).
+struct AffineSpec {
+  const double* center;
+  const double* scale;
+  int32_t memory;  // scxpca_memory of both vectors
+};
+
+std::vector<double> read_vec(const double* src, int64_t n, int32_t memory, double fill, cudaStream_t st) {
+  std::vector<double> v(n, fill);
+  if (!src) return v;
+  if (memory == SCXPCA_MEM_DEVICE) {
+    CK(cudaMemcpyAsync(v.data(), src, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  } else {
+    memcpy(v.data(), src, sizeof(double) * n);
+  }
+  return v;
+}
+
+scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const AffineSpec* aff = nullptr) {
   validate_params(x, p);
   auto pl = new scxpca_plan();
   try {
@@ -285,9 +314,10 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
     pl->dtype = p->math_mode == SCXPCA_MATH_STRICT_FP32 ? SCXPCA_F32
                 : p->math_mode == SCXPCA_MATH_MIXED_BF16 ? SCXPCA_BF16
                                                          : SCXPCA_F16;
-    pl->centered = p->zero_center != 0;
-    pl->scaled = p->scale != 0;
-    pl->clip = p->clip_max > 0 ? p->clip_max : 0.0;
+    pl->affine = aff != nullptr;
+    pl->centered = aff ? aff->center != nullptr : p->zero_center != 0;
+    pl->scaled = aff ? false : p->scale != 0;
+    pl->clip = (!aff && p->clip_max > 0) ? p->clip_max : 0.0;
     if (p->stream) {
       pl->stream = static_cast<cudaStream_t>(p->stream);
     } else {
@@ -359,6 +389,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
         }
         CK(launch_sort_rows(pl->in_dtype, pl->indptr, pl->b_idx.as<int32_t>(), pl->b_stage.p, n, st,
                             pl->num_sms));
+        pl->rows_resorted = true;
         // after sorting, any remaining "not strictly ascending" pair is a duplicate
         CK(cudaMemsetAsync(flags.p, 0, 16, st));
         CK(launch_validate_csr(pl->in_dtype, pl->indptr, pl->idx, vin, n, g, nnz, flags.as<int32_t>(),
@@ -387,7 +418,18 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
     for (int64_t j = 0; j < g; ++j) pl->mean_x[j] = sx[j] / (double)n;
 
     // ---- working values ----
-    const bool borrow = !pl->scaled && pl->in_dtype == pl->dtype;
+    std::vector<double> center_raw(g, 0.0), scale_raw(g, 1.0);
+    const bool affine_scaled = aff && aff->scale;
+    const bool borrow = !pl->scaled && !affine_scaled && pl->in_dtype == pl->dtype;
+    if (aff) {
+      center_raw = read_vec(aff->center, g, aff->memory, 0.0, st);
+      scale_raw = read_vec(aff->scale, g, aff->memory, 1.0, st);
+      for (int64_t j = 0; j < g; ++j) {
+        if (!std::isfinite(center_raw[j]) || !std::isfinite(scale_raw[j]) || scale_raw[j] == 0.0)
+          fail(SCXPCA_INVALID_ARGUMENT, "center and scale must be finite and scale non-zero (gene " +
+                                            std::to_string(j) + ")");
+      }
+    }
     if (borrow) {
       pl->val = vin;
       if (!dev_in || vin != x->values) {
@@ -404,7 +446,10 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
       pl->b_val.alloc(dtype_size(pl->dtype) * std::max<int64_t>(nnz, 1));
       int mode = 0;
       std::vector<double> mu(g, 0.0), inv_std(g, 1.0), cshift(g, 0.0);
-      if (pl->scaled) {
+      if (affine_scaled) {
+        inv_std = scale_raw;  // x -> x s, no clip; the centring stays implicit
+        mode = 2;
+      } else if (pl->scaled) {
         pl->std_x.resize(g);
         for (int64_t j = 0; j < g; ++j) {
           double m = pl->mean_x[j];
@@ -432,13 +477,34 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p) {
       stats_pass(pl, pl->val, pl->dtype, pl->col_sum, pl->col_sq);
       pl->b_stage.release();
     }
-    {
+    if (aff) {
+      // X~ = P - 1 (c s)^T: the centre is the given vector, not the column mean
+      std::vector<double> mu_w(g, 0.0);
+      double t = 0.0;
+      for (int64_t j = 0; j < g; ++j) {
+        if (pl->centered) mu_w[j] = center_raw[j] * scale_raw[j];
+        t += pl->col_sq[j] - 2.0 * mu_w[j] * pl->col_sum[j] + (double)n * mu_w[j] * mu_w[j];
+      }
+      upload(pl->d_mu, mu_w, st);
+      pl->total_var = t / std::max<double>((double)n - 1.0, 1.0);
+    } else {
       std::vector<double> mu_w(g, 0.0);
       if (pl->centered)
         for (int64_t j = 0; j < g; ++j) mu_w[j] = pl->col_sum[j] / (double)n;
       upload(pl->d_mu, mu_w, st);
+      compute_total_variance(pl);
+      // the same matrix as an affine map of the input, for the backward pass
+      for (int64_t j = 0; j < g; ++j) {
+        center_raw[j] = pl->centered ? pl->mean_x[j] : 0.0;
+        scale_raw[j] = pl->scaled ? 1.0 / pl->std_x[j] : 1.0;
+      }
     }
-    compute_total_variance(pl);
+    upload(pl->d_center_raw, center_raw, st);
+    upload(pl->d_scale_raw, scale_raw, st);
+    if (aff && aff->scale) {
+      pl->std_x.resize(g);
+      for (int64_t j = 0; j < g; ++j) pl->std_x[j] = 1.0 / scale_raw[j];
+    }
 
     // ---- tensor-core path: tile-chunk packed matrix, 16-bit operands, TMA maps ----
     if (pl->use_tc) {
@@ -787,13 +853,124 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
     for (int64_t j = 0; j < pl->g; ++j) out->mean[j] = pl->mean_x[j];
   }
   if (out->std) {
-    for (int64_t j = 0; j < pl->g; ++j) out->std[j] = pl->scaled ? pl->std_x[j] : 1.0;
+    for (int64_t j = 0; j < pl->g; ++j) out->std[j] = pl->std_x.empty() ? 1.0 : pl->std_x[j];
   }
   out->resident_csr = 1;
   out->total_var_recomputed = pl->total_var_recomputed ? 1 : 0;
   out->shifted_cholesky = hstatus[0] > 0 ? hstatus[0] : 0;
   out->eig_sweeps = hstatus[2];
   out->total_var = pl->total_var;
+  pl->run_valid = true;
+}
+
+// ---------------------------------------------------------------------------
+// Backward pass of the scores S = X~ V_c (truncated-SVD adjoint; the
+// derivation is in kernels_adjoint.cu).  Uses the last run's Ritz state: B in
+// Z, the eigenvectors E and eigenvalues lambda = sigma^2 of B^T B.
+// ---------------------------------------------------------------------------
+void backward(scxpca_plan* pl, const float* S, const float* GS, int iters, float* gvals, double* gcenter,
+              double* gscale) {
+  if (!pl->run_valid)
+    fail(SCXPCA_INVALID_ARGUMENT, "backward needs the state of a completed run: call scxpca_plan_run first, "
+                                  "with no other call on the plan in between");
+  if (pl->clip > 0) fail(SCXPCA_UNSUPPORTED, "the backward pass does not support clipped values (clip_max > 0)");
+  if (pl->rows_resorted)
+    fail(SCXPCA_UNSUPPORTED, "the plan re-sorted unsorted CSR rows, so gradients would not follow the caller's "
+                             "entry order; sort each row by gene before creating the plan");
+  if (iters < 0 || iters > 1000) fail(SCXPCA_INVALID_ARGUMENT, "solve_iterations must be in [0, 1000]");
+  if (!S || !GS || !gvals) fail(SCXPCA_INVALID_ARGUMENT, "null scores, grad_scores or grad_values");
+  pl->run_valid = false;
+  cudaStream_t st = pl->stream;
+  const int64_t n = pl->n, g = pl->g;
+  const int ld = (int)pl->ld, k = (int)pl->k, c = (int)pl->nc;
+  const double* mu = pl->centered ? pl->d_mu.as<double>() : nullptr;
+  const size_t gl = sizeof(double) * g * ld;
+  for (DevBuf* b : {&pl->bw_Vk, &pl->bw_H, &pl->bw_A, &pl->bw_X, &pl->bw_R, &pl->bw_P, &pl->bw_Ap, &pl->bw_Proj})
+    b->alloc(gl);
+  pl->bw_T.alloc(sizeof(double) * ld * ld);
+  pl->bw_M.alloc(sizeof(double) * ld * ld);
+  pl->bw_vec.alloc(sizeof(double) * ld * 8);
+  pl->bw_colD.alloc(sizeof(double) * g);
+  pl->bw_sumDP.alloc(sizeof(double) * g);
+  pl->bw_part.alloc(sizeof(double) * (size_t)pl->nchunks * g);
+  const int cparts = (int)std::max<int64_t>(1, std::min<int64_t>(2 * pl->num_sms, (n + 255) / 256));
+  pl->bw_cpart.alloc(sizeof(double) * (size_t)cparts * 256);
+  double* vec = pl->bw_vec.as<double>();
+  double *sG = vec, *sY = vec + ld, *sS = vec + 2 * ld, *sF = vec + 3 * ld, *rr = vec + 4 * ld,
+         *rr_new = vec + 5 * ld, *pAp = vec + 6 * ld;
+  double *Vk = pl->bw_Vk.as<double>(), *H = pl->bw_H.as<double>(), *A = pl->bw_A.as<double>(),
+         *X = pl->bw_X.as<double>(), *R = pl->bw_R.as<double>(), *P = pl->bw_P.as<double>(),
+         *Ap = pl->bw_Ap.as<double>(), *Proj = pl->bw_Proj.as<double>(), *T = pl->bw_T.as<double>(),
+         *M = pl->bw_M.as<double>();
+  const double* evals = pl->evals.as<double>();
+  const double* eye = pl->eye.as<double>();
+  float* Y = pl->Y.as<float>();
+  auto colsum = [&](const float* src, int ldsrc, int ncols, double* out) {
+    CK(launch_colsum_f32(src, n, ldsrc, ncols, pl->bw_cpart.as<double>(), cparts, out, st, pl->num_sms));
+  };
+  // X~^T (tall float in Y) -> (g x ld) FP64 in `out`, centring folded in
+  auto apply_t = [&](int split, double* out) {
+    colsum(Y, ld, ld, sY);
+    rmatmat_raw(pl, Y, split);
+    CK(launch_center_apply(pl->W.as<double>(), g, ld, mu, sY, eye, out, st));
+  };
+  // Y = X~ Vg for a gene-side FP64 block Vg
+  auto apply_f = [&](const double* Vg) {
+    CK(launch_round_v(Vg, g, ld, mu, pl->V.as<float>(), pl->mc.as<float>(), st));
+    forward(pl);
+  };
+
+  // Ritz vectors of the gene side: Vk = B E diag(1 / sigma)
+  CK(launch_ritz_scale(pl->evecs.as<double>(), evals, k, ld, M, st));
+  CK(launch_center_apply(pl->Z.as<double>(), g, ld, nullptr, nullptr, M, Vk, st));
+  // H = X~^T G
+  CK(cudaMemsetAsync(Y, 0, sizeof(float) * n * ld, st));
+  CK(cudaMemcpy2DAsync(Y, sizeof(float) * ld, GS, sizeof(float) * c, sizeof(float) * c, n, cudaMemcpyDeviceToDevice,
+                       st));
+  colsum(Y, ld, ld, sG);
+  apply_t(1, H);
+  // inside the sketch subspace: A_in = Vk Phi, Phi_ji = (Vk^T H)_ji / (lambda_i - lambda_j)
+  CK(launch_atb(Vk, H, g, ld, k, c, T, st));
+  CK(launch_phi(T, evals, k, c, ld, M, st));
+  CK(launch_center_apply(Vk, g, ld, nullptr, nullptr, M, A, st));
+  // outside it: (lambda_i I - X~^T X~) x_i = r_i on the complement, r = H - Vk (Vk^T H), by CG
+  CK(launch_center_apply(Vk, g, ld, nullptr, nullptr, T, Proj, st));
+  CK(launch_axpy_cols(H, Proj, -1.0, g, ld, c, R, st));
+  CK(cudaMemsetAsync(X, 0, gl, st));
+  CK(cudaMemcpyAsync(P, R, gl, cudaMemcpyDeviceToDevice, st));
+  CK(launch_coldot(R, R, g, ld, c, rr, st));
+  for (int m = 0; m < iters; ++m) {
+    apply_f(P);
+    apply_t(0, H);  // H <- X~^T X~ P
+    CK(launch_atb(Vk, H, g, ld, k, c, T, st));
+    CK(launch_center_apply(Vk, g, ld, nullptr, nullptr, T, Proj, st));
+    CK(launch_cg_ap(P, H, Proj, evals, g, ld, c, Ap, st));
+    CK(launch_coldot(P, Ap, g, ld, c, pAp, st));
+    CK(launch_cg_step(X, R, P, Ap, rr, pAp, g, ld, c, st));
+    CK(launch_coldot(R, R, g, ld, c, rr_new, st));
+    CK(launch_cg_dir(P, R, rr, rr_new, g, ld, c, st));
+  }
+  CK(launch_axpy_cols(A, X, 1.0, g, ld, c, A, st));
+  // F = G + X~ A ; column sums of F and S ; column sums of D
+  apply_f(A);
+  colsum(Y, ld, ld, sY);
+  colsum(S, c, c, sS);
+  CK(launch_axpy_cols(sG, sY, 1.0, 1, ld, c, sF, st));
+  CK(launch_col_d(Vk, A, sF, sS, g, ld, c, pl->bw_colD.as<double>(), st));
+  // SDDMM at the stored entries, 64 columns at a time
+  for (int c0 = 0; c0 < c; c0 += 64) {
+    const int cs = std::min(64, c - c0);
+    CK(launch_sddmm(pl->dtype, pl->indptr, pl->idx, pl->val, n, (int32_t)g, pl->rbp.as<int32_t>(), pl->nb,
+                    pl->nchunks, pl->rows_per_chunk, GS + c0, c, Y + c0, ld, S + c0, c, Vk + c0, A + c0, ld, cs,
+                    pl->d_scale_raw.as<double>(), c0 > 0, gvals, pl->bw_part.as<double>(), st));
+    CK(launch_reduce_rows_f64(pl->bw_part.as<double>(), pl->nchunks, g, pl->bw_sumDP.as<double>(), c0 > 0, st,
+                              pl->num_sms));
+  }
+  if (gcenter || gscale)
+    CK(launch_grad_vectors(pl->bw_colD.as<double>(), pl->bw_sumDP.as<double>(), pl->d_center_raw.as<double>(),
+                           pl->d_scale_raw.as<double>(), g, gcenter, gscale, st));
+  CK(cudaStreamSynchronize(st));
+  check_tc_error(pl);
 }
 
 template <typename F>
@@ -843,6 +1020,35 @@ int32_t scxpca_plan_create(const scxpca_csr* x, const scxpca_params* params, scx
     validate_params(x, params);
     DeviceGuard dg(params->device_ordinal);
     *plan = create_plan(x, params);
+  });
+}
+
+int32_t scxpca_plan_create_affine(const scxpca_csr* x, const scxpca_params* params, const double* center,
+                                  const double* scale, int32_t vectors_memory, scxpca_plan** plan, char* err,
+                                  size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!plan) fail(SCXPCA_INVALID_ARGUMENT, "null plan output");
+    *plan = nullptr;
+    if (!params) fail(SCXPCA_INVALID_ARGUMENT, "null params");
+    if (params->scale != 0 || params->clip_max > 0)
+      fail(SCXPCA_INVALID_ARGUMENT, "explicit center/scale vectors replace params.scale and params.clip_max "
+                                    "(set scale = 0 and clip_max <= 0)");
+    if (vectors_memory != SCXPCA_MEM_HOST && vectors_memory != SCXPCA_MEM_DEVICE)
+      fail(SCXPCA_INVALID_ARGUMENT, "bad vectors_memory");
+    validate_params(x, params);
+    DeviceGuard dg(params->device_ordinal);
+    AffineSpec aff{center, scale, vectors_memory};
+    *plan = create_plan(x, params, &aff);
+  });
+}
+
+int32_t scxpca_plan_backward(scxpca_plan* plan, const float* scores, const float* grad_scores,
+                             int32_t solve_iterations, float* grad_values, double* grad_center, double* grad_scale,
+                             char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!plan) fail(SCXPCA_INVALID_ARGUMENT, "null plan");
+    DeviceGuard dg(plan->device);
+    backward(plan, scores, grad_scores, solve_iterations, grad_values, grad_center, grad_scale);
   });
 }
 
@@ -927,6 +1133,7 @@ int32_t scxpca_plan_matmat(scxpca_plan* plan, const float* v, int64_t ld_v, floa
     if (!plan || !v || !y) fail(SCXPCA_INVALID_ARGUMENT, "null argument");
     if (ld_v < plan->k || ld_y < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "leading dimension < k");
     DeviceGuard dg(plan->device);
+    plan->run_valid = false;
     cudaStream_t st = plan->stream;
     const int64_t ld = plan->ld;
     CK(cudaMemsetAsync(plan->V.p, 0, sizeof(float) * plan->g * ld, st));
@@ -948,6 +1155,7 @@ int32_t scxpca_plan_rmatmat(scxpca_plan* plan, const float* q, int64_t ld_q, dou
     if (!plan || !q || !z) fail(SCXPCA_INVALID_ARGUMENT, "null argument");
     if (ld_q < plan->k || ld_z < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "leading dimension < k");
     DeviceGuard dg(plan->device);
+    plan->run_valid = false;
     cudaStream_t st = plan->stream;
     const int64_t ld = plan->ld;
     CK(cudaMemsetAsync(plan->Y.p, 0, sizeof(float) * plan->n * ld, st));
@@ -974,6 +1182,7 @@ int32_t scxpca_plan_qr(scxpca_plan* plan, float* a, int64_t m, int64_t ld_a, cha
     if (ld_a < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "leading dimension < k");
     if (m < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "CholeskyQR2 requires m >= k");
     DeviceGuard dg(plan->device);
+    plan->run_valid = false;
     cudaStream_t st = plan->stream;
     const int64_t ld = plan->ld;
     const int shift = plan->params.qr_method == SCXPCA_QR_HOUSEHOLDER ? 1 : 0;

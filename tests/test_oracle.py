@@ -195,3 +195,69 @@ def test_bf16_rounding_helper():
     # bf16 spacing at 1 is 2^-7: 1 + 2^-8 is a tie and rounds to even (1.0)
     assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0
     assert np.all(np.abs(r - x) <= np.abs(x) * 2 ** -8)
+
+
+# --------------------------------------------------------------------------
+# truncated-SVD adjoint (oracle/adjoint.py): pinned against torch autograd
+# through torch.linalg.svd in FP64 and against central finite differences
+# --------------------------------------------------------------------------
+
+def _torch_reference_grads(ip, ix, vv, shape, center, scale, W, c):
+    import torch
+
+    n, g = shape
+    rows = torch.from_numpy(np.repeat(np.arange(n), np.diff(ip)))
+    cols = torch.from_numpy(ix.astype(np.int64))
+    v = torch.tensor(vv, dtype=torch.float64, requires_grad=True)
+    cen = torch.tensor(center, dtype=torch.float64, requires_grad=True)
+    sca = torch.tensor(scale, dtype=torch.float64, requires_grad=True)
+    X = torch.zeros((n, g), dtype=torch.float64).index_put((rows, cols), v, accumulate=True)
+    Xt = (X - cen[None, :]) * sca[None, :]
+    _, _, vh = torch.linalg.svd(Xt, full_matrices=False)
+    S = Xt @ vh[:c].T
+    loss = (torch.from_numpy(W) * S * S).sum()
+    loss.backward()
+    return v.grad.numpy(), cen.grad.numpy(), sca.grad.numpy()
+
+
+def test_adjoint_matches_torch_svd_autograd():
+    from oracle import adjoint as ad
+
+    ip, ix, vv = ad.planted_csr(80, 24, 8, 0.5, seed=3, top=50.0, ratio=0.85, noise=0.2)
+    shape = (80, 24)
+    rng = np.random.default_rng(0)
+    X = ad.dense(ip, ix, vv, shape)
+    center = X.mean(axis=0)
+    scale = 1.0 / (X.std(axis=0, ddof=1) + 0.5)
+    W = rng.standard_normal((80, 6))
+    gv, gc, gs = ad.grads(ip, ix, vv, shape, center, scale, W, 6)
+    tv, tc, ts = _torch_reference_grads(ip, ix, vv.astype(np.float64), shape, center, scale, W, 6)
+    for a, b in ((gv, tv), (gc, tc), (gs, ts)):
+        assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(b)
+
+
+def test_adjoint_matches_finite_differences():
+    from oracle import adjoint as ad
+
+    n, g, c = 60, 20, 5
+    ip, ix, vv = ad.planted_csr(n, g, 7, 0.6, seed=5, top=40.0, ratio=0.8, noise=0.1)
+    rng = np.random.default_rng(1)
+    X = ad.dense(ip, ix, vv, (n, g))
+    center = X.mean(axis=0)
+    scale = 1.0 / (X.std(axis=0, ddof=1) + 0.3)
+    W = rng.standard_normal((n, c))
+    gv, gc, gs = ad.grads(ip, ix, vv, (n, g), center, scale, W, c)
+    vv64 = vv.astype(np.float64)
+
+    def L(v, cen, sca):
+        return ad.loss(ad.affine(ad.dense(ip, ix, v, (n, g)), cen, sca), W, c)
+
+    eps = 1e-6
+    for _ in range(3):
+        dv, dc, ds = rng.standard_normal(len(vv)), rng.standard_normal(g), rng.standard_normal(g)
+        fd_v = (L(vv64 + eps * dv, center, scale) - L(vv64 - eps * dv, center, scale)) / (2 * eps)
+        fd_c = (L(vv64, center + eps * dc, scale) - L(vv64, center - eps * dc, scale)) / (2 * eps)
+        fd_s = (L(vv64, center, scale + eps * ds) - L(vv64, center, scale - eps * ds)) / (2 * eps)
+        assert abs(fd_v - gv @ dv) <= 1e-5 * max(1.0, abs(fd_v))
+        assert abs(fd_c - gc @ dc) <= 1e-5 * max(1.0, abs(fd_c))
+        assert abs(fd_s - gs @ ds) <= 1e-5 * max(1.0, abs(fd_s))
