@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-rows", type=int, default=50_000)
+    ap.add_argument("--no-backward", action="store_true", help="skip the differentiable-PCA leg")
     return ap.parse_args()
 
 
@@ -384,6 +385,9 @@ def run_ours(args):
     else:
         host_csr = (ip.cpu().numpy(), ix.cpu().numpy(), vv.cpu().numpy())
 
+    if not args.no_backward:
+        out["differentiable"] = differentiable_leg(args, local, dev)
+
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cpu_ms, sample_nnz, sample_s = cpu_baseline(*host_csr, n_obs, args.cpu_sample_rows, threads)
@@ -397,6 +401,59 @@ def run_ours(args):
     if rank == 0:
         print(json.dumps(out), flush=True)
     _finish_dist()
+
+
+DIFF_N_OBS = 200_000
+
+
+def differentiable_leg(args, local, dev):
+    """Forward vs backward of the differentiable scores on the 200,000 x 2,000
+    NB-synthetic CSR, FP32, 50 PCs, oversample 10, 4 power iterations, centred
+    on the column means and scaled by 1 / std (explicit per-gene vectors), loss
+    sum(W * S**2) with W a seeded N(0, 1) 200,000 x 50 matrix.  Both legs are
+    timed with CUDA events on the plan's stream over the same steps."""
+    import torch
+
+    from scx_b200 import accel
+
+    n, g = DIFF_N_OBS, N_VARS
+    ip, ix, vv = accel.synth_nb_csr_device(n, g, seed=SEED + 1, loc=LOC, dispersion=DISPERSION, device=local)
+    sums = torch.bincount(ix.long(), weights=vv.double(), minlength=g)
+    sq = torch.bincount(ix.long(), weights=vv.double() ** 2, minlength=g)
+    mean = sums / n
+    std = ((sq - n * mean * mean) / (n - 1)).clamp_min(0).sqrt()
+    scale = torch.where(std > 0, 1.0 / std, torch.ones_like(std))
+    stream = torch.cuda.Stream(device=dev)
+    gen = torch.Generator(device=dev).manual_seed(SEED)
+    W = torch.randn((n, N_COMPS), generator=gen, device=dev, dtype=torch.float32)
+    plan = accel.Plan(ip, ix, vv, (n, g), n_components=N_COMPS, n_oversamples=N_OVERSAMPLES,
+                      n_power_iterations=N_POWER, seed=SEED, qr_method="householder",
+                      math_mode="strict_fp32", device=local, stream=stream.cuda_stream,
+                      center=mean, gene_scale=scale)
+    S = torch.empty((n, N_COMPS), dtype=torch.float32, device=dev)
+    solve = 8
+    fwd_ms, bwd_ms = [], []
+    steps = max(2, min(args.steps, 5))
+    for i in range(args.warmup + steps):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        plan.run(embeddings_out=S)
+        e1.record(stream)
+        with torch.cuda.stream(stream):
+            G = 2.0 * W * S
+        plan.backward(S, G, solve)
+        e2.record(stream)
+        torch.cuda.synchronize(dev)
+        if i >= args.warmup:
+            fwd_ms.append(e0.elapsed_time(e1))
+            bwd_ms.append(e1.elapsed_time(e2))
+    plan.close()
+    f = statistics.median(fwd_ms)
+    b = statistics.median(bwd_ms)
+    return {"workload": f"{n:,} x {g:,} NB-synthetic CSR ({int(ix.numel()):,} nnz), FP32, 50 PCs, "
+                        "oversample 10, 4 power iterations, loss sum(W * S^2)",
+            "forward_ms": round(f, 3), "backward_ms": round(b, 3), "backward_over_forward": round(b / f, 3),
+            "solve_iterations": solve, "steps": steps}
 
 
 def _finish_dist():

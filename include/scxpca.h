@@ -222,6 +222,44 @@ int32_t scxpca_plan_rmatmat(scxpca_plan* plan, const float* q, int64_t ld_q, dou
 int32_t scxpca_plan_qr(scxpca_plan* plan, float* a, int64_t m, int64_t ld_a,
                        char* err, size_t err_len);
 
+/* Batched sub-PCAs: an independent randomized PCA of every row segment
+ * [segment_offsets[q], segment_offsets[q + 1]) of one CSR (cell clusters of
+ * uneven sizes), each centred on its own column means, with the same
+ * parameters.  Creation builds one resident plan per segment (device CSR
+ * slices are borrowed, not copied), runs every segment once with plain
+ * launches to measure it, and records all runs into ONE CUDA graph whose
+ * parallel branches take the segments in a longest-first schedule of the
+ * measured times; `branches` fixes the branch count (1..32) or, with 0, an
+ * autotuner times the graph for 1, 2, 4, ... 32 branches and keeps the
+ * fastest.  params->omega must be NULL (seeded) or device memory, and
+ * params->stream NULL (the batch owns its streams).  The reference runs one
+ * PCA per call (scx-gpu/src/gpu_pca.rs:706-763); a caller with clusters
+ * loops over it, which scxpca_batch_run with use_graph = 0 reproduces. */
+typedef struct scxpca_batch scxpca_batch;
+
+int32_t scxpca_batch_create(const scxpca_csr* x, const int64_t* segment_offsets, int64_t n_segments,
+                            const scxpca_params* params, int32_t branches, scxpca_batch** batch,
+                            char* err, size_t err_len);
+
+/* Run every segment: use_graph = 1 launches the recorded graph once;
+ * use_graph = 0 runs one plain, synchronising plan run per segment.
+ * embeddings: n_obs x n_components float32 row-major (each segment's rows in
+ * place), host or device per embeddings_memory.  Host outputs (any may be
+ * NULL): components [segment][n_components][n_vars] float32, singular_values
+ * / variance_ratio / variance_explained [segment][n_components] double.
+ * device_ms (may be NULL) receives the device time of the runs. */
+int32_t scxpca_batch_run(scxpca_batch* batch, int32_t use_graph, float* embeddings,
+                         int32_t embeddings_memory, float* components, double* singular_values,
+                         double* variance_ratio, double* variance_explained, double* device_ms,
+                         char* err, size_t err_len);
+
+/* Chosen branch count, graph node count, and the autotuner's timings in ms
+ * for 1, 2, 4, 8, 16, 32 branches (0 where not tried; 6 entries). */
+int32_t scxpca_batch_info(const scxpca_batch* batch, int32_t* branches, int64_t* graph_nodes,
+                          double* tuned_ms);
+
+void scxpca_batch_destroy(scxpca_batch* batch);
+
 /* Opt-in per-stage device timing (the counterpart of SCX_GPU_PROFILE,
  * scx-gpu/src/profile.rs:1-60, and the SpMM timing hook of
  * cusparse.rs:501-528).  When enabled, plan_run brackets each stage's kernels

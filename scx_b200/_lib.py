@@ -42,6 +42,10 @@ EXPORTED = (
     "scxpca_plan_destroy",
     "scxpca_plan_create_affine",
     "scxpca_plan_backward",
+    "scxpca_batch_create",
+    "scxpca_batch_run",
+    "scxpca_batch_info",
+    "scxpca_batch_destroy",
     "scxpca_plan_info",
     "scxpca_plan_matmat",
     "scxpca_plan_rmatmat",
@@ -150,6 +154,12 @@ def load() -> C.CDLL:
         "scxpca_plan_create_affine": (C.c_int32, [C.POINTER(Csr), C.POINTER(Params), P, P, C.c_int32,
                                                   C.POINTER(P), *E]),
         "scxpca_plan_backward": (C.c_int32, [P, P, P, C.c_int32, P, P, P, *E]),
+        "scxpca_batch_create": (C.c_int32, [C.POINTER(Csr), P, C.c_int64, C.POINTER(Params), C.c_int32,
+                                            C.POINTER(P), *E]),
+        "scxpca_batch_run": (C.c_int32, [P, C.c_int32, P, C.c_int32, P, P, P, P,
+                                         C.POINTER(C.c_double), *E]),
+        "scxpca_batch_info": (C.c_int32, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int64), P]),
+        "scxpca_batch_destroy": (None, [P]),
         "scxpca_plan_info": (C.c_int32, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                          C.POINTER(C.c_int64)]),
         "scxpca_plan_matmat": (C.c_int32, [P, P, C.c_int64, P, C.c_int64, *E]),

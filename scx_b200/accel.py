@@ -430,6 +430,72 @@ class Plan:
         return s, q
 
 
+class Batch:
+    """Independent randomized PCAs of the row segments of one CSR matrix
+    (scxpca_batch_*): one resident plan per segment, all runs recorded into a
+    single CUDA graph over parallel branches (``branches=0`` autotunes the
+    branch count).  ``run(use_graph=False)`` runs one plain plan call per
+    segment instead, the loop a caller of the one-PCA API would write."""
+
+    def __init__(self, indptr, indices, values, shape, segment_offsets, n_components: int = 30,
+                 n_oversamples: int = 10, n_power_iterations: int = 3, zero_center: bool = True,
+                 seed: int = 0, qr_method: str = "householder", math_mode: str = "mixed_bf16",
+                 device: int = 0, branches: int = 0):
+        self._lib = _lib.load()
+        csr, keep, mem, dev = _prepare_csr(indptr, indices, values, shape)
+        if dev is not None:
+            device = dev
+        self.device = int(device)
+        self.shape = (int(shape[0]), int(shape[1]))
+        self.n_components = int(n_components)
+        offs = np.ascontiguousarray(np.asarray(segment_offsets, dtype=np.int64))
+        self.offsets = offs
+        self.n_segments = len(offs) - 1
+        self._keep = keep
+        p = _params(n_components, n_oversamples, n_power_iterations, zero_center, False, None, seed,
+                    qr_method, math_mode, "default", device)
+        handle = C.c_void_p()
+        err = _lib.errbuf()
+        st = self._lib.scxpca_batch_create(C.byref(csr), _ptr(offs), self.n_segments, C.byref(p),
+                                           int(branches), C.byref(handle), err, len(err))
+        _lib.check(st, err)
+        self._h = handle
+        nb = C.c_int32()
+        nodes = C.c_int64()
+        tuned = np.zeros(6, dtype=np.float64)
+        self._lib.scxpca_batch_info(self._h, C.byref(nb), C.byref(nodes), _ptr(tuned))
+        self.branches, self.graph_nodes = int(nb.value), int(nodes.value)
+        self.tuned_ms = {b: float(t) for b, t in zip((1, 2, 4, 8, 16, 32), tuned) if t > 0}
+
+    def run(self, use_graph: bool = True, embeddings_out=None, components: bool = True):
+        """Returns (embeddings, components [seg, nc, n_vars] or None, singular values
+        [seg, nc], variance ratios [seg, nc], device ms)."""
+        n, g = self.shape
+        nc, ns = self.n_components, self.n_segments
+        emb = embeddings_out if embeddings_out is not None else np.empty((n, nc), dtype=np.float32)
+        mem = _lib.MEM_DEVICE if (_is_torch(emb) and emb.is_cuda) else _lib.MEM_HOST
+        comps = np.empty((ns, nc, g), dtype=np.float32) if components else None
+        sv = np.empty((ns, nc), dtype=np.float64)
+        vr = np.empty((ns, nc), dtype=np.float64)
+        ms = C.c_double()
+        err = _lib.errbuf()
+        st = self._lib.scxpca_batch_run(self._h, 1 if use_graph else 0, _ptr(emb), mem, _ptr(comps),
+                                        _ptr(sv), _ptr(vr), None, C.byref(ms), err, len(err))
+        _lib.check(st, err)
+        return emb, comps, sv, vr, float(ms.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.scxpca_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def gaussian(n_rows: int, n_cols: int, seed: int, device: int = 0):
     """Seeded N(0,1) test matrix (n_rows x n_cols) as a CUDA float32 tensor."""
     import torch

@@ -531,6 +531,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       pl->tc_err.alloc(sizeof(int) * 4);
       CK(cudaMemsetAsync(pl->tc_err.p, 0, sizeof(int) * 4, st));
       pl->tc_row_groups = rmat_tc_groups((int)ld, pl->n_chunks, pl->num_sms, &pl->tc_gene_groups);
+      pl->tc_row_groups = (int)std::min<int64_t>(pl->tc_row_groups, n_tiles);  // no idle row groups
       pl->tc_part.alloc(sizeof(float) * (size_t)pl->tc_row_groups * g * ld);
       int r1 = make_tmap16(&pl->vmap, pl->V16.p, g, ld, 64, pl->fmt16);
       int r4 = make_tmap16(&pl->vmap_lo, pl->V16lo.p, g, ld, 64, pl->fmt16);
@@ -751,9 +752,8 @@ void load_omega(scxpca_plan* pl, const scxpca_params* p) {
                            pl->mc.as<float>(), st));
 }
 
-void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
-  if (!out) fail(SCXPCA_INVALID_ARGUMENT, "null result");
-  if (!out->embeddings) fail(SCXPCA_INVALID_ARGUMENT, "null embeddings output");
+// Parameters of one run: the plan's, with the per-run overrides of `over`.
+scxpca_params run_params(const scxpca_plan* pl, const scxpca_params* over) {
   scxpca_params p = pl->params;
   if (over) {
     p.seed = over->seed;
@@ -762,13 +762,20 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
     p.n_power_iterations = over->n_power_iterations;
     if (p.n_power_iterations < 0) fail(SCXPCA_INVALID_ARGUMENT, "n_power_iterations must be >= 0");
   }
+  return p;
+}
+
+// Enqueue one run on the plan's stream: power loop, Rayleigh-Ritz step and
+// embeddings into the device buffer U (n_obs x n_components).  No host
+// synchronisation and, when omega is NULL or device memory, no allocation:
+// the sequence can be captured into a CUDA graph.
+void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
   cudaStream_t st = pl->stream;
   const int ld = (int)pl->ld;
   const int shift = p.qr_method == SCXPCA_QR_HOUSEHOLDER ? 1 : 0;
   const double* mu = pl->centered ? pl->d_mu.as<double>() : nullptr;
   double* sY = pl->G.as<double>() + (size_t)ld * ld;  // column sums follow the Gram
 
-  const int64_t launches0 = launches_total();
   CK(cudaMemsetAsync(pl->status.p, 0, sizeof(int) * 4, st));
   int s = stage_begin(pl);
   load_omega(pl, &p);
@@ -814,34 +821,17 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
                         pl->comps.as<float>(), pl->M_emb.as<float>(), st));
   stage_end(pl, SCXPCA_STAGE_SMALL, s);
   // Embeddings U = Q R2^{-1} E Sigma (first n_components).
-  float* U = out->embeddings;
-  const bool host_out = out->embeddings_memory != SCXPCA_MEM_DEVICE;
-  if (host_out) {
-    pl->U.alloc(sizeof(float) * pl->n * pl->nc);
-    U = pl->U.as<float>();
-  }
   s = stage_begin(pl);
   CK(launch_embed(pl->Y.as<float>(), pl->n, ld, (int)pl->k, pl->M_emb.as<float>(), (int)pl->nc, U, st,
                   pl->num_sms));
   stage_end(pl, SCXPCA_STAGE_EMBED, s);
-  pl->prof.kernel_launches += launches_total() - launches0;
-  pl->prof.runs += 1;
-  if (host_out)
-    CK(cudaMemcpyAsync(out->embeddings, U, sizeof(float) * pl->n * pl->nc, cudaMemcpyDeviceToHost, st));
+}
 
-  int hstatus[4];
-  std::vector<double> sigma(pl->k);
-  CK(cudaMemcpyAsync(hstatus, pl->status.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(sigma.data(), pl->sigma.p, sizeof(double) * pl->k, cudaMemcpyDeviceToHost, st));
-  if (out->components)
-    CK(cudaMemcpyAsync(out->components, pl->comps.p, sizeof(float) * pl->nc * pl->g,
-                       cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  collect_stages(pl);
-  check_tc_error(pl);
+// Host side of a finished run: the status words and singular values copied
+// back from the device -> the result record.
+void finish_result(scxpca_plan* pl, const int* hstatus, const double* sigma, scxpca_result* out) {
   if (hstatus[0] < 0)
     fail(SCXPCA_NOT_SPD, "CholeskyQR2 failed: non-SPD; retry with qr_method='householder'");
-
   const double denom = std::max<double>((double)pl->n - 1.0, 1.0);
   for (int64_t c = 0; c < pl->nc; ++c) {
     double ve = sigma[c] * sigma[c] / denom;
@@ -861,6 +851,37 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   out->eig_sweeps = hstatus[2];
   out->total_var = pl->total_var;
   pl->run_valid = true;
+}
+
+void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
+  if (!out) fail(SCXPCA_INVALID_ARGUMENT, "null result");
+  if (!out->embeddings) fail(SCXPCA_INVALID_ARGUMENT, "null embeddings output");
+  const scxpca_params p = run_params(pl, over);
+  cudaStream_t st = pl->stream;
+  float* U = out->embeddings;
+  const bool host_out = out->embeddings_memory != SCXPCA_MEM_DEVICE;
+  if (host_out) {
+    pl->U.alloc(sizeof(float) * pl->n * pl->nc);
+    U = pl->U.as<float>();
+  }
+  const int64_t launches0 = launches_total();
+  enqueue_run(pl, p, U);
+  pl->prof.kernel_launches += launches_total() - launches0;
+  pl->prof.runs += 1;
+  if (host_out)
+    CK(cudaMemcpyAsync(out->embeddings, U, sizeof(float) * pl->n * pl->nc, cudaMemcpyDeviceToHost, st));
+
+  int hstatus[4];
+  std::vector<double> sigma(pl->k);
+  CK(cudaMemcpyAsync(hstatus, pl->status.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(sigma.data(), pl->sigma.p, sizeof(double) * pl->k, cudaMemcpyDeviceToHost, st));
+  if (out->components)
+    CK(cudaMemcpyAsync(out->components, pl->comps.p, sizeof(float) * pl->nc * pl->g,
+                       cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  collect_stages(pl);
+  check_tc_error(pl);
+  finish_result(pl, hstatus, sigma.data(), out);
 }
 
 // ---------------------------------------------------------------------------
@@ -993,7 +1014,386 @@ int32_t guarded(char* err, size_t err_len, F&& f) {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Batched sub-PCAs: one resident plan per row segment of one CSR, all runs
+// recorded into one CUDA graph whose parallel branches each take a list of
+// segments, launched as a single graph; or, for comparison, one plain
+// (synchronising) plan run per segment.
+// ---------------------------------------------------------------------------
+struct scxpca_batch {
+  int device = 0;
+  cudaStream_t main = nullptr;
+  bool own_main = false;
+  std::vector<cudaStream_t> branch;   // fork streams of the capture
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
+  std::vector<scxpca_plan*> plans;     // one per segment
+  std::vector<int64_t> offsets;        // segment row offsets (n_segments + 1)
+  std::vector<DevBuf*> indptrs;        // rebased device indptr of each segment (owned)
+  std::vector<double> seg_ms;          // measured plain-run time of each segment (schedule weights)
+  int64_t n_obs = 0, n_vars = 0, nc = 0, k = 0;
+  DevBuf emb;                          // n_obs x n_components, written by the graph
+  int32_t* h_status = nullptr;         // pinned: [seg][4]
+  double* h_sigma = nullptr;           // pinned: [seg][k]
+  float* h_comps = nullptr;            // pinned: [seg][nc][n_vars]
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int branches = 0;
+  size_t graph_nodes = 0;
+  double tuned_ms[6] = {0, 0, 0, 0, 0, 0};  // graph time per tried branch count (1, 2, 4, 8, 16, 32)
+  scxpca_params params{};
+
+  ~scxpca_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (scxpca_plan* pl : plans) delete pl;
+    for (DevBuf* b : indptrs) delete b;
+    for (cudaStream_t st : branch) cudaStreamDestroy(st);
+    for (cudaEvent_t e : join) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (h_status) cudaFreeHost(h_status);
+    if (h_sigma) cudaFreeHost(h_sigma);
+    if (h_comps) cudaFreeHost(h_comps);
+    if (own_main && main) cudaStreamDestroy(main);
+  }
+};
+
+namespace {
+
+constexpr int kMaxBranches = 32;
+
+void batch_free_graph(scxpca_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->graph_nodes = 0;
+}
+
+// Longest-processing-time schedule of the segments over `nb` branches, by
+// their measured plain-run times; each branch runs its list in order.
+std::vector<std::vector<int>> batch_schedule(const scxpca_batch* b, int nb) {
+  const int ns = (int)b->plans.size();
+  std::vector<int> order(ns);
+  for (int i = 0; i < ns; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](int x, int y) { return b->seg_ms[x] > b->seg_ms[y]; });
+  std::vector<std::vector<int>> lists(nb);
+  std::vector<double> load(nb, 0.0);
+  for (int i : order) {
+    const int t = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    lists[t].push_back(i);
+    load[t] += b->seg_ms[i];
+  }
+  return lists;
+}
+
+// Record every segment's run (and the copies of its status, singular values
+// and components to pinned host memory) into one graph over `nb` branches.
+void batch_capture(scxpca_batch* b, int nb) {
+  batch_free_graph(b);
+  while ((int)b->branch.size() < nb) {
+    cudaStream_t st;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    b->branch.push_back(st);
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->join.push_back(e);
+  }
+  const auto lists = batch_schedule(b, nb);
+  const scxpca_params p = b->params;
+  CK(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeRelaxed));
+  try {
+    CK(cudaEventRecord(b->fork, b->main));
+    for (int t = 0; t < nb; ++t) {
+      cudaStream_t st = b->branch[t];
+      CK(cudaStreamWaitEvent(st, b->fork, 0));
+      for (int q : lists[t]) {
+        scxpca_plan* pl = b->plans[q];
+        pl->stream = st;
+        enqueue_run(pl, p, b->emb.as<float>() + b->offsets[q] * b->nc);
+        CK(cudaMemcpyAsync(b->h_status + 4 * q, pl->status.p, sizeof(int) * 3, cudaMemcpyDeviceToHost, st));
+        if (pl->use_tc)
+          CK(cudaMemcpyAsync(b->h_status + 4 * q + 3, pl->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(b->h_sigma + b->k * q, pl->sigma.p, sizeof(double) * pl->k, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(b->h_comps + (size_t)b->nc * b->n_vars * q, pl->comps.p,
+                           sizeof(float) * pl->nc * pl->g, cudaMemcpyDeviceToHost, st));
+      }
+      CK(cudaEventRecord(b->join[t], st));
+      CK(cudaStreamWaitEvent(b->main, b->join[t], 0));
+    }
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(b->main, &g);
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    for (scxpca_plan* pl : b->plans) pl->stream = b->main;
+    throw;
+  }
+  CK(cudaStreamEndCapture(b->main, &b->graph));
+  for (scxpca_plan* pl : b->plans) pl->stream = b->main;
+  CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  size_t nodes = 0;
+  CK(cudaGraphGetNodes(b->graph, nullptr, &nodes));
+  b->graph_nodes = nodes;
+  b->branches = nb;
+}
+
+// One graph launch; returns its device time in ms.
+double batch_launch_timed(scxpca_batch* b) {
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, b->main));
+  CK(cudaGraphLaunch(b->exec, b->main));
+  CK(cudaEventRecord(e1, b->main));
+  CK(cudaStreamSynchronize(b->main));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms;
+}
+
+// Host results of every segment after a graph launch (pinned buffers).
+void batch_collect(scxpca_batch* b, float* components, double* singular_values, double* variance_ratio,
+                   double* variance_explained) {
+  const int ns = (int)b->plans.size();
+  std::vector<double> ve(b->nc), vr(b->nc), sv(b->nc);
+  for (int q = 0; q < ns; ++q) {
+    scxpca_plan* pl = b->plans[q];
+    if (pl->use_tc && b->h_status[4 * q + 3] != 0)
+      fail(SCXPCA_TIMEOUT, "segment " + std::to_string(q) + ": tensor-core pipeline wait timed out (site " +
+                               std::to_string(b->h_status[4 * q + 3]) + ")");
+    scxpca_result r{};
+    r.variance_explained = ve.data();
+    r.variance_ratio = vr.data();
+    r.singular_values = sv.data();
+    try {
+      finish_result(pl, b->h_status + 4 * q, b->h_sigma + b->k * q, &r);
+    } catch (const Failure& f) {
+      fail(f.code, "segment " + std::to_string(q) + ": " + f.msg);
+    }
+    for (int64_t c = 0; c < b->nc; ++c) {
+      if (singular_values) singular_values[q * b->nc + c] = sv[c];
+      if (variance_ratio) variance_ratio[q * b->nc + c] = vr[c];
+      if (variance_explained) variance_explained[q * b->nc + c] = ve[c];
+    }
+  }
+  if (components) memcpy(components, b->h_comps, sizeof(float) * (size_t)ns * b->nc * b->n_vars);
+}
+
+// Plain reference execution: one synchronising plan run per segment.
+void batch_run_plain(scxpca_batch* b, float* emb_dev, float* components, double* singular_values,
+                     double* variance_ratio, double* variance_explained, bool record_times) {
+  const int ns = (int)b->plans.size();
+  std::vector<double> ve(b->nc), vr(b->nc), sv(b->nc);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (record_times) {
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+  }
+  for (int q = 0; q < ns; ++q) {
+    scxpca_plan* pl = b->plans[q];
+    scxpca_result r{};
+    r.embeddings = emb_dev + b->offsets[q] * b->nc;
+    r.embeddings_memory = SCXPCA_MEM_DEVICE;
+    r.components = components ? components + (size_t)q * b->nc * b->n_vars : nullptr;
+    r.variance_explained = ve.data();
+    r.variance_ratio = vr.data();
+    r.singular_values = sv.data();
+    if (record_times) CK(cudaEventRecord(e0, pl->stream));
+    try {
+      run_plan(pl, &b->params, &r);
+    } catch (const Failure& f) {
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+      fail(f.code, "segment " + std::to_string(q) + ": " + f.msg);
+    }
+    if (record_times) {
+      CK(cudaEventRecord(e1, pl->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      b->seg_ms[q] = ms;
+    }
+    for (int64_t c = 0; c < b->nc; ++c) {
+      if (singular_values) singular_values[q * b->nc + c] = sv[c];
+      if (variance_ratio) variance_ratio[q * b->nc + c] = vr[c];
+      if (variance_explained) variance_explained[q * b->nc + c] = ve[c];
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+}
+
+scxpca_batch* create_batch(const scxpca_csr* x, const int64_t* offsets, int64_t n_segments,
+                           const scxpca_params* p, int32_t branches) {
+  if (!x || !offsets || !p) fail(SCXPCA_INVALID_ARGUMENT, "null csr, offsets or params");
+  if (n_segments <= 0) fail(SCXPCA_INVALID_ARGUMENT, "n_segments must be > 0");
+  if (branches < 0 || branches > kMaxBranches)
+    fail(SCXPCA_INVALID_ARGUMENT, "branches must be in [0, " + std::to_string(kMaxBranches) + "] (0 = autotune)");
+  if (p->omega && p->omega_memory != SCXPCA_MEM_DEVICE)
+    fail(SCXPCA_INVALID_ARGUMENT, "a batch takes a device omega (or NULL for the seeded test matrix)");
+  if (p->stream) fail(SCXPCA_INVALID_ARGUMENT, "a batch owns its streams: params.stream must be NULL");
+  if (offsets[0] != 0 || offsets[n_segments] != x->n_obs)
+    fail(SCXPCA_INVALID_ARGUMENT, "segment offsets must start at 0 and end at n_obs");
+  for (int64_t q = 0; q < n_segments; ++q)
+    if (offsets[q + 1] <= offsets[q]) fail(SCXPCA_INVALID_ARGUMENT, "segment offsets must increase strictly");
+  auto b = new scxpca_batch();
+  try {
+    b->device = p->device_ordinal;
+    b->params = *p;
+    b->n_obs = x->n_obs;
+    b->n_vars = x->n_vars;
+    b->nc = p->n_components;
+    CK(cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking));
+    b->own_main = true;
+    CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    b->offsets.assign(offsets, offsets + n_segments + 1);
+    // indptr on the host, to cut and rebase per segment
+    std::vector<int64_t> ip(x->n_obs + 1);
+    if (x->memory == SCXPCA_MEM_DEVICE)
+      CK(cudaMemcpy(ip.data(), x->indptr, sizeof(int64_t) * (x->n_obs + 1), cudaMemcpyDeviceToHost));
+    else
+      memcpy(ip.data(), x->indptr, sizeof(int64_t) * (x->n_obs + 1));
+    const size_t vsz = dtype_size(x->values_dtype);
+    int64_t kmax = 0;
+    for (int64_t q = 0; q < n_segments; ++q) {
+      const int64_t r0 = offsets[q], r1 = offsets[q + 1], nq = r1 - r0;
+      const int64_t e0 = ip[r0], nnz_q = ip[r1] - ip[r0];
+      std::vector<int64_t> seg(nq + 1);
+      for (int64_t i = 0; i <= nq; ++i) seg[i] = ip[r0 + i] - e0;
+      scxpca_csr xs = *x;
+      xs.n_obs = nq;
+      xs.nnz = nnz_q;
+      if (x->memory == SCXPCA_MEM_DEVICE) {
+        auto* d = new DevBuf();
+        b->indptrs.push_back(d);
+        d->alloc(sizeof(int64_t) * (nq + 1));
+        CK(cudaMemcpy(d->p, seg.data(), sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice));
+        xs.indptr = d->as<int64_t>();
+      } else {
+        xs.indptr = seg.data();
+      }
+      xs.indices = x->indices + e0;
+      xs.values = static_cast<const char*>(x->values) + vsz * e0;
+      scxpca_params ps = *p;
+      ps.stream = b->main;
+      if (p->n_components > std::min(nq, x->n_vars))
+        fail(SCXPCA_INVALID_ARGUMENT, "segment " + std::to_string(q) + " has " + std::to_string(nq) +
+                                          " rows, fewer than n_components");
+      b->plans.push_back(create_plan(&xs, &ps));
+      kmax = std::max<int64_t>(kmax, b->plans.back()->k);
+    }
+    b->k = kmax;
+    b->seg_ms.assign(n_segments, 1.0);
+    b->emb.alloc(sizeof(float) * b->n_obs * b->nc);
+    CK(cudaMallocHost(&b->h_status, sizeof(int32_t) * 4 * n_segments));
+    memset(b->h_status, 0, sizeof(int32_t) * 4 * n_segments);
+    CK(cudaMallocHost(&b->h_sigma, sizeof(double) * b->k * n_segments));
+    CK(cudaMallocHost(&b->h_comps, sizeof(float) * (size_t)b->nc * b->n_vars * n_segments));
+    // measured per-segment times: one plain pass (warms every plan up too)
+    batch_run_plain(b, b->emb.as<float>(), nullptr, nullptr, nullptr, nullptr, true);
+    if (branches > 0) {
+      batch_capture(b, branches);
+    } else {
+      // autotune the branch count: time one launch of each candidate graph
+      double best = 0.0;
+      int best_nb = 1;
+      const int cands[6] = {1, 2, 4, 8, 16, 32};
+      for (int i = 0; i < 6; ++i) {
+        const int nb = cands[i];
+        if (nb > n_segments) break;
+        batch_capture(b, nb);
+        batch_launch_timed(b);  // warm
+        const double ms = batch_launch_timed(b);
+        b->tuned_ms[i] = ms;
+        if (i == 0 || ms < best) {
+          best = ms;
+          best_nb = nb;
+        }
+      }
+      if (b->branches != best_nb) batch_capture(b, best_nb);
+    }
+    return b;
+  } catch (...) {
+    delete b;
+    throw;
+  }
+}
+
+}  // namespace
+
 extern "C" {
+
+int32_t scxpca_batch_create(const scxpca_csr* x, const int64_t* segment_offsets, int64_t n_segments,
+                            const scxpca_params* params, int32_t branches, scxpca_batch** batch, char* err,
+                            size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!batch) fail(SCXPCA_INVALID_ARGUMENT, "null batch output");
+    *batch = nullptr;
+    if (!params) fail(SCXPCA_INVALID_ARGUMENT, "null params");
+    validate_params(x, params);
+    DeviceGuard dg(params->device_ordinal);
+    *batch = create_batch(x, segment_offsets, n_segments, params, branches);
+  });
+}
+
+int32_t scxpca_batch_run(scxpca_batch* batch, int32_t use_graph, float* embeddings, int32_t embeddings_memory,
+                         float* components, double* singular_values, double* variance_ratio,
+                         double* variance_explained, double* device_ms, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!batch) fail(SCXPCA_INVALID_ARGUMENT, "null batch");
+    if (!embeddings) fail(SCXPCA_INVALID_ARGUMENT, "null embeddings output");
+    DeviceGuard dg(batch->device);
+    scxpca_batch* b = batch;
+    const size_t bytes = sizeof(float) * b->n_obs * b->nc;
+    const cudaMemcpyKind kind =
+        embeddings_memory == SCXPCA_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, b->main));
+    if (use_graph) {
+      CK(cudaGraphLaunch(b->exec, b->main));
+      CK(cudaEventRecord(e1, b->main));
+      CK(cudaMemcpyAsync(embeddings, b->emb.p, bytes, kind, b->main));
+      CK(cudaStreamSynchronize(b->main));
+      batch_collect(b, components, singular_values, variance_ratio, variance_explained);
+    } else {
+      batch_run_plain(b, b->emb.as<float>(), components, singular_values, variance_ratio, variance_explained,
+                      false);
+      CK(cudaEventRecord(e1, b->main));
+      CK(cudaMemcpyAsync(embeddings, b->emb.p, bytes, kind, b->main));
+      CK(cudaStreamSynchronize(b->main));
+    }
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (device_ms) *device_ms = ms;
+  });
+}
+
+int32_t scxpca_batch_info(const scxpca_batch* batch, int32_t* branches, int64_t* graph_nodes,
+                          double* tuned_ms) {
+  if (!batch) return SCXPCA_INVALID_ARGUMENT;
+  if (branches) *branches = batch->branches;
+  if (graph_nodes) *graph_nodes = (int64_t)batch->graph_nodes;
+  if (tuned_ms)
+    for (int i = 0; i < 6; ++i) tuned_ms[i] = batch->tuned_ms[i];
+  return SCXPCA_OK;
+}
+
+void scxpca_batch_destroy(scxpca_batch* batch) {
+  if (!batch) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(batch->device);
+  cudaStreamSynchronize(batch->main);
+  delete batch;
+  if (prev >= 0) cudaSetDevice(prev);
+}
 
 const char* scxpca_status_string(int32_t s) {
   switch (s) {
