@@ -68,6 +68,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-rows", type=int, default=50_000)
     ap.add_argument("--no-backward", action="store_true", help="skip the differentiable-PCA leg")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched sub-PCA leg")
     return ap.parse_args()
 
 
@@ -387,6 +388,8 @@ def run_ours(args):
 
     if not args.no_backward:
         out["differentiable"] = differentiable_leg(args, local, dev)
+    if not args.no_batched:
+        out["batched"] = batched_leg(args, local, dev)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -454,6 +457,59 @@ def differentiable_leg(args, local, dev):
                         "oversample 10, 4 power iterations, loss sum(W * S^2)",
             "forward_ms": round(f, 3), "backward_ms": round(b, 3), "backward_over_forward": round(b / f, 3),
             "solve_iterations": solve, "steps": steps}
+
+
+BATCH_CLUSTERS = 256
+BATCH_LOC = -3.2  # ~9 % density
+
+
+def batched_leg(args, local, dev):
+    """256 cell clusters (sizes LogNormal(log 4000, 1.0) clipped to [500,
+    50,000], seed 0) of 2,000 genes, each cluster from the NB generator with
+    its own seed -- its own gene-mean profile -- at ~9 % density, BF16 values;
+    a centred 30-PC randomized PCA (oversample 10, 3 power iterations) per
+    cluster.  Times one launch of the batch's graph against the 256 plain
+    per-cluster launches, both on the device (CUDA events)."""
+    import numpy as np
+    import torch
+
+    from scx_b200 import accel
+
+    rng = np.random.default_rng(SEED)
+    sizes = np.clip(np.round(rng.lognormal(np.log(4000.0), 1.0, BATCH_CLUSTERS)), 500, 50_000).astype(np.int64)
+    ips, ixs, vvs, base = [torch.zeros(1, dtype=torch.int64, device=dev)], [], [], 0
+    for q, nq in enumerate(sizes):
+        ip, ix, vv = accel.synth_nb_csr_device(int(nq), N_VARS, seed=1000 + q, loc=BATCH_LOC,
+                                               dispersion=DISPERSION, device=local)
+        ips.append(ip[1:] + base)
+        base += int(ix.numel())
+        ixs.append(ix)
+        vvs.append(vv.to(torch.bfloat16))
+    ip, ix, vv = torch.cat(ips), torch.cat(ixs), torch.cat(vvs)
+    n = int(sizes.sum())
+    offs = np.r_[0, np.cumsum(sizes)]
+    b = accel.Batch(ip, ix, vv, (n, N_VARS), offs, n_components=30, n_oversamples=10, n_power_iterations=3,
+                    seed=SEED, math_mode="mixed_bf16", device=local, branches=0)
+    emb = torch.empty((n, 30), dtype=torch.float32, device=dev)
+    graph_ms, plain_ms = [], []
+    for i in range(2 + max(2, min(args.steps, 3))):
+        _, _, sv_g, _, ms = b.run(use_graph=True, embeddings_out=emb, components=False)
+        if i >= 2:
+            graph_ms.append(ms)
+    for i in range(1 + 2):
+        _, _, sv_p, _, ms = b.run(use_graph=False, embeddings_out=emb, components=False)
+        if i >= 1:
+            plain_ms.append(ms)
+    out = {"workload": f"{BATCH_CLUSTERS} clusters, {n:,} cells x {N_VARS:,} genes ({int(ix.numel()):,} nnz, "
+                       f"{int(ix.numel()) / (n * N_VARS):.3f} density), BF16, 30 PCs, oversample 10, q = 3",
+           "cluster_sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)), "max": int(sizes.max())},
+           "graph_ms": round(statistics.median(graph_ms), 3), "plain_launches_ms": round(statistics.median(plain_ms), 3),
+           "speedup_graph_vs_plain": round(statistics.median(plain_ms) / statistics.median(graph_ms), 3),
+           "branches": b.branches, "graph_nodes": b.graph_nodes,
+           "autotune_ms": {str(k): round(v, 3) for k, v in b.tuned_ms.items()},
+           "sigma_max_rel_diff_graph_vs_plain": float(np.max(np.abs(sv_g - sv_p) / sv_p))}
+    b.close()
+    return out
 
 
 def _finish_dist():
