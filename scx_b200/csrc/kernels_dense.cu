@@ -512,18 +512,22 @@ cudaError_t launch_round_v(const double* A, int64_t g, int ld, const double* mu,
 
 // ---------------------------------------------------------------------------
 // Parallel cyclic Jacobi (round-robin pairing) for the symmetric k x k block
-// of C.  A round rotates kk/2 disjoint pairs in three barrier-separated
-// phases: (0) one lane per pair computes the angle from the round's starting
-// A (the pairing of every round is tabulated once); (1) one warp per pair
-// rotates columns p, q of A and E (no other pair touches them); (2) one warp
-// per pair rotates rows p, q of A and sets the rotated 2 x 2 block to its
-// exact diagonal form (rounding would otherwise leave residues of order
-// eps * max(app, aqq) that keep the criterion below, relative to
-// sqrt(app aqq), from ever being met).  Matrices are row-major in shared
-// memory with an odd stride so column walks are free of bank conflicts; E
-// moves to global scratch when both do not fit.  Stops after a sweep with no
-// rotation (every off-diagonal entry below 1e-15 of the geometric mean of its
-// two diagonal entries) or after 40 sweeps.
+// of C.  A round rotates the kk/2 disjoint pairs of the round's tabulated
+// pairing at once, A <- J^T A J, in two barrier-separated phases:
+//   (0) one lane per pair computes the rotation of its pair from the round's
+//       starting A;
+//   (1) the pairs partition the index set, so J^T A J splits into
+//       independent 2 x 2 blocks: block (i, j) of A (rows p_i, q_i, columns
+//       p_j, q_j) becomes J_i^T A_ij J_j.  One thread per block updates it in
+//       place, and one thread per (row, pair) rotates the two columns of E.
+//       A rotated diagonal block is set to its exact diagonal form
+//       diag(app', aqq') (rounding would otherwise leave residues of order
+//       eps * max(app, aqq) that keep the criterion below, relative to
+//       sqrt(app aqq), from ever being met).
+// Matrices are row-major in shared memory (odd stride); E moves to global
+// scratch when both do not fit.  Stops after a sweep with no rotation (every
+// off-diagonal entry below 1e-15 of the geometric mean of its two diagonal
+// entries) or after 40 sweeps.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, int k, int ld,
                                                  double* __restrict__ evals, double* __restrict__ evecs,
@@ -537,7 +541,7 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, i
   double* E = (Eglob != nullptr) ? Eglob : sm + kk * S + (m * npair + 3) / 4;
   __shared__ double cs[kMaxK / 2], sn[kMaxK / 2], dpp[kMaxK / 2], dqq[kMaxK / 2];
   __shared__ int done;
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const int tid = threadIdx.x, nt = blockDim.x;
   for (int t = tid; t < kk * S; t += nt) {
     const int r = t / S, c = t - r * S;
     A[t] = (r < k && c < k) ? C[r * ld + c] : 0.0;
@@ -556,7 +560,7 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, i
   for (; sweep < 40; ++sweep) {
     for (int round = 0; round < m; ++round) {
       const uint16_t* pr = sched + round * npair;
-      // phase 0: angles, one lane per pair
+      // phase 0: rotations, one lane per pair
       for (int i = tid; i < npair; i += nt) {
         const int p = pr[i] & 0xff, q = pr[i] >> 8;
         double c = 1.0, s = 0.0, npp = 0.0, nqq = 0.0;
@@ -578,40 +582,39 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, i
         dqq[i] = nqq;
       }
       __syncthreads();
-      // phase 1: columns p, q of A and E
-      for (int i = warp; i < npair; i += nw) {
-        const double s = sn[i];
-        if (s == 0.0) continue;
-        const double c = cs[i];
-        const int p = pr[i] & 0xff, q = pr[i] >> 8;
-        for (int r = lane; r < kk; r += 32) {
-          const double xp = A[r * S + p], xq = A[r * S + q];
-          A[r * S + p] = c * xp - s * xq;
-          A[r * S + q] = s * xp + c * xq;
-          const double ep = E[r * S + p], eq = E[r * S + q];
-          E[r * S + p] = c * ep - s * eq;
-          E[r * S + q] = s * ep + c * eq;
+      // phase 1: every 2 x 2 block of A, and the column pairs of E
+      for (int b = tid; b < npair * npair; b += nt) {
+        const int i = b / npair, j = b - i * npair;
+        const double si = sn[i], sj = sn[j];
+        if (si == 0.0 && sj == 0.0) continue;
+        const int pi = pr[i] & 0xff, qi = pr[i] >> 8, pj = pr[j] & 0xff, qj = pr[j] >> 8;
+        if (i == j) {  // rotated diagonal block: exact diagonal form
+          A[pi * S + pi] = dpp[i];
+          A[qi * S + qi] = dqq[i];
+          A[pi * S + qi] = 0.0;
+          A[qi * S + pi] = 0.0;
+          continue;
         }
+        const double ci = cs[i], cj = cs[j];
+        double a00 = A[pi * S + pj], a01 = A[pi * S + qj], a10 = A[qi * S + pj], a11 = A[qi * S + qj];
+        // columns: [a.0 a.1] <- [c a.0 - s a.1, s a.0 + c a.1] with (cj, sj)
+        double t0 = cj * a00 - sj * a01, t1 = sj * a00 + cj * a01;
+        double u0 = cj * a10 - sj * a11, u1 = sj * a10 + cj * a11;
+        // rows: [a0. ; a1.] <- [c a0. - s a1. ; s a0. + c a1.] with (ci, si)
+        A[pi * S + pj] = ci * t0 - si * u0;
+        A[pi * S + qj] = ci * t1 - si * u1;
+        A[qi * S + pj] = si * t0 + ci * u0;
+        A[qi * S + qj] = si * t1 + ci * u1;
       }
-      __syncthreads();
-      // phase 2: rows p, q of A, then the exact 2 x 2 block
-      for (int i = warp; i < npair; i += nw) {
-        const double s = sn[i];
-        if (s == 0.0) continue;
-        const double c = cs[i];
+      for (int t = tid; t < kk * npair; t += nt) {
+        const int r = t / npair, i = t - r * npair;
+        const double si = sn[i];
+        if (si == 0.0) continue;
+        const double ci = cs[i];
         const int p = pr[i] & 0xff, q = pr[i] >> 8;
-        for (int col = lane; col < kk; col += 32) {
-          const double xp = A[p * S + col], xq = A[q * S + col];
-          A[p * S + col] = c * xp - s * xq;
-          A[q * S + col] = s * xp + c * xq;
-        }
-        __syncwarp();
-        if (lane == 0) {
-          A[p * S + p] = dpp[i];
-          A[q * S + q] = dqq[i];
-          A[p * S + q] = 0.0;
-          A[q * S + p] = 0.0;
-        }
+        const double ep = E[r * S + p], eq = E[r * S + q];
+        E[r * S + p] = ci * ep - si * eq;
+        E[r * S + q] = si * ep + ci * eq;
       }
       __syncthreads();
     }
@@ -653,9 +656,10 @@ cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, dou
     smem = one + sched;
   }
   cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int warps = std::min(32, std::max(1, kk / 2));
+  // one thread per 2 x 2 block of a round, up to a full block of threads
+  const int threads = std::min(1024, std::max(32, ((kk / 2) * (kk / 2) + 31) / 32 * 32));
   note_launches(1);
-  k_jacobi<<<1, 32 * warps, smem, st>>>(C, k, ld, evals, evecs, eglob, sweeps);
+  k_jacobi<<<1, threads, smem, st>>>(C, k, ld, evals, evecs, eglob, sweeps);
   return cudaGetLastError();
 }
 

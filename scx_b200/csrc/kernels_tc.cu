@@ -23,9 +23,9 @@
 // epilogue adds the two halves: about 16 mantissa bits on the dense operand,
 // the matrix values being the only operand rounded to 16 bits.
 //
-// Warp roles (23 warps): warps 0-15 densify in four groups of four; group g
-// takes every fourth stage (its own A buffers: two in the forward kernel, one
-// in the transposed kernel, whose stages are twice as large).  Each densify warp reads its
+// Warp roles (23 warps): warps 0-15 densify in four groups of four (forward:
+// group g takes every fourth stage into its own two A buffers; transposed: a
+// pair of groups fills the two sub-tiles of every other stage).  Each densify warp reads its
 // quarter of a segment straight from global memory with 16-byte loads (the
 // tile's entries were prefetched into L2 a tile ahead), keeping the loads of
 // its group's next segment in flight in registers while the current one is
@@ -60,10 +60,12 @@ struct SegMeta {
 };
 static_assert(sizeof(SegMeta) == 16, "segment metadata is one 16-byte record");
 
-// Pipeline shapes.  Densify group g takes the stages it with it % G == g.  In
-// the forward kernel it owns A stage buffers g and g + G (S == 2 G), so it
-// densifies its next segment while the MMAs read the previous one; in the
-// transposed kernel it owns buffer g (S == G).  Either way each waiter runs at
+// Pipeline shapes.  In the forward kernel densify group g takes the stages
+// it with it % G == g and owns A stage buffers g and g + G (S == 2 G), so it
+// densifies its next segment while the MMAs read the previous one.  In the
+// transposed kernel a stage (two 64-gene sub-tiles) is filled by a pair of
+// groups, one sub-tile each; pair p takes the stages it with it % 2 == p and
+// owns buffers p and p + 2 (S == 4 at ld 64).  Either way each waiter runs at
 // most one barrier phase ahead of the phase it waits for, which is what a
 // parity wait can distinguish.  The forward kernel's dense operand has its
 // own ring of fwd_bslots(LD) chunk buffers, filled ahead of the MMAs.
@@ -73,7 +75,7 @@ __host__ __device__ constexpr int rmat_stages(int LD) { return LD == 64 ? 4 : 2;
 // 16-byte entry words a densify lane keeps in flight per segment quarter
 // (x 128 entries per warp); a larger quarter loads the rest on demand.
 constexpr int kFwdRegs = 4;
-constexpr int kRmatRegs = 3;
+constexpr int kRmatRegs = 4;
 
 __host__ __device__ __forceinline__ int padded4(int x) { return (x + 3) & ~3; }
 
@@ -378,9 +380,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
           for (int i = 0; i < 16; ++i)
             o[i] = __uint_as_float(h[i]) + __uint_as_float(l[i]) - __ldg(mc + cb * 16 + i);
-          float4* yr = reinterpret_cast<float4*>(Y + grow * LD + cb * 16);
+          if (Y) {  // the FP32 copy only when the caller reads it
+            float4* yr = reinterpret_cast<float4*>(Y + grow * LD + cb * 16);
 #pragma unroll
-          for (int i = 0; i < 4; ++i) yr[i] = make_float4(o[4 * i], o[4 * i + 1], o[4 * i + 2], o[4 * i + 3]);
+            for (int i = 0; i < 4; ++i) yr[i] = make_float4(o[4 * i], o[4 * i + 1], o[4 * i + 2], o[4 * i + 3]);
+          }
           uint32_t ph16[8], pl16[8];
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
@@ -403,7 +407,13 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == W_MMA) {
     // ---- MMA issuer ----
     if (lane == 0) {
+      // The issue loop is the pipeline's critical path: descriptors are
+      // formed once and advanced by constant offsets (their address field is
+      // in 16-byte units; shared addresses stay below 256 KB, so no carry).
       const uint32_t idesc = idesc_f16(128, N2, fmt, 0, 1);
+      const uint64_t adesc0 = sdesc_sw128(smem_u32(As), 16, 1024);
+      const uint64_t bdesc0 = sdesc_sw128(smem_u32(Bs), CW * 128, 1024);
+      static_assert((S & (S - 1)) == 0 && (NB & (NB - 1)) == 0, "power-of-two rings");
       uint32_t it = 0, k = 0;
       for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++k) {
         const uint32_t a = k & 1u, ph = (k >> 1) & 1u;
@@ -419,12 +429,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           tc_fence_after();
-          const uint32_t a_base = smem_u32(As + s * A_BYTES);
-          const uint32_t b_base = smem_u32(Bs + b * B_BYTES);
+          const uint64_t ad = adesc0 + (uint64_t)(s * (A_BYTES >> 4));
+          const uint64_t bd = bdesc0 + (uint64_t)(b * (B_BYTES >> 4));
+          umma_f16(d, ad, bd, idesc, c != 0);
 #pragma unroll
-          for (int kk = 0; kk < CW / 16; ++kk)
-            umma_f16(d, sdesc_sw128(a_base + kk * 32, 16, 1024), sdesc_sw128(b_base + kk * 2048, CW * 128, 1024),
-                     idesc, (c | kk) != 0);
+          for (int kk = 1; kk < CW / 16; ++kk)  // K steps: +32 B along A's rows, +2 KB down B
+            umma_f16(d, ad + 2 * kk, bd + 128 * kk, idesc, 1u);
           umma_commit(&empty[s]);
           umma_commit(&bempty[b]);
         }
@@ -491,7 +501,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               int64_t g, int n_gene_groups, const __grid_constant__ CUtensorMap qmap_hi,
               const __grid_constant__ CUtensorMap qmap_lo, float* __restrict__ part, int fmt, int* err) {
   constexpr int N2 = 2 * LD;
-  constexpr int S = rmat_stages(LD);     // A stages == active densify groups
+  constexpr int S = rmat_stages(LD);     // A stages (even: two per pair of densify groups at ld 64)
   constexpr int SUB = TM * CW * 2;       // one 64-gene sub-tile, 16 KB
   constexpr int A_BYTES = 2 * SUB;       // 128 genes
   constexpr int Q_PLANE = TM * LD * 2;   // 128 cells x LD
@@ -525,14 +535,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
-      mbar_init(&full[s], 4);  // one arrival per warp of the stage's densify group
+      mbar_init(&full[s], 8);  // one arrival per warp of the stage's two densify groups
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&qfull[b], 1);
       mbar_init(&qempty[b], 1);
       mbar_init(&mfull[b], 1);
-      mbar_init(&mempty[b], 4 * S);
+      mbar_init(&mempty[b], 4 * kGroups);
     }
     mbar_init(done_bar, 1);
     *abort_flag = 0;
@@ -548,34 +558,33 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp < W_EPI) {
-    // ---- densify: group (warp / 4) takes super-chunk stages it % S == group ----
+    // ---- densify: a stage (128-gene super-chunk) is split over a pair of
+    // groups, one 64-gene sub-tile each: group g fills sub-tile g & 1 of the
+    // stages it with it % 2 == g >> 1, so each pair owns every other stage
+    // buffer and has its next stage in hand while the MMAs read this one ----
     const int group = warp >> 2, q = warp & 3;
-    if (group >= S) goto done;  // spare warps of a narrower configuration
+    const int h = group & 1, pg = group >> 1;
     uint32_t it = 0, ti = 0;
-    uint4 w0[kRmatRegs], w1[kRmatRegs];
-    Span pre0{-1, -1}, pre1{-1, -1};  // spans whose loads are in flight in w0 / w1
+    uint4 w[kRmatRegs];
+    Span pre{-1, -1};  // span whose loads are in flight in w
     if (have_work)
       for (int64_t t = t0; t < t1; ++t, ++ti) {
         if (!warp_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 21)) goto done;
         const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
         for (int sc = sc0; sc < sc1; ++sc, ++it) {
-          if ((int)(it % S) != group) continue;
-          const bool two = 2 * sc + 1 < nc;
-          const Span s0 = quarter_span(mt[2 * sc], q);
-          const Span s1 = two ? quarter_span(mt[2 * sc + 1], q) : Span{s0.hi, s0.hi};
-          if (s0.lo != pre0.lo || s0.hi != pre0.hi) span_load<kRmatRegs>(ent, s0, lane, w0);
-          if (s1.lo != pre1.lo || s1.hi != pre1.hi) span_load<kRmatRegs>(ent, s1, lane, w1);
+          if ((int)(it & 1u) != pg) continue;
+          const int ch = 2 * sc + h;
+          const Span sp = ch < nc ? quarter_span(mt[ch], q) : Span{0, 0};
+          if (sp.lo != pre.lo || sp.hi != pre.hi) span_load<kRmatRegs>(ent, sp, lane, w);
           const int s = it % S;
           if (!warp_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 22)) goto done;
-          const uint32_t tile = smem_u32(As + s * A_BYTES);
+          const uint32_t tile = smem_u32(As + s * A_BYTES) + h * SUB;
           zero_rows(tile, q, lane);
-          zero_rows(tile + SUB, q, lane);
           __syncwarp();
-          span_scatter<kRmatRegs>(tile, ent, s0, lane, w0);
-          span_scatter<kRmatRegs>(tile + SUB, ent, s1, lane, w1);
-          // the group's next stage: super-chunk sc + S of this tile, or of the next
-          pre0 = pre1 = Span{-1, -1};
-          const int scn = sc + S;
+          span_scatter<kRmatRegs>(tile, ent, sp, lane, w);
+          // the pair's next stage: super-chunk sc + 2 of this tile, or of the next
+          pre = Span{-1, -1};
+          const int scn = sc + 2;
           const SegMeta* mn = nullptr;
           int scx = 0;
           if (scn < sc1) {
@@ -586,11 +595,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             mn = mring + ((ti + 1) & 1u) * kMaxChunks;
             scx = scn - nsc;
           }
-          if (mn) {
-            pre0 = quarter_span(mn[2 * scx], q);
-            pre1 = 2 * scx + 1 < nc ? quarter_span(mn[2 * scx + 1], q) : Span{pre0.hi, pre0.hi};
-            span_load<kRmatRegs>(ent, pre0, lane, w0);
-            span_load<kRmatRegs>(ent, pre1, lane, w1);
+          if (mn && 2 * scx + h < nc) {
+            pre = quarter_span(mn[2 * scx + h], q);
+            span_load<kRmatRegs>(ent, pre, lane, w);
           }
           fence_proxy_async_smem();
           __syncwarp();
@@ -633,7 +640,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == W_MMA) {
     // ---- MMA issuer ----
     if (lane == 0 && have_work) {
+      // descriptors formed once and advanced by constant offsets (see k_fwd_tc)
       const uint32_t idesc = idesc_f16(128, N2, fmt, 1, 1);
+      const uint64_t adesc0 = sdesc_sw128(smem_u32(As), SUB, 1024);
+      const uint64_t qdesc0 = sdesc_sw128(smem_u32(Qs), TM * 128, 1024);
       uint32_t it = 0, ti = 0;
       bool ok = true;
       for (int64_t t = t0; t < t1 && ok; ++t, ++ti) {
@@ -643,7 +653,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t qh = smem_u32(Qs + b * Q_BYTES);
+        const uint64_t qd = qdesc0 + (uint64_t)(b * (Q_BYTES >> 4));
         for (int sc = sc0; sc < sc1; ++sc, ++it) {
           const int s = it % S;
           if (!mbar_wait(&full[s], (it / S) & 1u, abort_flag, err, 26)) {
@@ -651,12 +661,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             break;
           }
           tc_fence_after();
-          const uint32_t a_base = smem_u32(As + s * A_BYTES);
+          const uint64_t ad = adesc0 + (uint64_t)(s * (A_BYTES >> 4));
           const uint32_t d = tmem + (sc - sc0) * N2;
+          umma_f16(d, ad, qd, idesc, ti != 0);
 #pragma unroll
-          for (int kk = 0; kk < TM / 16; ++kk)
-            umma_f16(d, sdesc_sw128(a_base + kk * 2048, SUB, 1024), sdesc_sw128(qh + kk * 2048, TM * 128, 1024),
-                     idesc, (ti | kk) != 0);
+          for (int kk = 1; kk < TM / 16; ++kk)  // K steps of 16 cells: +2 KB down both operands
+            umma_f16(d, ad + 128 * kk, qd + 128 * kk, idesc, 1u);
           umma_commit(&empty[s]);
         }
         if (!ok) break;

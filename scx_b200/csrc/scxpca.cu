@@ -12,7 +12,8 @@
 // stored FP32 Y; inside the loop Q = Y R^{-1} stays implicit
 // (Z = (X^T Y - mu (1^T Y)^T) R^{-1}), and the last Q is formed explicitly
 // and re-orthonormalised (second Cholesky pass folded into B and the
-// embeddings) before the final projection.  qr(Z) is CholeskyQR2 in FP64.
+// embeddings) before the final projection.  qr(Z) is one CholeskyQR pass in
+// FP64.
 // The SVD of B is an FP64 Jacobi eigendecomposition of B^T B on the device.
 #include <algorithm>
 #include <atomic>
@@ -651,17 +652,19 @@ void tall_chol(scxpca_plan* pl, const float* A, int64_t rows, double* Rinv, floa
 }
 
 // CholeskyQR2 of a gene-side FP64 matrix in place.
+// One CholeskyQR pass.  The Gram and the triangular apply are both FP64, so the
+// loss of orthogonality is about cond(A)^2 * 1e-16: the second pass of
+// CholeskyQR2, which repairs a Gram formed in working precision, is not needed
+// on this FP64 gene-side matrix (the tall FP32 Q keeps its second pass).
 void small_qr(scxpca_plan* pl, double* A, int shift) {
   cudaStream_t st = pl->stream;
   const int ld = (int)pl->ld;
-  for (int pass = 0; pass < 2; ++pass) {
-    CK(launch_gram_f64(A, pl->g, ld, pl->gpart.as<double>(), pl->gram_parts_small, st));
-    CK(launch_reduce_rows_f64(pl->gpart.as<double>(), pl->gram_parts_small, (int64_t)ld * ld + ld,
-                              pl->G.as<double>(), 0, st, pl->num_sms));
-    CK(launch_cholesky(pl->G.as<double>(), (int)pl->k, ld, pl->tau, shift, pl->R.as<double>(),
-                       pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), pl->status.as<int>(), st));
-    CK(launch_apply_right_f64(A, pl->g, ld, pl->Rinv.as<double>(), st));
-  }
+  CK(launch_gram_f64(A, pl->g, ld, pl->gpart.as<double>(), pl->gram_parts_small, st));
+  CK(launch_reduce_rows_f64(pl->gpart.as<double>(), pl->gram_parts_small, (int64_t)ld * ld + ld,
+                            pl->G.as<double>(), 0, st, pl->num_sms));
+  CK(launch_cholesky(pl->G.as<double>(), (int)pl->k, ld, pl->tau, shift, pl->R.as<double>(),
+                     pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), pl->status.as<int>(), st));
+  CK(launch_apply_right_f64(A, pl->g, ld, pl->Rinv.as<double>(), st));
 }
 
 // W = X^T A (raw, uncentred), FP64, for a tall float A (n x ld).
@@ -700,8 +703,10 @@ void rmatmat_raw(scxpca_plan* pl, float* A, int split) {
 }
 
 // Y = (X - mu) V.  On the tensor-core path V enters as hi/lo 16-bit planes and
-// the product also leaves the hi/lo planes of Y for the transposed product.
-void forward(scxpca_plan* pl) {
+// the product also leaves the hi/lo planes of Y for the Gram and the
+// transposed product; `f32` = false skips the FP32 copy of Y when nothing
+// reads it (inside the power loop at ld 64, whose Gram uses the planes).
+void forward(scxpca_plan* pl, bool f32 = true) {
   cudaStream_t st = pl->stream;
   if (pl->use_tc) {
     int s = stage_begin(pl);
@@ -710,7 +715,7 @@ void forward(scxpca_plan* pl) {
     stage_end(pl, SCXPCA_STAGE_SMALL, s);
     s = stage_begin(pl);
     CK(launch_fwd_tc((int)pl->ld, pl->tf_ent.as<uint32_t>(), pl->tf_meta.p, pl->n, pl->n_chunks, &pl->vmap,
-                     &pl->vmap_lo, pl->mc.as<float>(), pl->Y.as<float>(), pl->Y16.as<uint16_t>(),
+                     &pl->vmap_lo, pl->mc.as<float>(), f32 ? pl->Y.as<float>() : nullptr, pl->Y16.as<uint16_t>(),
                      pl->Q16lo.as<uint16_t>(), pl->fmt16, pl->tc_err.as<int>(), st, pl->num_sms));
     stage_end(pl, SCXPCA_STAGE_FORWARD, s);
     return;
@@ -780,8 +785,11 @@ void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
   int s = stage_begin(pl);
   load_omega(pl, &p);
   stage_end(pl, SCXPCA_STAGE_SMALL, s);
-  // Y = (X - mu) Omega ; qr(Y)
-  forward(pl);
+  // Y = (X - mu) Omega ; qr(Y).  Only the last forward product's FP32 Y is
+  // read (by the explicit Q below); the tensor-core Gram at ld 64 reads the
+  // 16-bit planes.
+  const bool planes_only = pl->use_tc && ld == 64;
+  forward(pl, !planes_only || p.n_power_iterations == 0);
   tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
   for (int64_t it = 0; it < p.n_power_iterations; ++it) {
     // Z = (X - mu)^T Q = (X^T Y - mu (1^T Y)) R^{-1}
@@ -792,7 +800,7 @@ void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
     small_qr(pl, pl->Z.as<double>(), shift);
     CK(launch_round_v(pl->Z.as<double>(), pl->g, ld, mu, pl->V.as<float>(), pl->mc.as<float>(), st));
     stage_end(pl, SCXPCA_STAGE_SMALL, s);
-    forward(pl);
+    forward(pl, !planes_only || it + 1 == p.n_power_iterations);
     tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
   }
   // Explicit Q = Y R^{-1}, re-orthonormalised by a second FP64 Cholesky pass.
