@@ -26,6 +26,38 @@ template <> __device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(flo
 }
 template <> __device__ __forceinline__ __half from_f32<__half>(float x) { return __float2half_rn(x); }
 
+// FP64 reciprocal and reciprocal square root by Newton-Raphson iteration
+// (y <- y (2 - x y) and y <- y (3 - x y^2) / 2; each step doubles the correct
+// bits) from a single-precision hardware seed.  The argument is first scaled
+// by a power of two into [1, 2) (reciprocal) or [1, 4) (rsqrt), so the seed
+// never overflows or underflows; two steps reach double precision.  For the
+// short dependent chains of the small eigensolver and Cholesky kernels, where
+// the division and square-root library sequences dominate the latency.
+// Arguments must be positive, finite and normal.
+__device__ __forceinline__ double pow2_int(int k) {  // 2^k for k in [-1022, 1023]
+  return __longlong_as_double((long long)(k + 1023) << 52);
+}
+__device__ __forceinline__ int exponent_of(double x) {  // floor(log2 x) for normal x > 0
+  return (int)((__double_as_longlong(x) >> 52) & 0x7ff) - 1023;
+}
+__device__ __forceinline__ double rcp_nr(double x) {
+  const int e = exponent_of(x);
+  const double xs = x * pow2_int(-e);  // [1, 2)
+  double y = (double)__frcp_rn((float)xs);
+  y = y * fma(-xs, y, 2.0);
+  y = y * fma(-xs, y, 2.0);
+  return y * pow2_int(-e);
+}
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  const int h = exponent_of(x) >> 1;
+  const double xs = x * pow2_int(-2 * h);  // [1, 4)
+  double y = (double)rsqrtf((float)xs);
+  const double hx = 0.5 * xs;
+  y = y * fma(-hx, y * y, 1.5);
+  y = y * fma(-hx, y * y, 1.5);
+  return y * pow2_int(-h);
+}
+
 // Grid size for a grid-stride loop over `work` items at `per_block` items per
 // block: a multiple of the SM count, never more blocks than there is work.
 inline int grid_for(int64_t work, int per_block, int num_sms, int blocks_per_sm = 8) {

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
       const bool ok = isfinite(d) && d > 0.0 && (attempt == 1 || d > tau * (dg[j] + shift));
       pv_ok[j] = ok ? 1 : 0;
       if (ok) {
-        const double rinv = rsqrt(d);
+        const double rinv = d >= 1e-300 ? rsqrt_nr(d) : rsqrt(d);
         pv_rinv[j] = rinv;
         pv_di[j] = rinv * rinv;
       }
@@ -511,41 +511,54 @@ cudaError_t launch_round_v(const double* A, int64_t g, int ld, const double* mu,
 }
 
 // ---------------------------------------------------------------------------
-// Parallel cyclic Jacobi (round-robin pairing) for the symmetric k x k block
-// of C.  A round rotates the kk/2 disjoint pairs of the round's tabulated
-// pairing at once, A <- J^T A J, in two barrier-separated phases:
-//   (0) one lane per pair computes the rotation of its pair from the round's
-//       starting A;
-//   (1) the pairs partition the index set, so J^T A J splits into
-//       independent 2 x 2 blocks: block (i, j) of A (rows p_i, q_i, columns
-//       p_j, q_j) becomes J_i^T A_ij J_j.  One thread per block updates it in
-//       place, and one thread per (row, pair) rotates the two columns of E.
-//       A rotated diagonal block is set to its exact diagonal form
-//       diag(app', aqq') (rounding would otherwise leave residues of order
-//       eps * max(app, aqq) that keep the criterion below, relative to
-//       sqrt(app aqq), from ever being met).
-// Matrices are row-major in shared memory (odd stride); E moves to global
-// scratch when both do not fit.  Stops after a sweep with no rotation (every
-// off-diagonal entry below 1e-15 of the geometric mean of its two diagonal
-// entries) or after 40 sweeps.
+// Symmetric eigendecomposition of the k x k block of C (SPD up to rounding:
+// C = B^T B) by one-sided (Hestenes) Jacobi on its Cholesky factor.
+//   1. C = R^T R (FP64, right-looking, in shared memory; a pivot below
+//      1e-300 or 1e-15 of the largest diagonal is clamped there -- those are
+//      null directions of C, whose eigenvalues are zero to working accuracy).
+//   2. Rotate pairs of columns of R from the right until all columns are
+//      mutually orthogonal: R J_1 J_2 ... = U Sigma, V = J_1 J_2 ...; then
+//      C = V Sigma^2 V^T, eigenvalue i = |column i|^2.
+//   3. V is not accumulated rotation by rotation (that doubles the FP64
+//      work of every round): it is recovered once as V = R0^{-1} (R0 V) by
+//      back substitution against the Cholesky factor R0, and its columns are
+//      renormalised.  Its error is about cond(R0) * 1e-16 = sqrt(cond(C)) *
+//      1e-16.
+// A round takes the kk/2 disjoint column pairs of a round-robin schedule;
+// a half-warp owns one pair (a warp serves two pairs with the same shuffle
+// instructions): the cross product p.q is a 16-lane partial reduced by
+// shuffles, every lane of the half computes the same rotation, and the half
+// rotates its two columns of R and of V.  Column norms are carried in closed
+// form (a' = a - t c, b' = b + t c for the rotation that zeroes c) and
+// recomputed at the start of every sweep.  Pairs are disjoint, so a round
+// needs one block barrier.  Columns are stored contiguously (column-major,
+// odd stride) so a column walk is conflict-free.  Stops after a sweep with no
+// rotation (|p.q| <= 1e-15 |p| |q| for every pair, or |p.q| <= 1e-150), after
+// a sweep whose largest rotation tangent is below 1e-8 (convergence is
+// quadratic: the next sweep would rotate by less than 1e-16), or after 40
+// sweeps.  FP64 issue bandwidth (one warp instruction per ~4 cycles per SM
+// sub-partition) bounds a round, so the work per round is kept minimal.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, int k, int ld,
                                                  double* __restrict__ evals, double* __restrict__ evecs,
                                                  double* __restrict__ Eglob, int* sweeps_out) {
   extern __shared__ double sm[];
-  const int kk = (k + 1) & ~1;  // even number of players; index k (if odd) is a dummy
+  const int kk = (k + 1) & ~1;  // even number of columns; column k (if odd) is a zero dummy
   const int S = kk + 1;
   const int npair = kk / 2, m = kk - 1;
-  double* A = sm;  // [kk][S]
+  double* R = sm;                                              // [kk cols][S]: R[c * S + r]
   uint16_t* sched = reinterpret_cast<uint16_t*>(sm + kk * S);  // [m][npair]: p | q << 8
-  double* E = (Eglob != nullptr) ? Eglob : sm + kk * S + (m * npair + 3) / 4;
-  __shared__ double cs[kMaxK / 2], sn[kMaxK / 2], dpp[kMaxK / 2], dqq[kMaxK / 2];
+  double* V = (Eglob != nullptr) ? Eglob : sm + kk * S + (m * npair + 3) / 4;  // [kk cols][S]: R0, then V
+  __shared__ double colnorm[kMaxK];
   __shared__ int done;
-  const int tid = threadIdx.x, nt = blockDim.x;
+  __shared__ unsigned long long maxt_bits;  // largest |t| of the sweep (non-negative doubles order as integers)
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const int hl = lane & 15, half = lane >> 4;  // lane within the half-warp, which half
+  const unsigned hmask = half ? 0xffff0000u : 0x0000ffffu;
+  // R starts as the upper triangle of C (column-major)
   for (int t = tid; t < kk * S; t += nt) {
-    const int r = t / S, c = t - r * S;
-    A[t] = (r < k && c < k) ? C[r * ld + c] : 0.0;
-    E[t] = (r == c) ? 1.0 : 0.0;
+    const int c = t / S, r = t - c * S;
+    R[t] = (r < k && c < k && r <= c) ? C[r * ld + c] : 0.0;
   }
   for (int t = tid; t < m * npair; t += nt) {
     const int round = t / npair, i = t - round * npair;
@@ -554,86 +567,140 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, i
     else { a = (round + i) % m; b = (round - i + m) % m; }
     sched[t] = (uint16_t)(min(a, b) | (max(a, b) << 8));
   }
-  if (tid == 0) done = 1;
   __syncthreads();
+  // ---- Cholesky in place (upper triangle, right-looking).  Every thread reads
+  // pivot j; the diagonal entry itself is written one step later (by thread
+  // 0), when nobody reads it any more. ----
+  double dmax = 0.0;
+  for (int j = 0; j < k; ++j) dmax = fmax(dmax, R[j * S + j]);
+  double prev_diag = 0.0;
+  for (int j = 0; j < k; ++j) {
+    double d = R[j * S + j];
+    if (!(d > 1e-15 * dmax) || !(d > 1e-300)) d = fmax(1e-15 * dmax, 1e-300);
+    const double rd = rsqrt_nr(d);
+    if (tid == 0 && j > 0) R[(j - 1) * S + (j - 1)] = prev_diag;
+    prev_diag = d * rd;
+    for (int c = j + 1 + tid; c < k; c += nt) R[c * S + j] *= rd;  // row j, right of the diagonal
+    __syncthreads();
+    // trailing update: R[a][c] -= R[j][a] R[j][c] for j < a <= c (column c by a
+    // warp, row a by a lane)
+    for (int c = j + 1 + warp; c < k; c += nw) {
+      const double rjc = R[c * S + j];
+      for (int a = j + 1 + lane; a <= c; a += 32) R[c * S + a] -= R[a * S + j] * rjc;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (k > 0) R[(k - 1) * S + (k - 1)] = prev_diag;
+    done = 1;
+    maxt_bits = 0ull;
+  }
+  __syncthreads();
+  // R0, kept for the back substitution; a unit diagonal for the dummy column
+  // (odd k) keeps it invertible
+  for (int t = tid; t < kk * S; t += nt) V[t] = (k < kk && t == k * S + k) ? 1.0 : R[t];
+  __syncthreads();
+  // ---- one-sided Jacobi on the columns of R ----
   int sweep = 0;
   for (; sweep < 40; ++sweep) {
+    // column norms from scratch once per sweep (a half-warp per column)
+    for (int col = 2 * warp + half; col < kk; col += 2 * nw) {
+      double a = 0.0;
+      for (int r = hl; r < kk; r += 16) a = fma(R[col * S + r], R[col * S + r], a);
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) a += __shfl_xor_sync(hmask, a, o);
+      if (hl == 0) colnorm[col] = a;
+    }
+    __syncthreads();
     for (int round = 0; round < m; ++round) {
       const uint16_t* pr = sched + round * npair;
-      // phase 0: rotations, one lane per pair
-      for (int i = tid; i < npair; i += nt) {
+      for (int i = 2 * warp + half; i < npair; i += 2 * nw) {
         const int p = pr[i] & 0xff, q = pr[i] >> 8;
-        double c = 1.0, s = 0.0, npp = 0.0, nqq = 0.0;
-        if (q < k) {
-          const double apq = A[p * S + q], app = A[p * S + p], aqq = A[q * S + q];
-          if (fabs(apq) > 1e-300 && fabs(apq) > 1e-15 * sqrt(fabs(app * aqq))) {
-            const double theta = (aqq - app) / (2.0 * apq);
-            const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-            c = rsqrt(t * t + 1.0);
-            s = t * c;
-            npp = app - t * apq;  // the rotated 2 x 2 block is diag(npp, nqq)
-            nqq = aqq + t * apq;
-            done = 0;
-          }
+        double* rp = R + p * S;
+        double* rq = R + q * S;
+        double c = 0.0;
+        for (int r = hl; r < kk; r += 16) c = fma(rp[r], rq[r], c);
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) c += __shfl_xor_sync(hmask, c, o);
+        const double a = colnorm[p], b = colnorm[q];
+        if (!(fabs(c) > 1e-150 && c * c > 1e-30 * a * b)) continue;  // uniform over the half-warp
+        // t = tan of the angle that zeroes p.q: the smaller root of
+        // t^2 + 2 zeta t - 1 = 0, zeta = (b - a) / 2c, written as
+        // 2c sgn(tau) / (|tau| + sqrt(tau^2 + 4c^2)) with tau = b - a.  The
+        // angle only sets how much of p.q a rotation removes, so t is formed
+        // in FP32 (inputs scaled by a power of two into range); the rotation
+        // itself stays exactly orthogonal in FP64: cs = 1 / sqrt(1 + t^2),
+        // sn = t cs.  Near convergence |t| is tiny and its FP32 relative error
+        // leaves a residual below 1e-7 |p.q|, cleared by the next sweep.
+        const double sc = pow2_int(-exponent_of(a + b));
+        const float tf = (float)((b - a) * sc), cf = (float)(2.0 * c * sc);
+        const float den = fabsf(tf) + sqrtf(fmaf(tf, tf, cf * cf));
+        const double t = (double)(__fdividef(tf >= 0.f ? cf : -cf, den));
+        if (t == 0.0) continue;  // below FP32 resolution: nothing to rotate
+        const double cs = rsqrt_nr(fma(t, t, 1.0)), sn = t * cs;
+        for (int r = hl; r < kk; r += 16) {
+          const double xp = rp[r], xq = rq[r];
+          rp[r] = cs * xp - sn * xq;
+          rq[r] = sn * xp + cs * xq;
         }
-        cs[i] = c;
-        sn[i] = s;
-        dpp[i] = npp;
-        dqq[i] = nqq;
-      }
-      __syncthreads();
-      // phase 1: every 2 x 2 block of A, and the column pairs of E
-      for (int b = tid; b < npair * npair; b += nt) {
-        const int i = b / npair, j = b - i * npair;
-        const double si = sn[i], sj = sn[j];
-        if (si == 0.0 && sj == 0.0) continue;
-        const int pi = pr[i] & 0xff, qi = pr[i] >> 8, pj = pr[j] & 0xff, qj = pr[j] >> 8;
-        if (i == j) {  // rotated diagonal block: exact diagonal form
-          A[pi * S + pi] = dpp[i];
-          A[qi * S + qi] = dqq[i];
-          A[pi * S + qi] = 0.0;
-          A[qi * S + pi] = 0.0;
-          continue;
+        if (hl == 0) {
+          const double cc = cs * cs, ss = sn * sn, x2 = 2.0 * cs * sn * c;
+          colnorm[p] = fma(cc, a, fma(ss, b, -x2));
+          colnorm[q] = fma(ss, a, fma(cc, b, x2));
+          done = 0;
+          atomicMax(&maxt_bits, (unsigned long long)__double_as_longlong(fabs(t)));
         }
-        const double ci = cs[i], cj = cs[j];
-        double a00 = A[pi * S + pj], a01 = A[pi * S + qj], a10 = A[qi * S + pj], a11 = A[qi * S + qj];
-        // columns: [a.0 a.1] <- [c a.0 - s a.1, s a.0 + c a.1] with (cj, sj)
-        double t0 = cj * a00 - sj * a01, t1 = sj * a00 + cj * a01;
-        double u0 = cj * a10 - sj * a11, u1 = sj * a10 + cj * a11;
-        // rows: [a0. ; a1.] <- [c a0. - s a1. ; s a0. + c a1.] with (ci, si)
-        A[pi * S + pj] = ci * t0 - si * u0;
-        A[pi * S + qj] = ci * t1 - si * u1;
-        A[qi * S + pj] = si * t0 + ci * u0;
-        A[qi * S + qj] = si * t1 + ci * u1;
-      }
-      for (int t = tid; t < kk * npair; t += nt) {
-        const int r = t / npair, i = t - r * npair;
-        const double si = sn[i];
-        if (si == 0.0) continue;
-        const double ci = cs[i];
-        const int p = pr[i] & 0xff, q = pr[i] >> 8;
-        const double ep = E[r * S + p], eq = E[r * S + q];
-        E[r * S + p] = ci * ep - si * eq;
-        E[r * S + q] = si * ep + ci * eq;
       }
       __syncthreads();
     }
-    const int converged = done;
-    __syncthreads();  // every thread has read the flag before it is reset
+    const int converged = done || __longlong_as_double((long long)maxt_bits) < 1e-8;
+    __syncthreads();  // every thread has read the flags before they are reset
     if (converged) break;
-    if (tid == 0) done = 1;
+    if (tid == 0) {
+      done = 1;
+      maxt_bits = 0ull;
+    }
     __syncthreads();
   }
-  // sort eigenvalues descending: rank of each by counting (ties by index)
+  // eigenvalues: squared column norms of R0 V
+  for (int col = 2 * warp + half; col < kk; col += 2 * nw) {
+    double a = 0.0;
+    for (int r = hl; r < kk; r += 16) a = fma(R[col * S + r], R[col * S + r], a);
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) a += __shfl_xor_sync(hmask, a, o);
+    if (hl == 0) colnorm[col] = a;
+  }
+  // V = R0^{-1} (R0 V): back substitution, one column per thread, then unit columns
+  __syncthreads();
+  for (int c = tid; c < kk; c += nt) {
+    double* rc = R + c * S;  // column c of R0 V, overwritten by column c of V
+    for (int r = kk - 1; r >= 0; --r) {
+      double x = rc[r];
+      for (int j = r + 1; j < kk; ++j) x = fma(-V[j * S + r], rc[j], x);
+      rc[r] = x * rcp_nr(V[r * S + r]);
+    }
+  }
+  __syncthreads();
+  // unit eigenvector columns (the squared norms of R0 V's columns, the
+  // eigenvalues, were taken before the back substitution)
+  for (int i = warp; i < kk; i += nw) {
+    double a = 0.0;
+    for (int r = lane; r < kk; r += 32) a = fma(R[i * S + r], R[i * S + r], a);
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    a = __shfl_sync(0xffffffffu, a, 0);
+    const double inv = a > 0.0 ? rsqrt_nr(a) : 0.0;
+    for (int r = lane; r < kk; r += 32) R[i * S + r] *= inv;
+  }
+  __syncthreads();
   for (int i = tid; i < k; i += nt) {
-    const double v = A[i * S + i];
+    const double v = colnorm[i];
     int rank = 0;
     for (int j = 0; j < k; ++j) {
-      const double w = A[j * S + j];
+      const double w = colnorm[j];
       if (w > v || (w == v && j < i)) ++rank;
     }
     evals[rank] = v;
-    for (int r = 0; r < ld; ++r) evecs[r * ld + rank] = (r < k) ? E[r * S + i] : 0.0;
+    for (int r = 0; r < ld; ++r) evecs[r * ld + rank] = (r < k) ? R[i * S + r] : 0.0;
   }
   for (int t = tid; t < ld * ld; t += nt) {
     const int c = t % ld;
@@ -647,7 +714,7 @@ cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, dou
   const int kk = (k + 1) & ~1;
   const size_t one = (size_t)kk * (kk + 1) * sizeof(double);
   const size_t sched = ((size_t)(kk - 1) * (kk / 2) + 3) / 4 * sizeof(double);
-  // E lives in shared memory when both matrices fit, else in the scratch that
+  // V lives in shared memory when both matrices fit, else in the scratch that
   // follows evecs (the plan allocates ld * ld + ld * (ld + 1) doubles there).
   double* eglob = nullptr;
   size_t smem = 2 * one + sched;
@@ -656,10 +723,9 @@ cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, dou
     smem = one + sched;
   }
   cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  // one thread per 2 x 2 block of a round, up to a full block of threads
-  const int threads = std::min(1024, std::max(32, ((kk / 2) * (kk / 2) + 31) / 32 * 32));
+  const int warps = std::min(32, std::max(1, (kk / 2 + 1) / 2));  // one half-warp per column pair
   note_launches(1);
-  k_jacobi<<<1, threads, smem, st>>>(C, k, ld, evals, evecs, eglob, sweeps);
+  k_jacobi<<<1, 32 * warps, smem, st>>>(C, k, ld, evals, evecs, eglob, sweeps);
   return cudaGetLastError();
 }
 
