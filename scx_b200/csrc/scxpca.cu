@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -76,30 +77,125 @@ struct DeviceGuard {
   }
 };
 
+// Device memory of the plans comes from one stream-ordered pool per device
+// that keeps what is freed (release threshold: unlimited), so a plan built
+// after another one reuses its memory without mapping pages again, and
+// freeing costs a stream operation instead of a device-wide cudaFree.  Every
+// pooled allocation and free is ordered on one allocation stream per device
+// (so freed blocks are always reusable by the next allocation), fenced
+// against the stream that uses the memory by events.  The pool's memory
+// stays reserved by the process until it exits.
+struct DevicePool {
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t st = nullptr;  // allocation stream
+};
+
+DevicePool& pool_for(int dev) {
+  static std::mutex mu;
+  static DevicePool pools[256];
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev < 0 || dev >= 256) fail(SCXPCA_INVALID_ARGUMENT, "device ordinal out of range");
+  DevicePool& dp = pools[dev];
+  if (!dp.pool) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    CK(cudaMemPoolCreate(&dp.pool, &props));
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(dp.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    CK(cudaStreamCreateWithFlags(&dp.st, cudaStreamNonBlocking));
+  }
+  return dp;
+}
+
+// Order `to` after the work enqueued so far on `from`.
+void stream_fence(cudaStream_t from, cudaStream_t to) {
+  cudaEvent_t e;
+  CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CK(cudaEventRecord(e, from));
+  CK(cudaStreamWaitEvent(to, e, 0));
+  cudaEventDestroy(e);
+}
+
+// Allocation context of the calling thread: DevBufs allocated inside a
+// PoolScope come from the device's pool and are used on the scope's stream.
+struct AllocCtx {
+  DevicePool* dp = nullptr;
+  cudaStream_t use = nullptr;
+};
+thread_local AllocCtx t_alloc;
+
+struct PoolScope {
+  AllocCtx prev;
+  PoolScope(int dev, cudaStream_t use) : prev(t_alloc) { t_alloc = AllocCtx{&pool_for(dev), use}; }
+  ~PoolScope() { t_alloc = prev; }
+};
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  DevicePool* dp = nullptr;   // pool of a pooled allocation
+  cudaStream_t st = nullptr;  // stream the pooled memory is used on
+  bool pooled = false;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (pooled) {  // after the work already enqueued on the using stream
+        cudaEvent_t e;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) {
+          cudaEventRecord(e, st);
+          cudaStreamWaitEvent(dp->st, e, 0);
+          cudaEventDestroy(e);
+        }
+        cudaFreeAsync(p, dp->st);
+      } else {
+        cudaFree(p);
+      }
+    }
     p = nullptr;
     bytes = 0;
+    pooled = false;
   }
   void alloc(size_t b) {
     if (b <= bytes && p) return;
     release();
     if (b == 0) b = 16;
-    cudaError_t e = cudaMalloc(&p, b);
+    cudaError_t e;
+    if (t_alloc.dp) {
+      e = cudaMallocFromPoolAsync(&p, b, t_alloc.dp->pool, t_alloc.dp->st);
+      if (e == cudaSuccess) {
+        dp = t_alloc.dp;
+        st = t_alloc.use;
+        pooled = true;
+        stream_fence(dp->st, st);  // the using stream starts after the allocation
+      }
+    } else {
+      e = cudaMalloc(&p, b);
+    }
     if (e != cudaSuccess) {
       cudaGetLastError();
       p = nullptr;
+      pooled = false;
       fail(SCXPCA_OUT_OF_MEMORY, "device allocation of " + std::to_string(b) + " bytes failed: " +
                                      cudaGetErrorString(e));
     }
     bytes = b;
+  }
+  // take over another buffer's memory
+  void adopt(DevBuf& o) {
+    release();
+    p = o.p;
+    bytes = o.bytes;
+    dp = o.dp;
+    st = o.st;
+    pooled = o.pooled;
+    o.p = nullptr;
+    o.bytes = 0;
+    o.pooled = false;
   }
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
@@ -326,6 +422,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       pl->own_stream = true;
     }
     cudaStream_t st = pl->stream;
+    PoolScope pool_scope(pl->device, st);
     const int64_t n = pl->n, g = pl->g, nnz = pl->nnz;
 
     // ---- pre-flight (gpu_pca.rs:450-462): resident CSR + work buffers ----
@@ -336,6 +433,13 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
                     (size_t)g * ldp * 4 * 400;
       size_t fr = 0, tot = 0;
       CK(cudaMemGetInfo(&fr, &tot));
+      {  // memory our pool holds but does not use is free for this plan
+        uint64_t reserved = 0, used = 0;
+        cudaMemPool_t pool = pool_for(pl->device).pool;
+        CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+        CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+        if (reserved > used) fr += (size_t)(reserved - used);
+      }
       double with_headroom = (double)need * 1.1;
       if (with_headroom > (double)fr)
         fail(SCXPCA_OUT_OF_MEMORY, "GPU PCA requires ~" + std::to_string((size_t)with_headroom >> 20) +
@@ -435,10 +539,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       pl->val = vin;
       if (!dev_in || vin != x->values) {
         // vin is our staging buffer: keep it
-        pl->b_val.p = pl->b_stage.p;
-        pl->b_val.bytes = pl->b_stage.bytes;
-        pl->b_stage.p = nullptr;
-        pl->b_stage.bytes = 0;
+        pl->b_val.adopt(pl->b_stage);
         pl->val = pl->b_val.p;
       }
       pl->col_sum = sx;
@@ -587,8 +688,11 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
                        pl->W.bytes + pl->Z.bytes + pl->V.bytes;
     return pl;
   } catch (...) {
-    if (pl->own_stream && pl->stream) cudaStreamDestroy(pl->stream);
+    // the buffers are freed in the stream's order: delete the plan first
+    const bool own = pl->own_stream;
+    cudaStream_t st = pl->stream;
     delete pl;
+    if (own && st) cudaStreamDestroy(st);
     throw;
   }
 }
@@ -1054,8 +1158,10 @@ struct scxpca_batch {
   ~scxpca_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+    // buffers are freed in the order of the main stream: before it goes
     for (scxpca_plan* pl : plans) delete pl;
     for (DevBuf* b : indptrs) delete b;
+    emb.release();
     for (cudaStream_t st : branch) cudaStreamDestroy(st);
     for (cudaEvent_t e : join) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
@@ -1258,6 +1364,7 @@ scxpca_batch* create_batch(const scxpca_csr* x, const int64_t* offsets, int64_t 
     b->own_main = true;
     CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
     b->offsets.assign(offsets, offsets + n_segments + 1);
+    PoolScope pool_scope(b->device, b->main);
     // indptr on the host, to cut and rebase per segment
     std::vector<int64_t> ip(x->n_obs + 1);
     if (x->memory == SCXPCA_MEM_DEVICE)
@@ -1456,6 +1563,7 @@ int32_t scxpca_plan_backward(scxpca_plan* plan, const float* scores, const float
   return guarded(err, err_len, [&] {
     if (!plan) fail(SCXPCA_INVALID_ARGUMENT, "null plan");
     DeviceGuard dg(plan->device);
+    PoolScope pool_scope(plan->device, plan->stream);
     backward(plan, scores, grad_scores, solve_iterations, grad_values, grad_center, grad_scale);
   });
 }
@@ -1478,6 +1586,7 @@ int32_t scxpca_plan_run(scxpca_plan* plan, const scxpca_params* params, scxpca_r
   return guarded(err, err_len, [&] {
     if (!plan) fail(SCXPCA_INVALID_ARGUMENT, "null plan");
     DeviceGuard dg(plan->device);
+    PoolScope pool_scope(plan->device, plan->stream);
     run_plan(plan, params, out);
   });
 }
@@ -1513,6 +1622,7 @@ int32_t scxpca_randomized(const scxpca_csr* x, const scxpca_params* params, scxp
     validate_params(x, params);
     DeviceGuard dg(params->device_ordinal);
     scxpca_plan* pl = create_plan(x, params);
+    PoolScope pool_scope(pl->device, pl->stream);
     try {
       run_plan(pl, nullptr, out);
     } catch (...) {
@@ -1528,6 +1638,7 @@ int32_t scxpca_plan_col_stats(scxpca_plan* plan, double* col_sums, double* col_s
   return guarded(err, err_len, [&] {
     if (!plan) fail(SCXPCA_INVALID_ARGUMENT, "null plan");
     DeviceGuard dg(plan->device);
+    PoolScope pool_scope(plan->device, plan->stream);
     std::vector<double> s, q;
     stats_pass(plan, plan->val, plan->dtype, s, q);
     if (col_sums) memcpy(col_sums, s.data(), sizeof(double) * plan->g);
@@ -1541,6 +1652,7 @@ int32_t scxpca_plan_matmat(scxpca_plan* plan, const float* v, int64_t ld_v, floa
     if (!plan || !v || !y) fail(SCXPCA_INVALID_ARGUMENT, "null argument");
     if (ld_v < plan->k || ld_y < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "leading dimension < k");
     DeviceGuard dg(plan->device);
+    PoolScope pool_scope(plan->device, plan->stream);
     plan->run_valid = false;
     cudaStream_t st = plan->stream;
     const int64_t ld = plan->ld;
@@ -1563,6 +1675,7 @@ int32_t scxpca_plan_rmatmat(scxpca_plan* plan, const float* q, int64_t ld_q, dou
     if (!plan || !q || !z) fail(SCXPCA_INVALID_ARGUMENT, "null argument");
     if (ld_q < plan->k || ld_z < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "leading dimension < k");
     DeviceGuard dg(plan->device);
+    PoolScope pool_scope(plan->device, plan->stream);
     plan->run_valid = false;
     cudaStream_t st = plan->stream;
     const int64_t ld = plan->ld;
@@ -1590,6 +1703,7 @@ int32_t scxpca_plan_qr(scxpca_plan* plan, float* a, int64_t m, int64_t ld_a, cha
     if (ld_a < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "leading dimension < k");
     if (m < plan->k) fail(SCXPCA_INVALID_ARGUMENT, "CholeskyQR2 requires m >= k");
     DeviceGuard dg(plan->device);
+    PoolScope pool_scope(plan->device, plan->stream);
     plan->run_valid = false;
     cudaStream_t st = plan->stream;
     const int64_t ld = plan->ld;
