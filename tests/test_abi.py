@@ -111,3 +111,30 @@ def test_python_layer_maps_statuses():
         _lib.check(_lib.INVALID_ARGUMENT, C.create_string_buffer(b"n_components must be > 0"))
     with pytest.raises(_lib.ScxPcaError, match="non-SPD"):
         _lib.check(_lib.NOT_SPD, C.create_string_buffer(b"CholeskyQR2 failed: non-SPD"))
+
+
+def test_new_entry_points_reject_bad_arguments_without_a_device():
+    """Null handles and contradictory arguments of the affine, backward and
+    batch entry points return INVALID_ARGUMENT before any device call."""
+    lib = _lib.load()
+    err = _lib.errbuf()
+    assert lib.scxpca_plan_backward(None, None, None, 8, None, None, None, err, len(err)) == _lib.INVALID_ARGUMENT
+    assert lib.scxpca_batch_run(None, 1, None, 0, None, None, None, None, None, err, len(err)) == _lib.INVALID_ARGUMENT
+    assert lib.scxpca_batch_info(None, None, None, None) == _lib.INVALID_ARGUMENT
+    lib.scxpca_batch_destroy(None)  # no-op
+    indptr = np.array([0, 1, 2, 3], dtype=np.int64)
+    idx = np.array([0, 1, 2], dtype=np.int32)
+    val = np.ones(3, dtype=np.float32)
+    csr = _lib.Csr(3, 3, 3, indptr.ctypes.data, idx.ctypes.data, val.ctypes.data, _lib.F32, _lib.MEM_HOST)
+    p = _lib.Params()
+    p.n_components, p.n_oversamples, p.scale = 1, 1, 1
+    h = C.c_void_p()
+    st = lib.scxpca_plan_create_affine(C.byref(csr), C.byref(p), None, None, _lib.MEM_HOST, C.byref(h), err,
+                                       len(err))
+    assert st == _lib.INVALID_ARGUMENT and b"replace params.scale" in err.value
+    p.scale = 0
+    st = lib.scxpca_plan_create_affine(C.byref(csr), C.byref(p), None, None, 9, C.byref(h), err, len(err))
+    assert st == _lib.INVALID_ARGUMENT and b"vectors_memory" in err.value
+    offs = np.array([0, 3], dtype=np.int64)
+    st = lib.scxpca_batch_create(C.byref(csr), offs.ctypes.data, 1, C.byref(p), 99, C.byref(h), err, len(err))
+    assert st != _lib.OK  # bad branch count (or no device here): never a crash
