@@ -66,7 +66,8 @@ def parse():
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 comparison leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-rows", type=int, default=50_000)
+    ap.add_argument("--cpu-sample-rows", type=int, default=None,
+                    help="rows of the CPU-baseline sample (default: all rows for ours, 50,000 for --impl reference)")
     ap.add_argument("--no-backward", action="store_true", help="skip the differentiable-PCA leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched sub-PCA leg")
     return ap.parse_args()
@@ -393,12 +394,14 @@ def run_ours(args):
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cpu_ms, sample_nnz, sample_s = cpu_baseline(*host_csr, n_obs, args.cpu_sample_rows, threads)
+        sample_rows = args.cpu_sample_rows or n_obs
+        cpu_ms, sample_nnz, sample_s = cpu_baseline(*host_csr, n_obs, sample_rows, threads)
         out["cpu_baseline"] = {
             "value": round(cpu_ms, 1), "unit": "ms", "cores": threads, "kind": "port",
-            "sample": f"first {min(args.cpu_sample_rows, n_obs):,} rows ({sample_nnz:,} nnz) of the "
-                      f"same matrix, FP64 C++ restatement of the reference CPU randomized PCA, "
-                      f"{sample_s:.2f} s, scaled by rows to {n_obs:,}",
+            "sample": (f"the whole matrix ({sample_nnz:,} nnz)" if sample_rows >= n_obs else
+                       f"first {sample_rows:,} rows ({sample_nnz:,} nnz) of the same matrix, scaled by "
+                       f"rows to {n_obs:,}") +
+                      f", FP64 C++ restatement of the reference CPU randomized PCA, {sample_s:.2f} s",
         }
 
     if rank == 0:
@@ -529,7 +532,7 @@ def run_reference(args):
 
     from scx_b200.synth import synth_nb_csr
 
-    rows = min(args.cpu_sample_rows, args.n_obs)
+    rows = min(args.cpu_sample_rows or 50_000, args.n_obs)
     ip, ix, vv = synth_nb_csr(rows, N_VARS, seed=SEED, loc=LOC, dispersion=DISPERSION)
     threads = os.cpu_count() or 1
     times = []
