@@ -231,10 +231,64 @@ def cpu_baseline(indptr, indices, values, n_full: int, rows: int, threads: int):
     om = rpca.gaussian_omega(N_VARS, k, SEED)
     build_cpu.load()
     t0 = time.perf_counter()
-    build_cpu.run(ip, ix, vv, (rows, N_VARS), N_COMPS, k, N_POWER, om, zero_center=True,
-                  scale=True, clip_max=CLIP, threads=threads)
+    res = build_cpu.run(ip, ix, vv, (rows, N_VARS), N_COMPS, k, N_POWER, om, zero_center=True,
+                        scale=True, clip_max=CLIP, threads=threads)
     dt = time.perf_counter() - t0
-    return dt * 1e3 * (n_full / rows), nnz, dt
+    return dt * 1e3 * (n_full / rows), nnz, dt, res
+
+
+SUBSAMPLE_ROWS = 50_000
+
+
+def precision_report(ours: dict, fp64_full: dict | None, sub_ours: dict, sub_csr) -> dict:
+    """Singular-value and principal-angle error of the GPU results against the
+    FP64 randomized result on the whole matrix (the C++ restatement, same
+    seeded Omega) and against the exact FP64 PCA of a 50,000-cell subsample
+    (dense Gram eigendecomposition of the same scaled, clipped, centred
+    matrix).  Checker only: nothing here is timed."""
+    import numpy as np
+
+    from oracle import rpca
+
+    def cmp(sv, comps, ref_sv, ref_comps):
+        sv = np.asarray(sv, dtype=np.float64)
+        rel = np.abs(sv - ref_sv) / ref_sv
+        a = np.asarray(comps, dtype=np.float64).T
+        b = np.asarray(ref_comps, dtype=np.float64).T
+        ang = rpca.per_component_angles(a, b)
+        return {"sigma_max_rel_err": float(rel.max()), "sigma_max_rel_err_top10": float(rel[:10].max()),
+                "angle_max_rad_top10": float(ang[:10].max()),
+                "subspace_angle_max_rad_top50": float(rpca.principal_angles(a, b).max())}
+
+    out = {}
+    if fp64_full is not None:
+        out["vs_fp64_randomized_full"] = {m: cmp(r["sv"], r["comps"], fp64_full["singular_values"],
+                                                 fp64_full["components"]) for m, r in ours.items()}
+    ip, ix, vv = sub_csr
+    n = len(ip) - 1
+    csr = rpca.Csr(ip, ix, vv, (n, N_VARS))
+    p, _, _, _ = rpca.scale_values(csr, CLIP, True)
+    dense = np.zeros((n, N_VARS))
+    rows = np.repeat(np.arange(n), np.diff(ip))
+    np.add.at(dense, (rows, ix.astype(np.int64)), p)
+    dense -= dense.mean(axis=0, keepdims=True)
+    lam, vec = np.linalg.eigh(dense.T @ dense)
+    order = np.argsort(lam)[::-1][:N_COMPS]
+    ex_sv, ex_comps = np.sqrt(np.maximum(lam[order], 0.0)), vec[:, order].T
+    out["subsample_vs_exact_fp64"] = {m: cmp(r["sv"], r["comps"], ex_sv, ex_comps) for m, r in sub_ours.items()}
+    # the FP64 randomized PCA of the subsample (same Omega) separates the
+    # algorithm's own error (q power iterations on a flat spectrum) from the
+    # arithmetic's
+    from oracle import build_cpu
+    sub64 = build_cpu.run(ip, ix, vv, (n, N_VARS), N_COMPS, N_COMPS + N_OVERSAMPLES, N_POWER,
+                          rpca.gaussian_omega(N_VARS, N_COMPS + N_OVERSAMPLES, SEED), zero_center=True,
+                          scale=True, clip_max=CLIP, threads=os.cpu_count() or 1)
+    out["subsample_vs_fp64_randomized"] = {m: cmp(r["sv"], r["comps"], sub64["singular_values"],
+                                                  sub64["components"]) for m, r in sub_ours.items()}
+    out["subsample_fp64_randomized_vs_exact"] = cmp(sub64["singular_values"], sub64["components"], ex_sv,
+                                                    ex_comps)
+    out["subsample"] = f"first {n:,} rows of the same matrix ({len(ix):,} nnz); exact PCA by dense FP64 Gram eigh"
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -351,6 +405,7 @@ def run_ours(args):
         ms32 = max_over_ranks(ms32, dev)
         p32.close()
         sv32 = np.asarray(res32.singular_values)
+        comps32 = np.asarray(res32.components)
         out["fp32"] = {"ms": round(ms32, 4), "speedup_mixed_vs_fp32": round(ms32 / ms_max, 3),
                        "sigma_max_rel_diff_mixed_vs_fp32":
                            float(np.max(np.abs(sv_main - sv32) / sv32))}
@@ -395,7 +450,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample_rows = args.cpu_sample_rows or n_obs
-        cpu_ms, sample_nnz, sample_s = cpu_baseline(*host_csr, n_obs, sample_rows, threads)
+        cpu_ms, sample_nnz, sample_s, fp64 = cpu_baseline(*host_csr, n_obs, sample_rows, threads)
         out["cpu_baseline"] = {
             "value": round(cpu_ms, 1), "unit": "ms", "cores": threads, "kind": "port",
             "sample": (f"the whole matrix ({sample_nnz:,} nnz)" if sample_rows >= n_obs else
@@ -403,6 +458,32 @@ def run_ours(args):
                        f"rows to {n_obs:,}") +
                       f", FP64 C++ restatement of the reference CPU randomized PCA, {sample_s:.2f} s",
         }
+        # precision of the GPU paths against FP64 (config 3): the whole matrix
+        # against the FP64 randomized result just computed (same seeded Omega),
+        # a 50,000-cell subsample against the exact PCA
+        ours = {args.mode: {"sv": res.singular_values, "comps": res.components}}
+        extra = [m for m in ("mixed_bf16", "mixed_f16", "strict_fp32") if m != args.mode]
+        sub_n = min(SUBSAMPLE_ROWS, n_obs)
+        sub_nnz = int(host_csr[0][sub_n])
+        sub_csr = (np.ascontiguousarray(host_csr[0][: sub_n + 1]), np.ascontiguousarray(host_csr[1][:sub_nnz]),
+                   np.ascontiguousarray(host_csr[2][:sub_nnz]))
+        sub_ours = {}
+        for m in [args.mode] + extra:
+            if m != args.mode and m in ("mixed_f16",):
+                pm = make_plan(m)
+                rm = pm.run()
+                pm.close()
+                ours[m] = {"sv": rm.singular_values, "comps": rm.components}
+            elif m == "strict_fp32" and "fp32" in out:
+                ours[m] = {"sv": sv32, "comps": comps32}
+            ps = accel.Plan(ip[: sub_n + 1], ix[:sub_nnz], vv[:sub_nnz], (sub_n, N_VARS), n_components=N_COMPS,
+                            n_oversamples=N_OVERSAMPLES, n_power_iterations=N_POWER, zero_center=True,
+                            scale=True, clip_max=CLIP, seed=SEED, qr_method="cholesky", math_mode=m,
+                            device=local)
+            rs = ps.run()
+            ps.close()
+            sub_ours[m] = {"sv": rs.singular_values, "comps": rs.components}
+        out["precision"] = precision_report(ours, fp64, sub_ours, sub_csr)
 
     if rank == 0:
         print(json.dumps(out), flush=True)
