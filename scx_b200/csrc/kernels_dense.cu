@@ -270,8 +270,9 @@ cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shif
 // its rows (two distinct addresses per warp: broadcast) and 4 OUTB/64
 // float4 of M, for 128 OUTB/64 FMAs.  A block loads a tile before it writes
 // any of its rows, and only ever writes its own tiles, so Out may alias In.
-// Optionally writes the hi/lo 16-bit planes of Out (hi = round16(x),
-// lo = round16(x - hi); fmt 1 = bf16, 0 = f16) in the same pass.
+// Optionally writes the 16-bit image of Out in the same pass: row stride
+// 2 ldo, column 2 j = hi = round16(x), 2 j + 1 = round16(x - hi) (fmt 1 =
+// bf16, 0 = f16).
 // ---------------------------------------------------------------------------
 constexpr int kTallRows = 128;
 
@@ -299,8 +300,7 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 template <int OUTB>
 __global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, int K, int ldi,
                                                     const float* __restrict__ M, int ldm, int cnt, float* Out,
-                                                    int ldo, uint16_t* __restrict__ hi,
-                                                    uint16_t* __restrict__ lo, int fmt) {
+                                                    int ldo, uint16_t* __restrict__ img, int fmt) {
   constexpr int H = OUTB / 64;
   constexpr int RPT = kTallRows / 16;  // rows per thread
   extern __shared__ __align__(16) float sm_f[];
@@ -375,21 +375,20 @@ __global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, 
         const float* v = &acc[i][4 * h];
         if (vec_out) {
           *reinterpret_cast<float4*>(out) = make_float4(v[0], v[1], v[2], v[3]);
-          if (hi) {
+          if (img) {
             uint16_t hh[4], ll[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) split16(v[j], fmt, hh[j], ll[j]);
-            *reinterpret_cast<uint2*>(hi + row * ldo + col) =
-                make_uint2(hh[0] | ((uint32_t)hh[1] << 16), hh[2] | ((uint32_t)hh[3] << 16));
-            *reinterpret_cast<uint2*>(lo + row * ldo + col) =
-                make_uint2(ll[0] | ((uint32_t)ll[1] << 16), ll[2] | ((uint32_t)ll[3] << 16));
+            *reinterpret_cast<uint4*>(img + (row * ldo + col) * 2) =
+                make_uint4(hh[0] | ((uint32_t)ll[0] << 16), hh[1] | ((uint32_t)ll[1] << 16),
+                           hh[2] | ((uint32_t)ll[2] << 16), hh[3] | ((uint32_t)ll[3] << 16));
           }
         } else {
 #pragma unroll
           for (int j = 0; j < 4; ++j)
             if (col + j < cnt) {
               out[j] = v[j];
-              if (hi) split16(v[j], fmt, hi[row * ldo + col + j], lo[row * ldo + col + j]);
+              if (img) split16(v[j], fmt, img[(row * ldo + col + j) * 2], img[(row * ldo + col + j) * 2 + 1]);
             }
         }
       }
@@ -400,7 +399,7 @@ __global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, 
 }
 
 static cudaError_t tall_mm(const float* In, int64_t n, int K, int ldi, const float* M, int ldm, int cnt,
-                           float* Out, int ldo, uint16_t* hi, uint16_t* lo, int fmt, cudaStream_t st,
+                           float* Out, int ldo, uint16_t* img, int fmt, cudaStream_t st,
                            int num_sms) {
   if (n == 0) return cudaSuccess;
   if ((K & 3) || (ldi & 3)) return cudaErrorInvalidValue;
@@ -411,22 +410,22 @@ static cudaError_t tall_mm(const float* In, int64_t n, int K, int ldi, const flo
   note_launches(1);
   if (outb == 64) {
     cudaFuncSetAttribute(k_tall_mm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_tall_mm<64><<<grid, 256, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo, hi, lo, fmt);
+    k_tall_mm<64><<<grid, 256, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo, img, fmt);
   } else {
     cudaFuncSetAttribute(k_tall_mm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_tall_mm<128><<<grid, 256, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo, hi, lo, fmt);
+    k_tall_mm<128><<<grid, 256, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo, img, fmt);
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_apply_right_f32(const float* In, int64_t n, int ld, const float* M, float* Out,
                                    cudaStream_t st, int num_sms) {
-  return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, nullptr, nullptr, 0, st, num_sms);
+  return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, nullptr, 0, st, num_sms);
 }
 
 cudaError_t launch_apply_right_split(const float* In, int64_t n, int ld, const float* M, float* Out,
-                                     uint16_t* hi, uint16_t* lo, int fmt, cudaStream_t st, int num_sms) {
-  return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, hi, lo, fmt, st, num_sms);
+                                     uint16_t* img, int fmt, cudaStream_t st, int num_sms) {
+  return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, img, fmt, st, num_sms);
 }
 
 // ---------------------------------------------------------------------------
@@ -783,7 +782,7 @@ cudaError_t launch_ritz_finish(const double* B, int64_t g, int ld, int k, int nc
 cudaError_t launch_embed(const float* Q, int64_t n, int ld, int k, const float* M_emb, int nc,
                          float* U, cudaStream_t st, int num_sms) {
   (void)k;  // rows k..ld-1 of M_emb are zero
-  return tall_mm(Q, n, ld, ld, M_emb, nc, nc, U, nc, nullptr, nullptr, 0, st, num_sms);
+  return tall_mm(Q, n, ld, ld, M_emb, nc, nc, U, nc, nullptr, 0, st, num_sms);
 }
 
 // ---------------------------------------------------------------------------

@@ -15,26 +15,34 @@
 //   4 bytes per stored entry instead of 6 (bf16 value + int32 index).
 //
 // Both products densify a segment into a 128 x 64 16-bit shared-memory tile
-// (128-byte swizzle, see tc.cuh) and run tcgen05.mma on it:
-//   forward    Y(128 cells x 2ld) += A(cells x 64 genes, K-major) [Vhi|Vlo]
-//   transposed Z(128 genes x 2ld) += A^T(genes x cells, MN-major) [Qhi|Qlo]
-// The dense operand enters as two 16-bit planes side by side, hi = round(x)
-// and lo = round(x - hi), so one N = 2 ld MMA multiplies both and the
-// epilogue adds the two halves: about 16 mantissa bits on the dense operand,
-// the matrix values being the only operand rounded to 16 bits.
+// (128-byte swizzle, see tc.cuh) and run tcgen05.mma on it.  The dense
+// operand enters as its 16-bit image: column 2 j holds hi = round(x_j),
+// column 2 j + 1 holds lo = round(x_j - hi), so one MMA multiplies both
+// halves and the epilogue adds each (hi, lo) pair of accumulator columns:
+// about 16 mantissa bits on the dense operand, the matrix values being the
+// only operand rounded to 16 bits.
 //
-// Warp roles (23 warps): warps 0-15 densify in four groups of four (forward:
-// group g takes every fourth stage into its own two A buffers; transposed: a
-// pair of groups fills the two sub-tiles of every other stage).  Each densify warp reads its
-// quarter of a segment straight from global memory with 16-byte loads (the
-// tile's entries were prefetched into L2 a tile ahead), keeping the loads of
-// its group's next segment in flight in registers while the current one is
-// scattered, so many warps -- not one issuing thread -- keep the entry stream
-// moving.  Warps 16-19 drain TMEM (one lane quarter each); warp 20 issues the
-// MMAs from one thread; warp 21 loads the dense operand by TMA into its own
-// ring (forward) or per row tile (transposed); warp 22 copies segment
-// metadata per tile and prefetches the entries of the tile after into L2.
-// All waits are bounded (tc.cuh).
+// At ld 64 (k_fwd_swap, k_rmat_swap) the image is the MMA's A operand
+// (M = 128 image columns, MN-major) and the densified tiles are its B:
+//   forward    Y^T(128 x 256 cells) += Vimg_c^T [A_(t0,c) | A_(t1,c)]^T
+//   transposed Z^T(128 x 256 genes) += Qimg_t^T [A_(t,4q) | ... | A_(t,4q+3)]
+// A tcgen05.mma at M = 128 costs about the same to issue whatever its N, so
+// spanning two row tiles (forward) or four gene chunks (transposed) in
+// N = 256 halves the instructions per segment against N = 128.  At ld 128
+// (k_fwd_tc, k_rmat_tc) the image is the B operand (N = 256) and the tiles
+// the A:
+//   forward    Y(128 cells x 256) += A(cells x 64 genes, K-major) Vimg_c
+//   transposed Z(128 genes x 256) += A^T(genes x cells, MN-major) Qimg_t
+//
+// Warp roles (23 warps): warps 0-15 densify in four groups of four; warps
+// 16-19 drain TMEM (one lane quarter each); warp 20 issues the MMAs from one
+// thread; warp 21 loads the dense operand by TMA; warp 22 copies segment
+// metadata per tile (or band of two tiles) and prefetches their entries into
+// L2.  Each densify warp reads its quarter of a segment straight from global
+// memory with 16-byte loads, keeping the loads of its group's next segment
+// in flight in registers while the current one is scattered, so many warps
+// -- not one issuing thread -- keep the entry stream moving.  All waits are
+// bounded (tc.cuh).
 #include <algorithm>
 
 #include "common.cuh"
@@ -185,6 +193,13 @@ __device__ __forceinline__ float unpack16(uint32_t bits, int fmt) {
   if (fmt) return __bfloat162float(__ushort_as_bfloat16((unsigned short)bits));
   return __half2float(__ushort_as_half((unsigned short)bits));
 }
+// The (hi, lo) pair of x as one word, hi in the low half: hi = round16(x),
+// lo = round16(x - hi) -- two adjacent columns of the 16-bit image.
+__device__ __forceinline__ uint32_t hilo16(float x, int fmt) {
+  const uint32_t h = pack16x2(x, 0.f, fmt) & 0xFFFFu;
+  const uint32_t l = pack16x2(x - unpack16(h, fmt), 0.f, fmt) & 0xFFFFu;
+  return h | (l << 16);
+}
 
 // Zero rows 32q .. 32q+31 of a 128 x 64 16-bit swizzled tile, lane = row.
 // Iteration i writes physical chunk i ^ (row % 8): the 32 lanes of one store
@@ -246,15 +261,16 @@ __device__ __forceinline__ void prefetch_segments(const uint32_t* __restrict__ e
   for (int64_t p = b; p < e; p += 8192) bulk_prefetch_l2(ent + p, (uint32_t)(min((int64_t)8192, e - p) * 4));
 }
 
-// Meta loader: metadata of tile t (nc records) into meta ring slot mi & 1.
-__device__ __forceinline__ bool load_meta(const SegMeta* __restrict__ meta, int64_t t, int nc,
-                                          SegMeta* mring, uint64_t* mfull, uint64_t* mempty, uint32_t mi,
+// Meta loader: `records` metadata records from `src` into slot mi & 1 of a
+// two-slot ring of `slot_records` records per slot.
+__device__ __forceinline__ bool load_meta(const SegMeta* __restrict__ src, int records, SegMeta* mring,
+                                          int slot_records, uint64_t* mfull, uint64_t* mempty, uint32_t mi,
                                           volatile int* abort_flag, int* err, int code) {
   const int ms = mi & 1u;
   if (!mbar_wait(&mempty[ms], ((mi >> 1) & 1u) ^ 1u, abort_flag, err, code)) return false;
-  const uint32_t bytes = (uint32_t)nc * 16u;
+  const uint32_t bytes = (uint32_t)records * 16u;
   mbar_arrive_expect_tx(&mfull[ms], bytes);
-  bulk_load(mring + (size_t)ms * kMaxChunks, meta + t * nc, bytes, &mfull[ms]);
+  bulk_load(mring + (size_t)ms * slot_records, src, bytes, &mfull[ms]);
   return true;
 }
 
@@ -264,16 +280,14 @@ __device__ __forceinline__ bool load_meta(const SegMeta* __restrict__ meta, int6
 template <int LD>
 __global__ void __launch_bounds__(kThreads, 1)
     k_fwd_tc(const uint32_t* __restrict__ ent, const SegMeta* __restrict__ meta, int64_t n_tiles, int nc,
-             int64_t n, const __grid_constant__ CUtensorMap vmap_hi, const __grid_constant__ CUtensorMap vmap_lo,
-             const float* __restrict__ mc, float* __restrict__ Y, uint16_t* __restrict__ Yhi,
-             uint16_t* __restrict__ Ylo, int fmt, int* err) {
+             int64_t n, const __grid_constant__ CUtensorMap vmap, const float* __restrict__ mc,
+             float* __restrict__ Y, uint16_t* __restrict__ Yimg, int fmt, int* err) {
   constexpr int N2 = 2 * LD;                // [hi | lo] columns
   constexpr int S = fwd_stages(LD);         // A stages, two per densify group
   constexpr int G = kGroups;
   constexpr int NB = fwd_bslots(LD);        // dense-operand ring
   constexpr int A_BYTES = TM * CW * 2;      // 16 KB
-  constexpr int B_PLANE = CW * LD * 2;      // 64 genes x LD, one 16-bit plane
-  constexpr int B_BYTES = 2 * B_PLANE;
+  constexpr int B_BYTES = CW * N2 * 2;      // 64 genes x N2 image columns
   static_assert(S == 2 * G, "two A stages per densify group");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = align1024(smem_raw);
@@ -370,34 +384,26 @@ __global__ void __launch_bounds__(kThreads, 1)
       const uint32_t tbase = tmem + ((32u * q) << 16) + a * N2;
       const int64_t grow = t * TM + row;
 #pragma unroll 1
-      for (int cb = 0; cb < LD / 16; ++cb) {
-        uint32_t h[16], l[16];
-        tmem_ld16(tbase + cb * 16, h);
-        tmem_ld16(tbase + LD + cb * 16, l);
+      for (int cb = 0; cb < N2 / 16; ++cb) {  // 16 image columns = 8 output columns
+        uint32_t r[16];
+        tmem_ld16(tbase + cb * 16, r);
         tmem_wait_ld();
         if (grow < n) {
-          float o[16];
-#pragma unroll
-          for (int i = 0; i < 16; ++i)
-            o[i] = __uint_as_float(h[i]) + __uint_as_float(l[i]) - __ldg(mc + cb * 16 + i);
-          if (Y) {  // the FP32 copy only when the caller reads it
-            float4* yr = reinterpret_cast<float4*>(Y + grow * LD + cb * 16);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) yr[i] = make_float4(o[4 * i], o[4 * i + 1], o[4 * i + 2], o[4 * i + 3]);
-          }
-          uint32_t ph16[8], pl16[8];
+          float o[8];
+          uint32_t w[8];
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
-            ph16[i] = pack16x2(o[2 * i], o[2 * i + 1], fmt);
-            pl16[i] = pack16x2(o[2 * i] - unpack16(ph16[i] & 0xFFFFu, fmt),
-                               o[2 * i + 1] - unpack16(ph16[i] >> 16, fmt), fmt);
+            o[i] = __uint_as_float(r[2 * i]) + __uint_as_float(r[2 * i + 1]) - __ldg(mc + cb * 8 + i);
+            w[i] = hilo16(o[i], fmt);
           }
-          uint4* hr = reinterpret_cast<uint4*>(Yhi + grow * LD + cb * 16);
-          uint4* lr = reinterpret_cast<uint4*>(Ylo + grow * LD + cb * 16);
-          hr[0] = make_uint4(ph16[0], ph16[1], ph16[2], ph16[3]);
-          hr[1] = make_uint4(ph16[4], ph16[5], ph16[6], ph16[7]);
-          lr[0] = make_uint4(pl16[0], pl16[1], pl16[2], pl16[3]);
-          lr[1] = make_uint4(pl16[4], pl16[5], pl16[6], pl16[7]);
+          if (Y) {  // the FP32 copy only when the caller reads it
+            float4* yr = reinterpret_cast<float4*>(Y + grow * LD + cb * 8);
+            yr[0] = make_float4(o[0], o[1], o[2], o[3]);
+            yr[1] = make_float4(o[4], o[5], o[6], o[7]);
+          }
+          uint4* ir = reinterpret_cast<uint4*>(Yimg + grow * N2 + cb * 16);
+          ir[0] = make_uint4(w[0], w[1], w[2], w[3]);
+          ir[1] = make_uint4(w[4], w[5], w[6], w[7]);
         }
       }
       tc_fence_before();
@@ -458,10 +464,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           uint8_t* bb = Bs + b * B_BYTES;
           mbar_arrive_expect_tx(&bfull[b], B_BYTES);
 #pragma unroll
-          for (int h = 0; h < LD / 64; ++h) {
-            tma_load_2d(bb + h * (CW * 128), &vmap_hi, &bfull[b], 64 * h, CW * c);
-            tma_load_2d(bb + B_PLANE + h * (CW * 128), &vmap_lo, &bfull[b], 64 * h, CW * c);
-          }
+          for (int h = 0; h < N2 / 64; ++h) tma_load_2d(bb + h * (CW * 128), &vmap, &bfull[b], 64 * h, CW * c);
         }
       }
     }
@@ -471,7 +474,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (lane == 0) {
       uint32_t ti = 0;
       for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++ti) {
-        if (!load_meta(meta, t, nc, mring, mfull, mempty, ti, abort_flag, err, 17)) break;
+        if (!load_meta(meta + t * nc, nc, mring, kMaxChunks, mfull, mempty, ti, abort_flag, err, 17)) break;
         if (!mbar_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 18)) break;
         prefetch_segments(ent, mring + (ti & 1u) * kMaxChunks, 0, nc);
       }
@@ -498,14 +501,13 @@ done:
 template <int LD>
 __global__ void __launch_bounds__(kThreads, 1)
     k_rmat_tc(const uint32_t* __restrict__ ent, const SegMeta* __restrict__ meta, int64_t n_tiles, int nc,
-              int64_t g, int n_gene_groups, const __grid_constant__ CUtensorMap qmap_hi,
-              const __grid_constant__ CUtensorMap qmap_lo, float* __restrict__ part, int fmt, int* err) {
+              int64_t g, int n_gene_groups, const __grid_constant__ CUtensorMap qmap, float* __restrict__ part,
+              int fmt, int* err) {
   constexpr int N2 = 2 * LD;
   constexpr int S = rmat_stages(LD);     // A stages (even: two per pair of densify groups at ld 64)
   constexpr int SUB = TM * CW * 2;       // one 64-gene sub-tile, 16 KB
   constexpr int A_BYTES = 2 * SUB;       // 128 genes
-  constexpr int Q_PLANE = TM * LD * 2;   // 128 cells x LD
-  constexpr int Q_BYTES = 2 * Q_PLANE;   // [hi | lo]
+  constexpr int Q_BYTES = TM * N2 * 2;   // 128 cells x N2 image columns
   constexpr int SPG = 512 / N2;          // 128-gene super-chunks per CTA (TMEM columns)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = align1024(smem_raw);
@@ -616,24 +618,23 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int64_t gene = (int64_t)(sc0 + j) * 128 + row;
       const uint32_t tbase = tmem + ((32u * q) << 16) + j * N2;
 #pragma unroll 1
-      for (int cb = 0; cb < LD / 16; ++cb) {
-        uint32_t h[16], l[16];
+      for (int cb = 0; cb < N2 / 16; ++cb) {  // 16 image columns = 8 output columns
+        uint32_t r[16];
         if (have_work) {
-          tmem_ld16(tbase + cb * 16, h);
-          tmem_ld16(tbase + LD + cb * 16, l);
+          tmem_ld16(tbase + cb * 16, r);
           tmem_wait_ld();
         } else {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) h[i] = l[i] = 0u;
+          for (int i = 0; i < 16; ++i) r[i] = 0u;
         }
         if (gene < g) {
-          float4* out = reinterpret_cast<float4*>(part + ((int64_t)rg * g + gene) * LD + cb * 16);
+          float4* out = reinterpret_cast<float4*>(part + ((int64_t)rg * g + gene) * LD + cb * 8);
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
-            out[i] = make_float4(__uint_as_float(h[4 * i]) + __uint_as_float(l[4 * i]),
-                                 __uint_as_float(h[4 * i + 1]) + __uint_as_float(l[4 * i + 1]),
-                                 __uint_as_float(h[4 * i + 2]) + __uint_as_float(l[4 * i + 2]),
-                                 __uint_as_float(h[4 * i + 3]) + __uint_as_float(l[4 * i + 3]));
+          for (int i = 0; i < 2; ++i)
+            out[i] = make_float4(__uint_as_float(r[8 * i]) + __uint_as_float(r[8 * i + 1]),
+                                 __uint_as_float(r[8 * i + 2]) + __uint_as_float(r[8 * i + 3]),
+                                 __uint_as_float(r[8 * i + 4]) + __uint_as_float(r[8 * i + 5]),
+                                 __uint_as_float(r[8 * i + 6]) + __uint_as_float(r[8 * i + 7]));
         }
       }
     }
@@ -685,10 +686,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         uint8_t* qb = Qs + b * Q_BYTES;
         mbar_arrive_expect_tx(&qfull[b], Q_BYTES);
 #pragma unroll
-        for (int h = 0; h < LD / 64; ++h) {
-          tma_load_2d(qb + h * (TM * 128), &qmap_hi, &qfull[b], 64 * h, (int)(t * TM));
-          tma_load_2d(qb + Q_PLANE + h * (TM * 128), &qmap_lo, &qfull[b], 64 * h, (int)(t * TM));
-        }
+        for (int h = 0; h < N2 / 64; ++h) tma_load_2d(qb + h * (TM * 128), &qmap, &qfull[b], 64 * h, (int)(t * TM));
       }
     }
     __syncwarp();
@@ -697,7 +695,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (lane == 0 && have_work) {
       uint32_t ti = 0;
       for (int64_t t = t0; t < t1; ++t, ++ti) {
-        if (!load_meta(meta, t, nc, mring, mfull, mempty, ti, abort_flag, err, 27)) break;
+        if (!load_meta(meta + t * nc, nc, mring, kMaxChunks, mfull, mempty, ti, abort_flag, err, 27)) break;
         if (!mbar_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 29)) break;
         prefetch_segments(ent, mring + (ti & 1u) * kMaxChunks, 2 * sc0, min(nc, 2 * sc1));
       }
@@ -715,18 +713,19 @@ done:
 }
 
 // ---------------------------------------------------------------------------
-// Tall Gram on tensor cores (ld = 64): for the rows of this CTA,
-//   D  = [h|l]^T [h|l]   (128 x 128, FP32 in TMEM)  -> G = hh + hl + lh + ll
-//   Ds = [h|l]^T 1       (128 x 64)                 -> column sums of h + l
-// from the hi/lo 16-bit planes of Y (TMA, 4-stage ring).  One MMA per 16 rows
+// Tall Gram on tensor cores (ld = 64): for the rows of this CTA, with I the
+// 16-bit image of Y (128 columns, (hi, lo) of column j at 2 j and 2 j + 1),
+//   D  = I^T I   (128 x 128, FP32 in TMEM)  -> G = hh + hl + lh + ll
+//   Ds = I^T 1   (128 x 64)                 -> column sums of h + l
+// (TMA, 4-stage ring).  One MMA per 16 rows
 // for each; the per-CTA partial is written in FP64 as [G (64 x 64), colsum
 // (64)], the layout the fixed-order reduction expects.
 // ---------------------------------------------------------------------------
 constexpr int kGramStages = 4;
 
 __global__ void __launch_bounds__(128, 1)
-    k_gram_tc(int64_t n_tiles, const __grid_constant__ CUtensorMap qmap_hi, const __grid_constant__ CUtensorMap qmap_lo,
-              double* __restrict__ part, int fmt, int* err) {
+    k_gram_tc(int64_t n_tiles, const __grid_constant__ CUtensorMap qmap, double* __restrict__ part, int fmt,
+              int* err) {
   constexpr int LD = 64;
   constexpr int PLANE = TM * LD * 2;  // 16 KB
   constexpr int TILE = 2 * PLANE;     // [h | l]
@@ -780,8 +779,8 @@ __global__ void __launch_bounds__(128, 1)
       if (!mbar_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 41)) break;
       uint8_t* tile = tiles + s * TILE;
       mbar_arrive_expect_tx(&full[s], TILE);
-      tma_load_2d(tile, &qmap_hi, &full[s], 0, (int)(t * TM));
-      tma_load_2d(tile + PLANE, &qmap_lo, &full[s], 0, (int)(t * TM));
+      tma_load_2d(tile, &qmap, &full[s], 0, (int)(t * TM));
+      tma_load_2d(tile + PLANE, &qmap, &full[s], 64, (int)(t * TM));
     }
   } else if (threadIdx.x == 32 && have_work) {
     // MMA issuer
@@ -817,13 +816,13 @@ __global__ void __launch_bounds__(128, 1)
     tc_fence_after();
     const uint32_t tb = tmem + ((32u * warp) << 16);
 #pragma unroll 1
-    for (int cb = 0; cb < 4; ++cb) {
-      uint32_t a[16], b[16];
+    for (int cb = 0; cb < 8; ++cb) {  // image columns (2 j', 2 j' + 1) -> column j'
+      uint32_t a[16];
       tmem_ld16(tb + cb * 16, a);
-      tmem_ld16(tb + 64 + cb * 16, b);
       tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < 16; ++i) pbuf[row * LD + cb * 16 + i] = __uint_as_float(a[i]) + __uint_as_float(b[i]);
+      for (int i = 0; i < 8; ++i)
+        pbuf[row * LD + cb * 8 + i] = __uint_as_float(a[2 * i]) + __uint_as_float(a[2 * i + 1]);
     }
     uint32_t c16[16];
     tmem_ld16(tb + 128, c16);
@@ -835,17 +834,17 @@ __global__ void __launch_bounds__(128, 1)
   __syncthreads();
   {
     double* out = part + (int64_t)blockIdx.x * (LD * LD + LD);
-    // row < 64 holds h-rows, row >= 64 the l-rows of the same column index
+    // image rows 2 i (hi) and 2 i + 1 (lo) belong to column i
     for (int t = threadIdx.x; t < LD * LD; t += blockDim.x) {
       const int i = t / LD, j = t % LD;
-      out[t] = (double)pbuf[i * LD + j] + (double)pbuf[(i + LD) * LD + j];
+      out[t] = (double)pbuf[(2 * i) * LD + j] + (double)pbuf[(2 * i + 1) * LD + j];
     }
     pbuf[row * LD] = srow;  // column sums of [h | l], one per row of Ds
   }
   __syncthreads();
   if (threadIdx.x < LD) {
     double* out = part + (int64_t)blockIdx.x * (LD * LD + LD);
-    out[LD * LD + threadIdx.x] = (double)pbuf[threadIdx.x * LD] + (double)pbuf[(threadIdx.x + LD) * LD];
+    out[LD * LD + threadIdx.x] = (double)pbuf[(2 * threadIdx.x) * LD] + (double)pbuf[(2 * threadIdx.x + 1) * LD];
   }
 done:
   if (*abort_flag) __nanosleep(500000);
@@ -857,25 +856,482 @@ done:
   }
 }
 
-// hi = round16(x), lo = round16(x - hi) (fmt 1 = bf16, 0 = f16); lo may be null.
-__global__ void k_split16(float* __restrict__ in, int64_t count, uint16_t* __restrict__ hi,
-                          uint16_t* __restrict__ lo, int fmt, int write_back) {
+// 16-bit image of x: words (hi | lo << 16), hi = round16(x), lo = round16(x - hi)
+// (fmt 1 = bf16, 0 = f16).
+__global__ void k_split16(const float* __restrict__ in, int64_t count, uint32_t* __restrict__ img, int fmt) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const float x = in[i];
-    float h;
-    if (fmt) {
-      const __nv_bfloat16 b = __float2bfloat16_rn(x);
-      hi[i] = __bfloat16_as_ushort(b);
-      h = __bfloat162float(b);
-      if (lo) lo[i] = __bfloat16_as_ushort(__float2bfloat16_rn(x - h));
-    } else {
-      const __half b = __float2half_rn(x);
-      hi[i] = __half_as_ushort(b);
-      h = __half2float(b);
-      if (lo) lo[i] = __half_as_ushort(__float2half_rn(x - h));
+       i += (int64_t)gridDim.x * blockDim.x)
+    img[i] = hilo16(in[i], fmt);
+}
+
+// ---------------------------------------------------------------------------
+// ld 64: the two products with the dense operand's image as the MMA's A and
+// the densified tiles as its B, so one instruction spans N = 256 cells (two
+// tiles, forward) or 256 genes (four chunks, transposed).  The issue cost of
+// a tcgen05.mma at M = 128 does not depend on N, so the wider N halves the
+// instructions per segment.  The accumulator is transposed: TMEM lane m is
+// image column m = 2 j + p ((hi, lo) of output column j), so lanes 2 j and
+// 2 j + 1 hold the two halves of one output column and a lane shuffle adds
+// them.
+// ---------------------------------------------------------------------------
+constexpr int kSwapFwdStages = 4;  // pair stages: the two tiles of a band, one chunk
+constexpr int kSwapFwdSlots = 5;   // dense-operand ring (16 KB image chunks)
+
+__host__ __device__ constexpr size_t fwd_swap_smem() {
+  return 1024 + (size_t)kSwapFwdStages * 2 * (TM * CW * 2) + (size_t)kSwapFwdSlots * (CW * 128 * 2) +
+         2 * 2 * (size_t)kMaxChunks * sizeof(SegMeta) + 64 * sizeof(uint64_t) + 64;
+}
+
+// A band is two consecutive row tiles.  Per band:
+// Y^T[m, its 256 cells] = sum over chunks c of Vimg_c^T (m x 64 genes) [A_(t0,c) | A_(t1,c)]^T.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_fwd_swap(const uint32_t* __restrict__ ent, const SegMeta* __restrict__ meta, int64_t n_tiles, int nc,
+               int64_t n, const __grid_constant__ CUtensorMap vmap, const float* __restrict__ mc,
+               float* __restrict__ Y, uint16_t* __restrict__ Yimg, int fmt, int* err) {
+  constexpr int LD = 64;
+  constexpr int S = kSwapFwdStages;
+  constexpr int NB = kSwapFwdSlots;
+  constexpr int TILE = TM * CW * 2;      // one 128 x 64 tile, 16 KB
+  constexpr int STAGE = 2 * TILE;        // the band's two tiles, 256 cell rows
+  constexpr int B_BYTES = CW * 128 * 2;  // 64 genes x 128 image columns
+  constexpr int MSLOT = 2 * kMaxChunks;
+  static_assert(S == 4, "stage of chunk counter cc is cc % 4; groups (cc & 1, tile) own two stages each");
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = align1024(smem_raw);
+  uint8_t* As = smem;
+  uint8_t* Bs = As + S * STAGE;
+  SegMeta* mring = reinterpret_cast<SegMeta*>(Bs + NB * B_BYTES);  // [2][2 * kMaxChunks]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(mring + 2 * MSLOT);
+  uint64_t* full = bars;            // [S]  stage densified (two groups x 4 warps)
+  uint64_t* empty = full + S;       // [S]  stage consumed (MMA commit)
+  uint64_t* bfull = empty + S;      // [NB] image chunk landed (TMA)
+  uint64_t* bempty = bfull + NB;    // [NB] image chunk consumed (MMA commit)
+  uint64_t* acc_full = bempty + NB;
+  uint64_t* acc_empty = acc_full + 2;
+  uint64_t* mfull = acc_empty + 2;
+  uint64_t* mempty = mfull + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mempty + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t n_bands = (n_tiles + 1) / 2;
+  auto band_tiles = [&](int64_t band) { return (int)min((int64_t)2, n_tiles - band * 2); };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 8);
+      mbar_init(&empty[s], 1);
     }
-    if (write_back) in[i] = h;
+    for (int b = 0; b < NB; ++b) {
+      mbar_init(&bfull[b], 1);
+      mbar_init(&bempty[b], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], 4);
+      mbar_init(&mfull[a], 1);
+      mbar_init(&mempty[a], 4 * kGroups);
+    }
+    *abort_flag = 0;
+    mbar_fence_init();
+  }
+  if (warp == W_MMA) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < W_EPI) {
+    // ---- densify: group (cc & 1, u) fills tile u of the stage of chunk
+    // counter cc; a band with one tile leaves its u = 1 groups idle, but they
+    // still take part in the stage handshake ----
+    const int group = warp >> 2, q = warp & 3;
+    const int par = group >> 1, u = group & 1;
+    uint32_t cc = 0, bi = 0;
+    uint4 w[kFwdRegs];
+    Span pre{-1, -1};  // span whose loads are in flight in w
+    for (int64_t band = blockIdx.x; band < n_bands; band += gridDim.x, ++bi) {
+      const int nt = band_tiles(band);
+      const bool has = u < nt;
+      if (!warp_wait(&mfull[bi & 1u], (bi >> 1) & 1u, abort_flag, err, 11)) goto done;
+      const SegMeta* mt = mring + (bi & 1u) * MSLOT;
+      for (int c = 0; c < nc; ++c, ++cc) {
+        if ((int)(cc & 1u) != par) continue;
+        const Span sp = has ? quarter_span(mt[u * nc + c], q) : Span{0, 0};
+        if (has && (sp.lo != pre.lo || sp.hi != pre.hi)) span_load<kFwdRegs>(ent, sp, lane, w);
+        const int s = cc % S;
+        if (!warp_wait(&empty[s], ((cc / S) & 1u) ^ 1u, abort_flag, err, 12)) goto done;
+        if (has) {
+          const uint32_t tile = smem_u32(As + s * STAGE + u * TILE);
+          zero_rows(tile, q, lane);
+          __syncwarp();
+          span_scatter<kFwdRegs>(tile, ent, sp, lane, w);
+        }
+        // the group's next segment: chunk c + 2 of this band, or of the next
+        pre = Span{-1, -1};
+        if (c + 2 < nc) {
+          if (has) pre = quarter_span(mt[u * nc + c + 2], q);
+        } else if (band + gridDim.x < n_bands && c + 2 - nc < nc && u < band_tiles(band + gridDim.x)) {
+          if (!warp_wait(&mfull[(bi + 1) & 1u], ((bi + 1) >> 1) & 1u, abort_flag, err, 11)) goto done;
+          pre = quarter_span(mring[((bi + 1) & 1u) * MSLOT + u * nc + (c + 2 - nc)], q);
+        }
+        if (pre.lo >= 0) span_load<kFwdRegs>(ent, pre, lane, w);
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&full[s]);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&mempty[bi & 1u]);
+    }
+  } else if (warp < W_MMA) {
+    // ---- epilogue: lane pair (2 j, 2 j + 1) -> column j of Y and its image ----
+    const int q = warp & 3;
+    const int p = lane & 1, j = 16 * q + (lane >> 1);
+    const float mcj = __ldg(mc + j);
+    uint32_t k = 0;
+    for (int64_t band = blockIdx.x; band < n_bands; band += gridDim.x, ++k) {
+      const int nt = band_tiles(band);
+      const uint32_t a = k & 1u, ph = (k >> 1) & 1u;
+      if (!warp_wait(&acc_full[a], ph, abort_flag, err, 14)) goto done;
+      tc_fence_after();
+      for (int u = 0; u < nt; ++u) {
+        const uint32_t tbase = tmem + ((32u * q) << 16) + a * 256 + u * 128;
+        const int64_t row0 = (band * 2 + u) * TM;
+#pragma unroll 1
+        for (int cb = 0; cb < TM / 16; ++cb) {  // 16 cells per TMEM load
+          uint32_t r[16];
+          tmem_ld16(tbase + cb * 16, r);
+          tmem_wait_ld();
+          float v[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const float x = __uint_as_float(r[i]);
+            v[i] = x + __shfl_xor_sync(0xffffffffu, x, 1) - mcj;
+          }
+          const int64_t c0 = row0 + cb * 16;
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            if (c0 + i < n) {
+              const uint32_t hl = hilo16(v[i], fmt);
+              Yimg[(c0 + i) * 128 + 32 * q + lane] = (uint16_t)(p ? hl >> 16 : hl & 0xFFFFu);
+            }
+          }
+          if (Y) {  // the FP32 copy only when the caller reads it: lane p writes cell 2 i + p
+#pragma unroll
+            for (int i = 0; i < 16; i += 2)
+              if (c0 + i + p < n) Y[(c0 + i + p) * LD + j] = p ? v[i + 1] : v[i];
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[a]);
+    }
+  } else if (warp == W_MMA) {
+    // ---- MMA issuer: per chunk, four K = 16 steps over both tiles of the band ----
+    if (lane == 0) {
+      const uint32_t idesc2 = idesc_f16(128, 256, fmt, 1, 0);
+      const uint32_t idesc1 = idesc_f16(128, 128, fmt, 1, 0);
+      const uint64_t vdesc0 = sdesc_sw128(smem_u32(Bs), CW * 128, 1024);  // MN-major, two 64-column blocks
+      const uint64_t tdesc0 = sdesc_sw128(smem_u32(As), 16, 1024);        // K-major, 256 cell rows
+      uint32_t cc = 0, k = 0;
+      bool ok = true;
+      for (int64_t band = blockIdx.x; band < n_bands && ok; band += gridDim.x, ++k) {
+        const uint32_t idesc = band_tiles(band) == 2 ? idesc2 : idesc1;
+        const uint32_t a = k & 1u, ph = (k >> 1) & 1u;
+        if (!mbar_wait(&acc_empty[a], ph ^ 1u, abort_flag, err, 15)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + a * 256;
+        for (int c = 0; c < nc; ++c, ++cc) {
+          const int b = cc % NB, s = cc % S;
+          if (!mbar_wait(&bfull[b], (cc / NB) & 1u, abort_flag, err, 16) ||
+              !mbar_wait(&full[s], (cc / S) & 1u, abort_flag, err, 16)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t vd = vdesc0 + (uint64_t)(b * (B_BYTES >> 4));
+          const uint64_t td = tdesc0 + (uint64_t)(s * (STAGE >> 4));
+          umma_f16(d, vd, td, idesc, c != 0);
+#pragma unroll
+          for (int kk = 1; kk < CW / 16; ++kk)  // K steps of 16 genes: +2 KB down the image, +32 B along the tiles
+            umma_f16(d, vd + 128 * kk, td + 2 * kk, idesc, 1u);
+          umma_commit(&empty[s]);
+          umma_commit(&bempty[b]);
+        }
+        if (ok) umma_commit(&acc_full[a]);
+      }
+    }
+    __syncwarp();
+  } else if (warp == W_DENSE) {
+    // ---- dense loader: image chunks into the ring, up to NB ahead ----
+    if (lane == 0) {
+      uint32_t cc = 0;
+      bool ok = true;
+      for (int64_t band = blockIdx.x; band < n_bands && ok; band += gridDim.x) {
+        for (int c = 0; c < nc; ++c, ++cc) {
+          const int b = cc % NB;
+          if (!mbar_wait(&bempty[b], ((cc / NB) & 1u) ^ 1u, abort_flag, err, 19)) {
+            ok = false;
+            break;
+          }
+          uint8_t* bb = Bs + b * B_BYTES;
+          mbar_arrive_expect_tx(&bfull[b], B_BYTES);
+          tma_load_2d(bb, &vmap, &bfull[b], 0, CW * c);
+          tma_load_2d(bb + CW * 128, &vmap, &bfull[b], 64, CW * c);
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == W_META) {
+    // ---- meta loader: band metadata, and the band's entries into L2 ----
+    if (lane == 0) {
+      uint32_t bi = 0;
+      for (int64_t band = blockIdx.x; band < n_bands; band += gridDim.x, ++bi) {
+        const int records = band_tiles(band) * nc;  // the band's tiles are consecutive in `meta`
+        if (!load_meta(meta + band * 2 * nc, records, mring, MSLOT, mfull, mempty, bi, abort_flag, err, 17))
+          break;
+        if (!mbar_wait(&mfull[bi & 1u], (bi >> 1) & 1u, abort_flag, err, 18)) break;
+        prefetch_segments(ent, mring + (bi & 1u) * MSLOT, 0, records);
+      }
+    }
+    __syncwarp();
+  }
+done:
+  if (*abort_flag) __nanosleep(500000);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == W_MMA) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+constexpr int kSwapRmatStages = 4;  // stages: one half tile (64 cells) of a quad's four chunks
+constexpr int kSwapQuads = 2;       // 256-gene quads per CTA (2 x 256 TMEM columns)
+
+__host__ __device__ constexpr size_t rmat_swap_smem() {
+  return 1024 + (size_t)kSwapRmatStages * 4 * (64 * CW * 2) + 2 * (size_t)(TM * 128 * 2) +
+         2 * (size_t)kMaxChunks * sizeof(SegMeta) + 64 * sizeof(uint64_t) + 64;
+}
+
+// part[row group][genes of this CTA, :64]: per quad of four chunks (256 genes)
+// Z^T[m, the quad's genes] = sum over the CTA's row tiles t of
+// Qimg_t^T (m x 128 cells) [A_(t,4qd) | ... | A_(t,4qd+3)].  grid = gene groups x row groups.
+// A stage holds one half (64 cells) of a tile for the quad's four chunks, so
+// K = 64 per stage and the densify warps split into two teams of eight, team
+// h filling the cells 64 h .. 64 h + 63 of every tile (warp = chunk x quarter).
+__global__ void __launch_bounds__(kThreads, 1)
+    k_rmat_swap(const uint32_t* __restrict__ ent, const SegMeta* __restrict__ meta, int64_t n_tiles, int nc,
+                int64_t g, int n_gene_groups, const __grid_constant__ CUtensorMap qmap, float* __restrict__ part,
+                int fmt, int* err) {
+  constexpr int LD = 64;
+  constexpr int S = kSwapRmatStages;
+  constexpr int HSUB = 64 * CW * 2;      // half a chunk tile (64 cells x 64 genes), 8 KB
+  constexpr int STAGE = 4 * HSUB;        // 64 cells x 256 genes
+  constexpr int Q_BYTES = TM * 128 * 2;  // 128 cells x 128 image columns
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = align1024(smem_raw);
+  uint8_t* As = smem;
+  uint8_t* Qs = As + S * STAGE;  // [2 buffers]
+  SegMeta* mring = reinterpret_cast<SegMeta*>(Qs + 2 * Q_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(mring + 2 * kMaxChunks);
+  uint64_t* full = bars;
+  uint64_t* empty = full + S;
+  uint64_t* qfull = empty + S;
+  uint64_t* qempty = qfull + 2;
+  uint64_t* mfull = qempty + 2;
+  uint64_t* mempty = mfull + 2;
+  uint64_t* done_bar = mempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done_bar + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gg = blockIdx.x % n_gene_groups;
+  const int rg = blockIdx.x / n_gene_groups;
+  const int R = gridDim.x / n_gene_groups;
+  const int64_t t0 = (int64_t)rg * n_tiles / R, t1 = (int64_t)(rg + 1) * n_tiles / R;
+  const int n_quads = (nc + 3) / 4;
+  const int qd0 = gg * kSwapQuads, qd1 = min(n_quads, qd0 + kSwapQuads);
+  const int nq = max(0, qd1 - qd0);
+  const bool have_work = (t1 > t0) && nq > 0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 8);  // the eight warps of one team
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&qfull[b], 1);
+      mbar_init(&qempty[b], 1);
+      mbar_init(&mfull[b], 1);
+      mbar_init(&mempty[b], 4 * kGroups);
+    }
+    mbar_init(done_bar, 1);
+    *abort_flag = 0;
+    mbar_fence_init();
+  }
+  if (warp == W_MMA) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < W_EPI) {
+    // ---- densify: team h (warps 8 h .. 8 h + 7) fills the half-tile stages
+    // of cells 64 h .. 64 h + 63; warp (c, r) of a team takes chunk 4 qd + c,
+    // quarter 2 h + r of the tile ----
+    const int h = warp >> 3, cofs = (warp >> 1) & 3, q = 2 * h + (warp & 1);
+    uint32_t ti = 0;
+    uint4 w[kRmatRegs];
+    Span pre{-1, -1};  // span whose loads are in flight in w
+    if (have_work)
+      for (int64_t t = t0; t < t1; ++t, ++ti) {
+        if (!warp_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 21)) goto done;
+        const SegMeta* mt = mring + (ti & 1u) * kMaxChunks;
+        for (int jq = 0; jq < nq; ++jq) {
+          const uint32_t it = (ti * (uint32_t)nq + jq) * 2u + h;  // this stage in the MMA's order
+          const int ch = 4 * (qd0 + jq) + cofs;
+          const bool has = ch < nc;
+          const Span sp = has ? quarter_span(mt[ch], q) : Span{0, 0};
+          if (has && (sp.lo != pre.lo || sp.hi != pre.hi)) span_load<kRmatRegs>(ent, sp, lane, w);
+          const int s = it % S;
+          if (!warp_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 22)) goto done;
+          if (has) {
+            // entry offsets address the whole 128-row tile: rows 64 h.. start 8 KB before the half
+            const uint32_t tile = smem_u32(As + s * STAGE + cofs * HSUB) - h * HSUB;
+            zero_rows(tile, q, lane);
+            __syncwarp();
+            span_scatter<kRmatRegs>(tile, ent, sp, lane, w);
+          }
+          // the warp's next segment: the next quad of this tile, or the first of the next tile
+          pre = Span{-1, -1};
+          if (jq + 1 < nq) {
+            if (ch + 4 < nc) pre = quarter_span(mt[ch + 4], q);
+          } else if (t + 1 < t1 && 4 * qd0 + cofs < nc) {
+            if (!warp_wait(&mfull[(ti + 1) & 1u], ((ti + 1) >> 1) & 1u, abort_flag, err, 21)) goto done;
+            pre = quarter_span(mring[((ti + 1) & 1u) * kMaxChunks + 4 * qd0 + cofs], q);
+          }
+          if (pre.lo >= 0) span_load<kRmatRegs>(ent, pre, lane, w);
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&full[s]);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&mempty[ti & 1u]);
+      }
+  } else if (warp < W_MMA) {
+    // ---- epilogue: lane pair (2 j, 2 j + 1) -> column j of the partial ----
+    const int q = warp & 3;
+    const int p = lane & 1, j = 16 * q + (lane >> 1);
+    if (have_work && !warp_wait(done_bar, 0, abort_flag, err, 24)) goto done;
+    tc_fence_after();
+    for (int jq = 0; jq < nq; ++jq) {
+      const uint32_t tbase = tmem + ((32u * q) << 16) + jq * 256;
+      const int64_t gene0 = (int64_t)(qd0 + jq) * 256;
+#pragma unroll 1
+      for (int gb = 0; gb < 16; ++gb) {  // 16 genes per TMEM load
+        uint32_t r[16];
+        if (have_work) {
+          tmem_ld16(tbase + gb * 16, r);
+          tmem_wait_ld();
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) r[i] = 0u;
+        }
+        float v[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const float x = __uint_as_float(r[i]);
+          v[i] = x + __shfl_xor_sync(0xffffffffu, x, 1);
+        }
+        // lane p writes genes 2 i + p: 16 consecutive columns per gene row
+#pragma unroll
+        for (int i = 0; i < 16; i += 2) {
+          const int64_t gene = gene0 + gb * 16 + i + p;
+          if (gene < g) part[((int64_t)rg * g + gene) * LD + j] = p ? v[i + 1] : v[i];
+        }
+      }
+    }
+  } else if (warp == W_MMA) {
+    // ---- MMA issuer: per stage, eight K = 16 steps over the quad's 256 genes ----
+    if (lane == 0 && have_work) {
+      const uint64_t qdesc0 = sdesc_sw128(smem_u32(Qs), TM * 128, 1024);  // MN-major, two 64-column blocks
+      const uint64_t tdesc0 = sdesc_sw128(smem_u32(As), HSUB, 1024);      // MN-major, four 64-gene blocks
+      uint32_t it = 0, ti = 0;
+      bool ok = true;
+      for (int64_t t = t0; t < t1 && ok; ++t, ++ti) {
+        const uint32_t b = ti & 1u;
+        if (!mbar_wait(&qfull[b], (ti >> 1) & 1u, abort_flag, err, 25)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint64_t qd = qdesc0 + (uint64_t)(b * (Q_BYTES >> 4));
+        for (int jq = 0; jq < nq && ok; ++jq) {
+          const int nch = min(4, nc - 4 * (qd0 + jq));  // chunk tiles in this quad
+          const uint32_t idesc = idesc_f16(128, 64 * nch, fmt, 1, 1);
+          const uint32_t d = tmem + jq * 256;
+          for (int h = 0; h < 2; ++h, ++it) {  // the two half tiles
+            const int s = it % S;
+            if (!mbar_wait(&full[s], (it / S) & 1u, abort_flag, err, 26)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint64_t td = tdesc0 + (uint64_t)(s * (STAGE >> 4));
+            const uint64_t qh = qd + (uint64_t)(h * (64 * 128 >> 4));  // cells 64 h.. of the image tile
+            umma_f16(d, qh, td, idesc, (ti | h) != 0);
+#pragma unroll
+            for (int kk = 1; kk < 64 / 16; ++kk)  // K steps of 16 cells: +2 KB down both operands
+              umma_f16(d, qh + 128 * kk, td + 128 * kk, idesc, 1u);
+            umma_commit(&empty[s]);
+          }
+        }
+        if (!ok) break;
+        umma_commit(&qempty[b]);
+      }
+      if (ok) umma_commit(done_bar);
+    }
+    __syncwarp();
+  } else if (warp == W_DENSE) {
+    // ---- dense loader: image tiles of Q, double-buffered per row tile ----
+    if (lane == 0 && have_work) {
+      uint32_t ti = 0;
+      for (int64_t t = t0; t < t1; ++t, ++ti) {
+        const uint32_t b = ti & 1u;
+        if (!mbar_wait(&qempty[b], ((ti >> 1) & 1u) ^ 1u, abort_flag, err, 28)) break;
+        uint8_t* qb = Qs + b * Q_BYTES;
+        mbar_arrive_expect_tx(&qfull[b], Q_BYTES);
+        tma_load_2d(qb, &qmap, &qfull[b], 0, (int)(t * TM));
+        tma_load_2d(qb + TM * 128, &qmap, &qfull[b], 64, (int)(t * TM));
+      }
+    }
+    __syncwarp();
+  } else if (warp == W_META) {
+    // ---- meta loader: tile metadata, and this gene group's entries of the tile into L2 ----
+    if (lane == 0 && have_work) {
+      uint32_t ti = 0;
+      for (int64_t t = t0; t < t1; ++t, ++ti) {
+        if (!load_meta(meta + t * nc, nc, mring, kMaxChunks, mfull, mempty, ti, abort_flag, err, 27)) break;
+        if (!mbar_wait(&mfull[ti & 1u], (ti >> 1) & 1u, abort_flag, err, 29)) break;
+        prefetch_segments(ent, mring + (ti & 1u) * kMaxChunks, 4 * qd0, min(nc, 4 * qd1));
+      }
+    }
+    __syncwarp();
+  }
+done:
+  if (*abort_flag) __nanosleep(500000);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == W_MMA) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
   }
 }
 
@@ -951,71 +1407,74 @@ int make_tmap16(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, 
   return (int)r;
 }
 
-cudaError_t launch_fwd_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc,
-                          const CUtensorMap* vhi, const CUtensorMap* vlo, const float* mc, float* Y,
-                          uint16_t* Yhi, uint16_t* Ylo, int fmt, int* err, cudaStream_t st, int num_sms) {
+cudaError_t launch_fwd_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc, const CUtensorMap* vmap,
+                          const float* mc, float* Y, uint16_t* Yimg, int fmt, int* err, cudaStream_t st, int num_sms) {
   const int64_t n_tiles = (n + TM - 1) / TM;
-  const int grid = (int)std::min<int64_t>(n_tiles, (int64_t)num_sms);
   const SegMeta* m = static_cast<const SegMeta*>(meta);
   note_launches(1);
   if (ld == 64) {
-    size_t smem = fwd_smem(64);
-    cudaFuncSetAttribute(k_fwd_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_fwd_tc<64><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, n, *vhi, *vlo, mc, Y, Yhi, Ylo, fmt, err);
+    const int grid = (int)std::min<int64_t>((n_tiles + 1) / 2, (int64_t)num_sms);
+    const size_t smem = fwd_swap_smem();
+    cudaFuncSetAttribute(k_fwd_swap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fwd_swap<<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, n, *vmap, mc, Y, Yimg, fmt, err);
   } else {
-    size_t smem = fwd_smem(128);
+    const int grid = (int)std::min<int64_t>(n_tiles, (int64_t)num_sms);
+    const size_t smem = fwd_smem(128);
     cudaFuncSetAttribute(k_fwd_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_fwd_tc<128><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, n, *vhi, *vlo, mc, Y, Yhi, Ylo, fmt, err);
+    k_fwd_tc<128><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, n, *vmap, mc, Y, Yimg, fmt, err);
   }
   return cudaGetLastError();
 }
 
 int rmat_tc_groups(int ld, int nc, int num_sms, int* gene_groups) {
-  const int spg = 256 / ld;  // 512 TMEM columns / (2 ld) per super-chunk
-  const int n_super = (nc + 1) / 2;
-  const int G = (n_super + spg - 1) / spg;
+  int G;
+  if (ld == 64) {
+    G = ((nc + 3) / 4 + kSwapQuads - 1) / kSwapQuads;  // 512 genes per CTA
+  } else {
+    const int spg = 256 / ld;  // 512 TMEM columns / (2 ld) per super-chunk
+    G = ((nc + 1) / 2 + spg - 1) / spg;
+  }
   *gene_groups = G;
   return std::max(1, num_sms / G);  // row groups
 }
 
 cudaError_t launch_rmat_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc, int64_t g,
-                           int gene_groups, int row_groups, const CUtensorMap* qhi, const CUtensorMap* qlo,
-                           float* part, int fmt, int* err, cudaStream_t st) {
+                           int gene_groups, int row_groups, const CUtensorMap* qmap, float* part, int fmt, int* err,
+                           cudaStream_t st) {
   const int64_t n_tiles = (n + TM - 1) / TM;
   const int grid = gene_groups * row_groups;
   const SegMeta* m = static_cast<const SegMeta*>(meta);
   note_launches(1);
   if (ld == 64) {
-    size_t smem = rmat_smem(64);
-    cudaFuncSetAttribute(k_rmat_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_rmat_tc<64><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, g, gene_groups, *qhi, *qlo, part, fmt, err);
+    const size_t smem = rmat_swap_smem();
+    cudaFuncSetAttribute(k_rmat_swap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_rmat_swap<<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, g, gene_groups, *qmap, part, fmt, err);
   } else {
-    size_t smem = rmat_smem(128);
+    const size_t smem = rmat_smem(128);
     cudaFuncSetAttribute(k_rmat_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_rmat_tc<128><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, g, gene_groups, *qhi, *qlo, part, fmt, err);
+    k_rmat_tc<128><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, g, gene_groups, *qmap, part, fmt, err);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_split16(float* in, int64_t count, uint16_t* hi, uint16_t* lo, int fmt, int write_back,
-                           cudaStream_t st, int num_sms) {
+cudaError_t launch_split16(const float* in, int64_t count, uint16_t* img, int fmt, cudaStream_t st, int num_sms) {
   note_launches(1);
-  k_split16<<<grid_for(count, 256, num_sms), 256, 0, st>>>(in, count, hi, lo, fmt, write_back);
+  k_split16<<<grid_for(count, 256, num_sms), 256, 0, st>>>(in, count, reinterpret_cast<uint32_t*>(img), fmt);
   return cudaGetLastError();
 }
 
-int launch_gram_tc(int64_t n, const CUtensorMap* qhi, const CUtensorMap* qlo, double* part, int fmt, int* err,
-                   cudaStream_t st, int num_sms) {
+int launch_gram_tc(int64_t n, const CUtensorMap* qmap, double* part, int fmt, int* err, cudaStream_t st,
+                   int num_sms) {
   const int64_t n_tiles = (n + TM - 1) / TM;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, num_sms));
   const size_t smem = 1024 + (size_t)kGramStages * 2 * TM * 64 * 2 + TM * 64 * 2 + TM * 64 * 4 + 256;
   cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   note_launches(1);
-  k_gram_tc<<<grid, 128, smem, st>>>(n_tiles, *qhi, *qlo, part, fmt, err);
+  k_gram_tc<<<grid, 128, smem, st>>>(n_tiles, *qmap, part, fmt, err);
   return cudaGetLastError() == cudaSuccess ? grid : -1;
 }
 
-size_t fwd_tc_smem_bytes(int ld) { return fwd_smem(ld); }
-size_t rmat_tc_smem_bytes(int ld) { return rmat_smem(ld); }
+size_t fwd_tc_smem_bytes(int ld) { return ld == 64 ? fwd_swap_smem() : fwd_smem(ld); }
+size_t rmat_tc_smem_bytes(int ld) { return ld == 64 ? rmat_swap_smem() : rmat_smem(ld); }
 
 }  // namespace scx

@@ -67,10 +67,9 @@ cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shif
 // Tall apply: Out[i, :] = In[i, :] * M (ld x ld float, upper-triangular or full).
 cudaError_t launch_apply_right_f32(const float* In, int64_t n, int ld, const float* M,
                                    float* Out, cudaStream_t st, int num_sms);
-// Same, also writing the hi/lo 16-bit planes of Out (row stride ld; fmt 1 =
-// bf16, 0 = f16).
+// Same, also writing the 16-bit image of Out (n x 2 ld; fmt 1 = bf16, 0 = f16).
 cudaError_t launch_apply_right_split(const float* In, int64_t n, int ld, const float* M, float* Out,
-                                     uint16_t* hi, uint16_t* lo, int fmt, cudaStream_t st, int num_sms);
+                                     uint16_t* img, int fmt, cudaStream_t st, int num_sms);
 // Gene-side ops (n_vars x ld, FP64):
 //   Z = (W - mu s^T) M        (mu may be null)
 cudaError_t launch_center_apply(const double* W, int64_t g, int ld, const double* mu,
@@ -121,24 +120,26 @@ cudaError_t tile_format_fill(const int64_t* indptr, const int32_t* idx, const vo
 // TMA map of a row-major [rows][cols] 16-bit matrix (fmt 1 = bf16, 0 = f16);
 // returns the CUresult.
 int make_tmap16(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, int box_rows, int fmt);
-// Y (n x ld, FP32) = A (Vhi + Vlo) - mc, plus the hi/lo 16-bit planes of Y.
-cudaError_t launch_fwd_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc,
-                          const CUtensorMap* vhi, const CUtensorMap* vlo, const float* mc, float* Y,
-                          uint16_t* Yhi, uint16_t* Ylo, int fmt, int* err, cudaStream_t st, int num_sms);
-// Partials part[row_group][g][ld] of A^T (Qhi + Qlo); returns row groups.
+// 16-bit image of a float matrix M (rows x ld): rows x 2 ld values, column
+// 2 j = hi(M[:, j]) = round16(M[:, j]), column 2 j + 1 = round16(M[:, j] - hi).
+// Y (n x ld, FP32; may be null) = A V - mc with V given by its image (map
+// vmap), plus the image of Y.
+cudaError_t launch_fwd_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc, const CUtensorMap* vmap,
+                          const float* mc, float* Y, uint16_t* Yimg, int fmt, int* err, cudaStream_t st, int num_sms);
+// Partials part[row_group][g][ld] of A^T Q, Q given by its image (map qmap);
+// returns row groups.
 int rmat_tc_groups(int ld, int nc, int num_sms, int* gene_groups);
 cudaError_t launch_rmat_tc(int ld, const uint32_t* ent, const void* meta, int64_t n, int nc, int64_t g,
-                           int gene_groups, int row_groups, const CUtensorMap* qhi, const CUtensorMap* qlo,
-                           float* part, int fmt, int* err, cudaStream_t st);
-// Gram partials [G (64 x 64), colsum (64)] of (hi + lo) on tensor cores, ld 64;
-// returns the number of partials written, or -1 on a launch error.
-int launch_gram_tc(int64_t n, const CUtensorMap* qhi, const CUtensorMap* qlo, double* part, int fmt, int* err,
-                   cudaStream_t st, int num_sms);
+                           int gene_groups, int row_groups, const CUtensorMap* qmap, float* part, int fmt, int* err,
+                           cudaStream_t st);
+// Gram partials [G (64 x 64), colsum (64)] of hi + lo from the image (ld 64)
+// on tensor cores; returns the number of partials written, or -1 on a launch
+// error.
+int launch_gram_tc(int64_t n, const CUtensorMap* qmap, double* part, int fmt, int* err, cudaStream_t st, int num_sms);
 size_t fwd_tc_smem_bytes(int ld);
 size_t rmat_tc_smem_bytes(int ld);
-// hi = round16(x), lo = round16(x - hi); lo may be null; write_back: x = hi.
-cudaError_t launch_split16(float* in, int64_t count, uint16_t* hi, uint16_t* lo, int fmt, int write_back,
-                           cudaStream_t st, int num_sms);
+// Image of count floats: img[2 i] = round16(x_i), img[2 i + 1] = round16(x_i - img[2 i]).
+cudaError_t launch_split16(const float* in, int64_t count, uint16_t* img, int fmt, cudaStream_t st, int num_sms);
 
 // ---- truncated-SVD adjoint (kernels_adjoint.cu) ----
 // Column sums (FP64) of a tall float matrix A (n x ld, first ncols columns)

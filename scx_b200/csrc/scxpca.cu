@@ -255,8 +255,10 @@ struct scxpca_plan {
   bool use_tc = false;
   int fmt16 = 1;  // 1 = bf16, 0 = f16
   int n_chunks = 0, tc_gene_groups = 0, tc_row_groups = 0;
-  DevBuf tf_meta, tf_ent, V16, V16lo, Y16, Q16lo, tc_part, tc_err;
-  CUtensorMap vmap{}, vmap_lo{}, qmap_hi{}, qmap_lo{};
+  // 16-bit images (column 2 j = hi, 2 j + 1 = lo of column j) of the dense
+  // operands of the tensor-core products: V (g x 2 ld) and the tall Y/Q (n x 2 ld)
+  DevBuf tf_meta, tf_ent, Vimg, Yimg, tc_part, tc_err;
+  CUtensorMap vmap{}, qmap{};
 
   // differentiation: raw per-gene centre c and scale s of X~ = (X - 1 c^T) diag(s)
   // (device, n_vars each), whether the last run's Ritz state (B in Z, E, evals)
@@ -626,23 +628,18 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       pl->tf_meta.alloc(tile_meta_bytes(n, pl->n_chunks));
       CK(tile_format_fill(pl->indptr, pl->idx, pl->val, n, pl->n_chunks, seg.as<int64_t>(),
                           pl->tf_ent.as<uint32_t>(), pl->tf_meta.p, st, pl->num_sms));
-      pl->V16.alloc(sizeof(uint16_t) * g * ld);
-      pl->V16lo.alloc(sizeof(uint16_t) * g * ld);
-      pl->Y16.alloc(sizeof(uint16_t) * n * ld);
-      pl->Q16lo.alloc(sizeof(uint16_t) * n * ld);
+      pl->Vimg.alloc(sizeof(uint16_t) * g * 2 * ld);
+      pl->Yimg.alloc(sizeof(uint16_t) * n * 2 * ld);
       pl->tc_err.alloc(sizeof(int) * 4);
       CK(cudaMemsetAsync(pl->tc_err.p, 0, sizeof(int) * 4, st));
       pl->tc_row_groups = rmat_tc_groups((int)ld, pl->n_chunks, pl->num_sms, &pl->tc_gene_groups);
       pl->tc_row_groups = (int)std::min<int64_t>(pl->tc_row_groups, n_tiles);  // no idle row groups
       pl->tc_part.alloc(sizeof(float) * (size_t)pl->tc_row_groups * g * ld);
-      int r1 = make_tmap16(&pl->vmap, pl->V16.p, g, ld, 64, pl->fmt16);
-      int r4 = make_tmap16(&pl->vmap_lo, pl->V16lo.p, g, ld, 64, pl->fmt16);
-      int r2 = make_tmap16(&pl->qmap_hi, pl->Y16.p, n, ld, 128, pl->fmt16);
-      int r3 = make_tmap16(&pl->qmap_lo, pl->Q16lo.p, n, ld, 128, pl->fmt16);
-      if (r1 || r2 || r3 || r4)
-        fail(SCXPCA_CUDA_ERROR, "cuTensorMapEncodeTiled failed (" + std::to_string(r1) + ", " +
-                                    std::to_string(r2) + ", " + std::to_string(r3) + ", " +
-                                    std::to_string(r4) + ")");
+      int r1 = make_tmap16(&pl->vmap, pl->Vimg.p, g, 2 * ld, 64, pl->fmt16);
+      int r2 = make_tmap16(&pl->qmap, pl->Yimg.p, n, 2 * ld, 128, pl->fmt16);
+      if (r1 || r2)
+        fail(SCXPCA_CUDA_ERROR,
+             "cuTensorMapEncodeTiled failed (" + std::to_string(r1) + ", " + std::to_string(r2) + ")");
     }
 
     // ---- transposed-product tables ----
@@ -732,8 +729,8 @@ void collect_stages(scxpca_plan* pl) {
 }
 
 // Tall Gram + Cholesky (FP64) of a tall matrix A.  With `planes` (tensor-core
-// path, ld 64) the Gram is taken on tensor cores from the hi/lo 16-bit planes
-// of A held in Y16/Q16lo; otherwise from the FP32 A with FP64 FMAs.
+// path, ld 64) the Gram is taken on tensor cores from the 16-bit image of A
+// held in Yimg; otherwise from the FP32 A with FP64 FMAs.
 void tall_chol(scxpca_plan* pl, const float* A, int64_t rows, double* Rinv, float* Rinv_f,
                int shift, bool planes = false) {
   cudaStream_t st = pl->stream;
@@ -741,7 +738,7 @@ void tall_chol(scxpca_plan* pl, const float* A, int64_t rows, double* Rinv, floa
   int parts = (int)std::max<int64_t>(1, std::min<int64_t>(pl->gram_parts, (rows + 31) / 32));
   int s = stage_begin(pl);
   if (planes && pl->use_tc && ld == 64) {
-    parts = launch_gram_tc(rows, &pl->qmap_hi, &pl->qmap_lo, pl->gpart.as<double>(), pl->fmt16,
+    parts = launch_gram_tc(rows, &pl->qmap, pl->gpart.as<double>(), pl->fmt16,
                            pl->tc_err.as<int>(), st, pl->num_sms);
     if (parts < 0) CK(cudaGetLastError());
   } else
@@ -773,21 +770,20 @@ void small_qr(scxpca_plan* pl, double* A, int shift) {
 
 // W = X^T A (raw, uncentred), FP64, for a tall float A (n x ld).
 // W = X^T A (raw, uncentred) into pl->W (FP64).  On the tensor-core path the
-// tall operand enters as two 16-bit planes Y16 (hi) and Q16lo (lo): `split`
-// != 0 first splits the FP32 A into them; otherwise they already hold the
-// forward product's planes of A.
+// tall operand enters as its 16-bit image Yimg: `split` != 0 first writes
+// the image of the FP32 A; otherwise it already holds the image of A (the
+// forward product's, or the explicit Q's).
 void rmatmat_raw(scxpca_plan* pl, float* A, int split) {
   cudaStream_t st = pl->stream;
   if (pl->use_tc) {
     int s = stage_begin(pl);
     if (split)
-      CK(launch_split16(A, pl->n * pl->ld, pl->Y16.as<uint16_t>(), pl->Q16lo.as<uint16_t>(), pl->fmt16, 0,
-                        st, pl->num_sms));
+      CK(launch_split16(A, pl->n * pl->ld, pl->Yimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
     stage_end(pl, SCXPCA_STAGE_APPLY, s);
     s = stage_begin(pl);
     CK(launch_rmat_tc((int)pl->ld, pl->tf_ent.as<uint32_t>(), pl->tf_meta.p, pl->n, pl->n_chunks, pl->g,
-                      pl->tc_gene_groups, pl->tc_row_groups, &pl->qmap_hi, &pl->qmap_lo,
-                      pl->tc_part.as<float>(), pl->fmt16, pl->tc_err.as<int>(), st));
+                      pl->tc_gene_groups, pl->tc_row_groups, &pl->qmap, pl->tc_part.as<float>(), pl->fmt16,
+                      pl->tc_err.as<int>(), st));
     stage_end(pl, SCXPCA_STAGE_TRANSPOSE, s);
     s = stage_begin(pl);
     CK(launch_reduce_rows_f32(pl->tc_part.as<float>(), pl->tc_row_groups, pl->g * pl->ld,
@@ -806,21 +802,20 @@ void rmatmat_raw(scxpca_plan* pl, float* A, int split) {
   stage_end(pl, SCXPCA_STAGE_REDUCE, s);
 }
 
-// Y = (X - mu) V.  On the tensor-core path V enters as hi/lo 16-bit planes and
-// the product also leaves the hi/lo planes of Y for the Gram and the
-// transposed product; `f32` = false skips the FP32 copy of Y when nothing
-// reads it (inside the power loop at ld 64, whose Gram uses the planes).
+// Y = (X - mu) V.  On the tensor-core path V enters as its 16-bit image and
+// the product also leaves the image of Y for the Gram and the transposed
+// product; `f32` = false skips the FP32 copy of Y when nothing reads it
+// (inside the power loop at ld 64, whose Gram uses the image).
 void forward(scxpca_plan* pl, bool f32 = true) {
   cudaStream_t st = pl->stream;
   if (pl->use_tc) {
     int s = stage_begin(pl);
-    CK(launch_split16(pl->V.as<float>(), pl->g * pl->ld, pl->V16.as<uint16_t>(), pl->V16lo.as<uint16_t>(),
-                      pl->fmt16, 0, st, pl->num_sms));
+    CK(launch_split16(pl->V.as<float>(), pl->g * pl->ld, pl->Vimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
     stage_end(pl, SCXPCA_STAGE_SMALL, s);
     s = stage_begin(pl);
     CK(launch_fwd_tc((int)pl->ld, pl->tf_ent.as<uint32_t>(), pl->tf_meta.p, pl->n, pl->n_chunks, &pl->vmap,
-                     &pl->vmap_lo, pl->mc.as<float>(), f32 ? pl->Y.as<float>() : nullptr, pl->Y16.as<uint16_t>(),
-                     pl->Q16lo.as<uint16_t>(), pl->fmt16, pl->tc_err.as<int>(), st, pl->num_sms));
+                     pl->mc.as<float>(), f32 ? pl->Y.as<float>() : nullptr, pl->Yimg.as<uint16_t>(), pl->fmt16,
+                     pl->tc_err.as<int>(), st, pl->num_sms));
     stage_end(pl, SCXPCA_STAGE_FORWARD, s);
     return;
   }
@@ -891,7 +886,7 @@ void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
   stage_end(pl, SCXPCA_STAGE_SMALL, s);
   // Y = (X - mu) Omega ; qr(Y).  Only the last forward product's FP32 Y is
   // read (by the explicit Q below); the tensor-core Gram at ld 64 reads the
-  // 16-bit planes.
+  // 16-bit image.
   const bool planes_only = pl->use_tc && ld == 64;
   forward(pl, !planes_only || p.n_power_iterations == 0);
   tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
@@ -909,9 +904,9 @@ void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
   }
   // Explicit Q = Y R^{-1}, re-orthonormalised by a second FP64 Cholesky pass.
   s = stage_begin(pl);
-  if (pl->use_tc)  // with the hi/lo planes of Q for the tensor-core Gram and transposed product
+  if (pl->use_tc)  // with the 16-bit image of Q for the tensor-core Gram and transposed product
     CK(launch_apply_right_split(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(),
-                                pl->Y16.as<uint16_t>(), pl->Q16lo.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
+                                pl->Yimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
   else
     CK(launch_apply_right_f32(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(), st,
                               pl->num_sms));

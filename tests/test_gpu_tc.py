@@ -23,6 +23,7 @@ SHAPES = [
     (77, 130, 10),      # fewer cells than a tile
     (4099, 2000, 60),   # the benchmark gene count
     (2500, 700, 100),   # ld 128
+    (40000, 520, 30),   # more two-tile bands than SMs, odd chunk count
 ]
 
 
