@@ -1000,28 +1000,26 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t tbase = tmem + ((32u * q) << 16) + a * 256 + u * 128;
         const int64_t row0 = (band * 2 + u) * TM;
 #pragma unroll 1
-        for (int cb = 0; cb < TM / 16; ++cb) {  // 16 cells per TMEM load
-          uint32_t r[16];
-          tmem_ld16(tbase + cb * 16, r);
+        for (int cb = 0; cb < TM / 32; ++cb) {  // 32 cells per TMEM load
+          uint32_t r[32];
+          tmem_ld32(tbase + cb * 32, r);
           tmem_wait_ld();
-          float v[16];
+          const int64_t c0 = row0 + cb * 32;
+          const int lim = (int)min((int64_t)32, n - c0);  // cells of this block inside the matrix
+          uint16_t* dst = Yimg + c0 * 128 + 32 * q + lane;  // this lane's image column
+          float* ydst = Y ? Y + c0 * LD + j : nullptr;
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            const float x = __uint_as_float(r[i]);
-            v[i] = x + __shfl_xor_sync(0xffffffffu, x, 1) - mcj;
-          }
-          const int64_t c0 = row0 + cb * 16;
-#pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            if (c0 + i < n) {
-              const uint32_t hl = hilo16(v[i], fmt);
-              Yimg[(c0 + i) * 128 + 32 * q + lane] = (uint16_t)(p ? hl >> 16 : hl & 0xFFFFu);
-            }
-          }
-          if (Y) {  // the FP32 copy only when the caller reads it: lane p writes cell 2 i + p
-#pragma unroll
-            for (int i = 0; i < 16; i += 2)
-              if (c0 + i + p < n) Y[(c0 + i + p) * LD + j] = p ? v[i + 1] : v[i];
+          for (int i = 0; i < 32; i += 2) {
+            const float x0 = __uint_as_float(r[i]), x1 = __uint_as_float(r[i + 1]);
+            const float s0 = x0 + __shfl_xor_sync(0xffffffffu, x0, 1) - mcj;
+            const float s1 = x1 + __shfl_xor_sync(0xffffffffu, x1, 1) - mcj;
+            // (hi, lo) of two cells at once; lane p keeps half p of each
+            const uint32_t h2 = pack16x2(s0, s1, fmt);
+            const uint32_t l2 = pack16x2(s0 - unpack16(h2 & 0xFFFFu, fmt), s1 - unpack16(h2 >> 16, fmt), fmt);
+            const uint32_t mine = p ? l2 : h2;
+            if (i < lim) dst[i * 128] = (uint16_t)(mine & 0xFFFFu);
+            if (i + 1 < lim) dst[(i + 1) * 128] = (uint16_t)(mine >> 16);
+            if (ydst && i + p < lim) ydst[(i + p) * LD] = p ? s1 : s0;  // lane p writes cell i + p
           }
         }
       }
