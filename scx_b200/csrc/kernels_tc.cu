@@ -68,18 +68,19 @@ struct SegMeta {
 };
 static_assert(sizeof(SegMeta) == 16, "segment metadata is one 16-byte record");
 
-// Pipeline shapes.  In the forward kernel densify group g takes the stages
-// it with it % G == g and owns A stage buffers g and g + G (S == 2 G), so it
-// densifies its next segment while the MMAs read the previous one.  In the
-// transposed kernel a stage (two 64-gene sub-tiles) is filled by a pair of
-// groups, one sub-tile each; pair p takes the stages it with it % 2 == p and
-// owns buffers p and p + 2 (S == 4 at ld 64).  Either way each waiter runs at
-// most one barrier phase ahead of the phase it waits for, which is what a
-// parity wait can distinguish.  The forward kernel's dense operand has its
-// own ring of fwd_bslots(LD) chunk buffers, filled ahead of the MMAs.
+// Pipeline shapes of the ld-128 kernels (k_fwd_tc, k_rmat_tc; ld 64 has its
+// own, next to k_fwd_swap / k_rmat_swap).  In the forward kernel densify group
+// g takes the stages it with it % G == g and owns A stage buffers g and g + G
+// (S == 2 G), so it densifies its next segment while the MMAs read the
+// previous one.  In the transposed kernel a stage (two 64-gene sub-tiles) is
+// filled by a pair of groups, one sub-tile each; pair p takes the stages it
+// with it % 2 == p.  Either way each waiter runs at most one barrier phase
+// ahead of the phase it waits for, which is what a parity wait can
+// distinguish.  The forward kernel's dense operand has its own ring of
+// fwd_bslots(LD) chunk buffers, filled ahead of the MMAs.
 __host__ __device__ constexpr int fwd_stages(int LD) { return 2 * kGroups; }
-__host__ __device__ constexpr int fwd_bslots(int LD) { return LD == 64 ? 4 : 2; }
-__host__ __device__ constexpr int rmat_stages(int LD) { return LD == 64 ? 4 : 2; }
+__host__ __device__ constexpr int fwd_bslots(int LD) { return 2; }
+__host__ __device__ constexpr int rmat_stages(int LD) { return 2; }
 // 16-byte entry words a densify lane keeps in flight per segment quarter
 // (x 128 entries per warp); a larger quarter loads the rest on demand.
 constexpr int kFwdRegs = 4;
