@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               int64_t g, int n_gene_groups, const __grid_constant__ CUtensorMap qmap, float* __restrict__ part,
               int fmt, int* err) {
   constexpr int N2 = 2 * LD;
-  constexpr int S = rmat_stages(LD);     // A stages (even: two per pair of densify groups at ld 64)
+  constexpr int S = rmat_stages(LD);     // A stages, one per pair of densify groups
   constexpr int SUB = TM * CW * 2;       // one 64-gene sub-tile, 16 KB
   constexpr int A_BYTES = 2 * SUB;       // 128 genes
   constexpr int Q_BYTES = TM * N2 * 2;   // 128 cells x N2 image columns
