@@ -218,8 +218,18 @@ __device__ __forceinline__ void scatter_one(uint32_t tile, uint32_t w) { sts_u16
 struct Span {
   int64_t lo, hi;
 };
+// `m` lives in shared memory (the metadata ring): one 16-byte load, then
+// warp-uniform selects (q is the warp's quarter).
 __device__ __forceinline__ Span quarter_span(const SegMeta& m, int q) {
-  return Span{m.start + (q ? (int64_t)m.q[q - 1] : 0), m.start + (int64_t)m.q[q]};
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(smem_u32(&m)));
+  const int64_t start = (int64_t)(((uint64_t)v.y << 32) | v.x);
+  const uint32_t q0 = v.z & 0xFFFFu, q1 = v.z >> 16, q2 = v.w & 0xFFFFu, q3 = v.w >> 16;
+  const uint32_t hi = q == 0 ? q0 : q == 1 ? q1 : q == 2 ? q2 : q3;
+  const uint32_t lo = q == 0 ? 0u : q == 1 ? q0 : q == 2 ? q1 : q2;
+  return Span{start + (int64_t)lo, start + (int64_t)hi};
 }
 
 // Issue the first R 16-byte loads of a span (its start rounded down to a
@@ -228,10 +238,12 @@ __device__ __forceinline__ Span quarter_span(const SegMeta& m, int q) {
 template <int R>
 __device__ __forceinline__ void span_load(const uint32_t* __restrict__ ent, Span sp, int lane, uint4 (&w)[R]) {
   const int64_t a0 = sp.lo & ~int64_t(3);
+  const int phi = (int)(sp.hi - a0);
+  const uint32_t* base = ent + a0;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    const int64_t e = a0 + 4 * (lane + 32 * r);
-    w[r] = e < sp.hi ? ldg_entries(ent + e) : make_uint4(0u, 0u, 0u, 0u);
+    const int p = 4 * (lane + 32 * r);
+    w[r] = p < phi ? ldg_entries(base + p) : make_uint4(0u, 0u, 0u, 0u);
   }
 }
 
