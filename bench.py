@@ -52,7 +52,7 @@ FALLBACK_HBM_GBS = 6650.0
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch / its 57,193,010
 # nonzeros).  Traffic grows in proportion to the nonzeros at fixed density, so
 # the figure scales to the bench workload.
-NCU_TRAFFIC_BYTES_PER_NNZ = {"transpose": 5.212, "forward": 6.131}
+NCU_TRAFFIC_BYTES_PER_NNZ = {"transpose": 5.210, "forward": 6.134}
 
 
 def parse():
