@@ -976,8 +976,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       const SegMeta* mt = mring + (bi & 1u) * MSLOT;
       for (int c = 0; c < nc; ++c, ++cc) {
         if ((int)(cc & 1u) != par) continue;
-        const Span sp = has ? quarter_span(mt[u * nc + c], q) : Span{0, 0};
-        if (has && (sp.lo != pre.lo || sp.hi != pre.hi)) span_load<kFwdRegs>(ent, sp, lane, w);
+        // the span loaded ahead (pre) is this segment's whenever one was loaded
+        const Span sp = !has ? Span{0, 0} : pre.lo >= 0 ? pre : quarter_span(mt[u * nc + c], q);
+        if (has && pre.lo < 0) span_load<kFwdRegs>(ent, sp, lane, w);
         const int s = cc % S;
         if (!warp_wait(&empty[s], ((cc / S) & 1u) ^ 1u, abort_flag, err, 12)) goto done;
         if (has) {
@@ -1214,8 +1215,9 @@ __global__ void __launch_bounds__(kThreads, 1)
           const uint32_t it = (ti * (uint32_t)nq + jq) * 2u + h;  // this stage in the MMA's order
           const int ch = 4 * (qd0 + jq) + cofs;
           const bool has = ch < nc;
-          const Span sp = has ? quarter_span(mt[ch], q) : Span{0, 0};
-          if (has && (sp.lo != pre.lo || sp.hi != pre.hi)) span_load<kRmatRegs>(ent, sp, lane, w);
+          // the span loaded ahead (pre) is this segment's whenever one was loaded
+          const Span sp = !has ? Span{0, 0} : pre.lo >= 0 ? pre : quarter_span(mt[ch], q);
+          if (has && pre.lo < 0) span_load<kRmatRegs>(ent, sp, lane, w);
           const int s = it % S;
           if (!warp_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 22)) goto done;
           if (has) {
