@@ -249,12 +249,13 @@ __device__ __forceinline__ void span_load(const uint32_t* __restrict__ ent, Span
 
 // The four words at span positions p .. p + 3 (counted from the span's 16-byte
 // aligned start); those outside [plo, phi) belong to the neighbouring spans.
-// 32-bit positions keep the bounds tests to one compare each.
-__device__ __forceinline__ void scatter4(uint32_t tile, const uint4& w, int p, int plo, int phi) {
-  if (p >= plo && p < phi) scatter_one(tile, w.x);
-  if (p + 1 >= plo && p + 1 < phi) scatter_one(tile, w.y);
-  if (p + 2 >= plo && p + 2 < phi) scatter_one(tile, w.z);
-  if (p + 3 >= plo && p + 3 < phi) scatter_one(tile, w.w);
+// With d = p - plo and n = phi - plo, word k is in the span iff
+// (unsigned)(d + k) < n: one 32-bit compare per word.
+__device__ __forceinline__ void scatter4(uint32_t tile, const uint4& w, int d, unsigned n) {
+  if ((unsigned)d < n) scatter_one(tile, w.x);
+  if ((unsigned)(d + 1) < n) scatter_one(tile, w.y);
+  if ((unsigned)(d + 2) < n) scatter_one(tile, w.z);
+  if ((unsigned)(d + 3) < n) scatter_one(tile, w.w);
 }
 
 // Scatter a span into `tile` (already zeroed): the R words in flight first,
@@ -264,9 +265,10 @@ __device__ __forceinline__ void span_scatter(uint32_t tile, const uint32_t* __re
                                              const uint4 (&w)[R]) {
   const int64_t a0 = sp.lo & ~int64_t(3);
   const int plo = (int)(sp.lo - a0), phi = (int)(sp.hi - a0);  // a quarter holds at most 2,048 entries
+  const unsigned n = (unsigned)(phi - plo);
 #pragma unroll
-  for (int r = 0; r < R; ++r) scatter4(tile, w[r], 4 * (lane + 32 * r), plo, phi);
-  for (int p = 4 * (lane + 32 * R); p < phi; p += 128) scatter4(tile, ldg_entries(ent + a0 + p), p, plo, phi);
+  for (int r = 0; r < R; ++r) scatter4(tile, w[r], 4 * (lane + 32 * r) - plo, n);
+  for (int p = 4 * (lane + 32 * R); p < phi; p += 128) scatter4(tile, ldg_entries(ent + a0 + p), p - plo, n);
 }
 
 // Meta loader: L2 prefetch of the entries of segments [c0, c1) of one tile
