@@ -1026,20 +1026,19 @@ __global__ void __launch_bounds__(kThreads, 1)
           tmem_wait_ld();
           const int64_t c0 = row0 + cb * 32;
           const int lim = (int)min((int64_t)32, n - c0);  // cells of this block inside the matrix
-          uint16_t* dst = Yimg + c0 * 128 + 32 * q + lane;  // this lane's image column
+          // word j of an image row holds (hi, lo) of column j; lane p handles cell i + p
+          uint32_t* dst = reinterpret_cast<uint32_t*>(Yimg) + c0 * 64 + 16 * q + (lane >> 1);
           float* ydst = Y ? Y + c0 * LD + j : nullptr;
 #pragma unroll
           for (int i = 0; i < 32; i += 2) {
             const float x0 = __uint_as_float(r[i]), x1 = __uint_as_float(r[i + 1]);
             const float s0 = x0 + __shfl_xor_sync(0xffffffffu, x0, 1) - mcj;
             const float s1 = x1 + __shfl_xor_sync(0xffffffffu, x1, 1) - mcj;
-            // (hi, lo) of two cells at once; lane p keeps half p of each
-            const uint32_t h2 = pack16x2(s0, s1, fmt);
-            const uint32_t l2 = pack16x2(s0 - unpack16(h2 & 0xFFFFu, fmt), s1 - unpack16(h2 >> 16, fmt), fmt);
-            const uint32_t mine = p ? l2 : h2;
-            if (i < lim) dst[i * 128] = (uint16_t)(mine & 0xFFFFu);
-            if (i + 1 < lim) dst[(i + 1) * 128] = (uint16_t)(mine >> 16);
-            if (ydst && i + p < lim) ydst[(i + p) * LD] = p ? s1 : s0;  // lane p writes cell i + p
+            const float sm = p ? s1 : s0;
+            if (i + p < lim) {
+              dst[(i + p) * 64] = hilo16(sm, fmt);
+              if (ydst) ydst[(i + p) * LD] = sm;
+            }
           }
         }
       }
