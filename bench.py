@@ -618,7 +618,7 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     times = []
     for i in range(args.warmup + args.steps):
-        ms, nnz, dt = cpu_baseline(ip, ix, vv, args.n_obs, rows, threads)
+        ms, nnz, _, _ = cpu_baseline(ip, ix, vv, args.n_obs, rows, threads)
         if i >= args.warmup:
             times.append(ms)
     value = float(np.mean(times))
