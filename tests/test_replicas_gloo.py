@@ -8,7 +8,6 @@ import socket
 import sys
 from pathlib import Path
 
-import pytest
 import torch.multiprocessing as mp
 
 ROOT = Path(__file__).resolve().parents[1]
