@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (lane == 0) mbar_arrive(&mempty[ti & 1u]);
     }
   } else if (warp < W_MMA) {
-    // ---- epilogue: TMEM -> hi + lo halves -> Y (FP32) and its hi/lo 16-bit planes ----
+    // ---- epilogue: TMEM (hi, lo) column pairs -> Y (FP32) and its 16-bit image ----
     const int q = warp & 3;
     const uint32_t row = 32u * q + lane;
     uint32_t k = 0;
@@ -746,8 +746,8 @@ __global__ void __launch_bounds__(128, 1)
     k_gram_tc(int64_t n_tiles, const __grid_constant__ CUtensorMap qmap, double* __restrict__ part, int fmt,
               int* err) {
   constexpr int LD = 64;
-  constexpr int PLANE = TM * LD * 2;  // 16 KB
-  constexpr int TILE = 2 * PLANE;     // [h | l]
+  constexpr int PLANE = TM * LD * 2;  // 64 image columns of 128 rows, 16 KB
+  constexpr int TILE = 2 * PLANE;     // the 128 image columns of a row tile
   constexpr int S = kGramStages;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = align1024(smem_raw);

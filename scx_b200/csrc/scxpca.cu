@@ -728,16 +728,16 @@ void collect_stages(scxpca_plan* pl) {
   pl->events_used = 0;
 }
 
-// Tall Gram + Cholesky (FP64) of a tall matrix A.  With `planes` (tensor-core
+// Tall Gram + Cholesky (FP64) of a tall matrix A.  With `from_image` (tensor-core
 // path, ld 64) the Gram is taken on tensor cores from the 16-bit image of A
 // held in Yimg; otherwise from the FP32 A with FP64 FMAs.
 void tall_chol(scxpca_plan* pl, const float* A, int64_t rows, double* Rinv, float* Rinv_f,
-               int shift, bool planes = false) {
+               int shift, bool from_image = false) {
   cudaStream_t st = pl->stream;
   const int ld = (int)pl->ld;
   int parts = (int)std::max<int64_t>(1, std::min<int64_t>(pl->gram_parts, (rows + 31) / 32));
   int s = stage_begin(pl);
-  if (planes && pl->use_tc && ld == 64) {
+  if (from_image && pl->use_tc && ld == 64) {
     parts = launch_gram_tc(rows, &pl->qmap, pl->gpart.as<double>(), pl->fmt16,
                            pl->tc_err.as<int>(), st, pl->num_sms);
     if (parts < 0) CK(cudaGetLastError());
@@ -887,8 +887,8 @@ void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
   // Y = (X - mu) Omega ; qr(Y).  Only the last forward product's FP32 Y is
   // read (by the explicit Q below); the tensor-core Gram at ld 64 reads the
   // 16-bit image.
-  const bool planes_only = pl->use_tc && ld == 64;
-  forward(pl, !planes_only || p.n_power_iterations == 0);
+  const bool image_only = pl->use_tc && ld == 64;
+  forward(pl, !image_only || p.n_power_iterations == 0);
   tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
   for (int64_t it = 0; it < p.n_power_iterations; ++it) {
     // Z = (X - mu)^T Q = (X^T Y - mu (1^T Y)) R^{-1}
@@ -899,7 +899,7 @@ void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
     small_qr(pl, pl->Z.as<double>(), shift);
     CK(launch_round_v(pl->Z.as<double>(), pl->g, ld, mu, pl->V.as<float>(), pl->mc.as<float>(), st));
     stage_end(pl, SCXPCA_STAGE_SMALL, s);
-    forward(pl, !planes_only || it + 1 == p.n_power_iterations);
+    forward(pl, !image_only || it + 1 == p.n_power_iterations);
     tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
   }
   // Explicit Q = Y R^{-1}, re-orthonormalised by a second FP64 Cholesky pass.

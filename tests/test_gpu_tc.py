@@ -1,8 +1,8 @@
 """Tensor-core (tcgen05) SpMM path of the mixed-precision mode vs the FP64 oracle.
 
 The oracle is fed the same 16-bit-rounded matrix values the tensor cores see;
-the dense operand (V or Q) enters the tensor cores as a hi/lo pair of 16-bit
-planes (about 16 mantissa bits), so the forward product agrees to 1e-4 and
+the dense operand (V or Q) enters the tensor cores as a 16-bit image holding a
+hi/lo pair per value (about 16 mantissa bits), so the forward product agrees to 1e-4 and
 the transposed product to 1e-4 relative to the output norm.  Shapes cover
 partial row tiles, partial gene chunks, a single tile, and both supported
 sketch widths (ld 64 and 128).
