@@ -315,11 +315,13 @@ int32_t scxpca_plan_col_stats(scxpca_plan* plan, double* col_sums, double* col_s
  * that every GPU which loads the library holds until the process exits, so
  * n_vars is limited to SCXPCA_NOALLOC_MAX_VARS; larger matrices get
  * SCXPCA_INVALID_ARGUMENT.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture.  All calls share the array and it keeps the last call's
- * contents: two calls whose kernels overlapped on the GPU would race on it, so
- * the library takes a process-wide lock around each call and synchronises the
- * stream before releasing it. */
+ * device address (cudaGetSymbolAddress).  No call can be recorded into a CUDA
+ * graph: each one copies the validation flags to the host and synchronises
+ * the stream, so a call on a stream that is being captured returns
+ * SCXPCA_INVALID_ARGUMENT without touching the capture.  All calls share the
+ * array and it keeps the last call's contents: two calls whose kernels
+ * overlapped on the GPU would race on it, so the library takes a process-wide
+ * lock around each call and synchronises the stream before releasing it. */
 #define SCXPCA_NOALLOC_SCRATCH_BYTES (8u << 20)
 #define SCXPCA_NOALLOC_MAX_VARS 12800
 int32_t scxpca_col_stats_noalloc(int32_t device_ordinal, const scxpca_csr* x, double* out_stats,

@@ -32,6 +32,7 @@ SOURCES = [
     "synth.cu",
     "kernels_adjoint.cu",
     "noalloc.cu",
+    "kernels_strict.cu",
 ]
 EXTRA_SOURCES_OPTIONAL = ["kernels_tc.cu"]
 

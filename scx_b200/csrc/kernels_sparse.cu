@@ -7,47 +7,108 @@
 //   V      : float [n_vars][ld]   gene-major, ld = k padded to 32, pad = 0
 //   Y, Q   : float [n_obs][ld]    cell-major
 //   partial: float [n_chunks][n_vars][ld] per-chunk partial X^T Q
+#include <algorithm>
+
 #include "common.cuh"
 #include "launch.h"
 
 namespace scx {
 
 // ---------------------------------------------------------------------------
-// Per-gene sums and sums of squares (FP64).  The nnz range is split evenly
-// across blocks; each block accumulates in shared memory and writes one
-// partial row pair, reduced in fixed block order by reduce_rows_f64.
-// Restates ScxCsr::col_sums_and_sum_sq (scx-sparse/src/csr.rs:570-580).
+// Per-gene sums and sums of squares (FP64), in a fixed order: the result is
+// bit-identical from run to run.  Restates ScxCsr::col_sums_and_sum_sq
+// (scx-sparse/src/csr.rs:570-580).
+//
+// Block b owns the stored entries [b * per, (b + 1) * per) and walks them in
+// windows of kStatsWindow entries staged in shared memory.  Its kStatsWarps
+// warps share one FP64 accumulator pair per gene, and warp w owns the genes
+// j with (j - lo) % kStatsWarps == w: every warp scans the whole window
+// (32 consecutive entries per step) and adds only its own genes, so no two
+// warps touch one accumulator and no atomics are needed.  Inside one step two
+// lanes may name the same gene only across a row boundary (a sorted row
+// holds a gene once); the step is cut into runs of strictly increasing gene
+// index, within which every gene is distinct, and the runs are applied one
+// after another in lane order.  Unsorted rows and duplicates are handled the
+// same way.  Genes beyond the shared-memory accumulator take further passes
+// over the block's entries, kStatsPassGenes at a time.  Each block writes one
+// partial row pair [sum | sum sq] (n_vars each); reduce_rows_f64 adds the
+// partials in block order.
 // ---------------------------------------------------------------------------
-template <typename ValT>
-__global__ void k_col_stats(const int32_t* __restrict__ idx, const ValT* __restrict__ val,
-                            int64_t nnz, int32_t g, double* __restrict__ partial) {
-  extern __shared__ double sm[];  // [2][g]
-  for (int i = threadIdx.x; i < 2 * g; i += blockDim.x) sm[i] = 0.0;
-  __syncthreads();
-  int64_t per = (nnz + gridDim.x - 1) / gridDim.x;
-  int64_t s = (int64_t)blockIdx.x * per;
-  int64_t e = min(nnz, s + per);
-  for (int64_t p = s + threadIdx.x; p < e; p += blockDim.x) {
-    int32_t j = __ldg(idx + p);
-    double x = (double)to_f32(val[p]);
-    atomicAdd(&sm[j], x);
-    atomicAdd(&sm[g + j], x * x);
-  }
-  __syncthreads();
-  double* out = partial + (int64_t)blockIdx.x * 2 * g;
-  for (int i = threadIdx.x; i < 2 * g; i += blockDim.x) out[i] = sm[i];
-}
+constexpr int kStatsWarps = 4;
+constexpr int kStatsWindow = 1024;
+constexpr int kStatsPassGenes = (int)((kStatsSmemMax - (size_t)kStatsWindow * 8) / 16);
 
-// Wide matrices (too many genes for shared memory): FP64 global atomics.
 template <typename ValT>
-__global__ void k_col_stats_global(const int32_t* __restrict__ idx, const ValT* __restrict__ val,
-                                   int64_t nnz, int32_t g, double* __restrict__ out) {
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nnz;
-       p += (int64_t)gridDim.x * blockDim.x) {
-    int32_t j = __ldg(idx + p);
-    double x = (double)to_f32(val[p]);
-    atomicAdd(&out[j], x);
-    atomicAdd(&out[g + j], x * x);
+__global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* __restrict__ idx,
+                                                                const ValT* __restrict__ val, int64_t nnz,
+                                                                int32_t g, int32_t pass_genes,
+                                                                double* __restrict__ partial) {
+  extern __shared__ double sm[];  // [2][pass_genes] accumulators, then the window
+  double* acc = sm;
+  int32_t* w_idx = reinterpret_cast<int32_t*>(sm + 2 * (int64_t)pass_genes);
+  float* w_val = reinterpret_cast<float*>(w_idx + kStatsWindow);
+  constexpr int kPer = kStatsWindow / (kStatsWarps * 32);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lanemask_le = 0xffffffffu >> (31 - lane);
+  const int64_t per = (nnz + gridDim.x - 1) / gridDim.x;
+  const int64_t s = min(nnz, (int64_t)blockIdx.x * per);
+  const int64_t e = min(nnz, s + per);
+  double* out = partial + (int64_t)blockIdx.x * 2 * g;
+  for (int32_t lo = 0; lo < g; lo += pass_genes) {
+    const int32_t gp = min(pass_genes, g - lo);
+    for (int i = threadIdx.x; i < 2 * gp; i += blockDim.x) acc[i] = 0.0;
+    for (int64_t w0 = s; w0 < e; w0 += kStatsWindow) {
+      const int cnt = (int)min((int64_t)kStatsWindow, e - w0);
+      int32_t ri[kPer];
+      float rv[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int t = threadIdx.x + u * kStatsWarps * 32;
+        ri[u] = t < cnt ? __ldg(idx + w0 + t) : -1;
+        rv[u] = t < cnt ? to_f32(val[w0 + t]) : 0.f;
+      }
+      __syncthreads();  // the previous window is consumed (and the accumulators zeroed)
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int t = threadIdx.x + u * kStatsWarps * 32;
+        w_idx[t] = ri[u];
+        w_val[t] = rv[u];
+      }
+      __syncthreads();
+      for (int b = 0; b < cnt; b += 32) {
+        const int t = b + lane;
+        const int32_t j = t < cnt ? w_idx[t] : -1;
+        const int32_t jl = __shfl_up_sync(0xffffffffu, j, 1);
+        const unsigned starts = __ballot_sync(0xffffffffu, lane > 0 && t < cnt && j <= jl);
+        const int32_t jr = j - lo;
+        const bool own = t < cnt && jr >= 0 && jr < gp && (jr % kStatsWarps) == warp;
+        if (starts == 0) {
+          if (own) {
+            const double x = (double)w_val[t];
+            acc[jr] += x;
+            acc[gp + jr] += x * x;
+          }
+          __syncwarp();  // the next step's lanes see these updates
+        } else {
+          const int run = __popc(starts & lanemask_le);
+          const int runs = __popc(starts) + 1;
+          for (int r = 0; r < runs; ++r) {
+            if (own && run == r) {
+              const double x = (double)w_val[t];
+              acc[jr] += x;
+              acc[gp + jr] += x * x;
+            }
+            __syncwarp();
+          }
+        }
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < gp; i += blockDim.x) {
+      out[lo + i] = acc[i];
+      out[g + lo + i] = acc[gp + i];
+    }
+    __syncthreads();
   }
 }
 
@@ -279,18 +340,15 @@ static cudaError_t col_stats_t(const int32_t* idx, const void* val, int64_t nnz,
                                double* partial, int nparts, double* out, cudaStream_t st,
                                int num_sms) {
   const ValT* v = static_cast<const ValT*>(val);
-  size_t smem = (size_t)2 * g * sizeof(double);
-  if (smem <= kStatsSmemMax) {
-    if (smem > 48 * 1024)
-      cudaFuncSetAttribute(k_col_stats<ValT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_col_stats<ValT><<<nparts, 512, smem, st>>>(idx, v, nnz, g, partial);
-    k_reduce_rows<double><<<grid_for(2 * g, 256, num_sms), 256, 0, st>>>(partial, nparts, 2 * g, out, 0);
-    note_launches(2);
-  } else {
-    cudaMemsetAsync(out, 0, sizeof(double) * 2 * g, st);
-    k_col_stats_global<ValT><<<grid_for(nnz, 256, num_sms), 256, 0, st>>>(idx, v, nnz, g, out);
-    note_launches(1);
+  const int32_t pass_genes = std::min<int32_t>(g, kStatsPassGenes);
+  const size_t smem = (size_t)2 * pass_genes * sizeof(double) + (size_t)kStatsWindow * 8;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_col_stats<ValT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
   }
+  k_col_stats<ValT><<<nparts, kStatsWarps * 32, smem, st>>>(idx, v, nnz, g, pass_genes, partial);
+  k_reduce_rows<double><<<grid_for(2 * g, 256, num_sms), 256, 0, st>>>(partial, nparts, 2 * g, out, 0);
+  note_launches(2);
   return cudaGetLastError();
 }
 

@@ -1,0 +1,500 @@
+// CUDA-core SpMM pair with FP32 products and a fixed summation order (the
+// strict FP32 path, and the CUDA-core path of 16-bit values when the tensor
+// cores cannot take a matrix).  Both kernels read their dense operand from
+// shared memory and accumulate in registers; neither uses atomics, so every
+// result is bit-identical from run to run.
+//
+//   forward    Y = P V - 1 mc^T   (CSR rows, V staged in gene chunks)
+//   transposed W_part = P^T Q     (tile-CSC copy, Q staged one row tile at a time)
+//
+// Restate spmm_forward_row (scx-accel/src/pca/cpu.rs:1500-1523) with the mean
+// correction of forward_mean_prefactor (scx-gpu/src/gpu_pca.rs:218-237), and
+// spmm_transpose_block (scx-accel/src/pca/cpu.rs:1282-1328) with the output-
+// partitioned reduction of spmm_transpose_into (cpu.rs:1330-1389).
+//
+// Layouts (device memory):
+//   CSR      : int64 indptr[n+1], int32 idx[nnz], values[nnz], rows sorted by gene
+//   V        : float [n_vars][ld] gene-major;  Y, Q: float [n_obs][ld] cell-major
+//   tile CSC : for row tile t (kStrictTile rows, entries indptr[t T] .. indptr[(t+1) T]),
+//              the same entries reordered by (slot, row): cell[p] = row within the
+//              tile (uint8), cval[p] = value; tptr[t (S + 1) + s] = offset of slot
+//              s's first entry from indptr[t T] (S + 1 offsets per tile).  Genes are
+//              relabelled to slots (gene2slot) so that each warp of the transposed
+//              product owns GPW consecutive slots of about equal stored-entry count.
+//   partial  : float [ranges][n_vars][ld], summed in range order by k_reduce_rows
+#include <algorithm>
+#include <functional>
+#include <queue>
+#include <utility>
+#include <vector>
+
+#include "common.cuh"
+#include "launch.h"
+
+namespace scx {
+
+namespace {
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Copy `bytes` (a multiple of 16, both addresses 16-byte aligned) with the
+// whole block, as 16-byte asynchronous copies.
+__device__ __forceinline__ void block_copy_async(void* smem, const void* gmem, int bytes) {
+  for (int o = threadIdx.x * 16; o < bytes; o += blockDim.x * 16)
+    cp_async16(static_cast<char*>(smem) + o, static_cast<const char*>(gmem) + o);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Tile-CSC build, one warp per row tile (once per plan).  Counting sort of
+// the tile's entries by slot (the relabelled gene); rows are visited in
+// order, so within a slot the entries keep row order.  Within one 32-entry
+// step two lanes can name the same gene only across a duplicate; the step is
+// cut into runs of strictly increasing gene, applied in lane order, which
+// keeps the placement (and so the later summation order) deterministic.
+// k_gene_counts gives the stored entries per gene that the slot assignment
+// balances.
+// ---------------------------------------------------------------------------
+__global__ void k_gene_counts(const int32_t* __restrict__ idx, int64_t nnz, int32_t* __restrict__ counts) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(counts + __ldg(idx + p), 1);
+}
+
+template <typename ValT>
+__global__ void k_tile_csc(const int64_t* __restrict__ indptr, const int32_t* __restrict__ idx,
+                           const ValT* __restrict__ val, int64_t n, const int32_t* __restrict__ gene2slot,
+                           int32_t nslots, int64_t n_tiles, int32_t* __restrict__ tptr, uint8_t* __restrict__ cell,
+                           ValT* __restrict__ cval) {
+  extern __shared__ int32_t cur_all[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int warps = blockDim.x >> 5;
+  int32_t* cur = cur_all + (int64_t)wib * (nslots + 1);
+  const unsigned lanemask_le = 0xffffffffu >> (31 - lane);
+  for (int64_t t = (int64_t)blockIdx.x * warps + wib; t < n_tiles; t += (int64_t)gridDim.x * warps) {
+    const int64_t r0 = t * kStrictTile;
+    const int64_t r1 = min(n, r0 + kStrictTile);
+    const int64_t base = indptr[r0];
+    const int64_t end = indptr[r1];
+    for (int j = lane; j <= nslots; j += 32) cur[j] = 0;
+    __syncwarp();
+    // counts (integer atomics: the counts do not depend on the order)
+    for (int64_t p = base + lane; p < end; p += 32) atomicAdd(&cur[__ldg(gene2slot + __ldg(idx + p))], 1);
+    __syncwarp();
+    // exclusive scan of cur[0..nslots] -> offsets; lane owns a contiguous segment
+    const int per = (nslots + 1 + 31) / 32;
+    const int j0 = min(nslots + 1, lane * per), j1 = min(nslots + 1, j0 + per);
+    int32_t sum = 0;
+    for (int j = j0; j < j1; ++j) sum += cur[j];
+    int32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    int32_t run = incl - sum;
+    for (int j = j0; j < j1; ++j) {
+      const int32_t c = cur[j];
+      cur[j] = run;
+      tptr[t * (nslots + 1) + j] = run;
+      run += c;
+    }
+    __syncwarp();
+    // fill, rows in order
+    for (int64_t r = r0; r < r1; ++r) {
+      const int64_t s = indptr[r], e = indptr[r + 1];
+      const uint8_t rl = (uint8_t)(r - r0);
+      for (int64_t b = s; b < e; b += 32) {
+        const int64_t p = b + lane;
+        const bool ok = p < e;
+        const int32_t j = ok ? __ldg(idx + p) : -1;
+        const ValT x = ok ? val[p] : ValT();
+        const int32_t jl = __shfl_up_sync(0xffffffffu, j, 1);
+        const unsigned starts = __ballot_sync(0xffffffffu, lane > 0 && ok && j <= jl);
+        const int my_run = __popc(starts & lanemask_le);
+        const int runs = __popc(starts) + 1;
+        const int32_t slot = ok ? __ldg(gene2slot + j) : 0;
+        for (int rr = 0; rr < runs; ++rr) {
+          if (ok && my_run == rr) {
+            const int32_t q = cur[slot]++;
+            cell[base + q] = rl;
+            cval[base + q] = x;
+          }
+          __syncwarp();
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Forward product.  A block owns a tile of 8 * RPW rows (RPW per warp) and
+// walks the genes in chunks of GC, each chunk of V (GC x LD floats) staged in
+// shared memory by asynchronous copies, double-buffered.  A warp keeps, for
+// each of its rows, a 32-entry window of the row (one entry per lane) in
+// registers and consumes the window entries whose gene falls in the current
+// chunk (rows are sorted, so they are the next unconsumed ones); lane l
+// accumulates columns l, l + 32, ... of every row in registers.  A consumed
+// entry is marked by gene -1 (0xffffffff as unsigned, above every chunk
+// bound), an entry past the row's end by INT32_MAX; the window is reloaded
+// once all 32 of its entries are consumed.  The window position and end of
+// row r live in lane r.  Each stored entry is loaded from memory once.
+// ---------------------------------------------------------------------------
+template <int LD, int RPW, int GC, typename ValT>
+__global__ void __launch_bounds__(256, 2) k_fwd_strict(const int64_t* __restrict__ indptr,
+                                                       const int32_t* __restrict__ idx,
+                                                       const ValT* __restrict__ val, int64_t n, int32_t g,
+                                                       const float* __restrict__ V, const float* __restrict__ mc,
+                                                       float* __restrict__ Y) {
+  constexpr int C = LD / 32;
+  constexpr int32_t kDone = -1;
+  extern __shared__ __align__(16) float vs[];  // [2][GC][LD]
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t row0 = (int64_t)blockIdx.x * (8 * RPW) + (int64_t)wib * RPW;
+  // lane r < RPW: window start and end of row row0 + r
+  int64_t my_base = 0, my_end = 0;
+  if (lane < RPW && row0 + lane < n) {
+    my_base = indptr[row0 + lane];
+    my_end = indptr[row0 + lane + 1];
+  }
+  float acc[RPW][C];
+  int32_t wi[RPW];
+  float wv[RPW];
+#pragma unroll
+  for (int r = 0; r < RPW; ++r) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[r][c] = 0.f;
+    const int64_t base = __shfl_sync(0xffffffffu, my_base, r);
+    const int64_t end = __shfl_sync(0xffffffffu, my_end, r);
+    const int64_t p = base + lane;
+    wi[r] = p < end ? __ldg(idx + p) : INT32_MAX;
+    wv[r] = p < end ? to_f32(val[p]) : 0.f;
+  }
+  const int nchunk = (g + GC - 1) / GC;
+  block_copy_async(vs, V, min(GC, (int)g) * LD * 4);
+  cp_async_commit();
+  for (int ch = 0; ch < nchunk; ++ch) {
+    const int g0 = ch * GC;
+    const int g1 = min((int)g, g0 + GC);
+    if (ch + 1 < nchunk) {
+      const int n1 = min(GC, (int)g - g1);
+      block_copy_async(vs + ((ch + 1) & 1) * GC * LD, V + (int64_t)g1 * LD, n1 * LD * 4);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const float* vc = vs + (ch & 1) * GC * LD + lane;
+#pragma unroll
+    for (int r = 0; r < RPW; ++r) {
+      while (true) {
+        const bool take = (unsigned)wi[r] < (unsigned)g1;
+        const unsigned m = __ballot_sync(0xffffffffu, take);
+        if (m) {
+          const int t0 = __ffs(m) - 1;
+          const int t1 = t0 + __popc(m);
+          for (int t = t0; t < t1; ++t) {
+            const int32_t j = __shfl_sync(0xffffffffu, wi[r], t);
+            const float x = __shfl_sync(0xffffffffu, wv[r], t);
+            // j is in [g0, g1) for a sorted row; the clamp keeps any other
+            // index inside the staged chunk
+            const unsigned jl = min((unsigned)(j - g0), (unsigned)(GC - 1));
+            const float* vr = vc + jl * LD;
+#pragma unroll
+            for (int c = 0; c < C; ++c) acc[r][c] = fmaf(x, vr[32 * c], acc[r][c]);
+          }
+          if (take) wi[r] = kDone;
+        }
+        if (__ballot_sync(0xffffffffu, wi[r] == kDone) != 0xffffffffu) break;
+        // all 32 window entries consumed: load the next 32 entries of the row
+        if (lane == r) my_base += 32;
+        const int64_t base = __shfl_sync(0xffffffffu, my_base, r);
+        const int64_t end = __shfl_sync(0xffffffffu, my_end, r);
+        const int64_t p = base + lane;
+        wi[r] = p < end ? __ldg(idx + p) : INT32_MAX;
+        wv[r] = p < end ? to_f32(val[p]) : 0.f;
+      }
+    }
+    __syncthreads();  // everyone is done with this buffer before it is refilled
+  }
+  cp_async_wait<0>();
+  float m[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) m[c] = mc ? mc[lane + 32 * c] : 0.f;
+#pragma unroll
+  for (int r = 0; r < RPW; ++r) {
+    const int64_t row = row0 + r;
+    if (row < n) {
+#pragma unroll
+      for (int c = 0; c < C; ++c) Y[row * LD + lane + 32 * c] = acc[r][c] - m[c];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Transposed product.  Block (range, b) owns the slots [b * 8 GPW, (b + 1) *
+// 8 GPW) -- warp w the GPW consecutive slots from b * 8 GPW + w GPW -- and the
+// row tiles of one contiguous range.  For each tile, Q's rows (kStrictTile x
+// LD floats) are staged in shared memory (double-buffered, asynchronous
+// copies); a warp walks the tile-CSC entries of each of its slots in row
+// order and lane l accumulates columns l, l + 32, ... of every slot in
+// registers.  The block writes one partial row per gene it owns.
+// ---------------------------------------------------------------------------
+template <int LD, int GPW, typename ValT>
+__global__ void __launch_bounds__(256, 2) k_rmat_strict(const int64_t* __restrict__ indptr,
+                                                        const int32_t* __restrict__ tptr,
+                                                        const uint8_t* __restrict__ cell,
+                                                        const ValT* __restrict__ cval, int64_t n, int32_t g,
+                                                        int32_t nslots, const int32_t* __restrict__ slot2gene,
+                                                        int64_t tiles_per_range, const float* __restrict__ Q,
+                                                        float* __restrict__ part) {
+  constexpr int C = LD / 32;
+  constexpr int T = kStrictTile;
+  extern __shared__ __align__(16) float qs[];  // [2][T][LD]
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t n_tiles = (n + T - 1) / T;
+  const int64_t t0 = (int64_t)blockIdx.x * tiles_per_range;
+  const int64_t t1 = min(n_tiles, t0 + tiles_per_range);
+  const int slot0 = (blockIdx.y * 8 + wib) * GPW;
+  // lane jj < GPW reads the pointers of slot slot0 + jj (coalesced)
+  const int my_slot = slot0 + (lane % GPW);
+  float acc[GPW][C];
+#pragma unroll
+  for (int jj = 0; jj < GPW; ++jj)
+#pragma unroll
+    for (int c = 0; c < C; ++c) acc[jj][c] = 0.f;
+  if (t0 < t1) {
+    auto stage = [&](int64_t t, int buf) {
+      const int64_t r0 = t * T;
+      const int rows = (int)min((int64_t)T, n - r0);
+      block_copy_async(qs + buf * T * LD, Q + r0 * LD, rows * LD * 4);
+    };
+    stage(t0, 0);
+    cp_async_commit();
+    for (int64_t t = t0; t < t1; ++t) {
+      const int buf = (int)((t - t0) & 1);
+      if (t + 1 < t1) stage(t + 1, buf ^ 1);
+      cp_async_commit();
+      const int64_t tb = indptr[t * T];
+      int32_t p0 = 0, p1 = 0;
+      if (my_slot < nslots) {
+        p0 = __ldg(tptr + t * (nslots + 1) + my_slot);
+        p1 = __ldg(tptr + t * (nslots + 1) + my_slot + 1);
+      }
+      cp_async_wait<1>();
+      __syncthreads();
+      const float* qt = qs + buf * T * LD + lane;
+#pragma unroll
+      for (int jj = 0; jj < GPW; ++jj) {
+        const int32_t s = __shfl_sync(0xffffffffu, p0, jj);
+        const int32_t e = __shfl_sync(0xffffffffu, p1, jj);
+        for (int32_t b = s; b < e; b += 32) {
+          const int32_t q = b + lane;
+          const int cnt = min(32, e - b);
+          int cl = 0;
+          float x = 0.f;
+          if (q < e) {
+            cl = __ldg(cell + tb + q);
+            x = to_f32(cval[tb + q]);
+          }
+          for (int u = 0; u < cnt; ++u) {
+            const int cu = __shfl_sync(0xffffffffu, cl, u) & (T - 1);
+            const float xu = __shfl_sync(0xffffffffu, x, u);
+            const float* qr = qt + cu * LD;
+#pragma unroll
+            for (int c = 0; c < C; ++c) acc[jj][c] = fmaf(xu, qr[32 * c], acc[jj][c]);
+          }
+        }
+      }
+      __syncthreads();  // this buffer is read before it is refilled
+    }
+    cp_async_wait<0>();
+  }
+  float* out = part + (int64_t)blockIdx.x * g * LD;
+#pragma unroll
+  for (int jj = 0; jj < GPW; ++jj) {
+    const int slot = slot0 + jj;
+    const int j = slot < nslots ? __ldg(slot2gene + slot) : -1;
+    if (j >= 0) {
+#pragma unroll
+      for (int c = 0; c < C; ++c) out[(int64_t)j * LD + lane + 32 * c] = acc[jj][c];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+int strict_genes_per_warp(int ld) { return ld <= 64 ? 32 : 16; }
+
+int strict_slot_count(int64_t g, int ld) {
+  const int per_block = 8 * strict_genes_per_warp(ld);
+  return (int)((g + per_block - 1) / per_block) * per_block;
+}
+
+// Longest-processing-time assignment of genes to the warps of the
+// transposed product: genes in decreasing stored-entry count (ties by gene
+// index) each go to the warp group with the smallest count so far that still
+// has a free slot (ties by group index).  slot2gene[s] = -1 marks an empty
+// slot.  Deterministic for given counts.
+void strict_assign_slots(const std::vector<int32_t>& counts, int ld, std::vector<int32_t>& gene2slot,
+                         std::vector<int32_t>& slot2gene) {
+  const int64_t g = (int64_t)counts.size();
+  const int gpw = strict_genes_per_warp(ld);
+  const int nslots = strict_slot_count(g, ld);
+  const int groups = nslots / gpw;
+  std::vector<int32_t> order(g);
+  for (int64_t j = 0; j < g; ++j) order[j] = (int32_t)j;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return counts[a] > counts[b]; });
+  // min-heap of (load, group) over groups with a free slot
+  using Item = std::pair<int64_t, int32_t>;
+  std::priority_queue<Item, std::vector<Item>, std::greater<Item>> heap;
+  for (int32_t q = 0; q < groups; ++q) heap.push({0, q});
+  std::vector<int32_t> fill(groups, 0);
+  gene2slot.assign(g, 0);
+  slot2gene.assign(nslots, -1);
+  for (int32_t j : order) {
+    Item it = heap.top();
+    heap.pop();
+    const int32_t q = it.second;
+    const int32_t slot = q * gpw + fill[q]++;
+    gene2slot[j] = slot;
+    slot2gene[slot] = j;
+    if (fill[q] < gpw) heap.push({it.first + counts[j], q});
+  }
+}
+
+cudaError_t launch_gene_counts(const int32_t* idx, int64_t nnz, int32_t* counts, cudaStream_t st, int num_sms) {
+  if (nnz == 0) return cudaSuccess;
+  k_gene_counts<<<grid_for(nnz, 256, num_sms), 256, 0, st>>>(idx, nnz, counts);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+size_t strict_tile_smem_bytes(int nslots) { return sizeof(int32_t) * (size_t)(nslots + 1); }
+
+template <typename ValT>
+static cudaError_t tile_csc_t(const int64_t* indptr, const int32_t* idx, const void* val, int64_t n,
+                              const int32_t* gene2slot, int32_t nslots, int32_t* tptr, uint8_t* cell, void* cval,
+                              cudaStream_t st, int num_sms) {
+  const int64_t n_tiles = (n + kStrictTile - 1) / kStrictTile;
+  const size_t per_warp = strict_tile_smem_bytes(nslots);
+  if (per_warp > kStatsSmemMax) return cudaErrorInvalidValue;
+  const int warps = (int)std::min<size_t>(8, kStatsSmemMax / per_warp);
+  const size_t smem = per_warp * warps;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_tile_csc<ValT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_tiles + warps - 1) / warps, (int64_t)num_sms * 4));
+  k_tile_csc<ValT><<<grid, warps * 32, smem, st>>>(indptr, idx, static_cast<const ValT*>(val), n, gene2slot, nslots,
+                                                   n_tiles, tptr, cell, static_cast<ValT*>(cval));
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tile_csc(int dtype, const int64_t* indptr, const int32_t* idx, const void* val, int64_t n,
+                            const int32_t* gene2slot, int32_t nslots, int32_t* tptr, uint8_t* cell, void* cval,
+                            cudaStream_t st, int num_sms) {
+  if (n == 0) return cudaSuccess;
+  switch (dtype) {
+    case 0: return tile_csc_t<float>(indptr, idx, val, n, gene2slot, nslots, tptr, cell, cval, st, num_sms);
+    case 1: return tile_csc_t<__nv_bfloat16>(indptr, idx, val, n, gene2slot, nslots, tptr, cell, cval, st, num_sms);
+    default: return tile_csc_t<__half>(indptr, idx, val, n, gene2slot, nslots, tptr, cell, cval, st, num_sms);
+  }
+}
+
+template <int LD, typename ValT>
+static cudaError_t fwd_strict_t(const int64_t* indptr, const int32_t* idx, const void* val, int64_t n, int32_t g,
+                                const float* V, const float* mc, float* Y, cudaStream_t st) {
+  constexpr int RPW = LD <= 64 ? 16 : 8;
+  constexpr int GC = (8192 / LD) & ~7;
+  const size_t smem = (size_t)2 * GC * LD * sizeof(float);
+  auto kern = k_fwd_strict<LD, RPW, GC, ValT>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  const int64_t rows_per_block = 8 * RPW;
+  const int64_t grid = (n + rows_per_block - 1) / rows_per_block;
+  kern<<<(unsigned)grid, 256, smem, st>>>(indptr, idx, static_cast<const ValT*>(val), n, g, V, mc, Y);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+template <typename ValT>
+static cudaError_t fwd_strict_v(int ld, const int64_t* indptr, const int32_t* idx, const void* val, int64_t n,
+                                int32_t g, const float* V, const float* mc, float* Y, cudaStream_t st) {
+  switch (ld) {
+    case 32: return fwd_strict_t<32, ValT>(indptr, idx, val, n, g, V, mc, Y, st);
+    case 64: return fwd_strict_t<64, ValT>(indptr, idx, val, n, g, V, mc, Y, st);
+    case 96: return fwd_strict_t<96, ValT>(indptr, idx, val, n, g, V, mc, Y, st);
+    case 128: return fwd_strict_t<128, ValT>(indptr, idx, val, n, g, V, mc, Y, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_fwd_strict(int dtype, int ld, const int64_t* indptr, const int32_t* idx, const void* val,
+                              int64_t n, int32_t g, const float* V, const float* mc, float* Y, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  switch (dtype) {
+    case 0: return fwd_strict_v<float>(ld, indptr, idx, val, n, g, V, mc, Y, st);
+    case 1: return fwd_strict_v<__nv_bfloat16>(ld, indptr, idx, val, n, g, V, mc, Y, st);
+    default: return fwd_strict_v<__half>(ld, indptr, idx, val, n, g, V, mc, Y, st);
+  }
+}
+
+template <int LD, typename ValT>
+static cudaError_t rmat_strict_t(const int64_t* indptr, const int32_t* tptr, const uint8_t* cell, const void* cval,
+                                 int64_t n, int32_t g, int32_t nslots, const int32_t* slot2gene, int ranges,
+                                 const float* Q, float* part, cudaStream_t st) {
+  constexpr int GPW = LD <= 64 ? 32 : 16;
+  const size_t smem = (size_t)2 * kStrictTile * LD * sizeof(float);
+  auto kern = k_rmat_strict<LD, GPW, ValT>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  if (nslots % (8 * GPW) != 0) return cudaErrorInvalidValue;
+  const int64_t n_tiles = (n + kStrictTile - 1) / kStrictTile;
+  const int64_t per = (n_tiles + ranges - 1) / ranges;
+  dim3 grid((unsigned)ranges, (unsigned)(nslots / (8 * GPW)));
+  kern<<<grid, 256, smem, st>>>(indptr, tptr, cell, static_cast<const ValT*>(cval), n, g, nslots, slot2gene, per, Q,
+                                part);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+template <typename ValT>
+static cudaError_t rmat_strict_v(int ld, const int64_t* indptr, const int32_t* tptr, const uint8_t* cell,
+                                 const void* cval, int64_t n, int32_t g, int32_t nslots, const int32_t* slot2gene,
+                                 int ranges, const float* Q, float* part, cudaStream_t st) {
+  switch (ld) {
+    case 32: return rmat_strict_t<32, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
+    case 64: return rmat_strict_t<64, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
+    case 96: return rmat_strict_t<96, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
+    case 128: return rmat_strict_t<128, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_rmat_strict(int dtype, int ld, const int64_t* indptr, const int32_t* tptr, const uint8_t* cell,
+                               const void* cval, int64_t n, int32_t g, int32_t nslots, const int32_t* slot2gene,
+                               int ranges, const float* Q, float* part, cudaStream_t st) {
+  switch (dtype) {
+    case 0: return rmat_strict_v<float>(ld, indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
+    case 1:
+      return rmat_strict_v<__nv_bfloat16>(ld, indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
+    default: return rmat_strict_v<__half>(ld, indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
+  }
+}
+
+}  // namespace scx

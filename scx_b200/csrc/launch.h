@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace scx {
 
 // Process-wide count of kernels launched by this library (every launcher
@@ -37,6 +39,28 @@ cudaError_t launch_spmm_t(int dtype, int ld, const int64_t* indptr, const int32_
                           cudaStream_t st);
 cudaError_t launch_reduce_rows_f32(const float* part, int nparts, int64_t len, double* out,
                                    int accumulate, cudaStream_t st, int num_sms);
+
+// ---- CUDA-core SpMM pair in a fixed summation order (kernels_strict.cu) ----
+constexpr int kStrictTile = 128;  // rows per tile of the tile-CSC copy (a power of two <= 256)
+int strict_genes_per_warp(int ld);
+// Slots of the tile-CSC copy: n_vars rounded up to whole blocks of the transposed product.
+int strict_slot_count(int64_t g, int ld);
+// Balanced gene -> slot assignment from per-gene stored-entry counts.
+void strict_assign_slots(const std::vector<int32_t>& counts, int ld, std::vector<int32_t>& gene2slot,
+                         std::vector<int32_t>& slot2gene);
+size_t strict_tile_smem_bytes(int nslots);
+cudaError_t launch_gene_counts(const int32_t* idx, int64_t nnz, int32_t* counts, cudaStream_t st, int num_sms);
+// Tile-CSC copy of a row-sorted CSR: tptr [n_tiles][nslots + 1], cell/cval [nnz].
+cudaError_t launch_tile_csc(int dtype, const int64_t* indptr, const int32_t* idx, const void* val, int64_t n,
+                            const int32_t* gene2slot, int32_t nslots, int32_t* tptr, uint8_t* cell, void* cval,
+                            cudaStream_t st, int num_sms);
+// Y (n x ld) = P V - 1 mc^T (mc may be null) from a row-sorted CSR; ld in {32, 64, 96, 128}.
+cudaError_t launch_fwd_strict(int dtype, int ld, const int64_t* indptr, const int32_t* idx, const void* val,
+                              int64_t n, int32_t g, const float* V, const float* mc, float* Y, cudaStream_t st);
+// part[range][g][ld] = partial P^T Q over the row tiles of each of `ranges` contiguous ranges.
+cudaError_t launch_rmat_strict(int dtype, int ld, const int64_t* indptr, const int32_t* tptr, const uint8_t* cell,
+                               const void* cval, int64_t n, int32_t g, int32_t nslots, const int32_t* slot2gene,
+                               int ranges, const float* Q, float* part, cudaStream_t st);
 cudaError_t launch_reduce_rows_f64(const double* part, int nparts, int64_t len, double* out,
                                    int accumulate, cudaStream_t st, int num_sms);
 

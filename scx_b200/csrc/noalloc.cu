@@ -15,7 +15,10 @@
 // address; a kernel given it would fault or, where the GPU can reach host
 // memory, silently use the wrong memory.  The device address is taken once
 // per device with cudaGetSymbolAddress (with that device current) on the
-// first call there, so that first call should come before any stream capture.
+// first call there.  No call can be recorded into a CUDA graph: every call
+// reads the validation flags back to the host and waits for its stream, so a
+// call on a stream that is being captured is refused with
+// SCXPCA_INVALID_ARGUMENT instead of breaking the caller's capture.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -33,8 +36,8 @@ constexpr size_t kNoAllocScratchBytes = (size_t)SCXPCA_NOALLOC_SCRATCH_BYTES;
 constexpr size_t kFlagBytes = 256;  // four int32 flags, padded to keep the partials 256-byte aligned
 constexpr int64_t kPartialDoubles = (int64_t)((kNoAllocScratchBytes - kFlagBytes) / sizeof(double));
 constexpr int kMaxDevices = 256;
-static_assert(SCXPCA_NOALLOC_MAX_VARS * 2 * sizeof(double) <= kStatsSmemMax,
-              "the no-allocation statistics use the shared-memory accumulator path only");
+static_assert(kPartialDoubles / (2 * SCXPCA_NOALLOC_MAX_VARS) >= 32,
+              "the scratch must hold at least 32 per-block partials at the widest matrix");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -94,6 +97,15 @@ void col_stats_noalloc(int32_t dev, const scxpca_csr* x, double* out, cudaStream
     }
   } restore{prev};
   na_check(cudaSetDevice(dev), "cudaSetDevice");
+  // A non-sticky error left by the caller's earlier work is not this call's
+  // failure: clear it so the launch checks below report only our own.
+  cudaGetLastError();
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  na_check(cudaStreamIsCapturing(st, &capture), "cudaStreamIsCapturing");
+  if (capture != cudaStreamCaptureStatusNone)
+    throw NoAllocError{SCXPCA_INVALID_ARGUMENT,
+                       "scxpca_col_stats_noalloc cannot run on a stream that is being captured: it reads "
+                       "the validation flags back to the host and waits for the stream"};
   int sms = 148;
   na_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
 
@@ -104,21 +116,29 @@ void col_stats_noalloc(int32_t dev, const scxpca_csr* x, double* out, cudaStream
   const int64_t g = x->n_vars;
   const int nparts = (int)std::min<int64_t>(2 * (int64_t)sms, kPartialDoubles / (2 * g));
 
+  // Once work is queued, an error must not release the lock while our
+  // kernels may still touch the shared array: wait for the stream first
+  // (its own status is already being reported) and then throw.
+  auto check_queued = [st](cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    cudaStreamSynchronize(st);
+    na_check(e, what);
+  };
   // The flags accumulate with atomicOr: they must start at zero.  The
   // partials are overwritten whole by every call and need no clearing.
-  na_check(cudaMemsetAsync(flags, 0, 4 * sizeof(int32_t), st), "cudaMemsetAsync(flags)");
-  na_check(launch_validate_csr(x->values_dtype, x->indptr, x->indices, x->values, x->n_obs, g, x->nnz, flags,
-                               st, sms),
-           "launch_validate_csr");
+  check_queued(cudaMemsetAsync(flags, 0, 4 * sizeof(int32_t), st), "cudaMemsetAsync(flags)");
+  check_queued(launch_validate_csr(x->values_dtype, x->indptr, x->indices, x->values, x->n_obs, g, x->nnz, flags,
+                                   st, sms),
+               "launch_validate_csr");
   int32_t hf[4] = {0, 0, 0, 0};
-  na_check(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(flags)");
-  na_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  check_queued(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync(flags)");
+  check_queued(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   if (hf[0]) throw NoAllocError{SCXPCA_INVALID_CSR, "invalid CSR: indptr is not monotone within [0, nnz]"};
   if (hf[1]) throw NoAllocError{SCXPCA_INVALID_CSR, "invalid CSR: column index out of range [0, n_vars)"};
   if (hf[3]) throw NoAllocError{SCXPCA_INVALID_CSR, "invalid CSR: non-finite value"};
-  na_check(launch_col_stats(x->values_dtype, x->indices, x->values, x->nnz, (int32_t)g, partial, nparts, out, st,
-                            sms),
-           "launch_col_stats");
+  check_queued(launch_col_stats(x->values_dtype, x->indices, x->values, x->nnz, (int32_t)g, partial, nparts, out,
+                                st, sms),
+               "launch_col_stats");
   // Wait before releasing the lock, so the next call cannot touch the
   // partials while this call's kernels still read them.
   na_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");

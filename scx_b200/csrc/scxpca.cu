@@ -237,9 +237,16 @@ struct scxpca_plan {
   double total_var = 0.0;
   bool total_var_recomputed = false;
 
-  // transposed product
+  // CUDA-core transposed product: the tile-CSC copy (slots balanced by
+  // stored-entry count) and its per-range partials; the row-block pointer
+  // table of the gradient's SDDMM (and of the atomic fallback for matrices
+  // too wide for the tile-CSC copy) is built on first use
+  bool strict_csc = false;
+  int nslots = 0, strict_ranges = 0;
+  DevBuf csc_tptr, csc_cell, csc_val, d_slot2gene;
   int nb = 0, nchunks = 0;
   int64_t rows_per_chunk = 0;
+  bool rbp_built = false;
   DevBuf rbp, wpart;
 
   // dense work
@@ -394,6 +401,53 @@ std::vector<double> read_vec(const double* src, int64_t n, int32_t memory, doubl
     memcpy(v.data(), src, sizeof(double) * n);
   }
   return v;
+}
+
+// Row-block pointer table (the SDDMM of the gradient, and the transposed
+// product of matrices too wide for the tile-CSC copy), built on first use.
+void ensure_rbp(scxpca_plan* pl) {
+  if (pl->rbp_built) return;
+  PoolScope pool_scope(pl->device, pl->stream);
+  pl->rbp.alloc(sizeof(int32_t) * pl->n * (pl->nb + 1));
+  CK(launch_row_block_ptr(pl->indptr, pl->idx, pl->n, pl->nb, kTransposeGeneBlock, pl->rbp.as<int32_t>(),
+                          pl->stream, pl->num_sms));
+  if (!pl->strict_csc && !pl->use_tc)
+    pl->wpart.alloc(sizeof(float) * (size_t)pl->nchunks * pl->g * pl->ld);
+  pl->rbp_built = true;
+}
+
+// Tile-CSC copy of the working matrix for the CUDA-core transposed product:
+// per-gene stored-entry counts -> balanced slot assignment (host) -> the
+// copy, and the per-range partial buffer.
+void build_tile_csc(scxpca_plan* pl) {
+  cudaStream_t st = pl->stream;
+  const int64_t n = pl->n, g = pl->g, nnz = pl->nnz;
+  DevBuf counts;
+  counts.alloc(sizeof(int32_t) * g);
+  CK(cudaMemsetAsync(counts.p, 0, sizeof(int32_t) * g, st));
+  CK(launch_gene_counts(pl->idx, nnz, counts.as<int32_t>(), st, pl->num_sms));
+  std::vector<int32_t> hc(g);
+  CK(cudaMemcpyAsync(hc.data(), counts.p, sizeof(int32_t) * g, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::vector<int32_t> gene2slot, slot2gene;
+  strict_assign_slots(hc, (int)pl->ld, gene2slot, slot2gene);
+  DevBuf d_g2s;
+  d_g2s.alloc(sizeof(int32_t) * g);
+  CK(cudaMemcpyAsync(d_g2s.p, gene2slot.data(), sizeof(int32_t) * g, cudaMemcpyHostToDevice, st));
+  pl->d_slot2gene.alloc(sizeof(int32_t) * pl->nslots);
+  CK(cudaMemcpyAsync(pl->d_slot2gene.p, slot2gene.data(), sizeof(int32_t) * pl->nslots, cudaMemcpyHostToDevice,
+                     st));
+  const int64_t n_tiles = (n + kStrictTile - 1) / kStrictTile;
+  pl->csc_tptr.alloc(sizeof(int32_t) * (size_t)n_tiles * (pl->nslots + 1));
+  pl->csc_cell.alloc(std::max<int64_t>(nnz, 1));
+  pl->csc_val.alloc(dtype_size(pl->dtype) * std::max<int64_t>(nnz, 1));
+  CK(launch_tile_csc(pl->dtype, pl->indptr, pl->idx, pl->val, n, d_g2s.as<int32_t>(), pl->nslots,
+                     pl->csc_tptr.as<int32_t>(), pl->csc_cell.as<uint8_t>(), pl->csc_val.p, st, pl->num_sms));
+  // ranges: about four blocks per SM over all gene blocks, for balance
+  const int gblocks = pl->nslots / (8 * strict_genes_per_warp((int)pl->ld));
+  pl->strict_ranges = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, (4 * pl->num_sms + gblocks - 1) / gblocks));
+  pl->wpart.alloc(sizeof(float) * (size_t)pl->strict_ranges * g * pl->ld);
+  CK(cudaStreamSynchronize(st));  // the host vectors above go out of scope
 }
 
 scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const AffineSpec* aff = nullptr) {
@@ -642,15 +696,17 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
              "cuTensorMapEncodeTiled failed (" + std::to_string(r1) + ", " + std::to_string(r2) + ")");
     }
 
-    // ---- transposed-product tables ----
+    // ---- CUDA-core products: tile-CSC copy for the transposed product ----
     pl->nb = (int)((g + kTransposeGeneBlock - 1) / kTransposeGeneBlock);
     pl->nchunks = std::max(1, (2 * pl->num_sms + pl->nb - 1) / pl->nb);
     pl->nchunks = (int)std::min<int64_t>(pl->nchunks, n);
     pl->rows_per_chunk = (n + pl->nchunks - 1) / pl->nchunks;
-    pl->rbp.alloc(sizeof(int32_t) * n * (pl->nb + 1));
-    CK(launch_row_block_ptr(pl->indptr, pl->idx, n, pl->nb, kTransposeGeneBlock, pl->rbp.as<int32_t>(),
-                            st, pl->num_sms));
-    pl->wpart.alloc(sizeof(float) * (size_t)pl->nchunks * g * ld);
+    if (!pl->use_tc) {
+      pl->nslots = strict_slot_count(g, (int)ld);
+      pl->strict_csc = strict_tile_smem_bytes(pl->nslots) <= kStatsSmemMax;
+    }
+    if (pl->strict_csc) build_tile_csc(pl);
+    else if (!pl->use_tc) ensure_rbp(pl);
 
     // ---- dense work buffers ----
     pl->gram_parts = 2 * pl->num_sms;
@@ -682,7 +738,8 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
     CK(cudaMemGetInfo(&fr, &tot));
     pl->device_bytes = pl->b_indptr.bytes + pl->b_idx.bytes + pl->b_val.bytes + pl->stats_part.bytes +
                        pl->rbp.bytes + pl->wpart.bytes + pl->Y.bytes + pl->gpart.bytes +
-                       pl->W.bytes + pl->Z.bytes + pl->V.bytes;
+                       pl->W.bytes + pl->Z.bytes + pl->V.bytes + pl->csc_tptr.bytes + pl->csc_cell.bytes +
+                       pl->csc_val.bytes + pl->tf_ent.bytes + pl->Yimg.bytes + pl->tc_part.bytes;
     return pl;
   } catch (...) {
     // the buffers are freed in the stream's order: delete the plan first
@@ -792,12 +849,20 @@ void rmatmat_raw(scxpca_plan* pl, float* A, int split) {
     return;
   }
   int s = stage_begin(pl);
-  CK(launch_spmm_t(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, (int32_t)pl->g,
-                   pl->rbp.as<int32_t>(), pl->nb, pl->nchunks, pl->rows_per_chunk, A,
-                   pl->wpart.as<float>(), st));
+  int parts = pl->nchunks;
+  if (pl->strict_csc) {
+    CK(launch_rmat_strict(pl->dtype, (int)pl->ld, pl->indptr, pl->csc_tptr.as<int32_t>(), pl->csc_cell.as<uint8_t>(),
+                          pl->csc_val.p, pl->n, (int32_t)pl->g, pl->nslots, pl->d_slot2gene.as<int32_t>(),
+                          pl->strict_ranges, A, pl->wpart.as<float>(), st));
+    parts = pl->strict_ranges;
+  } else {
+    CK(launch_spmm_t(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, (int32_t)pl->g,
+                     pl->rbp.as<int32_t>(), pl->nb, pl->nchunks, pl->rows_per_chunk, A,
+                     pl->wpart.as<float>(), st));
+  }
   stage_end(pl, SCXPCA_STAGE_TRANSPOSE, s);
   s = stage_begin(pl);
-  CK(launch_reduce_rows_f32(pl->wpart.as<float>(), pl->nchunks, pl->g * pl->ld, pl->W.as<double>(), 0,
+  CK(launch_reduce_rows_f32(pl->wpart.as<float>(), parts, pl->g * pl->ld, pl->W.as<double>(), 0,
                             st, pl->num_sms));
   stage_end(pl, SCXPCA_STAGE_REDUCE, s);
 }
@@ -820,8 +885,8 @@ void forward(scxpca_plan* pl, bool f32 = true) {
     return;
   }
   int s = stage_begin(pl);
-  CK(launch_spmm_fwd(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, pl->V.as<float>(),
-                     pl->centered ? pl->mc.as<float>() : nullptr, pl->Y.as<float>(), st, pl->num_sms));
+  CK(launch_fwd_strict(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, (int32_t)pl->g,
+                       pl->V.as<float>(), pl->centered ? pl->mc.as<float>() : nullptr, pl->Y.as<float>(), st));
   stage_end(pl, SCXPCA_STAGE_FORWARD, s);
 }
 
@@ -912,6 +977,22 @@ void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
                               pl->num_sms));
   stage_end(pl, SCXPCA_STAGE_APPLY, s);
   tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
+  if (shift) {
+    // Householder contract (an orthonormal Q whatever the conditioning): when
+    // the first factorisation had to be shifted, CholeskyQR2 leaves Q with an
+    // orthogonality error of about u cond(Q1); a third pass (shifted
+    // CholeskyQR3) brings it to working precision.  Applied unconditionally in
+    // this mode, so the enqueued sequence does not depend on device results.
+    s = stage_begin(pl);
+    if (pl->use_tc)
+      CK(launch_apply_right_split(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(),
+                                  pl->Yimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
+    else
+      CK(launch_apply_right_f32(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(), st,
+                                pl->num_sms));
+    stage_end(pl, SCXPCA_STAGE_APPLY, s);
+    tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
+  }
   // B = (X - mu)^T Q R2^{-1}
   rmatmat_raw(pl, pl->Y.as<float>(), 0);
   s = stage_begin(pl);
@@ -1021,6 +1102,7 @@ void backward(scxpca_plan* pl, const float* S, const float* GS, int iters, float
   pl->bw_colD.alloc(sizeof(double) * g);
   pl->bw_sumDP.alloc(sizeof(double) * g);
   pl->bw_part.alloc(sizeof(double) * (size_t)pl->nchunks * g);
+  ensure_rbp(pl);
   const int cparts = (int)std::max<int64_t>(1, std::min<int64_t>(2 * pl->num_sms, (n + 255) / 256));
   pl->bw_cpart.alloc(sizeof(double) * (size_t)cparts * 256);
   double* vec = pl->bw_vec.as<double>();
@@ -1709,7 +1791,9 @@ int32_t scxpca_plan_qr(scxpca_plan* plan, float* a, int64_t m, int64_t ld_a, cha
     CK(cudaMemcpy2DAsync(tmp.p, sizeof(float) * ld, a, sizeof(float) * ld_a, sizeof(float) * plan->k, m,
                          cudaMemcpyDeviceToDevice, st));
     CK(cudaMemsetAsync(plan->status.p, 0, sizeof(int) * 4, st));
-    for (int pass = 0; pass < 2; ++pass) {
+    // CholeskyQR2; with the Householder contract a third pass (shifted
+    // CholeskyQR3), which restores orthogonality after a shifted first pass.
+    for (int pass = 0; pass < (shift ? 3 : 2); ++pass) {
       tall_chol(plan, tmp.as<float>(), m, plan->Rinv.as<double>(), plan->Rinv_f.as<float>(), shift);
       CK(launch_apply_right_f32(tmp.as<float>(), m, (int)ld, plan->Rinv_f.as<float>(), tmp.as<float>(), st,
                                 plan->num_sms));

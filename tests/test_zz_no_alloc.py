@@ -84,6 +84,47 @@ def test_noalloc_col_stats_match_plan_col_stats_on_two_calls():
         val = vv.cpu().numpy().astype(np.float64)
         np.testing.assert_allclose(got[:g], np.bincount(idx, weights=val, minlength=g), rtol=1e-10,
                                    atol=1e-10 * scale_s)
+        np.testing.assert_allclose(got[g:], np.bincount(idx, weights=val * val, minlength=g), rtol=1e-10,
+                                   atol=1e-10 * scale_q)
+
+
+@pytest.mark.gpu
+def test_noalloc_at_the_gene_limit():
+    """n_vars == NOALLOC_MAX_VARS: the widest matrix the static scratch serves
+    (the fewest per-block partials, and more genes than one shared-memory
+    accumulator pass holds).  Checked against the allocating entry point and
+    against FP64 sums on the host, on two calls in a row."""
+    import torch
+
+    from scx_b200 import accel
+
+    lib = _lib.load()
+    torch.cuda.init()
+    n, g = 2000, _lib.NOALLOC_MAX_VARS
+    ip, ix, vv = accel.synth_nb_csr_device(n, g, seed=21, loc=-1.5)
+    torch.cuda.synchronize()
+    plan = accel.Plan(ip, ix, vv, (n, g), n_components=5, n_oversamples=5, zero_center=True, scale=False,
+                      math_mode="strict_fp32")
+    try:
+        want_s, want_q = plan.col_stats()
+    finally:
+        plan.close()
+    idx = ix.cpu().numpy()
+    val = vv.cpu().numpy().astype(np.float64)
+    host_s = np.bincount(idx, weights=val, minlength=g)
+    host_q = np.bincount(idx, weights=val * val, minlength=g)
+    for _ in range(2):
+        out = torch.full((2 * g,), float("nan"), dtype=torch.float64, device="cuda:0")
+        x = _csr(ip, ix, vv, (n, g))
+        err = _lib.errbuf()
+        st = lib.scxpca_col_stats_noalloc(0, C.byref(x), C.c_void_p(out.data_ptr()), None, err, len(err))
+        _lib.check(st, err)
+        got = out.cpu().numpy()
+        # the same kernel over a different block partition (fewer partials)
+        np.testing.assert_allclose(got[:g], want_s, rtol=RTOL, atol=RTOL * np.abs(want_s).max())
+        np.testing.assert_allclose(got[g:], want_q, rtol=RTOL, atol=RTOL * np.abs(want_q).max())
+        np.testing.assert_allclose(got[:g], host_s, rtol=1e-10, atol=1e-10 * np.abs(host_s).max())
+        np.testing.assert_allclose(got[g:], host_q, rtol=1e-10, atol=1e-10 * np.abs(host_q).max())
 
 
 @pytest.mark.gpu
