@@ -406,39 +406,25 @@ def run_ours(args):
         p32.close()
         sv32 = np.asarray(res32.singular_values)
         comps32 = np.asarray(res32.components)
+        st32 = prof32["stages"]
+        tot32 = sum(v["device_ms"] for v in st32.values())
+        kern32 = {}
+        for stg in ("forward", "transpose"):
+            lm = st32[stg]["device_ms"] / max(st32[stg]["launches"], 1)
+            kb32 = kernel_bytes(stg, nnz, n_obs, N_VARS, k, 4)
+            kern32[stg] = {"launch_ms": round(lm, 4), "algorithmic_bytes_per_launch": kb32,
+                           "gbs": round(kb32 / (lm * 1e-3) / 1e9, 1),
+                           "frac": round(kb32 / (lm * 1e-3) / 1e9 / peak, 4)}
         out["fp32"] = {"ms": round(ms32, 4), "speedup_mixed_vs_fp32": round(ms32 / ms_max, 3),
                        "sigma_max_rel_diff_mixed_vs_fp32":
-                           float(np.max(np.abs(sv_main - sv32) / sv32))}
+                           float(np.max(np.abs(sv_main - sv32) / sv32)),
+                       "stage_share": {s_: round(v["device_ms"] / tot32, 4) for s_, v in st32.items()
+                                       if v["launches"]},
+                       "kernels": kern32}
 
     if not args.no_e2e:
-        # host (pinned) CSR through the one-shot C ABI call
-        h_ip = ip.cpu().pin_memory()
-        h_ix = ix.cpu().pin_memory()
-        h_vv = vv.cpu().pin_memory()
-        h_emb = torch.empty((n_obs, N_COMPS), dtype=torch.float32).pin_memory()
-        a_ip, a_ix, a_vv, a_emb = h_ip.numpy(), h_ix.numpy(), h_vv.numpy(), h_emb.numpy()
-
-        def one():
-            return accel.randomized_pca(a_ip, a_ix, a_vv, (n_obs, N_VARS), n_components=N_COMPS,
-                                        n_oversamples=N_OVERSAMPLES, n_power_iterations=N_POWER,
-                                        zero_center=True, scale=True, clip_max=CLIP, seed=SEED,
-                                        qr_method="cholesky", math_mode=args.mode, device=local,
-                                        embeddings_out=a_emb)
-
-        one()
-        e2e_steps = max(1, min(3, args.steps))
-        barrier(dev)
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            one()
-        e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
-        e2e_ms = max_over_ranks(e2e_ms, dev)
-        h2d = a_ip.nbytes + a_ix.nbytes + a_vv.nbytes
-        d2h = a_emb.nbytes + N_COMPS * N_VARS * 4 + N_COMPS * 8 * 3 + N_VARS * 8 * 2
-        out["e2e"] = {"value": round(e2e_ms / world, 3), "unit": "ms", "h2d_bytes_per_step": h2d,
-                      "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-                      "path": "scxpca_randomized (host pinned CSR -> host embeddings)"}
-        host_csr = (a_ip, a_ix, a_vv)
+        out["e2e"], host_csr = e2e_leg(args, ip, ix, vv, n_obs, local, dev, world)
+        out["device_one_shot"] = device_one_shot_leg(args, ip, ix, vv, n_obs, local, dev, stream)
     else:
         host_csr = (ip.cpu().numpy(), ix.cpu().numpy(), vv.cpu().numpy())
 
@@ -490,15 +476,119 @@ def run_ours(args):
     _finish_dist()
 
 
+def e2e_leg(args, ip, ix, vv, n_obs, local, dev, world):
+    """The PCA through the one-shot C ABI call from pinned host memory to host
+    embeddings (upload, validation, statistics, value transform, packing, the
+    PCA, download and teardown inside every timed step).  Values go up in the
+    precision the mode computes in (BF16 or FP16 for the mixed modes, FP32 for
+    the strict mode); indices int32, indptr int64.  Reports the median of the
+    library's own per-phase times (device clock on the call's stream) and the
+    host-to-device bandwidth of a plain copy of the same pinned bytes measured
+    in the same run, which sets the upload phase."""
+    import numpy as np
+    import torch
+
+    from scx_b200 import accel
+
+    vdt = {"mixed_bf16": torch.bfloat16, "mixed_f16": torch.float16, "strict_fp32": torch.float32}[args.mode]
+    h_ip = ip.cpu().pin_memory()
+    h_ix = ix.cpu().pin_memory()
+    h_vv = vv.to(vdt).cpu().pin_memory()
+    h_emb = torch.empty((n_obs, N_COMPS), dtype=torch.float32).pin_memory()
+    a_ip, a_ix, a_emb = h_ip.numpy(), h_ix.numpy(), h_emb.numpy()
+    a_vv = h_vv if vdt == torch.bfloat16 else h_vv.numpy()
+
+    def one():
+        return accel.randomized_pca(a_ip, a_ix, a_vv, (n_obs, N_VARS), n_components=N_COMPS,
+                                    n_oversamples=N_OVERSAMPLES, n_power_iterations=N_POWER,
+                                    zero_center=True, scale=True, clip_max=CLIP, seed=SEED,
+                                    qr_method="cholesky", math_mode=args.mode, device=local,
+                                    embeddings_out=a_emb)
+
+    one()
+    steps = max(1, min(10, args.steps))
+    phases = []
+    barrier(dev)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+        phases.append(accel.last_call_phases())
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / steps
+    e2e_ms = max_over_ranks(e2e_ms, dev)
+    h2d = h_ip.numel() * 8 + h_ix.numel() * 4 + h_vv.numel() * h_vv.element_size()
+    d2h = a_emb.nbytes + N_COMPS * N_VARS * 4 + N_COMPS * 8 * 3 + N_VARS * 8 * 2
+    # plain pinned host-to-device copy of the same bytes, for the upload phase
+    d_ix = torch.empty_like(ix)
+    d_vv = torch.empty(h_vv.shape, dtype=vdt, device=dev)
+    torch.cuda.synchronize(dev)
+    cs = torch.cuda.Stream(device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(cs):
+        e0.record(cs)
+        d_ix.copy_(h_ix, non_blocking=True)
+        d_vv.copy_(h_vv, non_blocking=True)
+        e1.record(cs)
+    torch.cuda.synchronize(dev)
+    copy_ms = e0.elapsed_time(e1)
+    del d_ix, d_vv
+    med = {k: round(statistics.median(p[k] for p in phases), 3) for k in phases[0]}
+    out = {"value": round(e2e_ms / world, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "steps": steps,
+           "path": "scxpca_randomized (host pinned CSR -> host embeddings)",
+           "values_on_host": str(vdt).replace("torch.", ""),
+           "phases_ms": med,
+           "h2d_copy": {"ms": round(copy_ms, 3),
+                        "gbs": round((h_ix.numel() * 4 + h_vv.numel() * h_vv.element_size()) / copy_ms / 1e6, 1)}}
+    host_csr = (a_ip, a_ix, vv.cpu().numpy())
+    return out, host_csr
+
+
+def device_one_shot_leg(args, ip, ix, vv, n_obs, local, dev, stream):
+    """Plan creation + run + destruction from the DEVICE CSR (FP32 values, so
+    validation, statistics, the value transform and packing all run), timed
+    with CUDA events on the plan's stream: the per-matrix set-up that the
+    resident headline excludes, counted like-for-like with the reference's
+    per-call host work."""
+    import torch
+
+    from scx_b200 import accel
+
+    emb = torch.empty((n_obs, N_COMPS), dtype=torch.float32, device=dev)
+    times = []
+    for i in range(2 + max(1, min(3, args.steps))):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        plan = accel.Plan(ip, ix, vv, (n_obs, N_VARS), n_components=N_COMPS, n_oversamples=N_OVERSAMPLES,
+                          n_power_iterations=N_POWER, zero_center=True, scale=True, clip_max=CLIP, seed=SEED,
+                          qr_method="cholesky", math_mode=args.mode, device=local, stream=stream.cuda_stream)
+        plan.run(embeddings_out=emb)
+        plan.close()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if i >= 2:
+            times.append(e0.elapsed_time(e1))
+    return {"ms": round(statistics.median(times), 3), "steps": len(times),
+            "path": "scxpca_plan_create + scxpca_plan_run + scxpca_plan_destroy on the device CSR (FP32 values)"}
+
+
 DIFF_N_OBS = 200_000
+CONVERGED_SOLVE = 64
+SOLVE_SWEEP = (4, 8, 16, 32)
+GRAD_RTOL = 2e-3
 
 
 def differentiable_leg(args, local, dev):
     """Forward vs backward of the differentiable scores on the 200,000 x 2,000
     NB-synthetic CSR, FP32, 50 PCs, oversample 10, 4 power iterations, centred
     on the column means and scaled by 1 / std (explicit per-gene vectors), loss
-    sum(W * S**2) with W a seeded N(0, 1) 200,000 x 50 matrix.  Both legs are
-    timed with CUDA events on the plan's stream over the same steps."""
+    sum(W * S**2) with W a seeded N(0, 1) 200,000 x 50 matrix.
+
+    The gradient's conjugate-gradient solve is first checked for accuracy: the
+    gradients (values, centre, scale) after 4, 8, 16 and 32 steps against a
+    converged solve of 64 steps of the same run; the smallest step count that
+    agrees to 2e-3 relative is the one timed.  Forward and backward are timed
+    with CUDA events on the plan's stream over the same steps."""
     import torch
 
     from scx_b200 import accel
@@ -518,7 +608,26 @@ def differentiable_leg(args, local, dev):
                       math_mode="strict_fp32", device=local, stream=stream.cuda_stream,
                       center=mean, gene_scale=scale)
     S = torch.empty((n, N_COMPS), dtype=torch.float32, device=dev)
-    solve = 8
+
+    def grads(iters):
+        plan.run(embeddings_out=S)
+        with torch.cuda.stream(stream):
+            G = 2.0 * W * S
+        gv, gc, gs = plan.backward(S, G, iters)
+        torch.cuda.synchronize(dev)
+        return gv.double(), gc.double(), gs.double()
+
+    def rel(a, b):
+        return float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+
+    ref = grads(CONVERGED_SOLVE)
+    errs = {}
+    for iters in SOLVE_SWEEP:
+        gv, gc, gs = grads(iters)
+        errs[iters] = {"values": rel(gv, ref[0]), "center": rel(gc, ref[1]), "scale": rel(gs, ref[2])}
+    enough = [i for i in SOLVE_SWEEP if max(errs[i].values()) <= GRAD_RTOL]
+    solve = enough[0] if enough else SOLVE_SWEEP[-1]
+
     fwd_ms, bwd_ms = [], []
     steps = max(2, min(args.steps, 5))
     for i in range(args.warmup + steps):
@@ -540,7 +649,10 @@ def differentiable_leg(args, local, dev):
     return {"workload": f"{n:,} x {g:,} NB-synthetic CSR ({int(ix.numel()):,} nnz), FP32, 50 PCs, "
                         "oversample 10, 4 power iterations, loss sum(W * S^2)",
             "forward_ms": round(f, 3), "backward_ms": round(b, 3), "backward_over_forward": round(b / f, 3),
-            "solve_iterations": solve, "steps": steps}
+            "solve_iterations": solve, "steps": steps,
+            "grad_rel_err": {str(i): {k_: float(f"{v:.3e}") for k_, v in e.items()} for i, e in errs.items()},
+            "grad_rel_err_reference": f"{CONVERGED_SOLVE} CG steps on the same run",
+            "grad_rtol": GRAD_RTOL, "solve_reaches_rtol": bool(enough)}
 
 
 BATCH_CLUSTERS = 256
@@ -593,7 +705,39 @@ def batched_leg(args, local, dev):
            "autotune_ms": {str(k): round(v, 3) for k, v in b.tuned_ms.items()},
            "sigma_max_rel_diff_graph_vs_plain": float(np.max(np.abs(sv_g - sv_p) / sv_p))}
     b.close()
+    # correctness at the timed setting: clusters from smallest to largest
+    # against the FP64 randomized PCA (C++ restatement, same seeded Omega) of
+    # the same BF16-rounded values
+    out["vs_oracle"] = batched_oracle_check(sizes, offs, ip, ix, vv, sv_g)
     return out
+
+
+BATCH_CHECKED = 8
+
+
+def batched_oracle_check(sizes, offs, ip, ix, vv, sv):
+    import numpy as np
+
+    from oracle import build_cpu, rpca
+
+    order = np.argsort(sizes, kind="stable")
+    pick = sorted({int(order[0]), int(order[-1])} |
+                  {int(order[i]) for i in np.linspace(0, len(order) - 1, BATCH_CHECKED).round().astype(int)})
+    h_ip = ip.cpu().numpy()
+    h_ix = ix.cpu().numpy()
+    h_vv = vv.float().cpu().numpy()  # the BF16 values the GPU saw, widened exactly
+    om = rpca.gaussian_omega(N_VARS, 40, SEED)
+    errs = {}
+    for q in pick:
+        r0, r1 = int(offs[q]), int(offs[q + 1])
+        p0, p1 = int(h_ip[r0]), int(h_ip[r1])
+        res = build_cpu.run(h_ip[r0:r1 + 1] - p0, h_ix[p0:p1], h_vv[p0:p1], (r1 - r0, N_VARS), 30, 40, 3, om,
+                            zero_center=True, threads=os.cpu_count() or 1)
+        ref = res["singular_values"]
+        errs[str(q)] = {"cells": r1 - r0, "sigma_max_rel_err": float(np.max(np.abs(sv[q] - ref) / ref))}
+    return {"clusters": errs, "sigma_max_rel_err": max(e["sigma_max_rel_err"] for e in errs.values()),
+            "reference": "FP64 C++ restatement of the reference CPU randomized PCA, same seeded Omega, "
+                         "BF16-rounded values"}
 
 
 def _finish_dist():
@@ -604,36 +748,53 @@ def _finish_dist():
 
 
 def run_reference(args):
-    """Reference arm: the reference's CPU randomized PCA (its C++ restatement,
-    the Rust reference being unbuildable here) on the host cores."""
+    """Reference arm: the reference's CPU randomized PCA (its multithreaded C++
+    restatement, the Rust reference being unbuildable here) on all host
+    cores, on the whole matrix of the GPU arm: the same device generator and
+    seed, copied to host memory once before timing.  Warm-up steps run on the
+    first 50,000 rows (the CPU has nothing to warm); every timed step is one
+    complete PCA of the whole matrix."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import numpy as np
+    import torch
 
-    from scx_b200.synth import synth_nb_csr
+    from scx_b200 import accel
 
-    rows = min(args.cpu_sample_rows or 50_000, args.n_obs)
-    ip, ix, vv = synth_nb_csr(rows, N_VARS, seed=SEED, loc=LOC, dispersion=DISPERSION)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if torch.cuda.is_available():
+        ip_d, ix_d, vv_d = accel.synth_nb_csr_device(args.n_obs, N_VARS, seed=SEED, loc=LOC,
+                                                     dispersion=DISPERSION, device=local)
+        ip, ix, vv = ip_d.cpu().numpy(), ix_d.cpu().numpy(), vv_d.cpu().numpy()
+        del ip_d, ix_d, vv_d
+        torch.cuda.empty_cache()
+        data = "synthetic (seeded negative-binomial CSR generated on device, copied to host before timing)"
+    else:  # no device: the host restatement of the generator (a different matrix of the same law)
+        from scx_b200.synth import synth_nb_csr
+        ip, ix, vv = synth_nb_csr(args.n_obs, N_VARS, seed=SEED, loc=LOC, dispersion=DISPERSION)
+        data = "synthetic (seeded negative-binomial CSR, host generator; no device present)"
+    nnz = int(ip[-1])
     threads = os.cpu_count() or 1
+    warm_rows = min(SUBSAMPLE_ROWS, args.n_obs)
+    for _ in range(args.warmup):
+        cpu_baseline(ip, ix, vv, warm_rows, warm_rows, threads)
     times = []
-    for i in range(args.warmup + args.steps):
-        ms, nnz, _, _ = cpu_baseline(ip, ix, vv, args.n_obs, rows, threads)
-        if i >= args.warmup:
-            times.append(ms)
+    for _ in range(args.steps):
+        ms, _, _, _ = cpu_baseline(ip, ix, vv, args.n_obs, args.n_obs, threads)
+        times.append(ms)
     value = float(np.mean(times))
-    nnz_full_est = int(nnz * args.n_obs / rows)
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "ms", "impl": "reference",
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(value, 1), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded negative-binomial CSR, host generator)",
-        "config": base_config(args.n_obs, nnz_full_est, "f32 input, f64 compute", 1),
+        "data": data,
+        "config": base_config(args.n_obs, nnz, "f32 input, f64 compute", 1),
         "cpu_baseline": {"value": round(value, 1), "unit": "ms", "cores": threads, "kind": "port",
-                         "sample": f"{rows:,} rows ({nnz:,} nnz) per step, scaled by rows to "
-                                   f"{args.n_obs:,}; reference is Rust (unbuildable here), "
-                                   "timed via its FP64 C++ restatement"},
+                         "sample": f"the whole matrix ({args.n_obs:,} rows, {nnz:,} nnz) per timed step; "
+                                   f"warm-up on the first {warm_rows:,} rows; reference is Rust (unbuildable "
+                                   "here), timed via its FP64 C++ restatement"},
         "e2e": {"value": round(value, 1), "unit": "ms", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -285,6 +285,29 @@ typedef struct {
   int64_t runs;                        /* plan_run calls since reset */
 } scxpca_profile;
 
+/* Phases of the calling thread's last scxpca_randomized call, in device
+ * milliseconds between consecutive phase boundaries recorded on the call's
+ * stream (host gaps between phases included), except DESTROY, which is host
+ * time.  The counterpart of the reference's per-call timing log
+ * (scx-gpu/src/profile.rs:1-60, gpu_pca.rs:465-697). */
+enum {
+  SCXPCA_PHASE_UPLOAD = 0,    /* pre-flight, allocations, host-to-device copy */
+  SCXPCA_PHASE_VALIDATE = 1,  /* CSR validation (and row sort) */
+  SCXPCA_PHASE_STATS = 2,     /* per-gene statistics of the input */
+  SCXPCA_PHASE_TRANSFORM = 3, /* value transform, working statistics, total variance */
+  SCXPCA_PHASE_PACK = 4,      /* packed tile copy for the products */
+  SCXPCA_PHASE_BUFFERS = 5,   /* work buffers */
+  SCXPCA_PHASE_PCA = 6,       /* power loop, Rayleigh-Ritz step, embeddings */
+  SCXPCA_PHASE_DOWNLOAD = 7,  /* device-to-host copy of the results */
+  SCXPCA_PHASE_DESTROY = 8,   /* plan teardown (host time) */
+  SCXPCA_NUM_PHASES = 9
+};
+
+/* Writes min(capacity, SCXPCA_NUM_PHASES) phase times (-1 when the call failed
+ * before its phases completed) and the call's host wall time; returns
+ * SCXPCA_NUM_PHASES. */
+int32_t scxpca_last_call_phases(double* ms, int32_t capacity, double* wall_ms);
+
 /* Enable (1) or disable (0) stage timing; any call resets the counters. */
 int32_t scxpca_plan_set_profiling(scxpca_plan* plan, int32_t enable);
 int32_t scxpca_plan_get_profile(const scxpca_plan* plan, scxpca_profile* out);

@@ -56,9 +56,12 @@ EXPORTED = (
     "scxpca_plan_get_profile",
     "scxpca_gaussian",
     "scxpca_synth_nb_csr",
+    "scxpca_last_call_phases",
 )
 
 STAGES = ("prepare", "forward", "transpose", "reduce", "gram", "apply", "small", "embed")
+# Phases of a one-shot call (scxpca_last_call_phases).
+PHASES = ("upload", "validate", "stats", "transform", "pack", "buffers", "pca", "download", "destroy")
 
 
 class ScxLibraryError(RuntimeError):
@@ -172,6 +175,7 @@ def load() -> C.CDLL:
         "scxpca_gaussian": (C.c_int32, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, P, *E]),
         "scxpca_synth_nb_csr": (C.c_int32, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, C.c_double,
                                             C.c_double, P, P, P, C.POINTER(C.c_int64), *E]),
+        "scxpca_last_call_phases": (C.c_int32, [P, C.c_int32, C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -88,8 +88,24 @@ def _prepare_csr(indptr, indices, values, shape):
     n_obs, n_vars = int(shape[0]), int(shape[1])
     if _is_torch(values):
         import torch
+        if not values.is_cuda and values.dtype == torch.bfloat16:
+            # host BF16 values (numpy has no bfloat16): passed by pointer, so a
+            # pinned tensor is copied to the device at full link speed
+            values = values.contiguous()
+            indptr = np.ascontiguousarray(indptr.numpy() if _is_torch(indptr) else indptr, dtype=np.int64)
+            indices = np.ascontiguousarray(indices.numpy() if _is_torch(indices) else indices, dtype=np.int32)
+            if indptr.shape[0] != n_obs + 1:
+                raise ValueError(f"indptr must have n_obs + 1 = {n_obs + 1} entries, got {indptr.shape[0]}")
+            nnz = int(values.numel())
+            if indices.shape[0] != nnz:
+                raise ValueError("indices and values lengths differ")
+            csr = _lib.Csr(n_obs, n_vars, nnz, _ptr(indptr), _ptr(indices), _ptr(values), _lib.BF16,
+                           _lib.MEM_HOST)
+            return csr, (indptr, indices, values), _lib.MEM_HOST, None
         if not values.is_cuda:
-            values = values.numpy() if values.dtype != torch.bfloat16 else values
+            values = values.numpy()
+            indptr = indptr.numpy() if _is_torch(indptr) else indptr
+            indices = indices.numpy() if _is_torch(indices) else indices
         else:
             indptr = indptr.to(torch.int64).contiguous()
             indices = indices.to(torch.int32).contiguous()
@@ -250,6 +266,19 @@ def randomized_pca(indptr, indices, values, shape, n_components: int = 50,
     _lib.check(st, err)
     del keep, okeep
     return _finish(res, bufs, n_obs, n_vars, nc, zero_center, scale, k)
+
+
+def last_call_phases() -> dict:
+    """Phases of this thread's last one-shot call (scxpca_last_call_phases):
+    device ms per phase (upload, validate, stats, transform, pack, buffers,
+    pca, download; destroy in host ms) and the call's host wall time."""
+    lib = _lib.load()
+    ms = np.zeros(len(_lib.PHASES), dtype=np.float64)
+    wall = C.c_double()
+    lib.scxpca_last_call_phases(_ptr(ms), len(ms), C.byref(wall))
+    out = {name: float(v) for name, v in zip(_lib.PHASES, ms)}
+    out["wall"] = float(wall.value)
+    return out
 
 
 class Plan:

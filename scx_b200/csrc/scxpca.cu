@@ -16,6 +16,7 @@
 // FP64.
 // The SVD of B is an FP64 Jacobi eigendecomposition of B^T B on the device.
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -116,6 +117,43 @@ void stream_fence(cudaStream_t from, cudaStream_t to) {
   CK(cudaEventRecord(e, from));
   CK(cudaStreamWaitEvent(to, e, 0));
   cudaEventDestroy(e);
+}
+
+// Phase timing of the calling thread's one-shot call (scxpca_randomized):
+// when on, each phase boundary records an event on the plan's stream, and
+// the intervals between consecutive boundaries (device clock, idle gaps
+// while the host prepares the next phase included) become the phases.
+struct PhaseRec {
+  bool on = false;
+  cudaStream_t st = nullptr;
+  int next = 0;
+  cudaEvent_t ev[SCXPCA_NUM_PHASES + 1] = {};
+  double ms[SCXPCA_NUM_PHASES] = {};
+  double wall_ms = 0.0;
+};
+thread_local PhaseRec t_phase;
+
+// Mark the end of phase `ph` (and of every phase before it not yet marked).
+void phase_mark(int ph, cudaStream_t st) {
+  PhaseRec& r = t_phase;
+  if (!r.on) return;
+  if (r.next == 0) {  // the first mark opens the clock
+    if (cudaEventCreate(&r.ev[0]) != cudaSuccess || cudaEventRecord(r.ev[0], st) != cudaSuccess) {
+      cudaGetLastError();
+      r.on = false;
+      return;
+    }
+    r.st = st;
+    r.next = 1;
+  }
+  while (r.next <= ph + 1 && r.next <= SCXPCA_NUM_PHASES) {
+    if (cudaEventCreate(&r.ev[r.next]) != cudaSuccess || cudaEventRecord(r.ev[r.next], st) != cudaSuccess) {
+      cudaGetLastError();
+      r.on = false;
+      return;
+    }
+    ++r.next;
+  }
 }
 
 // Allocation context of the calling thread: DevBufs allocated inside a
@@ -480,6 +518,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
     cudaStream_t st = pl->stream;
     PoolScope pool_scope(pl->device, st);
     const int64_t n = pl->n, g = pl->g, nnz = pl->nnz;
+    phase_mark(-1, st);  // opens the phase clock of a one-shot call
 
     // ---- pre-flight (gpu_pca.rs:450-462): resident CSR + work buffers ----
     {
@@ -523,6 +562,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
                          cudaMemcpyHostToDevice, st));
       vin = pl->b_stage.p;
     }
+    phase_mark(SCXPCA_PHASE_UPLOAD, st);
 
     // ---- validation ----
     {
@@ -568,6 +608,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       pl->fmt16 = pl->dtype == SCXPCA_BF16 ? 1 : 0;
     }
     const int64_t ld = pl->ld;
+    phase_mark(SCXPCA_PHASE_VALIDATE, st);
 
     // ---- statistics of the input ----
     pl->stats_parts = 2 * pl->num_sms;
@@ -577,6 +618,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
     stats_pass(pl, vin, pl->in_dtype, sx, sxx);
     pl->mean_x.resize(g);
     for (int64_t j = 0; j < g; ++j) pl->mean_x[j] = sx[j] / (double)n;
+    phase_mark(SCXPCA_PHASE_STATS, st);
 
     // ---- working values ----
     std::vector<double> center_raw(g, 0.0), scale_raw(g, 1.0);
@@ -663,6 +705,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       pl->std_x.resize(g);
       for (int64_t j = 0; j < g; ++j) pl->std_x[j] = 1.0 / scale_raw[j];
     }
+    phase_mark(SCXPCA_PHASE_TRANSFORM, st);
 
     // ---- tensor-core path: tile-chunk packed matrix, 16-bit operands, TMA maps ----
     if (pl->use_tc) {
@@ -707,6 +750,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
     }
     if (pl->strict_csc) build_tile_csc(pl);
     else if (!pl->use_tc) ensure_rbp(pl);
+    phase_mark(SCXPCA_PHASE_PACK, st);
 
     // ---- dense work buffers ----
     pl->gram_parts = 2 * pl->num_sms;
@@ -733,6 +777,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       for (int64_t i = 0; i < ld; ++i) eye[i * ld + i] = 1.0;
       upload(pl->eye, eye, st);
     }
+    phase_mark(SCXPCA_PHASE_BUFFERS, st);
     CK(cudaStreamSynchronize(st));
     size_t fr = 0, tot = 0;
     CK(cudaMemGetInfo(&fr, &tot));
@@ -1056,6 +1101,7 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   enqueue_run(pl, p, U);
   pl->prof.kernel_launches += launches_total() - launches0;
   pl->prof.runs += 1;
+  phase_mark(SCXPCA_PHASE_PCA, st);
   if (host_out)
     CK(cudaMemcpyAsync(out->embeddings, U, sizeof(float) * pl->n * pl->nc, cudaMemcpyDeviceToHost, st));
 
@@ -1066,6 +1112,7 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   if (out->components)
     CK(cudaMemcpyAsync(out->components, pl->comps.p, sizeof(float) * pl->nc * pl->g,
                        cudaMemcpyDeviceToHost, st));
+  phase_mark(SCXPCA_PHASE_DOWNLOAD, st);
   CK(cudaStreamSynchronize(st));
   collect_stages(pl);
   check_tc_error(pl);
@@ -1698,6 +1745,30 @@ int32_t scxpca_randomized(const scxpca_csr* x, const scxpca_params* params, scxp
     if (!out || !out->embeddings) fail(SCXPCA_INVALID_ARGUMENT, "null embeddings output");
     validate_params(x, params);
     DeviceGuard dg(params->device_ordinal);
+    // phase timing of this call (scxpca_last_call_phases)
+    struct PhaseScope {
+      std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+      PhaseScope() {
+        for (cudaEvent_t& e : t_phase.ev)
+          if (e) cudaEventDestroy(e);
+        t_phase = PhaseRec{};
+        t_phase.on = true;
+      }
+      ~PhaseScope() {
+        PhaseRec& r = t_phase;
+        if (r.on && r.next == SCXPCA_NUM_PHASES) {  // every device phase marked (destroy is host-timed)
+          for (int i = 0; i + 1 < SCXPCA_NUM_PHASES; ++i) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, r.ev[i], r.ev[i + 1]) == cudaSuccess) r.ms[i] = ms;
+          }
+        } else {
+          for (double& m : r.ms) m = -1.0;
+        }
+        cudaGetLastError();
+        r.wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        r.on = false;
+      }
+    } phases;
     scxpca_plan* pl = create_plan(x, params);
     PoolScope pool_scope(pl->device, pl->stream);
     try {
@@ -1706,8 +1777,19 @@ int32_t scxpca_randomized(const scxpca_csr* x, const scxpca_params* params, scxp
       scxpca_plan_destroy(pl);
       throw;
     }
+    const auto t_destroy = std::chrono::steady_clock::now();
     scxpca_plan_destroy(pl);
+    if (t_phase.on && t_phase.next == SCXPCA_NUM_PHASES)
+      t_phase.ms[SCXPCA_PHASE_DESTROY] =
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_destroy).count();
   });
+}
+
+int32_t scxpca_last_call_phases(double* ms, int32_t capacity, double* wall_ms) {
+  const int n = std::min<int32_t>(std::max<int32_t>(capacity, 0), SCXPCA_NUM_PHASES);
+  for (int i = 0; i < n; ++i) ms[i] = t_phase.ms[i];
+  if (wall_ms) *wall_ms = t_phase.wall_ms;
+  return SCXPCA_NUM_PHASES;
 }
 
 int32_t scxpca_plan_col_stats(scxpca_plan* plan, double* col_sums, double* col_sum_sq, char* err,

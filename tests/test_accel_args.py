@@ -64,3 +64,20 @@ def test_component_count_checked_by_the_library(n_components):
     ip, ix, vv, shape = _csr()
     with pytest.raises(ValueError):
         accel.randomized_pca(ip, ix, vv, shape, n_components=n_components)
+
+
+def test_host_bf16_values_pass_by_pointer():
+    """Host BF16 values (a torch CPU bfloat16 tensor) reach the C ABI as
+    values_dtype BF16 in host memory, without a conversion copy."""
+    import torch
+
+    from scx_b200 import _lib
+
+    ip, ix, vv, shape = _csr()
+    t = torch.from_numpy(vv).to(torch.bfloat16)
+    csr, keep, mem, dev = accel._prepare_csr(torch.from_numpy(ip), torch.from_numpy(ix), t, shape)
+    assert mem == _lib.MEM_HOST and dev is None
+    assert csr.values_dtype == _lib.BF16 and csr.values == t.data_ptr()
+    assert csr.nnz == len(vv)
+    with pytest.raises(ValueError, match="indptr must have n_obs"):
+        accel._prepare_csr(ip[:-1], ix, t, shape)
