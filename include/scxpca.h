@@ -350,6 +350,58 @@ int32_t scxpca_plan_col_stats(scxpca_plan* plan, double* col_sums, double* col_s
 int32_t scxpca_col_stats_noalloc(int32_t device_ordinal, const scxpca_csr* x, double* out_stats,
                                  void* stream, char* err, size_t err_len);
 
+/* Per-row normalize_total + log1p of a device CSR with float32 values,
+ * producing the PCA's input without leaving the device.  For every row with a
+ * non-zero sum: v <- v * target_sum / rowsum (FP64 row sum and factor; skipped
+ * when target_sum <= 0), then v <- log1p(v) when log1p != 0, then v <- v *
+ * row_factors[row] when row_factors (device, n_obs floats) is not NULL.  Rows
+ * that sum to zero are only multiplied by their factor.  Writes values_out
+ * (device, nnz floats; may be x->values itself for an in-place transform);
+ * indptr and indices are unchanged.  The CSR's indptr and indices are validated
+ * first (SCXPCA_INVALID_CSR).  `stream` may be NULL; the call synchronises it.
+ * Replaces gpu_apply_fused_ops and its wrappers gpu_normalize_log1p /
+ * gpu_normalize / gpu_log1p / gpu_row_scale (scx-gpu/src/gpu_preprocess.rs:
+ * 252-391, kernels in scx-gpu/kernels/normalize_log1p.cu:17-140). */
+int32_t scxpca_preprocess(int32_t device_ordinal, const scxpca_csr* x, float* values_out, double target_sum,
+                          int32_t log1p, const float* row_factors, void* stream, char* err, size_t err_len);
+
+/* Column projection of a device CSR with float32 values to the kept columns
+ * `cols` (host array of n_cols sorted, unique indices into [0, n_vars)); kept
+ * column cols[i] becomes column i, entries keep their row order.  The mask_var
+ * / highly_variable selection in front of the PCA, on the device.  Call with
+ * out_indices == out_values == NULL first: fills out_indptr (device, n_obs + 1)
+ * and *nnz_out; then again with device buffers of *nnz_out entries.  Replaces
+ * ProjectedShardSource (scx-accel/src/projected_source.rs:28-80) over
+ * scx_engine::project_csr. */
+int32_t scxpca_project_columns(int32_t device_ordinal, const scxpca_csr* x, const int32_t* cols, int64_t n_cols,
+                               int64_t* out_indptr, int32_t* out_indices, float* out_values, int64_t* nnz_out,
+                               void* stream, char* err, size_t err_len);
+
+/* PFlog (v4) representation of a raw-count device CSR (float32 values): the
+ * sparse delta = log1p(four_alpha * x) at the stored entries (delta_out,
+ * device, nnz floats; may be x->values for in place) and the per-cell
+ * baseline b_i = -(1 / n_vars) sum_j delta_ij in FP64 (baseline_out, device,
+ * n_obs doubles).  Negative or non-finite counts are rejected
+ * (SCXPCA_INVALID_ARGUMENT), as the reference's raw-count guard does.
+ * Replaces pflog_baseline_from_raw (scx-accel/src/pflog.rs:122-193) together
+ * with the lazy Scale{4 alpha} -> Log1p source it pairs with. */
+int32_t scxpca_pflog_prepare(int32_t device_ordinal, const scxpca_csr* x, double four_alpha, float* delta_out,
+                             double* baseline_out, void* stream, char* err, size_t err_len);
+
+/* Baseline-aware randomized PCA of Z = delta + baseline 1^T (the exact PFlog
+ * matrix, never densified): centring subtracts colmean(delta)_j +
+ * mean(baseline); `baseline` holds n_obs doubles in `baseline_memory`.  The
+ * baseline enters as one extra column of the working matrix, so both rank-1
+ * terms ride on the ordinary products.  params->scale must be 0 (clip_max is
+ * ignored); every other parameter and every output field means what it means
+ * for scxpca_randomized (mean = the column means of Z).  Total variance in
+ * closed form from the column statistics of delta, sum b_i^2 and
+ * sum b_i rowsum(delta_i).  Replaces pflog_pca / pflog_pca_with_depth
+ * (scx-accel/src/pca/cpu.rs:791-882, with the offset products of :618-687 and
+ * pflog_total_variance :689-786); the reference runs it on the CPU only. */
+int32_t scxpca_pflog_pca(const scxpca_csr* delta, const double* baseline, int32_t baseline_memory,
+                         const scxpca_params* params, scxpca_result* out, char* err, size_t err_len);
+
 /* Seeded N(0,1) test matrix, n_rows x n_cols column-major float32, into device
  * memory `out` on `device_ordinal`.  Replaces random_gaussian_gpu
  * (scx-gpu/src/curand.rs:76-157); the stream is Philox4x32-10 + Box-Muller,

@@ -428,3 +428,112 @@ def gaussian_omega(n_vars: int, k: int, seed: int) -> np.ndarray:
     z = np.where((e & np.uint64(1)) == 0, r * np.cos(2.0 * np.pi * u2), r * np.sin(2.0 * np.pi * u2))
     z = z.astype(np.float32).astype(np.float64)
     return z.reshape(k, n_vars).T.copy()
+
+
+# --------------------------------------------------------------------------
+# Upstream producers (scx-gpu/kernels/normalize_log1p.cu:17-140 dispatched by
+# gpu_apply_fused_ops, scx-gpu/src/gpu_preprocess.rs:340-391; the CPU
+# counterpart scx-engine fused_normalize_log1p forms value_f64 * factor, rounds
+# to f32 and takes ln_1p) and the column projection of ProjectedShardSource
+# (scx-accel/src/projected_source.rs:28-80 over scx_engine::project_csr)
+# --------------------------------------------------------------------------
+
+def normalize_log1p(csr: Csr, target_sum=1e4, log1p=True, row_factors=None) -> np.ndarray:
+    """New FP32 values: per row v * target_sum / rowsum (FP64 factor, result
+    rounded to f32; rows summing to zero untouched), then log1p, then the
+    explicit per-row factor."""
+    v = csr.data.astype(np.float64)
+    rows = csr.row_ids()
+    out = csr.data.astype(np.float32).copy()
+    if target_sum and target_sum > 0:
+        rs = np.bincount(rows, weights=v, minlength=csr.shape[0])
+        nz = rs[rows] != 0.0
+        scaled = (v * (target_sum / np.where(rs == 0.0, 1.0, rs))[rows]).astype(np.float32)
+        out = np.where(nz, scaled, out)
+        if log1p:
+            out = np.where(nz, np.log1p(out.astype(np.float64)).astype(np.float32), out)
+    elif log1p:
+        out = np.log1p(out.astype(np.float64)).astype(np.float32)
+    if row_factors is not None:
+        out = (out * np.asarray(row_factors, dtype=np.float32)[rows]).astype(np.float32)
+    return out
+
+
+def project_columns(csr: Csr, cols) -> Csr:
+    """Keep the sorted unique columns ``cols``; column cols[i] becomes i."""
+    cols = np.asarray(cols, dtype=np.int64)
+    cmap = np.full(csr.shape[1], -1, dtype=np.int64)
+    cmap[cols] = np.arange(len(cols))
+    new = cmap[csr.indices.astype(np.int64)]
+    keep = new >= 0
+    rows = csr.row_ids()[keep]
+    indptr = np.r_[0, np.cumsum(np.bincount(rows, minlength=csr.shape[0]))].astype(np.int64)
+    return Csr(indptr, new[keep].astype(np.int32), csr.data[keep], (csr.shape[0], len(cols)))
+
+
+# --------------------------------------------------------------------------
+# PFlog (v4) baseline-aware PCA (scx-accel/src/pflog.rs:122-193,
+# scx-accel/src/pca/cpu.rs:618-882)
+# --------------------------------------------------------------------------
+
+def pflog_prepare(csr: Csr, four_alpha: float):
+    """delta = log1p(four_alpha * x) at the stored entries (FP64, rounded to
+    f32 as the reference stores it) and b_i = -(1/D) sum_j delta_ij in FP64
+    (pflog_baseline_from_raw, pflog.rs:122-193)."""
+    x = csr.data.astype(np.float64)
+    if not np.all(np.isfinite(x)):
+        raise ValueError("PFlog input contains a non-finite value")
+    if np.any(x < 0):
+        raise ValueError("PFlog: negative count")
+    d = np.log1p(four_alpha * x)
+    base = -np.bincount(csr.row_ids(), weights=d, minlength=csr.shape[0]) / csr.shape[1]
+    return d.astype(np.float32), base
+
+
+def pflog_total_variance(col_sum_sq_delta, colmean_delta, baseline, n_obs: int, n_vars: int) -> float:
+    """Closed form of pflog_total_variance (cpu.rs:689-786)."""
+    s_dd = float(np.sum(col_sum_sq_delta))
+    b2 = float(np.sum(np.asarray(baseline) ** 2))
+    denom = max(n_obs - 1.0, 1.0)
+    if colmean_delta is None:
+        tss = s_dd - n_vars * b2
+    else:
+        mu = np.asarray(colmean_delta) + float(np.sum(baseline)) / max(n_obs, 1)
+        tss = s_dd - n_vars * b2 - n_obs * float(np.sum(mu * mu))
+    return max(tss / denom, 0.0)
+
+
+def pflog_pca(delta: Csr, baseline, n_components: int, n_oversamples: int, n_power_iterations: int,
+              zero_center: bool, omega, ordering: str = "gpu"):
+    """Randomized PCA of Z = delta + b 1^T with the offset products
+    streaming_spmm_forward_offset / streaming_spmm_transpose_offset
+    (cpu.rs:618-687) and the loop of pflog_pca_with_depth (cpu.rs:815-882);
+    explicit Omega, GPU step order by default (as randomized_pca)."""
+    n_obs, n_vars = delta.shape
+    validate_inputs(n_obs, n_vars, n_components)
+    k = effective_k(n_obs, n_vars, n_components, n_oversamples)
+    b = np.asarray(baseline, dtype=np.float64)
+    omega = np.asarray(omega, dtype=np.float64)
+    col_sums, col_sum_sq = col_sums_and_sum_sq(delta)
+    colmean = col_sums / n_obs if zero_center else None
+    means = colmean + b.mean() if zero_center else None
+
+    def fwd(m):  # (delta + b 1^T - 1 mu^T) m
+        return spmm_forward(delta, m, means) + np.outer(b, m.sum(axis=0))
+
+    def tr(q):  # (delta + b 1^T - 1 mu^T)^T q
+        return spmm_transpose(delta, q, means) + (b @ q)[None, :]
+
+    q = qr_thin_q(fwd(omega))
+    for _ in range(n_power_iterations):
+        z = tr(q)
+        if ordering == "gpu" or n_power_iterations > 2:
+            z = qr_thin_q(z)
+        q = qr_thin_q(fwd(z))
+    bm = tr(q)
+    total_var = pflog_total_variance(col_sum_sq, colmean, b, n_obs, n_vars)
+    res = build_pca_result(q, bm, n_components, n_obs, total_var)
+    res["mean"] = means
+    res["total_var"] = total_var
+    res["k"] = k
+    return res

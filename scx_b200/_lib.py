@@ -57,6 +57,10 @@ EXPORTED = (
     "scxpca_gaussian",
     "scxpca_synth_nb_csr",
     "scxpca_last_call_phases",
+    "scxpca_preprocess",
+    "scxpca_project_columns",
+    "scxpca_pflog_prepare",
+    "scxpca_pflog_pca",
 )
 
 STAGES = ("prepare", "forward", "transpose", "reduce", "gram", "apply", "small", "embed")
@@ -176,6 +180,11 @@ def load() -> C.CDLL:
         "scxpca_synth_nb_csr": (C.c_int32, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, C.c_double,
                                             C.c_double, P, P, P, C.POINTER(C.c_int64), *E]),
         "scxpca_last_call_phases": (C.c_int32, [P, C.c_int32, C.POINTER(C.c_double)]),
+        "scxpca_preprocess": (C.c_int32, [C.c_int32, C.POINTER(Csr), P, C.c_double, C.c_int32, P, P, *E]),
+        "scxpca_project_columns": (C.c_int32, [C.c_int32, C.POINTER(Csr), P, C.c_int64, P, P, P,
+                                               C.POINTER(C.c_int64), P, *E]),
+        "scxpca_pflog_prepare": (C.c_int32, [C.c_int32, C.POINTER(Csr), C.c_double, P, P, P, *E]),
+        "scxpca_pflog_pca": (C.c_int32, [C.POINTER(Csr), P, C.c_int32, C.POINTER(Params), C.POINTER(Result), *E]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

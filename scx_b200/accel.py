@@ -268,6 +268,113 @@ def randomized_pca(indptr, indices, values, shape, n_components: int = 50,
     return _finish(res, bufs, n_obs, n_vars, nc, zero_center, scale, k)
 
 
+def preprocess(indptr, indices, values, shape, target_sum: float | None = 1e4, log1p: bool = True,
+               row_factors=None, inplace: bool = False):
+    """normalize_total(target_sum) + log1p (+ an explicit per-row factor) of a
+    device CSR (CUDA torch tensors, float32 values) on the device
+    (scxpca_preprocess; gpu_apply_fused_ops in scx-gpu/src/gpu_preprocess.rs).
+    Returns the new values tensor (``values`` itself when ``inplace``)."""
+    import torch
+    lib = _lib.load()
+    csr, keep, mem, dev = _prepare_csr(indptr, indices, values, shape)
+    if mem != _lib.MEM_DEVICE:
+        raise ValueError("preprocess needs CUDA tensors")
+    vals = keep[2]
+    if vals.dtype != torch.float32:
+        raise ValueError("preprocess needs float32 values")
+    out = vals if inplace else torch.empty_like(vals)
+    rf = None
+    if row_factors is not None:
+        rf = row_factors.to(device=vals.device, dtype=torch.float32).contiguous()
+        if rf.numel() != int(shape[0]):
+            raise ValueError(f"row_factors must have n_obs = {int(shape[0])} entries")
+    err = _lib.errbuf()
+    st = lib.scxpca_preprocess(dev, C.byref(csr), _ptr(out), float(target_sum or 0.0), 1 if log1p else 0,
+                               _ptr(rf) or None, None, err, len(err))
+    _lib.check(st, err)
+    return out
+
+
+def project_columns(indptr, indices, values, shape, cols):
+    """Keep the columns ``cols`` (sorted, unique) of a device CSR on the device
+    (scxpca_project_columns; ProjectedShardSource in
+    scx-accel/src/projected_source.rs).  Returns (indptr, indices, values, shape)."""
+    import torch
+    lib = _lib.load()
+    csr, keep, mem, dev = _prepare_csr(indptr, indices, values, shape)
+    if mem != _lib.MEM_DEVICE:
+        raise ValueError("project_columns needs CUDA tensors")
+    c = np.ascontiguousarray(np.asarray(cols.cpu() if _is_torch(cols) else cols), dtype=np.int32)
+    d = keep[2].device
+    out_ip = torch.empty(int(shape[0]) + 1, dtype=torch.int64, device=d)
+    nnz = C.c_int64()
+    err = _lib.errbuf()
+    st = lib.scxpca_project_columns(dev, C.byref(csr), _ptr(c), len(c), _ptr(out_ip), None, None, C.byref(nnz),
+                                    None, err, len(err))
+    _lib.check(st, err)
+    out_ix = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=d)
+    out_vv = torch.empty(max(nnz.value, 1), dtype=torch.float32, device=d)
+    st = lib.scxpca_project_columns(dev, C.byref(csr), _ptr(c), len(c), _ptr(out_ip), _ptr(out_ix), _ptr(out_vv),
+                                    C.byref(nnz), None, err, len(err))
+    _lib.check(st, err)
+    return out_ip, out_ix[: nnz.value], out_vv[: nnz.value], (int(shape[0]), len(c))
+
+
+def pflog_prepare(indptr, indices, values, shape, alpha: float):
+    """PFlog (v4) representation of a raw-count device CSR: (delta values,
+    baseline) with delta = log1p(4 alpha x) and b_i = -(1 / n_vars) sum_j
+    delta_ij (scxpca_pflog_prepare; pflog_baseline_from_raw in
+    scx-accel/src/pflog.rs).  Returns CUDA tensors (float32 nnz, float64 n_obs)."""
+    import torch
+    lib = _lib.load()
+    csr, keep, mem, dev = _prepare_csr(indptr, indices, values, shape)
+    if mem != _lib.MEM_DEVICE:
+        raise ValueError("pflog_prepare needs CUDA tensors")
+    vals = keep[2]
+    delta = torch.empty_like(vals)
+    base = torch.empty(int(shape[0]), dtype=torch.float64, device=vals.device)
+    err = _lib.errbuf()
+    st = lib.scxpca_pflog_prepare(dev, C.byref(csr), 4.0 * float(alpha), _ptr(delta), _ptr(base), None, err,
+                                  len(err))
+    _lib.check(st, err)
+    return delta, base
+
+
+def pflog_pca(indptr, indices, values, shape, alpha: float, n_components: int = 50, n_oversamples: int = 10,
+              n_power_iterations: int = 2, zero_center: bool = True, seed: int = 0, omega=None,
+              qr_method: str = "householder", math_mode: str = "strict_fp32", device: int = 0,
+              device_embeddings: bool = False):
+    """Baseline-aware (PFlog v4) randomized PCA of raw counts on the GPU:
+    delta = log1p(4 alpha x) and the per-cell baseline on the device, then the
+    PCA of Z = delta + baseline 1^T without densifying it (scxpca_pflog_pca;
+    pflog_pca in scx-accel/src/pca/cpu.rs, which the reference runs on the
+    CPU).  ``values`` are raw counts (host numpy or CUDA torch, float32).
+    Returns (PcaResult, baseline as a CUDA float64 tensor)."""
+    import torch
+    lib = _lib.load()
+    if not (_is_torch(values) and values.is_cuda):
+        d = torch.device("cuda", int(device))
+        indptr = torch.as_tensor(np.ascontiguousarray(indptr, dtype=np.int64)).to(d)
+        indices = torch.as_tensor(np.ascontiguousarray(indices, dtype=np.int32)).to(d)
+        values = torch.as_tensor(np.ascontiguousarray(values, dtype=np.float32)).to(d)
+    delta, base = pflog_prepare(indptr, indices, values, shape, alpha)
+    csr, keep, mem, dev = _prepare_csr(indptr, indices, delta, shape)
+    n_obs, n_vars = int(shape[0]), int(shape[1])
+    p = _params(n_components, n_oversamples, n_power_iterations, zero_center, False, None, seed, qr_method,
+                math_mode, "default", dev)
+    k = min(int(n_components) + int(n_oversamples), n_vars, n_obs)
+    optr, omem, okeep = _prepare_omega(omega, n_vars, k)
+    p.omega = optr or None
+    p.omega_memory = omem
+    nc = int(n_components)
+    res, bufs = _alloc_outputs(n_obs, n_vars, max(nc, 0), device_embeddings, dev)
+    err = _lib.errbuf()
+    st = lib.scxpca_pflog_pca(C.byref(csr), _ptr(base), _lib.MEM_DEVICE, C.byref(p), C.byref(res), err, len(err))
+    _lib.check(st, err)
+    del keep, okeep
+    return _finish(res, bufs, n_obs, n_vars, nc, zero_center, False, k), base
+
+
 def last_call_phases() -> dict:
     """Phases of this thread's last one-shot call (scxpca_last_call_phases):
     device ms per phase (upload, validate, stats, transform, pack, buffers,

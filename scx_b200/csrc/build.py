@@ -33,6 +33,7 @@ SOURCES = [
     "kernels_adjoint.cu",
     "noalloc.cu",
     "kernels_strict.cu",
+    "kernels_preprocess.cu",
 ]
 EXTRA_SOURCES_OPTIONAL = ["kernels_tc.cu"]
 

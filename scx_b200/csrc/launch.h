@@ -202,6 +202,33 @@ cudaError_t launch_sddmm(int dtype, const int64_t* indptr, const int32_t* idx, c
                          const float* Y, int ldy, const float* S, int lds, const double* V, const double* A, int ldv,
                          int cs, const double* scale, int accumulate, float* grad, double* part, cudaStream_t st);
 
+// ---- upstream producers (kernels_preprocess.cu) ----
+// out = [log1p](x * target_sum / rowsum) [* row_factor[row]] per row; target_sum <= 0 skips the
+// normalisation; in may equal out.
+cudaError_t launch_normalize_log1p(const int64_t* indptr, const float* in, float* out, int64_t n,
+                                   double target_sum, int do_log1p, const float* row_factor, cudaStream_t st,
+                                   int num_sms);
+// Kept entries per row under col_map (new index or -1), then the compacted CSR.
+cudaError_t launch_project_count(const int64_t* indptr, const int32_t* idx, int64_t n, const int32_t* col_map,
+                                 int64_t* counts, cudaStream_t st, int num_sms);
+cudaError_t launch_project_fill(const int64_t* indptr, const int32_t* idx, const float* val, int64_t n,
+                                const int32_t* col_map, const int64_t* out_ptr, int32_t* out_idx, float* out_val,
+                                cudaStream_t st, int num_sms);
+
+// PFlog: delta = log1p(four_alpha x), baseline b_i = -sum_j delta_ij / d (FP64);
+// flags[0] negative count, flags[1] non-finite count.
+cudaError_t launch_pflog_prepare(const int64_t* indptr, const float* x, int64_t n, int64_t d, double four_alpha,
+                                 float* delta, double* baseline, int32_t* flags, cudaStream_t st, int num_sms);
+// Augmented CSR [delta | b] (column g = b_i, one extra entry per row) and
+// cross[i] = b_i * rowsum(delta_i).
+cudaError_t launch_pflog_augment(int dtype, const int64_t* indptr, const int32_t* idx, const void* val, int64_t n,
+                                 int32_t g, const double* baseline, int64_t* aptr, int32_t* aidx, void* aval,
+                                 double* cross, cudaStream_t st, int num_sms);
+// V[g] = sum_{j<g} V[j] (gene-major float, rows of ld).
+cudaError_t launch_aug_colsum(float* V, int32_t g, int ld, cudaStream_t st);
+// W[j] += W[g] (j < g), W[g] = 0 (gene-major FP64, rows of ld).
+cudaError_t launch_aug_fold(double* W, int32_t g, int ld, cudaStream_t st, int num_sms);
+
 // ---- synthetic generator (synth.cu) ----
 cudaError_t launch_synth_count(uint64_t seed, int64_t n, int64_t g, double loc, double disp,
                                const float* mu_g, int64_t* row_nnz, float* rowsum,

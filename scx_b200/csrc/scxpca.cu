@@ -315,6 +315,12 @@ struct scxpca_plan {
   DevBuf bw_Vk, bw_H, bw_A, bw_X, bw_R, bw_P, bw_Ap, bw_Proj, bw_T, bw_M, bw_vec, bw_colD, bw_sumDP, bw_part,
       bw_cpart;
 
+  // baseline-aware (PFlog) plan: the working matrix is [delta | b] with the
+  // baseline as its last column; g_user = the caller's gene count (g - 1 for
+  // PFlog, g otherwise)
+  bool pflog = false;
+  int64_t g_user = 0;
+
   // opt-in stage timing
   bool profiling = false;
   std::vector<cudaEvent_t> events;
@@ -488,8 +494,16 @@ void build_tile_csc(scxpca_plan* pl) {
   CK(cudaStreamSynchronize(st));  // the host vectors above go out of scope
 }
 
-scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const AffineSpec* aff = nullptr) {
-  validate_params(x, p);
+// The baseline of a PFlog plan: the working matrix's last column holds b.
+struct PflogSpec {
+  double b_mean;  // mean of the FP64 baseline (total variance)
+  double b2;      // sum_i b_i^2
+  double cross;   // sum_i b_i * (row sum of delta_i)
+};
+
+scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const AffineSpec* aff = nullptr,
+                         const PflogSpec* pf = nullptr) {
+  if (!pf) validate_params(x, p);
   auto pl = new scxpca_plan();
   try {
     pl->device = p->device_ordinal;
@@ -497,8 +511,10 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
     pl->params = *p;
     pl->n = x->n_obs;
     pl->g = x->n_vars;
+    pl->pflog = pf != nullptr;
+    pl->g_user = pf ? x->n_vars - 1 : x->n_vars;
     pl->nnz = x->nnz;
-    pl->k = std::min({p->n_components + p->n_oversamples, x->n_vars, x->n_obs});
+    pl->k = std::min({p->n_components + p->n_oversamples, pl->g_user, x->n_obs});
     pl->ld = padded_k(pl->k);
     pl->nc = p->n_components;
     pl->in_dtype = x->values_dtype;
@@ -687,6 +703,34 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       }
       upload(pl->d_mu, mu_w, st);
       pl->total_var = t / std::max<double>((double)n - 1.0, 1.0);
+    } else if (pf) {
+      // Z = delta + b 1^T: column means colmean(delta)_j + mean(b) (cpu.rs:836-842);
+      // the baseline column itself is not centred.  Total variance in closed
+      // form: sum_ij (delta_ij + b_i)^2 = S_dd + 2 sum_i b_i r_i + D sum_i b_i^2
+      // (r_i the row sums of delta), minus n sum_j mu_j^2 when centred; with
+      // the PFlog baseline b_i = -r_i / D this is pflog_total_variance's
+      // S_dd - D B2 - n sum mu^2 (cpu.rs:689-786).
+      // The centring takes the mean baseline from the stored baseline column
+      // (the values the products see, in the compute type), so it is
+      // consistent with the products; the total variance uses the FP64
+      // baseline.
+      const int64_t gu = pl->g_user;
+      const double b_mean = pl->col_sum[gu] / (double)n;
+      std::vector<double> mu_w(g, 0.0);
+      double s_dd = 0.0, m2 = 0.0;
+      for (int64_t j = 0; j < gu; ++j) {
+        s_dd += pl->col_sq[j];
+        if (pl->centered) {
+          mu_w[j] = pl->col_sum[j] / (double)n + b_mean;
+          const double mu64 = pl->col_sum[j] / (double)n + pf->b_mean;
+          m2 += mu64 * mu64;
+        }
+      }
+      for (int64_t j = 0; j < gu; ++j) pl->mean_x[j] = pl->col_sum[j] / (double)n + b_mean;
+      pl->mean_x.resize(gu);
+      upload(pl->d_mu, mu_w, st);
+      const double tss = s_dd + 2.0 * pf->cross + (double)gu * pf->b2 - (double)n * m2;
+      pl->total_var = std::max(tss, 0.0) / std::max<double>((double)n - 1.0, 1.0);
     } else {
       std::vector<double> mu_w(g, 0.0);
       if (pl->centered)
@@ -949,19 +993,20 @@ void check_tc_error(scxpca_plan* pl) {
 
 void load_omega(scxpca_plan* pl, const scxpca_params* p) {
   cudaStream_t st = pl->stream;
-  const int64_t g = pl->g, k = pl->k, ld = pl->ld;
+  const int64_t g = pl->g, gu = pl->g_user, k = pl->k, ld = pl->ld;
   CK(cudaMemsetAsync(pl->V.p, 0, sizeof(float) * g * ld, st));
   if (p->omega) {
     const float* src = p->omega;
     if (p->omega_memory != SCXPCA_MEM_DEVICE) {
-      pl->omega_stage.alloc(sizeof(float) * g * k);
-      CK(cudaMemcpyAsync(pl->omega_stage.p, p->omega, sizeof(float) * g * k, cudaMemcpyHostToDevice, st));
+      pl->omega_stage.alloc(sizeof(float) * gu * k);
+      CK(cudaMemcpyAsync(pl->omega_stage.p, p->omega, sizeof(float) * gu * k, cudaMemcpyHostToDevice, st));
       src = pl->omega_stage.as<float>();
     }
-    CK(launch_colmajor_to_padded(src, g, k, (int)ld, pl->V.as<float>(), st, pl->num_sms));
+    CK(launch_colmajor_to_padded(src, gu, k, (int)ld, pl->V.as<float>(), st, pl->num_sms));
   } else {
-    CK(launch_gaussian(p->seed, g, k, pl->V.as<float>(), (int)ld, st, pl->num_sms));
+    CK(launch_gaussian(p->seed, gu, k, pl->V.as<float>(), (int)ld, st, pl->num_sms));
   }
+  if (pl->pflog) CK(launch_aug_colsum(pl->V.as<float>(), (int32_t)gu, (int)ld, st));
   CK(launch_mean_prefactor(pl->V.as<float>(), g, (int)ld, pl->centered ? pl->d_mu.as<double>() : nullptr,
                            pl->mc.as<float>(), st));
 }
@@ -1004,10 +1049,12 @@ void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
     // Z = (X - mu)^T Q = (X^T Y - mu (1^T Y)) R^{-1}
     rmatmat_raw(pl, pl->Y.as<float>(), 0);
     s = stage_begin(pl);
+    if (pl->pflog) CK(launch_aug_fold(pl->W.as<double>(), (int32_t)pl->g_user, ld, st, pl->num_sms));
     CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->Rinv.as<double>(),
                            pl->Z.as<double>(), st));
     small_qr(pl, pl->Z.as<double>(), shift);
     CK(launch_round_v(pl->Z.as<double>(), pl->g, ld, mu, pl->V.as<float>(), pl->mc.as<float>(), st));
+    if (pl->pflog) CK(launch_aug_colsum(pl->V.as<float>(), (int32_t)pl->g_user, ld, st));
     stage_end(pl, SCXPCA_STAGE_SMALL, s);
     forward(pl, !image_only || it + 1 == p.n_power_iterations);
     tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
@@ -1041,6 +1088,7 @@ void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
   // B = (X - mu)^T Q R2^{-1}
   rmatmat_raw(pl, pl->Y.as<float>(), 0);
   s = stage_begin(pl);
+  if (pl->pflog) CK(launch_aug_fold(pl->W.as<double>(), (int32_t)pl->g_user, ld, st, pl->num_sms));
   CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->R2inv.as<double>(),
                          pl->Z.as<double>(), st));
   // SVD of B through the FP64 eigendecomposition of B^T B.
@@ -1073,10 +1121,10 @@ void finish_result(scxpca_plan* pl, const int* hstatus, const double* sigma, scx
     if (out->singular_values) out->singular_values[c] = sigma[c];
   }
   if (out->mean) {
-    for (int64_t j = 0; j < pl->g; ++j) out->mean[j] = pl->mean_x[j];
+    for (int64_t j = 0; j < pl->g_user; ++j) out->mean[j] = pl->mean_x[j];
   }
   if (out->std) {
-    for (int64_t j = 0; j < pl->g; ++j) out->std[j] = pl->std_x.empty() ? 1.0 : pl->std_x[j];
+    for (int64_t j = 0; j < pl->g_user; ++j) out->std[j] = pl->std_x.empty() ? 1.0 : pl->std_x[j];
   }
   out->resident_csr = 1;
   out->total_var_recomputed = pl->total_var_recomputed ? 1 : 0;
@@ -1109,9 +1157,9 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   std::vector<double> sigma(pl->k);
   CK(cudaMemcpyAsync(hstatus, pl->status.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(sigma.data(), pl->sigma.p, sizeof(double) * pl->k, cudaMemcpyDeviceToHost, st));
-  if (out->components)
-    CK(cudaMemcpyAsync(out->components, pl->comps.p, sizeof(float) * pl->nc * pl->g,
-                       cudaMemcpyDeviceToHost, st));
+  if (out->components)  // the first g_user loadings of every component row
+    CK(cudaMemcpy2DAsync(out->components, sizeof(float) * pl->g_user, pl->comps.p, sizeof(float) * pl->g,
+                         sizeof(float) * pl->g_user, pl->nc, cudaMemcpyDeviceToHost, st));
   phase_mark(SCXPCA_PHASE_DOWNLOAD, st);
   CK(cudaStreamSynchronize(st));
   collect_stages(pl);
@@ -1898,6 +1946,215 @@ int32_t scxpca_gaussian(int32_t device_ordinal, uint64_t seed, int64_t n_rows, i
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal));
     CK(launch_gaussian(seed, n_rows, n_cols, out, 0, nullptr, sms));
     CK(cudaStreamSynchronize(nullptr));
+  });
+}
+
+// Shared argument checks of the device-CSR producers: a device CSR with FP32
+// values whose indptr is monotone within [0, nnz] and whose column indices
+// lie in [0, n_vars) (validated on the device before any kernel indexes with
+// them).
+void check_device_csr_f32(const scxpca_csr* x, cudaStream_t st, int sms) {
+  if (!x) fail(SCXPCA_INVALID_ARGUMENT, "null csr");
+  if (x->memory != SCXPCA_MEM_DEVICE) fail(SCXPCA_INVALID_ARGUMENT, "a device CSR (memory = DEVICE) is required");
+  if (x->values_dtype != SCXPCA_F32) fail(SCXPCA_INVALID_ARGUMENT, "values must be float32");
+  if (x->n_obs < 0 || x->n_vars <= 0 || x->nnz < 0) fail(SCXPCA_INVALID_ARGUMENT, "bad matrix dimensions");
+  if (x->n_vars > INT32_MAX) fail(SCXPCA_INVALID_ARGUMENT, "n_vars exceeds int32 index range");
+  if (!x->indptr || (x->nnz > 0 && (!x->indices || !x->values))) fail(SCXPCA_INVALID_ARGUMENT, "null CSR arrays");
+  DevBuf flags;
+  flags.alloc(16);
+  CK(cudaMemsetAsync(flags.p, 0, 16, st));
+  CK(launch_validate_csr(SCXPCA_F32, x->indptr, x->indices, x->values, x->n_obs, x->n_vars, x->nnz,
+                         flags.as<int32_t>(), st, sms));
+  int32_t hf[4];
+  CK(cudaMemcpyAsync(hf, flags.p, 16, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (hf[0]) fail(SCXPCA_INVALID_CSR, "invalid CSR: indptr is not monotone within [0, nnz]");
+  if (hf[1]) fail(SCXPCA_INVALID_CSR, "invalid CSR: column index out of range [0, n_vars)");
+}
+
+int32_t scxpca_preprocess(int32_t device_ordinal, const scxpca_csr* x, float* values_out, double target_sum,
+                          int32_t log1p, const float* row_factors, void* stream, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!values_out) fail(SCXPCA_INVALID_ARGUMENT, "null values_out");
+    if (!std::isfinite(target_sum)) fail(SCXPCA_INVALID_ARGUMENT, "target_sum must be finite");
+    DeviceGuard dg(device_ordinal);
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    PoolScope pool_scope(device_ordinal, st);
+    check_device_csr_f32(x, st, sms);
+    CK(launch_normalize_log1p(x->indptr, static_cast<const float*>(x->values), values_out, x->n_obs, target_sum,
+                              log1p ? 1 : 0, row_factors, st, sms));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t scxpca_project_columns(int32_t device_ordinal, const scxpca_csr* x, const int32_t* cols, int64_t n_cols,
+                               int64_t* out_indptr, int32_t* out_indices, float* out_values, int64_t* nnz_out,
+                               void* stream, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!cols || n_cols <= 0 || !out_indptr || !nnz_out) fail(SCXPCA_INVALID_ARGUMENT, "bad projection arguments");
+    if ((out_indices == nullptr) != (out_values == nullptr))
+      fail(SCXPCA_INVALID_ARGUMENT, "out_indices and out_values must both be given or both be NULL");
+    if (!x) fail(SCXPCA_INVALID_ARGUMENT, "null csr");
+    // the kept columns: sorted, unique, in range (ProjectedShardSource's contract)
+    std::vector<int32_t> col_map(x->n_vars > 0 ? x->n_vars : 0, -1);
+    for (int64_t i = 0; i < n_cols; ++i) {
+      if (cols[i] < 0 || cols[i] >= x->n_vars) fail(SCXPCA_INVALID_ARGUMENT, "column index out of range");
+      if (i > 0 && cols[i] <= cols[i - 1]) fail(SCXPCA_INVALID_ARGUMENT, "cols must be sorted and unique");
+      col_map[cols[i]] = (int32_t)i;
+    }
+    DeviceGuard dg(device_ordinal);
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    PoolScope pool_scope(device_ordinal, st);
+    check_device_csr_f32(x, st, sms);
+    const int64_t n = x->n_obs;
+    DevBuf d_map, counts;
+    d_map.alloc(sizeof(int32_t) * col_map.size());
+    CK(cudaMemcpyAsync(d_map.p, col_map.data(), sizeof(int32_t) * col_map.size(), cudaMemcpyHostToDevice, st));
+    counts.alloc(sizeof(int64_t) * std::max<int64_t>(n, 1));
+    CK(launch_project_count(x->indptr, x->indices, n, d_map.as<int32_t>(), counts.as<int64_t>(), st, sms));
+    CK(launch_exclusive_scan_i64(counts.as<int64_t>(), n, out_indptr, st));
+    CK(cudaMemcpyAsync(nnz_out, out_indptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (out_indices)
+      CK(launch_project_fill(x->indptr, x->indices, static_cast<const float*>(x->values), n, d_map.as<int32_t>(),
+                             out_indptr, out_indices, out_values, st, sms));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t scxpca_pflog_prepare(int32_t device_ordinal, const scxpca_csr* x, double four_alpha, float* delta_out,
+                             double* baseline_out, void* stream, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!delta_out || !baseline_out) fail(SCXPCA_INVALID_ARGUMENT, "null delta or baseline output");
+    if (!(four_alpha > 0.0) || !std::isfinite(four_alpha))
+      fail(SCXPCA_INVALID_ARGUMENT, "PFlog four_alpha (= 4 alpha) must be positive and finite, got " +
+                                        std::to_string(four_alpha));
+    DeviceGuard dg(device_ordinal);
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    PoolScope pool_scope(device_ordinal, st);
+    check_device_csr_f32(x, st, sms);
+    DevBuf flags;
+    flags.alloc(16);
+    CK(cudaMemsetAsync(flags.p, 0, 16, st));
+    CK(launch_pflog_prepare(x->indptr, static_cast<const float*>(x->values), x->n_obs, x->n_vars, four_alpha,
+                            delta_out, baseline_out, flags.as<int32_t>(), st, sms));
+    int32_t hf[4];
+    CK(cudaMemcpyAsync(hf, flags.p, 16, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hf[1])
+      fail(SCXPCA_INVALID_ARGUMENT, "PFlog input contains a non-finite value; PFlog requires finite raw counts");
+    if (hf[0]) fail(SCXPCA_INVALID_ARGUMENT, "PFlog: negative count; counts must be non-negative");
+  });
+}
+
+int32_t scxpca_pflog_pca(const scxpca_csr* delta, const double* baseline, int32_t baseline_memory,
+                         const scxpca_params* params, scxpca_result* out, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!params) fail(SCXPCA_INVALID_ARGUMENT, "null params");
+    if (!out || !out->embeddings) fail(SCXPCA_INVALID_ARGUMENT, "null embeddings output");
+    if (!baseline) fail(SCXPCA_INVALID_ARGUMENT, "null baseline");
+    validate_params(delta, params);
+    if (params->scale) fail(SCXPCA_UNSUPPORTED, "PFlog PCA does not take per-gene scaling");
+    if (delta->n_vars + 1 > INT32_MAX) fail(SCXPCA_INVALID_ARGUMENT, "n_vars exceeds int32 index range");
+    DeviceGuard dg(params->device_ordinal);
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, params->device_ordinal));
+    scxpca_params p = *params;
+    p.clip_max = 0.0;
+    cudaStream_t own = nullptr;
+    if (!p.stream) {
+      CK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+      p.stream = own;
+    }
+    struct StreamGuard {
+      cudaStream_t s;
+      ~StreamGuard() {
+        if (s) {
+          cudaStreamSynchronize(s);
+          cudaStreamDestroy(s);
+        }
+      }
+    } own_guard{own};
+    cudaStream_t st = static_cast<cudaStream_t>(p.stream);
+    PoolScope pool_scope(params->device_ordinal, st);
+    const int64_t n = delta->n_obs, g = delta->n_vars, nnz = delta->nnz;
+    const size_t vs = dtype_size(delta->values_dtype);
+    // the delta CSR and the baseline on the device
+    DevBuf d_ip, d_ix, d_vv, d_b, a_ip, a_ix, a_vv, d_cross;
+    const int64_t* ip = delta->indptr;
+    const int32_t* ix = delta->indices;
+    const void* vv = delta->values;
+    if (delta->memory != SCXPCA_MEM_DEVICE) {
+      d_ip.alloc(sizeof(int64_t) * (n + 1));
+      d_ix.alloc(sizeof(int32_t) * std::max<int64_t>(nnz, 1));
+      d_vv.alloc(vs * std::max<int64_t>(nnz, 1));
+      CK(cudaMemcpyAsync(d_ip.p, ip, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
+      if (nnz) {
+        CK(cudaMemcpyAsync(d_ix.p, ix, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_vv.p, vv, vs * nnz, cudaMemcpyHostToDevice, st));
+      }
+      ip = d_ip.as<int64_t>();
+      ix = d_ix.as<int32_t>();
+      vv = d_vv.p;
+    }
+    const double* b = baseline;
+    std::vector<double> hb(n);
+    if (baseline_memory == SCXPCA_MEM_DEVICE) {
+      CK(cudaMemcpyAsync(hb.data(), baseline, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    } else {
+      memcpy(hb.data(), baseline, sizeof(double) * n);
+      d_b.alloc(sizeof(double) * n);
+      CK(cudaMemcpyAsync(d_b.p, baseline, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+      b = d_b.as<double>();
+    }
+    // validate the delta CSR before the augmentation kernel indexes with it
+    {
+      DevBuf flags;
+      flags.alloc(16);
+      CK(cudaMemsetAsync(flags.p, 0, 16, st));
+      CK(launch_validate_csr(delta->values_dtype, ip, ix, vv, n, g, nnz, flags.as<int32_t>(), st, sms));
+      int32_t hf[4];
+      CK(cudaMemcpyAsync(hf, flags.p, 16, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (hf[0]) fail(SCXPCA_INVALID_CSR, "invalid CSR: indptr is not monotone within [0, nnz]");
+      if (hf[1]) fail(SCXPCA_INVALID_CSR, "invalid CSR: column index out of range [0, n_vars)");
+      if (hf[3]) fail(SCXPCA_INVALID_CSR, "invalid CSR: non-finite value");
+    }
+    for (int64_t i = 0; i < n; ++i)
+      if (!std::isfinite(hb[i])) fail(SCXPCA_INVALID_ARGUMENT, "baseline must be finite (cell " + std::to_string(i) + ")");
+    // the augmented matrix [delta | b]
+    a_ip.alloc(sizeof(int64_t) * (n + 1));
+    a_ix.alloc(sizeof(int32_t) * (nnz + n));
+    a_vv.alloc(vs * (nnz + n));
+    d_cross.alloc(sizeof(double) * n);
+    CK(launch_pflog_augment(delta->values_dtype, ip, ix, vv, n, (int32_t)g, b, a_ip.as<int64_t>(),
+                            a_ix.as<int32_t>(), a_vv.p, d_cross.as<double>(), st, sms));
+    std::vector<double> hc(n);
+    CK(cudaMemcpyAsync(hc.data(), d_cross.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    PflogSpec spec{0.0, 0.0, 0.0};
+    for (int64_t i = 0; i < n; ++i) {
+      spec.b_mean += hb[i];
+      spec.b2 += hb[i] * hb[i];
+      spec.cross += hc[i];
+    }
+    spec.b_mean /= (double)std::max<int64_t>(n, 1);
+    scxpca_csr xa{n, g + 1, nnz + n, a_ip.as<int64_t>(), a_ix.as<int32_t>(), a_vv.p, delta->values_dtype,
+                  SCXPCA_MEM_DEVICE};
+    scxpca_plan* pl = create_plan(&xa, &p, nullptr, &spec);
+    try {
+      run_plan(pl, nullptr, out);
+    } catch (...) {
+      scxpca_plan_destroy(pl);
+      throw;
+    }
+    scxpca_plan_destroy(pl);
   });
 }
 

@@ -280,3 +280,27 @@ def test_cpp_restatement_matches_numpy_oracle():
                             clip_max=clip, threads=4)
         np.testing.assert_allclose(got["singular_values"], ref["singular_values"], rtol=1e-9)
         assert rpca.principal_angles(got["components"].T, ref["components"].T).max() < 1e-6
+
+
+def test_pflog_oracle_equals_dense_z():
+    """The PFlog restatement's offset products are the products with the dense
+    Z = delta + b 1^T, its closed-form total variance is the dense variance, and
+    its PCA is the dense PCA of Z at k = n_vars (cpu.rs:618-786)."""
+    rng = np.random.default_rng(4)
+    n, g = 300, 40
+    counts = rng.negative_binomial(3, 0.5, size=(n, g)).astype(np.float32) * (rng.random((n, g)) < 0.3)
+    rr, cc = np.nonzero(counts)
+    ip = np.r_[0, np.cumsum(np.bincount(rr, minlength=n))]
+    raw = rpca.Csr(ip, cc, counts[rr, cc], (n, g))
+    delta_v, base = rpca.pflog_prepare(raw, 4 * 0.3)
+    delta = raw.with_values(delta_v)
+    z = delta.to_dense() + base[:, None]
+    # the baseline is minus the mean of each row of delta
+    np.testing.assert_allclose(z.sum(axis=1), 0.0, atol=1e-6)
+    om = rng.standard_normal((g, g))
+    res = rpca.pflog_pca(delta, base, 10, g - 10, 2, True, om)
+    ex = rpca.dense_pca(z, 10)
+    np.testing.assert_allclose(res["singular_values"], ex["singular_values"], rtol=1e-8)
+    zc = z - z.mean(axis=0)
+    np.testing.assert_allclose(res["total_var"], (zc ** 2).sum() / (n - 1), rtol=1e-6)
+    np.testing.assert_allclose(res["mean"], z.mean(axis=0), rtol=1e-10, atol=1e-12)
