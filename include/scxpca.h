@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define SCXPCA_ABI_VERSION 1
+#define SCXPCA_ABI_VERSION 2
 
 /* Status codes.  They mirror the GpuError classes of scx-gpu/src/error.rs:
  * ShapeMismatch -> INVALID_ARGUMENT, OutOfMemory -> OUT_OF_MEMORY,
@@ -105,6 +105,16 @@ typedef struct {
   int32_t device_ordinal;
   int32_t reserved0;
   void* stream;           /* cudaStream_t; NULL = a stream owned by the plan */
+  int64_t device_budget;  /* bytes of device memory a plan of a HOST matrix may
+                             hold (0 = all free memory).  When the resident plan
+                             would not fit, the matrix stays in host memory and
+                             every product streams it in row shards
+                             (result.resident_csr = 0), as the reference's
+                             StreamingPcaOperator does
+                             (scx-gpu/src/linear_operator.rs:61-288).  The
+                             environment variable SCXPCA_RESIDENT=0 forces
+                             streaming (SCX_GPU_PCA_RESIDENT=0 in the
+                             reference, gpu_pca_resident.rs:56-73). */
 } scxpca_params;
 
 /* Outputs, caller-allocated.  Replaces GpuPcaResult (gpu_pca.rs:76-98) and
@@ -121,12 +131,14 @@ typedef struct {
   double* mean;                 /* n_vars: column means of the input matrix */
   double* std;                  /* n_vars: per-gene std used for scaling */
   int32_t embeddings_memory;    /* scxpca_memory */
-  int32_t resident_csr;         /* out: 1, the matrix was resident on device */
+  int32_t resident_csr;         /* out: 1 when the matrix was resident on the device,
+                                   0 when it was streamed from host memory */
   int32_t total_var_recomputed; /* out: 1 when the cancellation guard fired */
   int32_t shifted_cholesky;     /* out: number of shifted Gram factorisations */
   double total_var;             /* out: total variance used for the ratios */
   int32_t eig_sweeps;           /* out: Jacobi sweeps of the k x k eigensolver */
-  int32_t reserved1;
+  int32_t n_shards;             /* out: row shards a streamed matrix was taken in
+                                   (0 when resident) */
 } scxpca_result;
 
 typedef struct scxpca_plan scxpca_plan;

@@ -102,6 +102,7 @@ class Params(C.Structure):
         ("device_ordinal", C.c_int32),
         ("reserved0", C.c_int32),
         ("stream", C.c_void_p),
+        ("device_budget", C.c_int64),
     ]
 
 
@@ -120,7 +121,7 @@ class Result(C.Structure):
         ("shifted_cholesky", C.c_int32),
         ("total_var", C.c_double),
         ("eig_sweeps", C.c_int32),
-        ("reserved1", C.c_int32),
+        ("n_shards", C.c_int32),
     ]
 
 

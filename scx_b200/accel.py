@@ -48,6 +48,7 @@ class PcaResult:
     shifted_cholesky: int = 0
     eig_sweeps: int = 0
     resident_csr: bool = True
+    n_shards: int = 0
     k: int = 0
     extra: dict = field(default_factory=dict)
 
@@ -219,7 +220,8 @@ def _finish(res, bufs, n_obs, n_vars, nc, zero_center, scale, k):
         singular_values=sv, mean=mean if zero_center or scale else None,
         std=std if scale else None, n_components=nc, n_obs=n_obs, n_vars=n_vars,
         total_var=float(res.total_var), total_var_recomputed=bool(res.total_var_recomputed),
-        shifted_cholesky=int(res.shifted_cholesky), resident_csr=bool(res.resident_csr), k=k,
+        shifted_cholesky=int(res.shifted_cholesky), resident_csr=bool(res.resident_csr),
+        n_shards=int(res.n_shards), k=k,
         eig_sweeps=int(res.eig_sweeps))
 
 
@@ -233,13 +235,17 @@ def randomized_pca(indptr, indices, values, shape, n_components: int = 50,
                    seed: int = 0, omega=None, qr_method: str = "householder",
                    math_mode: str = "strict_fp32", spmm_policy: str = "default",
                    device: int = 0, device_embeddings: bool = False,
-                   embeddings_out=None) -> PcaResult:
+                   embeddings_out=None, device_budget: int | None = None) -> PcaResult:
     """One-shot randomized PCA of a CSR matrix (host numpy or CUDA torch arrays).
 
     Same contract as ``scx_gpu::gpu_randomized_pca`` (scx-gpu/src/gpu_pca.rs:706-763)
     with an optional explicit ``omega`` (n_vars x k) and per-gene scaling.
     ``embeddings_out`` may be a preallocated (n_obs, n_components) float32
     buffer: a numpy array (e.g. pinned host memory) or a CUDA torch tensor.
+    ``device_budget`` (bytes) caps the device memory of a host matrix's plan:
+    a matrix whose resident plan does not fit is streamed from host memory in
+    row shards (``resident_csr`` False), like the reference's streaming
+    operator.
     """
     lib = _lib.load()
     csr, keep, mem, dev = _prepare_csr(indptr, indices, values, shape)
@@ -248,6 +254,7 @@ def randomized_pca(indptr, indices, values, shape, n_components: int = 50,
     n_obs, n_vars = int(shape[0]), int(shape[1])
     p = _params(n_components, n_oversamples, n_power_iterations, zero_center, scale, clip_max,
                 seed, qr_method, math_mode, spmm_policy, device)
+    p.device_budget = int(device_budget or 0)
     k = min(int(n_components) + int(n_oversamples), n_vars, n_obs)
     optr, omem, okeep = _prepare_omega(omega, n_vars, k)
     p.omega = optr or None
@@ -400,7 +407,7 @@ class Plan:
                  scale: bool = False, clip_max: float | None = None, seed: int = 0,
                  qr_method: str = "householder", math_mode: str = "strict_fp32",
                  spmm_policy: str = "default", device: int = 0, stream: int | None = None,
-                 center=None, gene_scale=None):
+                 center=None, gene_scale=None, device_budget: int | None = None):
         """``stream`` is a raw ``cudaStream_t`` handle (e.g. ``torch.cuda.Stream().cuda_stream``)
         every kernel of this plan is ordered on; None lets the plan own a stream.
 
@@ -421,7 +428,10 @@ class Plan:
                                scale, clip_max, seed, qr_method, math_mode, spmm_policy, device)
         if stream:
             self._params.stream = int(stream)
-        self._keep = keep if mem == _lib.MEM_DEVICE else None  # borrowed device CSR must live
+        self._params.device_budget = int(device_budget or 0)
+        # a borrowed device CSR must live as long as the plan, and so must a
+        # host CSR that the plan streams from
+        self._keep = keep
         self.nnz = int(csr.nnz)
         handle = C.c_void_p()
         err = _lib.errbuf()

@@ -276,4 +276,15 @@ cudaError_t launch_aug_fold(double* W, int32_t g, int ld, cudaStream_t st, int n
   return cudaGetLastError();
 }
 
+__global__ void k_rebase_indptr(int64_t* __restrict__ indptr, int64_t n, int64_t base) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x)
+    indptr[i] -= base;
+}
+
+cudaError_t launch_rebase_indptr(int64_t* indptr, int64_t n, int64_t base, cudaStream_t st, int num_sms) {
+  k_rebase_indptr<<<grid_for(n + 1, 256, num_sms, 4), 256, 0, st>>>(indptr, n, base);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
 }  // namespace scx

@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(512) k_spmm_t(const int64_t* __restrict__ indp
 template <typename ValT>
 static cudaError_t col_stats_t(const int32_t* idx, const void* val, int64_t nnz, int32_t g,
                                double* partial, int nparts, double* out, cudaStream_t st,
-                               int num_sms) {
+                               int num_sms, int accumulate) {
   const ValT* v = static_cast<const ValT*>(val);
   const int32_t pass_genes = std::min<int32_t>(g, kStatsPassGenes);
   const size_t smem = (size_t)2 * pass_genes * sizeof(double) + (size_t)kStatsWindow * 8;
@@ -347,18 +347,18 @@ static cudaError_t col_stats_t(const int32_t* idx, const void* val, int64_t nnz,
     if (e != cudaSuccess) return e;
   }
   k_col_stats<ValT><<<nparts, kStatsWarps * 32, smem, st>>>(idx, v, nnz, g, pass_genes, partial);
-  k_reduce_rows<double><<<grid_for(2 * g, 256, num_sms), 256, 0, st>>>(partial, nparts, 2 * g, out, 0);
+  k_reduce_rows<double><<<grid_for(2 * g, 256, num_sms), 256, 0, st>>>(partial, nparts, 2 * g, out, accumulate);
   note_launches(2);
   return cudaGetLastError();
 }
 
 cudaError_t launch_col_stats(int dtype, const int32_t* idx, const void* val, int64_t nnz,
                              int32_t g, double* partial, int nparts, double* out,
-                             cudaStream_t st, int num_sms) {
+                             cudaStream_t st, int num_sms, int accumulate) {
   switch (dtype) {
-    case 0: return col_stats_t<float>(idx, val, nnz, g, partial, nparts, out, st, num_sms);
-    case 1: return col_stats_t<__nv_bfloat16>(idx, val, nnz, g, partial, nparts, out, st, num_sms);
-    default: return col_stats_t<__half>(idx, val, nnz, g, partial, nparts, out, st, num_sms);
+    case 0: return col_stats_t<float>(idx, val, nnz, g, partial, nparts, out, st, num_sms, accumulate);
+    case 1: return col_stats_t<__nv_bfloat16>(idx, val, nnz, g, partial, nparts, out, st, num_sms, accumulate);
+    default: return col_stats_t<__half>(idx, val, nnz, g, partial, nparts, out, st, num_sms, accumulate);
   }
 }
 

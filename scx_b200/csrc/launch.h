@@ -20,9 +20,11 @@ constexpr size_t kStatsSmemMax = 200 * 1024;  // per-block FP64 gene accumulator
 constexpr int kTransposeGeneBlock = 256;       // genes per block, CUDA-core transposed product
 
 // ---- sparse side (kernels_sparse.cu) ----
+// out = [sum x (g) | sum x^2 (g)] in FP64, fixed order; accumulate != 0 adds
+// to out instead of overwriting it (a matrix taken in row shards).
 cudaError_t launch_col_stats(int dtype, const int32_t* idx, const void* val, int64_t nnz,
                              int32_t g, double* partial, int nparts, double* out,
-                             cudaStream_t st, int num_sms);
+                             cudaStream_t st, int num_sms, int accumulate = 0);
 cudaError_t launch_transform_values(int in_dtype, int out_dtype, const int32_t* idx,
                                     const void* in, void* out, int64_t nnz, int mode,
                                     const double* mu, const double* inv_std,
@@ -228,6 +230,9 @@ cudaError_t launch_pflog_augment(int dtype, const int64_t* indptr, const int32_t
 cudaError_t launch_aug_colsum(float* V, int32_t g, int ld, cudaStream_t st);
 // W[j] += W[g] (j < g), W[g] = 0 (gene-major FP64, rows of ld).
 cudaError_t launch_aug_fold(double* W, int32_t g, int ld, cudaStream_t st, int num_sms);
+
+// indptr[i] -= base for i <= n (a row shard's pointers made relative to its first entry).
+cudaError_t launch_rebase_indptr(int64_t* indptr, int64_t n, int64_t base, cudaStream_t st, int num_sms);
 
 // ---- synthetic generator (synth.cu) ----
 cudaError_t launch_synth_count(uint64_t seed, int64_t n, int64_t g, double loc, double disp,

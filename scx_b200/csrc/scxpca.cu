@@ -315,6 +315,32 @@ struct scxpca_plan {
   DevBuf bw_Vk, bw_H, bw_A, bw_X, bw_R, bw_P, bw_Ap, bw_Proj, bw_T, bw_M, bw_vec, bw_colD, bw_sumDP, bw_part,
       bw_cpart;
 
+  // streamed plan: the matrix stays in the caller's host memory and every
+  // product uploads it again in row shards of whole 128-row tiles, two device
+  // slots deep (the copy of shard s + 1 overlaps the work on shard s)
+  struct Shard {
+    int64_t r0, r1, p0, p1;  // rows [r0, r1), stored entries [p0, p1)
+    CUtensorMap qmap;        // TMA map of the shard's rows of the tall image
+    int row_groups;          // partials of its tensor-core transposed product
+    int ranges;              // partials of its CUDA-core transposed product
+  };
+  struct Slot {
+    DevBuf ip, idx, vin, vwork, counts, seg, ent, meta, tptr, cell, cval;
+  };
+  bool streaming = false;
+  bool stream_sort = false;       // re-sort every shard after its upload
+  bool stream_transform = false;  // working values differ from the input's
+  int stream_mode = 0;            // value transform mode (k_transform_values)
+  const int64_t* h_indptr = nullptr;
+  const int32_t* h_idx = nullptr;
+  const void* h_val = nullptr;
+  std::vector<Shard> shards;
+  int64_t shard_rows_max = 0, shard_nnz_max = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+  Slot slot[2];
+  DevBuf t_mu, t_inv_std, t_cshift, d_gene2slot;
+
   // baseline-aware (PFlog) plan: the working matrix is [delta | b] with the
   // baseline as its last column; g_user = the caller's gene count (g - 1 for
   // PFlog, g otherwise)
@@ -330,6 +356,14 @@ struct scxpca_plan {
 
   ~scxpca_plan() {
     for (cudaEvent_t e : events) cudaEventDestroy(e);
+    if (copy_stream) {
+      cudaStreamSynchronize(copy_stream);
+      cudaStreamDestroy(copy_stream);
+    }
+    for (int i = 0; i < 2; ++i) {
+      if (ev_copied[i]) cudaEventDestroy(ev_copied[i]);
+      if (ev_free[i]) cudaEventDestroy(ev_free[i]);
+    }
   }
 };
 
@@ -494,6 +528,465 @@ void build_tile_csc(scxpca_plan* pl) {
   CK(cudaStreamSynchronize(st));  // the host vectors above go out of scope
 }
 
+// ---------------------------------------------------------------------------
+// Streamed plan: the matrix stays in host memory, products take it in row
+// shards (the counterpart of StreamingPcaOperator and drive_row_segments,
+// scx-gpu/src/linear_operator.rs:61-288).  Each shard is uploaded on a copy
+// stream into one of two device slots and prepared on the plan's stream
+// (indptr rebased, rows sorted when the input needs it, values transformed,
+// and the shard packed into the tile format of the product that reads it),
+// so the upload of shard s + 1 overlaps the work on shard s.  Everything
+// tall (Y, its 16-bit image) stays resident; a shard's rows are whole
+// 128-row tiles of it.
+// ---------------------------------------------------------------------------
+constexpr int64_t kShardEntriesMax = int64_t(1) << 26;  // stored entries per shard at most
+
+void alloc_work_buffers(scxpca_plan* pl);
+
+// Bytes one device slot needs per stored entry and per row.
+double slot_bytes_per_entry(const scxpca_plan* pl, bool tc) {
+  double b = 4.0 + (double)dtype_size(pl->in_dtype) + (double)dtype_size(pl->dtype);
+  b += tc ? 4.0 * 1.2 : 1.0 + (double)dtype_size(pl->dtype);
+  return b;
+}
+
+void shard_upload(scxpca_plan* pl, size_t s, int k) {
+  const scxpca_plan::Shard& sh = pl->shards[s];
+  scxpca_plan::Slot& sl = pl->slot[k];
+  cudaStream_t cs = pl->copy_stream;
+  const int64_t rows = sh.r1 - sh.r0, cnt = sh.p1 - sh.p0;
+  CK(cudaStreamWaitEvent(cs, pl->ev_free[k], 0));
+  CK(cudaMemcpyAsync(sl.ip.p, pl->h_indptr + sh.r0, sizeof(int64_t) * (rows + 1), cudaMemcpyHostToDevice, cs));
+  if (cnt) {
+    CK(cudaMemcpyAsync(sl.idx.p, pl->h_idx + sh.p0, sizeof(int32_t) * cnt, cudaMemcpyHostToDevice, cs));
+    const size_t vs = dtype_size(pl->in_dtype);
+    CK(cudaMemcpyAsync(sl.vin.p, static_cast<const char*>(pl->h_val) + vs * sh.p0, vs * cnt, cudaMemcpyHostToDevice,
+                       cs));
+  }
+  CK(cudaEventRecord(pl->ev_copied[k], cs));
+}
+
+// Bring an uploaded shard to the working form on the plan's stream: the
+// rebased indptr, sorted rows when needed, working values (`work`), and, per
+// `pack` (0 none, 1 tensor-core tiles, 2 tile-CSC), the packed copy.
+const void* shard_prepare(scxpca_plan* pl, size_t s, int k, bool work, int pack) {
+  const scxpca_plan::Shard& sh = pl->shards[s];
+  scxpca_plan::Slot& sl = pl->slot[k];
+  cudaStream_t st = pl->stream;
+  const int64_t rows = sh.r1 - sh.r0, cnt = sh.p1 - sh.p0;
+  CK(cudaStreamWaitEvent(st, pl->ev_copied[k], 0));
+  CK(launch_rebase_indptr(sl.ip.as<int64_t>(), rows, sh.p0, st, pl->num_sms));
+  if (pl->stream_sort) CK(launch_sort_rows(pl->in_dtype, sl.ip.as<int64_t>(), sl.idx.as<int32_t>(), sl.vin.p, rows, st,
+                                           pl->num_sms));
+  const void* vals = sl.vin.p;
+  if (work && pl->stream_transform) {
+    CK(launch_transform_values(pl->in_dtype, pl->dtype, sl.idx.as<int32_t>(), sl.vin.p, sl.vwork.p, cnt,
+                               pl->stream_mode, pl->t_mu.as<double>(), pl->t_inv_std.as<double>(),
+                               pl->t_cshift.as<double>(), pl->clip, st, pl->num_sms));
+    vals = sl.vwork.p;
+  }
+  if (pack == 1) {
+    const int64_t nseg = (rows + 127) / 128 * pl->n_chunks;
+    CK(tile_format_count(sl.ip.as<int64_t>(), sl.idx.as<int32_t>(), rows, pl->n_chunks, sl.counts.as<int64_t>(), st,
+                         pl->num_sms));
+    CK(launch_exclusive_scan_i64(sl.counts.as<int64_t>(), nseg, sl.seg.as<int64_t>(), st));
+    CK(cudaMemsetAsync(sl.ent.p, 0, sizeof(uint32_t) * (size_t)(cnt + 3 * nseg + 4), st));
+    CK(tile_format_fill(sl.ip.as<int64_t>(), sl.idx.as<int32_t>(), vals, rows, pl->n_chunks, sl.seg.as<int64_t>(),
+                        sl.ent.as<uint32_t>(), sl.meta.p, st, pl->num_sms));
+  } else if (pack == 2) {
+    CK(launch_tile_csc(pl->dtype, sl.ip.as<int64_t>(), sl.idx.as<int32_t>(), vals, rows, pl->d_gene2slot.as<int32_t>(),
+                       pl->nslots, sl.tptr.as<int32_t>(), sl.cell.as<uint8_t>(), sl.cval.p, st, pl->num_sms));
+  }
+  return vals;
+}
+
+void shard_release(scxpca_plan* pl, int k) { CK(cudaEventRecord(pl->ev_free[k], pl->stream)); }
+
+// Run `body(s, slot)` over every shard in order, each after its upload, with
+// the upload of the next shard issued ahead.
+template <typename F>
+void for_each_shard(scxpca_plan* pl, F&& body) {
+  const size_t ns = pl->shards.size();
+  for (size_t s = 0; s < ns; ++s) {
+    shard_upload(pl, s, (int)(s & 1));
+    if (s >= 1) {
+      body(s - 1, (int)((s - 1) & 1));
+      shard_release(pl, (int)((s - 1) & 1));
+    }
+  }
+  if (ns) {
+    body(ns - 1, (int)((ns - 1) & 1));
+    shard_release(pl, (int)((ns - 1) & 1));
+  }
+}
+
+// Per-gene statistics over the shards, of the input (work = false) or the
+// working values (work = true); optional validation flags and gene counts.
+void stream_stats(scxpca_plan* pl, bool work, std::vector<double>& sums, std::vector<double>& sq, int32_t* flags,
+                  int32_t* gene_counts) {
+  cudaStream_t st = pl->stream;
+  const int64_t g = pl->g;
+  for_each_shard(pl, [&](size_t s, int k) {
+    const scxpca_plan::Shard& sh = pl->shards[s];
+    scxpca_plan::Slot& sl = pl->slot[k];
+    const int64_t rows = sh.r1 - sh.r0, cnt = sh.p1 - sh.p0;
+    const void* vals = shard_prepare(pl, s, k, work, 0);
+    if (flags)
+      CK(launch_validate_csr(pl->in_dtype, sl.ip.as<int64_t>(), sl.idx.as<int32_t>(), sl.vin.p, rows, g, cnt, flags,
+                             st, pl->num_sms));
+    if (gene_counts) CK(launch_gene_counts(sl.idx.as<int32_t>(), cnt, gene_counts, st, pl->num_sms));
+    CK(launch_col_stats(work ? pl->dtype : pl->in_dtype, sl.idx.as<int32_t>(), vals, cnt, (int32_t)g,
+                        pl->stats_part.as<double>(), pl->stats_parts, pl->stats_out.as<double>(), st, pl->num_sms,
+                        s > 0 ? 1 : 0));
+  });
+  std::vector<double> host(2 * g);
+  CK(cudaMemcpyAsync(host.data(), pl->stats_out.p, sizeof(double) * 2 * g, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  sums.assign(host.begin(), host.begin() + g);
+  sq.assign(host.begin() + g, host.end());
+}
+
+// Streamed products (the tall operands and outputs stay resident).
+void stream_forward(scxpca_plan* pl, bool f32) {
+  cudaStream_t st = pl->stream;
+  const int64_t ld = pl->ld;
+  for_each_shard(pl, [&](size_t s, int k) {
+    const scxpca_plan::Shard& sh = pl->shards[s];
+    scxpca_plan::Slot& sl = pl->slot[k];
+    const int64_t rows = sh.r1 - sh.r0;
+    const void* vals = shard_prepare(pl, s, k, true, pl->use_tc ? 1 : 0);
+    if (pl->use_tc) {
+      CK(launch_fwd_tc((int)ld, sl.ent.as<uint32_t>(), sl.meta.p, rows, pl->n_chunks, &pl->vmap, pl->mc.as<float>(),
+                       f32 ? pl->Y.as<float>() + sh.r0 * ld : nullptr, pl->Yimg.as<uint16_t>() + sh.r0 * 2 * ld,
+                       pl->fmt16, pl->tc_err.as<int>(), st, pl->num_sms));
+    } else {
+      CK(launch_fwd_strict(pl->dtype, (int)ld, sl.ip.as<int64_t>(), sl.idx.as<int32_t>(), vals, rows, (int32_t)pl->g,
+                           pl->V.as<float>(), pl->centered ? pl->mc.as<float>() : nullptr,
+                           pl->Y.as<float>() + sh.r0 * ld, st));
+    }
+  });
+}
+
+void stream_rmat(scxpca_plan* pl, const float* A) {
+  cudaStream_t st = pl->stream;
+  const int64_t ld = pl->ld, g = pl->g;
+  for_each_shard(pl, [&](size_t s, int k) {
+    const scxpca_plan::Shard& sh = pl->shards[s];
+    scxpca_plan::Slot& sl = pl->slot[k];
+    const int64_t rows = sh.r1 - sh.r0;
+    shard_prepare(pl, s, k, true, pl->use_tc ? 1 : 2);
+    if (pl->use_tc) {
+      CK(launch_rmat_tc((int)ld, sl.ent.as<uint32_t>(), sl.meta.p, rows, pl->n_chunks, g, pl->tc_gene_groups,
+                        sh.row_groups, &sh.qmap, pl->tc_part.as<float>(), pl->fmt16, pl->tc_err.as<int>(), st));
+      CK(launch_reduce_rows_f32(pl->tc_part.as<float>(), sh.row_groups, g * ld, pl->W.as<double>(), s > 0 ? 1 : 0,
+                                st, pl->num_sms));
+    } else {
+      CK(launch_rmat_strict(pl->dtype, (int)ld, sl.ip.as<int64_t>(), sl.tptr.as<int32_t>(), sl.cell.as<uint8_t>(),
+                            sl.cval.p, rows, (int32_t)g, pl->nslots, pl->d_slot2gene.as<int32_t>(), sh.ranges,
+                            A + sh.r0 * ld, pl->wpart.as<float>(), st));
+      CK(launch_reduce_rows_f32(pl->wpart.as<float>(), sh.ranges, g * ld, pl->W.as<double>(), s > 0 ? 1 : 0, st,
+                                pl->num_sms));
+    }
+  });
+}
+
+// The transform of the input values into the working values (scaling with
+// clipping; or a plain conversion to the compute type) from the input
+// statistics: fills mode/mu/inv_std/cshift like the resident path and
+// returns whether the working values differ from the input's.
+bool value_transform(scxpca_plan* pl, const std::vector<double>& sx, const std::vector<double>& sxx, int& mode,
+                     std::vector<double>& mu, std::vector<double>& inv_std, std::vector<double>& cshift) {
+  const int64_t g = pl->g, n = pl->n;
+  mu.assign(g, 0.0);
+  inv_std.assign(g, 1.0);
+  cshift.assign(g, 0.0);
+  mode = 0;
+  if (pl->scaled) {
+    pl->std_x.resize(g);
+    for (int64_t j = 0; j < g; ++j) {
+      const double m = pl->mean_x[j];
+      const double var = (sxx[j] - (double)n * m * m) / std::max<double>((double)n - 1.0, 1.0);
+      double sd = std::sqrt(std::max(var, 0.0));
+      if (sd == 0.0) sd = 1.0;
+      pl->std_x[j] = sd;
+      mu[j] = m;
+      inv_std[j] = 1.0 / sd;
+      if (pl->centered) {
+        double c = -m / sd;
+        if (pl->clip > 0) c = std::min(std::max(c, -pl->clip), pl->clip);
+        cshift[j] = c;
+      }
+    }
+    mode = pl->centered ? 1 : 2;
+  }
+  (void)sx;
+  return pl->scaled || pl->in_dtype != pl->dtype;
+}
+
+// Streamed plan set-up (called by create_plan for a host matrix that does not
+// fit the device budget).  `limit` = the device bytes the plan may hold.
+void setup_streaming(scxpca_plan* pl, const scxpca_csr* x, size_t limit) {
+  cudaStream_t st = pl->stream;
+  const int64_t n = pl->n, g = pl->g, nnz = pl->nnz;
+  pl->streaming = true;
+  pl->h_indptr = x->indptr;
+  pl->h_idx = x->indices;
+  pl->h_val = x->values;
+  // the row pointers are in host memory: check them there
+  if (x->indptr[0] != 0 || x->indptr[n] != nnz)
+    fail(SCXPCA_INVALID_CSR, "invalid CSR: indptr is not monotone within [0, nnz]");
+  for (int64_t i = 0; i < n; ++i)
+    if (x->indptr[i + 1] < x->indptr[i]) fail(SCXPCA_INVALID_CSR, "invalid CSR: indptr is not monotone within [0, nnz]");
+  const bool tc_allowed = !(getenv("SCXPCA_TC") && getenv("SCXPCA_TC")[0] == '0');
+  pl->use_tc = tc_allowed && pl->dtype != SCXPCA_F32 && g <= 64 * 128;
+  if (pl->use_tc) pl->ld = (pl->k + 63) / 64 * 64;
+  pl->fmt16 = pl->dtype == SCXPCA_BF16 ? 1 : 0;
+  const int64_t ld = pl->ld;
+  // what stays resident: the tall buffers (Y; the 16-bit image), the gene-side
+  // and statistics buffers; the rest of `limit` is the two shard slots
+  const double resident = (double)n * ld * 4 * (pl->use_tc ? 2 : 1) + (double)n * pl->nc * 4 +
+                          (double)g * ld * 8 * 8 + (double)2 * g * 8 * (2 * pl->num_sms + 1) + (64 << 20);
+  const double per_entry = slot_bytes_per_entry(pl, pl->use_tc) + (pl->use_tc ? 0.0 : 1.0);
+  const double room = ((double)limit / 1.1 - resident) / 2.0;
+  int64_t cap = (int64_t)std::min<double>((double)kShardEntriesMax, room / per_entry);
+  // shards: whole 128-row tiles, at most `cap` stored entries (or one tile)
+  pl->shards.clear();
+  for (int64_t r0 = 0; r0 < n;) {
+    int64_t r1 = std::min(n, r0 + 128);
+    while (r1 < n) {
+      const int64_t nr = std::min(n, r1 + 128);
+      if (x->indptr[nr] - x->indptr[r0] > cap) break;
+      r1 = nr;
+    }
+    scxpca_plan::Shard sh{};
+    sh.r0 = r0;
+    sh.r1 = r1;
+    sh.p0 = x->indptr[r0];
+    sh.p1 = x->indptr[r1];
+    pl->shards.push_back(sh);
+    pl->shard_rows_max = std::max(pl->shard_rows_max, r1 - r0);
+    pl->shard_nnz_max = std::max(pl->shard_nnz_max, sh.p1 - sh.p0);
+    r0 = r1;
+  }
+  if (room <= 0.0 || (double)pl->shard_nnz_max * per_entry > room * 1.5)
+    fail(SCXPCA_OUT_OF_MEMORY, "streamed GPU PCA: the device budget of " + std::to_string(limit >> 20) +
+                                   " MB does not hold the resident buffers and two shard slots");
+  CK(cudaStreamCreateWithFlags(&pl->copy_stream, cudaStreamNonBlocking));
+  for (int i = 0; i < 2; ++i) {
+    CK(cudaEventCreateWithFlags(&pl->ev_copied[i], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&pl->ev_free[i], cudaEventDisableTiming));
+  }
+  const int64_t rmax = pl->shard_rows_max, emax = std::max<int64_t>(pl->shard_nnz_max, 1);
+  for (auto& sl : pl->slot) {
+    sl.ip.alloc(sizeof(int64_t) * (rmax + 1));
+    sl.idx.alloc(sizeof(int32_t) * emax);
+    sl.vin.alloc(dtype_size(pl->in_dtype) * emax);
+  }
+  phase_mark(SCXPCA_PHASE_UPLOAD, st);
+
+  // ---- validation, input statistics (and gene counts) over the shards ----
+  pl->stats_parts = 2 * pl->num_sms;
+  pl->stats_part.alloc(sizeof(double) * 2 * g * pl->stats_parts);
+  pl->stats_out.alloc(sizeof(double) * 2 * g);
+  DevBuf flags, counts;
+  flags.alloc(16);
+  CK(cudaMemsetAsync(flags.p, 0, 16, st));
+  counts.alloc(sizeof(int32_t) * g);
+  CK(cudaMemsetAsync(counts.p, 0, sizeof(int32_t) * g, st));
+  std::vector<double> sx, sxx;
+  stream_stats(pl, false, sx, sxx, flags.as<int32_t>(), counts.as<int32_t>());
+  int32_t hf[4];
+  CK(cudaMemcpyAsync(hf, flags.p, 16, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (hf[1]) fail(SCXPCA_INVALID_CSR, "invalid CSR: column index out of range [0, n_vars)");
+  if (hf[3]) fail(SCXPCA_INVALID_CSR, "invalid CSR: non-finite value");
+  if (hf[2]) {
+    // unsorted or duplicated rows: every upload sorts its shard; duplicates
+    // (found after sorting) take the CUDA-core path
+    pl->stream_sort = true;
+    pl->rows_resorted = true;
+    CK(cudaMemsetAsync(flags.p, 0, 16, st));
+    for_each_shard(pl, [&](size_t s, int k) {
+      const scxpca_plan::Shard& sh = pl->shards[s];
+      scxpca_plan::Slot& sl = pl->slot[k];
+      shard_prepare(pl, s, k, false, 0);
+      CK(launch_validate_csr(pl->in_dtype, sl.ip.as<int64_t>(), sl.idx.as<int32_t>(), sl.vin.p, sh.r1 - sh.r0, g,
+                             sh.p1 - sh.p0, flags.as<int32_t>(), st, pl->num_sms));
+    });
+    CK(cudaMemcpyAsync(hf, flags.p, 16, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hf[2] && pl->use_tc) {
+      pl->use_tc = false;
+      pl->ld = padded_k(pl->k);
+    }
+  }
+  pl->mean_x.resize(g);
+  for (int64_t j = 0; j < g; ++j) pl->mean_x[j] = sx[j] / (double)n;
+  phase_mark(SCXPCA_PHASE_VALIDATE, st);
+  phase_mark(SCXPCA_PHASE_STATS, st);
+
+  // ---- working values and their statistics ----
+  std::vector<double> mu, inv_std, cshift;
+  pl->stream_transform = value_transform(pl, sx, sxx, pl->stream_mode, mu, inv_std, cshift);
+  if (pl->stream_transform) {
+    upload(pl->t_mu, mu, st);
+    upload(pl->t_inv_std, inv_std, st);
+    upload(pl->t_cshift, cshift, st);
+    for (auto& sl : pl->slot) sl.vwork.alloc(dtype_size(pl->dtype) * emax);
+    stream_stats(pl, true, pl->col_sum, pl->col_sq, nullptr, nullptr);
+  } else {
+    pl->col_sum = sx;
+    pl->col_sq = sxx;
+  }
+  {
+    std::vector<double> mu_w(g, 0.0);
+    if (pl->centered)
+      for (int64_t j = 0; j < g; ++j) mu_w[j] = pl->col_sum[j] / (double)n;
+    upload(pl->d_mu, mu_w, st);
+    // closed-form total variance with the cancellation guard; the recompute
+    // takes one more pass over the shards (the working values minus mu)
+    const double denom = std::max<double>((double)n - 1.0, 1.0);
+    double sumsq = 0.0, meansq = 0.0, total = 0.0;
+    for (int64_t j = 0; j < g; ++j) {
+      sumsq += pl->col_sq[j];
+      meansq += mu_w[j] * mu_w[j];
+      total += pl->col_sq[j] - (double)n * mu_w[j] * mu_w[j];
+    }
+    pl->total_var = (pl->centered ? total : sumsq) / denom;
+    if (pl->centered && sumsq > 0.0 && sumsq - meansq * (double)n <= 1e-7 * sumsq) {
+      DevBuf d_shift, d_one, d_zero, shifted;
+      std::vector<double> one(g, 1.0), zero(g, 0.0);
+      upload(d_shift, mu_w, st);
+      upload(d_one, one, st);
+      upload(d_zero, zero, st);
+      shifted.alloc(sizeof(float) * emax);
+      for_each_shard(pl, [&](size_t s, int k) {
+        const scxpca_plan::Shard& sh = pl->shards[s];
+        scxpca_plan::Slot& sl = pl->slot[k];
+        const int64_t cnt = sh.p1 - sh.p0;
+        const void* vals = shard_prepare(pl, s, k, true, 0);
+        CK(launch_transform_values(pl->stream_transform ? pl->dtype : pl->in_dtype, 0, sl.idx.as<int32_t>(), vals,
+                                   shifted.p, cnt, 1, d_shift.as<double>(), d_one.as<double>(), d_zero.as<double>(),
+                                   0.0, st, pl->num_sms));
+        CK(launch_col_stats(0, sl.idx.as<int32_t>(), shifted.p, cnt, (int32_t)g, pl->stats_part.as<double>(),
+                            pl->stats_parts, pl->stats_out.as<double>(), st, pl->num_sms, s > 0 ? 1 : 0));
+      });
+      std::vector<double> host(2 * g);
+      CK(cudaMemcpyAsync(host.data(), pl->stats_out.p, sizeof(double) * 2 * g, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      double t = 0.0;
+      for (int64_t j = 0; j < g; ++j) {
+        const double nnz_j = mu_w[j] != 0.0 ? std::round((pl->col_sum[j] - host[j]) / mu_w[j]) : 0.0;
+        t += host[g + j] + std::max((double)n - nnz_j, 0.0) * mu_w[j] * mu_w[j];
+      }
+      pl->total_var = t / denom;
+      pl->total_var_recomputed = true;
+    }
+  }
+  {
+    std::vector<double> c(g), sc(g);
+    for (int64_t j = 0; j < g; ++j) {
+      c[j] = pl->centered ? pl->mean_x[j] : 0.0;
+      sc[j] = pl->scaled ? 1.0 / pl->std_x[j] : 1.0;
+    }
+    upload(pl->d_center_raw, c, st);
+    upload(pl->d_scale_raw, sc, st);
+    CK(cudaStreamSynchronize(st));
+  }
+  phase_mark(SCXPCA_PHASE_TRANSFORM, st);
+
+  // ---- the packed per-shard copies and the resident image ----
+  const int64_t tiles_max = (rmax + 127) / 128;
+  if (pl->use_tc) {
+    pl->n_chunks = (int)((g + 63) / 64);
+    const int64_t nseg_max = tiles_max * pl->n_chunks;
+    for (auto& sl : pl->slot) {
+      sl.counts.alloc(sizeof(int64_t) * nseg_max);
+      sl.seg.alloc(sizeof(int64_t) * (nseg_max + 1));
+      sl.ent.alloc(sizeof(uint32_t) * (size_t)(emax + 3 * nseg_max + 4));
+      sl.meta.alloc(tile_meta_bytes(rmax, pl->n_chunks));
+    }
+    pl->Vimg.alloc(sizeof(uint16_t) * g * 2 * ld);
+    pl->Yimg.alloc(sizeof(uint16_t) * n * 2 * ld);
+    pl->tc_err.alloc(sizeof(int) * 4);
+    CK(cudaMemsetAsync(pl->tc_err.p, 0, sizeof(int) * 4, st));
+    const int rg = rmat_tc_groups((int)ld, pl->n_chunks, pl->num_sms, &pl->tc_gene_groups);
+    int rg_max = 1;
+    for (auto& sh : pl->shards) {
+      sh.row_groups = (int)std::min<int64_t>(rg, (sh.r1 - sh.r0 + 127) / 128);
+      rg_max = std::max(rg_max, sh.row_groups);
+      const int r = make_tmap16(&sh.qmap, pl->Yimg.as<uint16_t>() + sh.r0 * 2 * ld, sh.r1 - sh.r0, 2 * ld, 128,
+                                pl->fmt16);
+      if (r) fail(SCXPCA_CUDA_ERROR, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")");
+    }
+    pl->tc_row_groups = rg_max;
+    pl->tc_part.alloc(sizeof(float) * (size_t)rg_max * g * ld);
+    const int r1 = make_tmap16(&pl->vmap, pl->Vimg.p, g, 2 * ld, 64, pl->fmt16);
+    const int r2 = make_tmap16(&pl->qmap, pl->Yimg.p, n, 2 * ld, 128, pl->fmt16);
+    if (r1 || r2)
+      fail(SCXPCA_CUDA_ERROR, "cuTensorMapEncodeTiled failed (" + std::to_string(r1) + ", " + std::to_string(r2) + ")");
+  } else {
+    pl->nslots = strict_slot_count(g, (int)ld);
+    if (strict_tile_smem_bytes(pl->nslots) > kStatsSmemMax)
+      fail(SCXPCA_UNSUPPORTED, "a streamed CUDA-core PCA takes at most " +
+                                   std::to_string(kStatsSmemMax / sizeof(int32_t) - 1) + " genes");
+    std::vector<int32_t> hc(g), gene2slot, slot2gene;
+    CK(cudaMemcpyAsync(hc.data(), counts.p, sizeof(int32_t) * g, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    strict_assign_slots(hc, (int)ld, gene2slot, slot2gene);
+    pl->d_gene2slot.alloc(sizeof(int32_t) * g);
+    pl->d_slot2gene.alloc(sizeof(int32_t) * pl->nslots);
+    CK(cudaMemcpyAsync(pl->d_gene2slot.p, gene2slot.data(), sizeof(int32_t) * g, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(pl->d_slot2gene.p, slot2gene.data(), sizeof(int32_t) * pl->nslots, cudaMemcpyHostToDevice,
+                       st));
+    for (auto& sl : pl->slot) {
+      sl.tptr.alloc(sizeof(int32_t) * (size_t)tiles_max * (pl->nslots + 1));
+      sl.cell.alloc(emax);
+      sl.cval.alloc(dtype_size(pl->dtype) * emax);
+    }
+    const int gblocks = pl->nslots / (8 * strict_genes_per_warp((int)ld));
+    int ranges_max = 1;
+    for (auto& sh : pl->shards) {
+      const int64_t nt = (sh.r1 - sh.r0 + kStrictTile - 1) / kStrictTile;
+      sh.ranges = (int)std::max<int64_t>(1, std::min<int64_t>(nt, (4 * pl->num_sms + gblocks - 1) / gblocks));
+      ranges_max = std::max(ranges_max, sh.ranges);
+    }
+    pl->strict_csc = true;
+    pl->wpart.alloc(sizeof(float) * (size_t)ranges_max * g * ld);
+    CK(cudaStreamSynchronize(st));  // the host vectors above go out of scope
+  }
+  phase_mark(SCXPCA_PHASE_PACK, st);
+  alloc_work_buffers(pl);
+}
+
+// The dense work buffers of a run (tall Y, gene-side factors, k x k FP64).
+void alloc_work_buffers(scxpca_plan* pl) {
+  const int64_t n = pl->n, g = pl->g, ld = pl->ld;
+  pl->gram_parts = 2 * pl->num_sms;
+  pl->gram_parts_small = (int)std::max<int64_t>(1, std::min<int64_t>(2 * pl->num_sms, (g + 31) / 32));
+  pl->Y.alloc(sizeof(float) * n * ld);
+  pl->W.alloc(sizeof(double) * g * ld);
+  pl->Z.alloc(sizeof(double) * g * ld);
+  pl->V.alloc(sizeof(float) * g * ld);
+  pl->mc.alloc(sizeof(float) * ld);
+  pl->gpart.alloc(sizeof(double) * pl->gram_parts * (ld * ld + ld));
+  pl->G.alloc(sizeof(double) * (ld * ld + ld));
+  pl->R.alloc(sizeof(double) * ld * ld);
+  pl->Rinv.alloc(sizeof(double) * ld * ld);
+  pl->Rinv_f.alloc(sizeof(float) * ld * ld);
+  pl->R2inv.alloc(sizeof(double) * ld * ld);
+  pl->evals.alloc(sizeof(double) * ld);
+  pl->evecs.alloc(sizeof(double) * (ld * ld + ld * (ld + 1)));  // + eigensolver scratch
+  pl->sigma.alloc(sizeof(double) * ld);
+  pl->comps.alloc(sizeof(float) * pl->nc * g);
+  pl->M_emb.alloc(sizeof(float) * ld * pl->nc);
+  pl->status.alloc(sizeof(int) * 4);
+  std::vector<double> eye(ld * ld, 0.0);
+  for (int64_t i = 0; i < ld; ++i) eye[i * ld + i] = 1.0;
+  upload(pl->eye, eye, pl->stream);
+  CK(cudaStreamSynchronize(pl->stream));  // `eye` goes out of scope
+}
+
 // The baseline of a PFlog plan: the working matrix's last column holds b.
 struct PflogSpec {
   double b_mean;  // mean of the FP64 baseline (total variance)
@@ -552,6 +1045,25 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
         if (reserved > used) fr += (size_t)(reserved - used);
       }
       double with_headroom = (double)need * 1.1;
+      // A host matrix that does not fit (the free memory, or the caller's
+      // device budget) is streamed from host memory instead of held resident
+      // (gpu_pca.rs:520-590); SCXPCA_RESIDENT=0 forces it.
+      size_t limit = fr;
+      if (p->device_budget > 0) limit = std::min(limit, (size_t)p->device_budget);
+      const char* res_env = getenv("SCXPCA_RESIDENT");
+      const bool force_stream = res_env && res_env[0] == '0';
+      if (x->memory != SCXPCA_MEM_DEVICE && !aff && !pf && (force_stream || with_headroom > (double)limit)) {
+        setup_streaming(pl, x, limit);
+        phase_mark(SCXPCA_PHASE_BUFFERS, st);
+        CK(cudaStreamSynchronize(st));
+        pl->device_bytes = pl->stats_part.bytes + pl->Y.bytes + pl->Yimg.bytes + pl->tc_part.bytes +
+                           pl->wpart.bytes + pl->gpart.bytes + pl->W.bytes + pl->Z.bytes + pl->V.bytes;
+        for (auto& sl : pl->slot)
+          pl->device_bytes += sl.ip.bytes + sl.idx.bytes + sl.vin.bytes + sl.vwork.bytes + sl.counts.bytes +
+                              sl.seg.bytes + sl.ent.bytes + sl.meta.bytes + sl.tptr.bytes + sl.cell.bytes +
+                              sl.cval.bytes;
+        return pl;
+      }
       if (with_headroom > (double)fr)
         fail(SCXPCA_OUT_OF_MEMORY, "GPU PCA requires ~" + std::to_string((size_t)with_headroom >> 20) +
                                        " MB but only " + std::to_string(fr >> 20) +
@@ -797,30 +1309,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
     phase_mark(SCXPCA_PHASE_PACK, st);
 
     // ---- dense work buffers ----
-    pl->gram_parts = 2 * pl->num_sms;
-    pl->gram_parts_small = (int)std::max<int64_t>(1, std::min<int64_t>(2 * pl->num_sms, (g + 31) / 32));
-    pl->Y.alloc(sizeof(float) * n * ld);
-    pl->W.alloc(sizeof(double) * g * ld);
-    pl->Z.alloc(sizeof(double) * g * ld);
-    pl->V.alloc(sizeof(float) * g * ld);
-    pl->mc.alloc(sizeof(float) * ld);
-    pl->gpart.alloc(sizeof(double) * pl->gram_parts * (ld * ld + ld));
-    pl->G.alloc(sizeof(double) * (ld * ld + ld));
-    pl->R.alloc(sizeof(double) * ld * ld);
-    pl->Rinv.alloc(sizeof(double) * ld * ld);
-    pl->Rinv_f.alloc(sizeof(float) * ld * ld);
-    pl->R2inv.alloc(sizeof(double) * ld * ld);
-    pl->evals.alloc(sizeof(double) * ld);
-    pl->evecs.alloc(sizeof(double) * (ld * ld + ld * (ld + 1)));  // + eigensolver scratch
-    pl->sigma.alloc(sizeof(double) * ld);
-    pl->comps.alloc(sizeof(float) * pl->nc * g);
-    pl->M_emb.alloc(sizeof(float) * ld * pl->nc);
-    pl->status.alloc(sizeof(int) * 4);
-    {
-      std::vector<double> eye(ld * ld, 0.0);
-      for (int64_t i = 0; i < ld; ++i) eye[i * ld + i] = 1.0;
-      upload(pl->eye, eye, st);
-    }
+    alloc_work_buffers(pl);
     phase_mark(SCXPCA_PHASE_BUFFERS, st);
     CK(cudaStreamSynchronize(st));
     size_t fr = 0, tot = 0;
@@ -921,6 +1410,16 @@ void small_qr(scxpca_plan* pl, double* A, int shift) {
 // forward product's, or the explicit Q's).
 void rmatmat_raw(scxpca_plan* pl, float* A, int split) {
   cudaStream_t st = pl->stream;
+  if (pl->streaming) {
+    int s = stage_begin(pl);
+    if (pl->use_tc && split)
+      CK(launch_split16(A, pl->n * pl->ld, pl->Yimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
+    stage_end(pl, SCXPCA_STAGE_APPLY, s);
+    s = stage_begin(pl);
+    stream_rmat(pl, A);
+    stage_end(pl, SCXPCA_STAGE_TRANSPOSE, s);
+    return;
+  }
   if (pl->use_tc) {
     int s = stage_begin(pl);
     if (split)
@@ -962,6 +1461,16 @@ void rmatmat_raw(scxpca_plan* pl, float* A, int split) {
 // (inside the power loop at ld 64, whose Gram uses the image).
 void forward(scxpca_plan* pl, bool f32 = true) {
   cudaStream_t st = pl->stream;
+  if (pl->streaming) {
+    int s = stage_begin(pl);
+    if (pl->use_tc)
+      CK(launch_split16(pl->V.as<float>(), pl->g * pl->ld, pl->Vimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
+    stage_end(pl, SCXPCA_STAGE_SMALL, s);
+    s = stage_begin(pl);
+    stream_forward(pl, f32);
+    stage_end(pl, SCXPCA_STAGE_FORWARD, s);
+    return;
+  }
   if (pl->use_tc) {
     int s = stage_begin(pl);
     CK(launch_split16(pl->V.as<float>(), pl->g * pl->ld, pl->Vimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
@@ -1126,7 +1635,8 @@ void finish_result(scxpca_plan* pl, const int* hstatus, const double* sigma, scx
   if (out->std) {
     for (int64_t j = 0; j < pl->g_user; ++j) out->std[j] = pl->std_x.empty() ? 1.0 : pl->std_x[j];
   }
-  out->resident_csr = 1;
+  out->resident_csr = pl->streaming ? 0 : 1;
+  out->n_shards = pl->streaming ? (int32_t)pl->shards.size() : 0;
   out->total_var_recomputed = pl->total_var_recomputed ? 1 : 0;
   out->shifted_cholesky = hstatus[0] > 0 ? hstatus[0] : 0;
   out->eig_sweeps = hstatus[2];
@@ -1181,6 +1691,9 @@ void backward(scxpca_plan* pl, const float* S, const float* GS, int iters, float
   if (pl->rows_resorted)
     fail(SCXPCA_UNSUPPORTED, "the plan re-sorted unsorted CSR rows, so gradients would not follow the caller's "
                              "entry order; sort each row by gene before creating the plan");
+  if (pl->streaming)
+    fail(SCXPCA_UNSUPPORTED, "the backward pass needs the matrix resident on the device; this plan streams it "
+                             "from host memory");
   if (iters < 0 || iters > 1000) fail(SCXPCA_INVALID_ARGUMENT, "solve_iterations must be in [0, 1000]");
   if (!S || !GS || !gvals) fail(SCXPCA_INVALID_ARGUMENT, "null scores, grad_scores or grad_values");
   pl->run_valid = false;
@@ -1847,7 +2360,8 @@ int32_t scxpca_plan_col_stats(scxpca_plan* plan, double* col_sums, double* col_s
     DeviceGuard dg(plan->device);
     PoolScope pool_scope(plan->device, plan->stream);
     std::vector<double> s, q;
-    stats_pass(plan, plan->val, plan->dtype, s, q);
+    if (plan->streaming) stream_stats(plan, true, s, q, nullptr, nullptr);
+    else stats_pass(plan, plan->val, plan->dtype, s, q);
     if (col_sums) memcpy(col_sums, s.data(), sizeof(double) * plan->g);
     if (col_sum_sq) memcpy(col_sum_sq, q.data(), sizeof(double) * plan->g);
   });

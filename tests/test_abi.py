@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     lib = _lib.load()
-    assert lib.scxpca_abi_version() == 1
+    assert lib.scxpca_abi_version() == 2
     assert lib.scxpca_status_string(_lib.NOT_SPD) == b"not SPD"
     assert lib.scxpca_status_string(999) == b"unknown status"
 
