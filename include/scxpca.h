@@ -121,7 +121,15 @@ typedef struct {
  * GpuPcaDeviceResult (gpu_pca.rs:108-128).  `embeddings` is n_obs x
  * n_components row-major float32 in `embeddings_memory` (device: on the plan's
  * device, written asynchronously before the call returns synchronised).  All
- * other arrays are host memory; any of them except `embeddings` may be NULL. */
+ * other arrays are host memory; any of them except `embeddings` may be NULL.
+ *
+ * Device hand-off (gpu_randomized_pca_device -> CAGRA kNN,
+ * scx-gpu/src/gpu_pca.rs:775-838, scx-accel/src/fused/gpu.rs:36-60): with
+ * embeddings_memory = DEVICE the caller owns the buffer (n_obs * n_components
+ * floats, contiguous rows, the layout of the reference's DeviceEmbedding); the
+ * library writes it in place on the plan's stream and returns only after that
+ * write completed, so a consumer on any stream of the device may read it at
+ * once, and the embedding never crosses to the host. */
 typedef struct {
   float* embeddings;            /* n_obs x n_components, row-major */
   float* components;            /* n_components x n_vars, row-major */

@@ -28,6 +28,7 @@
 #include "../../include/scxpca.h"
 #include "common.cuh"
 #include "launch.h"
+#include "power_loop.h"
 
 using namespace scx;
 
@@ -1533,6 +1534,81 @@ scxpca_params run_params(const scxpca_plan* pl, const scxpca_params* over) {
   return p;
 }
 
+// The plan's power-loop operator (the steps run_power_loop drives).  The Y
+// factor stays implicit inside the loop: qr(Y) is the FP64 Cholesky R of
+// Y^T Y, and the next transposed product applies R^{-1}
+// (Z = (X^T Y - mu (1^T Y)) R^{-1}).  qr(Z) is one FP64 CholeskyQR pass and
+// rounds Z into V, the next forward product's operand.  finalize_q forms
+// Q = Y R^{-1} and factors it again (R2; a third pass under the Householder
+// contract), so the closing product gives B = (X - mu)^T Q R2^{-1}.
+struct DeviceOperator {
+  scxpca_plan* pl;
+  const scxpca_params& p;
+  int shift;           // Householder contract: shifted factorisations allowed
+  bool image_only;     // tensor-core Gram at ld 64: the loop needs only Y's image
+  const double* mu;    // working-matrix centre (null without centring)
+  double* sY;          // column sums of Y, written after its Gram
+  bool closing = false;
+
+  void matmat(Operand src, bool last) {
+    if (src == Operand::kOmega) {
+      int s = stage_begin(pl);
+      load_omega(pl, &p);
+      stage_end(pl, SCXPCA_STAGE_SMALL, s);
+    }
+    // Only the last forward product's FP32 Y is read (by finalize_q); the
+    // tensor-core Gram at ld 64 reads the 16-bit image.
+    forward(pl, !image_only || last);
+  }
+  void qr(Buf b) {
+    if (b == Buf::kY) {
+      tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
+      return;
+    }
+    const int ld = (int)pl->ld;
+    int s = stage_begin(pl);
+    small_qr(pl, pl->Z.as<double>(), shift);
+    CK(launch_round_v(pl->Z.as<double>(), pl->g, ld, mu, pl->V.as<float>(), pl->mc.as<float>(), pl->stream));
+    if (pl->pflog) CK(launch_aug_colsum(pl->V.as<float>(), (int32_t)pl->g_user, ld, pl->stream));
+    stage_end(pl, SCXPCA_STAGE_SMALL, s);
+  }
+  void rmatmat() {
+    const int ld = (int)pl->ld;
+    rmatmat_raw(pl, pl->Y.as<float>(), 0);
+    int s = stage_begin(pl);
+    if (pl->pflog) CK(launch_aug_fold(pl->W.as<double>(), (int32_t)pl->g_user, ld, pl->stream, pl->num_sms));
+    CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY,
+                           closing ? pl->R2inv.as<double>() : pl->Rinv.as<double>(), pl->Z.as<double>(), pl->stream));
+    stage_end(pl, SCXPCA_STAGE_SMALL, s);
+  }
+  void apply_q() {  // Y <- Y Rinv_f, with the 16-bit image on the tensor-core path
+    const int ld = (int)pl->ld;
+    int s = stage_begin(pl);
+    if (pl->use_tc)
+      CK(launch_apply_right_split(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(),
+                                  pl->Yimg.as<uint16_t>(), pl->fmt16, pl->stream, pl->num_sms));
+    else
+      CK(launch_apply_right_f32(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(), pl->stream,
+                                pl->num_sms));
+    stage_end(pl, SCXPCA_STAGE_APPLY, s);
+  }
+  void finalize_q() {
+    // Explicit Q = Y R^{-1}, re-orthonormalised by a second FP64 Cholesky pass.
+    apply_q();
+    tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
+    if (shift) {
+      // Householder contract (an orthonormal Q whatever the conditioning):
+      // when the first factorisation had to be shifted, CholeskyQR2 leaves Q
+      // with an orthogonality error of about u cond(Q1); a third pass (shifted
+      // CholeskyQR3) brings it to working precision.  Applied unconditionally
+      // in this mode, so the enqueued sequence does not depend on device results.
+      apply_q();
+      tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
+    }
+    closing = true;
+  }
+};
+
 // Enqueue one run on the plan's stream: power loop, Rayleigh-Ritz step and
 // embeddings into the device buffer U (n_obs x n_components).  No host
 // synchronisation and, when omega is NULL or device memory, no allocation:
@@ -1540,67 +1616,13 @@ scxpca_params run_params(const scxpca_plan* pl, const scxpca_params* over) {
 void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
   cudaStream_t st = pl->stream;
   const int ld = (int)pl->ld;
-  const int shift = p.qr_method == SCXPCA_QR_HOUSEHOLDER ? 1 : 0;
-  const double* mu = pl->centered ? pl->d_mu.as<double>() : nullptr;
-  double* sY = pl->G.as<double>() + (size_t)ld * ld;  // column sums follow the Gram
-
   CK(cudaMemsetAsync(pl->status.p, 0, sizeof(int) * 4, st));
+  DeviceOperator op{pl, p, p.qr_method == SCXPCA_QR_HOUSEHOLDER ? 1 : 0, pl->use_tc && ld == 64,
+                    pl->centered ? pl->d_mu.as<double>() : nullptr,
+                    pl->G.as<double>() + (size_t)ld * ld};  // column sums follow the Gram
+  run_power_loop(op, p.n_power_iterations);
+  // SVD of B (in Z) through the FP64 eigendecomposition of B^T B.
   int s = stage_begin(pl);
-  load_omega(pl, &p);
-  stage_end(pl, SCXPCA_STAGE_SMALL, s);
-  // Y = (X - mu) Omega ; qr(Y).  Only the last forward product's FP32 Y is
-  // read (by the explicit Q below); the tensor-core Gram at ld 64 reads the
-  // 16-bit image.
-  const bool image_only = pl->use_tc && ld == 64;
-  forward(pl, !image_only || p.n_power_iterations == 0);
-  tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
-  for (int64_t it = 0; it < p.n_power_iterations; ++it) {
-    // Z = (X - mu)^T Q = (X^T Y - mu (1^T Y)) R^{-1}
-    rmatmat_raw(pl, pl->Y.as<float>(), 0);
-    s = stage_begin(pl);
-    if (pl->pflog) CK(launch_aug_fold(pl->W.as<double>(), (int32_t)pl->g_user, ld, st, pl->num_sms));
-    CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->Rinv.as<double>(),
-                           pl->Z.as<double>(), st));
-    small_qr(pl, pl->Z.as<double>(), shift);
-    CK(launch_round_v(pl->Z.as<double>(), pl->g, ld, mu, pl->V.as<float>(), pl->mc.as<float>(), st));
-    if (pl->pflog) CK(launch_aug_colsum(pl->V.as<float>(), (int32_t)pl->g_user, ld, st));
-    stage_end(pl, SCXPCA_STAGE_SMALL, s);
-    forward(pl, !image_only || it + 1 == p.n_power_iterations);
-    tall_chol(pl, pl->Y.as<float>(), pl->n, pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
-  }
-  // Explicit Q = Y R^{-1}, re-orthonormalised by a second FP64 Cholesky pass.
-  s = stage_begin(pl);
-  if (pl->use_tc)  // with the 16-bit image of Q for the tensor-core Gram and transposed product
-    CK(launch_apply_right_split(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(),
-                                pl->Yimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
-  else
-    CK(launch_apply_right_f32(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(), st,
-                              pl->num_sms));
-  stage_end(pl, SCXPCA_STAGE_APPLY, s);
-  tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
-  if (shift) {
-    // Householder contract (an orthonormal Q whatever the conditioning): when
-    // the first factorisation had to be shifted, CholeskyQR2 leaves Q with an
-    // orthogonality error of about u cond(Q1); a third pass (shifted
-    // CholeskyQR3) brings it to working precision.  Applied unconditionally in
-    // this mode, so the enqueued sequence does not depend on device results.
-    s = stage_begin(pl);
-    if (pl->use_tc)
-      CK(launch_apply_right_split(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(),
-                                  pl->Yimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
-    else
-      CK(launch_apply_right_f32(pl->Y.as<float>(), pl->n, ld, pl->Rinv_f.as<float>(), pl->Y.as<float>(), st,
-                                pl->num_sms));
-    stage_end(pl, SCXPCA_STAGE_APPLY, s);
-    tall_chol(pl, pl->Y.as<float>(), pl->n, pl->R2inv.as<double>(), pl->Rinv_f.as<float>(), shift, true);
-  }
-  // B = (X - mu)^T Q R2^{-1}
-  rmatmat_raw(pl, pl->Y.as<float>(), 0);
-  s = stage_begin(pl);
-  if (pl->pflog) CK(launch_aug_fold(pl->W.as<double>(), (int32_t)pl->g_user, ld, st, pl->num_sms));
-  CK(launch_center_apply(pl->W.as<double>(), pl->g, ld, mu, sY, pl->R2inv.as<double>(),
-                         pl->Z.as<double>(), st));
-  // SVD of B through the FP64 eigendecomposition of B^T B.
   CK(launch_gram_f64(pl->Z.as<double>(), pl->g, ld, pl->gpart.as<double>(), pl->gram_parts_small, st));
   CK(launch_reduce_rows_f64(pl->gpart.as<double>(), pl->gram_parts_small, (int64_t)ld * ld + ld,
                             pl->G.as<double>(), 0, st, pl->num_sms));
