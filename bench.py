@@ -743,8 +743,9 @@ def batched_leg(args, local, dev):
            "cluster_sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)), "max": int(sizes.max())},
            "graph_ms": round(statistics.median(graph_ms), 3), "plain_launches_ms": round(statistics.median(plain_ms), 3),
            "speedup_graph_vs_plain": round(statistics.median(plain_ms) / statistics.median(graph_ms), 3),
-           "branches": b.branches, "graph_nodes": b.graph_nodes,
-           "autotune_ms": {str(k): round(v, 3) for k, v in b.tuned_ms.items()},
+           "branches": abs(b.branches), "schedule": "lockstep" if b.lockstep else "segment per branch",
+           "graph_nodes": b.graph_nodes,
+           "autotune_ms": {(f"lockstep {-k}" if k < 0 else str(k)): round(v, 3) for k, v in b.tuned_ms.items()},
            "sigma_max_rel_diff_graph_vs_plain": float(np.max(np.abs(sv_g - sv_p) / sv_p))}
     b.close()
     # correctness at the timed setting: clusters from smallest to largest

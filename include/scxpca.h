@@ -249,9 +249,13 @@ int32_t scxpca_plan_qr(scxpca_plan* plan, float* a, int64_t m, int64_t ld_a,
  * slices are borrowed, not copied), runs every segment once with plain
  * launches to measure it, and records all runs into ONE CUDA graph whose
  * parallel branches take the segments in a longest-first schedule of the
- * measured times; `branches` fixes the branch count (1..32) or, with 0, an
- * autotuner times the graph for 1, 2, 4, ... 32 branches and keeps the
- * fastest.  params->omega must be NULL (seeded) or device memory, and
+ * measured times.  Two schedules: segment per branch (each branch runs whole
+ * segments one after another) or lockstep (all segments take each step of
+ * the power loop together, so their products run together and then their
+ * small factorisations run together).  `branches` = b in 1..32 fixes the
+ * segment-per-branch schedule over b branches, -b the lockstep schedule over
+ * b streams; 0 lets an autotuner time both schedules for 1, 2, 4, ... 32 and
+ * keep the fastest.  params->omega must be NULL (seeded) or device memory, and
  * params->stream NULL (the batch owns its streams).  The reference runs one
  * PCA per call (scx-gpu/src/gpu_pca.rs:706-763); a caller with clusters
  * loops over it, which scxpca_batch_run with use_graph = 0 reproduces. */
@@ -273,8 +277,10 @@ int32_t scxpca_batch_run(scxpca_batch* batch, int32_t use_graph, float* embeddin
                          double* variance_ratio, double* variance_explained, double* device_ms,
                          char* err, size_t err_len);
 
-/* Chosen branch count, graph node count, and the autotuner's timings in ms
- * for 1, 2, 4, 8, 16, 32 branches (0 where not tried; 6 entries). */
+/* Chosen schedule (branch count; negative = lockstep over that many
+ * streams), graph node count, and the autotuner's timings in ms (0 where not
+ * tried; 12 entries): [0..5] segment-per-branch schedules with 1, 2, 4, 8,
+ * 16, 32 branches, [6..11] lockstep schedules over as many streams. */
 int32_t scxpca_batch_info(const scxpca_batch* batch, int32_t* branches, int64_t* graph_nodes,
                           double* tuned_ms);
 

@@ -579,8 +579,10 @@ class Plan:
 class Batch:
     """Independent randomized PCAs of the row segments of one CSR matrix
     (scxpca_batch_*): one resident plan per segment, all runs recorded into a
-    single CUDA graph over parallel branches (``branches=0`` autotunes the
-    branch count).  ``run(use_graph=False)`` runs one plain plan call per
+    single CUDA graph over parallel branches.  ``branches=b > 0`` runs whole
+    segments per branch on b branches, ``-b`` the lockstep schedule (all
+    segments take each power-loop step together) over b streams, and 0
+    autotunes both.  ``run(use_graph=False)`` runs one plain plan call per
     segment instead, the loop a caller of the one-PCA API would write."""
 
     def __init__(self, indptr, indices, values, shape, segment_offsets, n_components: int = 30,
@@ -608,10 +610,14 @@ class Batch:
         self._h = handle
         nb = C.c_int32()
         nodes = C.c_int64()
-        tuned = np.zeros(6, dtype=np.float64)
+        tuned = np.zeros(12, dtype=np.float64)
         self._lib.scxpca_batch_info(self._h, C.byref(nb), C.byref(nodes), _ptr(tuned))
+        # branches < 0: the lockstep schedule over -branches streams
         self.branches, self.graph_nodes = int(nb.value), int(nodes.value)
-        self.tuned_ms = {b: float(t) for b, t in zip((1, 2, 4, 8, 16, 32), tuned) if t > 0}
+        self.lockstep = self.branches < 0
+        cand = (1, 2, 4, 8, 16, 32)
+        self.tuned_ms = {b: float(t) for b, t in zip(cand, tuned[:6]) if t > 0}
+        self.tuned_ms.update({-b: float(t) for b, t in zip(cand, tuned[6:]) if t > 0})
 
     def run(self, use_graph: bool = True, embeddings_out=None, components: bool = True):
         """Returns (embeddings, components [seg, nc, n_vars] or None, singular values

@@ -89,7 +89,7 @@ cudaError_t launch_gram_f64(const double* A, int64_t n, int ld, double* part, in
 
 // ---------------------------------------------------------------------------
 // Cholesky of the leading k x k block of G (ld x ld) and the inverse of its
-// factor, one block of 1024 threads.  A pivot j fails when its Schur
+// factor, one block of T x T threads.  A pivot j fails when its Schur
 // complement d_j <= tau * G_jj (the column is numerically dependent on the
 // previous ones) or is not finite.  With shift_on_fail the factorisation
 // restarts once on G + s I, s = 10 tau max_j G_jj, which always succeeds on
@@ -101,14 +101,14 @@ cudaError_t launch_gram_f64(const double* A, int64_t n, int ld, double* part, in
 // triangular), where A = L D L^T.  Then R = D^{1/2} L^T and
 // R^{-1} = X^T D^{-1/2}: R_jc = A_jc / sqrt(d_j), R^{-1}_ca = X_ac / sqrt(d_a).
 // Every matrix entry lives in a register of its owner, thread (ty, tx) owning
-// rows ty + 32u and columns tx + 32v; one register holds A_ac above the
+// rows ty + T u and columns tx + T v; one register holds A_ac above the
 // diagonal (c >= a) or X_ac below it.  Per step the owners of row j + 1
 // publish it (double-buffered rows in shared memory) and the owner of the
 // next diagonal entry computes the next pivot's reciprocals, so a step is
 // one barrier plus a short dependent chain.
 // ---------------------------------------------------------------------------
-template <int U>
-__global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G, int k, int ld, double tau,
+template <int U, int T>
+__global__ void __launch_bounds__(T * T) k_cholesky(const double* __restrict__ G, int k, int ld, double tau,
                                                    int shift_on_fail, double* __restrict__ R,
                                                    double* __restrict__ Rinv, float* __restrict__ Rinv_f,
                                                    int* __restrict__ status) {
@@ -117,19 +117,20 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
   __shared__ int pv_ok[kMaxK];
   __shared__ double maxdiag_s;
   __shared__ int fail_s;
-  const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
-  for (int j = tid; j < k; j += 1024) dg[j] = G[(int64_t)j * ld + j];
-  for (int t = tid; t < ld * ld; t += 1024) {
+  constexpr int NT = T * T;
+  const int tid = threadIdx.x, tx = tid % T, ty = tid / T;
+  for (int j = tid; j < k; j += NT) dg[j] = G[(int64_t)j * ld + j];
+  for (int t = tid; t < ld * ld; t += NT) {
     R[t] = 0.0;
     Rinv[t] = 0.0;
     Rinv_f[t] = 0.f;
   }
   __syncthreads();
-  if (ty == 0) {
+  if (tid < 32) {
     double m = 0.0;
-    for (int j = tx; j < k; j += 32) m = fmax(m, dg[j]);
+    for (int j = tid; j < k; j += 32) m = fmax(m, dg[j]);
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (tx == 0) maxdiag_s = m;
+    if (tid == 0) maxdiag_s = m;
   }
   double shift = 0.0;
   int fail = -1;
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
     for (int u = 0; u < U; ++u)
 #pragma unroll
       for (int v = 0; v < U; ++v) {
-        const int a = ty + 32 * u, c = tx + 32 * v;
+        const int a = ty + T * u, c = tx + T * v;
         double x = 0.0;
         if (a < k && c < k) {
           if (c >= a) x = G[(int64_t)a * ld + c] + (a == c ? shift : 0.0);
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
     if (ty == 0) {
 #pragma unroll
       for (int v = 0; v < U; ++v) {
-        const int c = tx + 32 * v;
+        const int c = tx + T * v;
         if (c < k) {
           rowA[0][c] = val[0][v];
           rowX[0][c] = c == 0 ? 1.0 : 0.0;
@@ -180,11 +181,11 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
       const double di = pv_di[j], rj = pv_rinv[j];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int a = ty + 32 * u;
+        const int a = ty + T * u;
         if (a == j) {  // row j is final: R_jc = A_jc / sqrt(d_j)
 #pragma unroll
           for (int v = 0; v < U; ++v) {
-            const int c = tx + 32 * v;
+            const int c = tx + T * v;
             if (c >= j && c < k) R[(int64_t)j * ld + c] = val[u][v] * rj;
           }
         }
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
           const double m = rowA[b][a] * di;
 #pragma unroll
           for (int v = 0; v < U; ++v) {
-            const int c = tx + 32 * v;
+            const int c = tx + T * v;
             if (c < k) {
               if (c >= a) val[u][v] -= m * rowA[b][c];
               else if (c <= j) val[u][v] -= m * rowX[b][c];
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
           if (a == j + 1) {  // publish row j + 1 for the next step
 #pragma unroll
             for (int v = 0; v < U; ++v) {
-              const int c = tx + 32 * v;
+              const int c = tx + T * v;
               if (c < k) {
                 if (c >= a) rowA[b ^ 1][c] = val[u][v];
                 if (c < a) rowX[b ^ 1][c] = val[u][v];
@@ -222,7 +223,7 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
     if (!shift_on_fail || attempt == 1) {
       if (tid == 0) status[0] = -(fail + 1);
       // Leave well-defined (identity) factors so downstream kernels stay finite.
-      for (int t = tid; t < ld * ld; t += 1024) {
+      for (int t = tid; t < ld * ld; t += NT) {
         const int r = t / ld, c = t % ld;
         const double v = (r == c && r < k) ? 1.0 : 0.0;
         R[t] = v;
@@ -240,7 +241,7 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ G,
   for (int u = 0; u < U; ++u)
 #pragma unroll
     for (int v = 0; v < U; ++v) {
-      const int a = ty + 32 * u, c = tx + 32 * v;
+      const int a = ty + T * u, c = tx + T * v;
       if (a < k && c <= a) {
         const double x = (c == a ? 1.0 : val[u][v]) * pv_rinv[a];
         Rinv[(int64_t)c * ld + a] = x;
@@ -253,10 +254,13 @@ cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shif
                             double* R, double* Rinv, float* Rinv_f, int* status, cudaStream_t st) {
   if (k > kMaxK) return cudaErrorInvalidValue;
   note_launches(1);
+  // 16 x 16 threads with 4 x 4 entries each for k <= 64: every owner reads the
+  // published pivot row from shared memory each step, so fewer threads that
+  // hold more entries each move less of it per step
   if (k <= 64)
-    k_cholesky<2><<<1, 1024, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
+    k_cholesky<4, 16><<<1, 256, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
   else
-    k_cholesky<4><<<1, 1024, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
+    k_cholesky<4, 32><<<1, 1024, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
   return cudaGetLastError();
 }
 

@@ -1613,15 +1613,27 @@ struct DeviceOperator {
 // embeddings into the device buffer U (n_obs x n_components).  No host
 // synchronisation and, when omega is NULL or device memory, no allocation:
 // the sequence can be captured into a CUDA graph.
+DeviceOperator device_operator(scxpca_plan* pl, const scxpca_params& p) {
+  const int ld = (int)pl->ld;
+  return DeviceOperator{pl, p, p.qr_method == SCXPCA_QR_HOUSEHOLDER ? 1 : 0, pl->use_tc && ld == 64,
+                        pl->centered ? pl->d_mu.as<double>() : nullptr,
+                        pl->G.as<double>() + (size_t)ld * ld};  // column sums follow the Gram
+}
+
+void enqueue_finish(scxpca_plan* pl, float* U);
+
 void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
+  CK(cudaMemsetAsync(pl->status.p, 0, sizeof(int) * 4, pl->stream));
+  DeviceOperator op = device_operator(pl, p);
+  run_power_loop(op, p.n_power_iterations);
+  enqueue_finish(pl, U);
+}
+
+// After the loop: the SVD of B (in Z) through the FP64 eigendecomposition of
+// B^T B, the components, and the embeddings U = Q R2^{-1} E Sigma.
+void enqueue_finish(scxpca_plan* pl, float* U) {
   cudaStream_t st = pl->stream;
   const int ld = (int)pl->ld;
-  CK(cudaMemsetAsync(pl->status.p, 0, sizeof(int) * 4, st));
-  DeviceOperator op{pl, p, p.qr_method == SCXPCA_QR_HOUSEHOLDER ? 1 : 0, pl->use_tc && ld == 64,
-                    pl->centered ? pl->d_mu.as<double>() : nullptr,
-                    pl->G.as<double>() + (size_t)ld * ld};  // column sums follow the Gram
-  run_power_loop(op, p.n_power_iterations);
-  // SVD of B (in Z) through the FP64 eigendecomposition of B^T B.
   int s = stage_begin(pl);
   CK(launch_gram_f64(pl->Z.as<double>(), pl->g, ld, pl->gpart.as<double>(), pl->gram_parts_small, st));
   CK(launch_reduce_rows_f64(pl->gpart.as<double>(), pl->gram_parts_small, (int64_t)ld * ld + ld,
@@ -1858,8 +1870,11 @@ struct scxpca_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int branches = 0;
+  bool lockstep = false;               // schedule of the recorded graph (see batch_capture)
   size_t graph_nodes = 0;
-  double tuned_ms[6] = {0, 0, 0, 0, 0, 0};  // graph time per tried branch count (1, 2, 4, 8, 16, 32)
+  // graph time per tried schedule: [0..5] segment-per-branch with 1, 2, 4, 8,
+  // 16, 32 branches; [6..11] lockstep over as many streams
+  double tuned_ms[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   scxpca_params params{};
 
   ~scxpca_batch() {
@@ -1908,9 +1923,55 @@ std::vector<std::vector<int>> batch_schedule(const scxpca_batch* b, int nb) {
   return lists;
 }
 
+// The copies of a segment's status, singular values and components to the
+// batch's pinned host buffers, on the segment's current stream.
+void batch_copy_out(scxpca_batch* b, int q) {
+  scxpca_plan* pl = b->plans[q];
+  cudaStream_t st = pl->stream;
+  CK(cudaMemcpyAsync(b->h_status + 4 * q, pl->status.p, sizeof(int) * 3, cudaMemcpyDeviceToHost, st));
+  if (pl->use_tc)
+    CK(cudaMemcpyAsync(b->h_status + 4 * q + 3, pl->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(b->h_sigma + b->k * q, pl->sigma.p, sizeof(double) * pl->k, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(b->h_comps + (size_t)b->nc * b->n_vars * q, pl->comps.p, sizeof(float) * pl->nc * pl->g,
+                     cudaMemcpyDeviceToHost, st));
+}
+
+// The lockstep schedule's operator: every step of run_power_loop is taken by
+// all segments at once, each segment on its branch stream (the branches fork
+// from the main stream before the step and join it after), so the segments'
+// products run together and then their small factorisations run together.
+struct BatchOperator {
+  scxpca_batch* b;
+  std::vector<DeviceOperator> ops;  // one per segment
+  std::vector<int> branch_of;       // segment -> branch
+  int nb;
+
+  template <class F>
+  void each(F&& f) {
+    CK(cudaEventRecord(b->fork, b->main));
+    for (int t = 0; t < nb; ++t) CK(cudaStreamWaitEvent(b->branch[t], b->fork, 0));
+    for (size_t q = 0; q < ops.size(); ++q) {
+      ops[q].pl->stream = b->branch[branch_of[q]];
+      f((int)q, ops[q]);
+    }
+    for (int t = 0; t < nb; ++t) {
+      CK(cudaEventRecord(b->join[t], b->branch[t]));
+      CK(cudaStreamWaitEvent(b->main, b->join[t], 0));
+    }
+  }
+  void matmat(Operand src, bool last) { each([&](int, DeviceOperator& o) { o.matmat(src, last); }); }
+  void rmatmat() { each([&](int, DeviceOperator& o) { o.rmatmat(); }); }
+  void qr(Buf x) { each([&](int, DeviceOperator& o) { o.qr(x); }); }
+  void finalize_q() { each([&](int, DeviceOperator& o) { o.finalize_q(); }); }
+};
+
 // Record every segment's run (and the copies of its status, singular values
 // and components to pinned host memory) into one graph over `nb` branches.
-void batch_capture(scxpca_batch* b, int nb) {
+// Two schedules: segment per branch (a branch runs whole segments one after
+// another, the longest first) or lockstep (all segments take each power-loop
+// step together; BatchOperator).  Segments go to branches by a
+// longest-processing-time schedule of their measured times either way.
+void batch_capture(scxpca_batch* b, int nb, bool lockstep) {
   batch_free_graph(b);
   while ((int)b->branch.size() < nb) {
     cudaStream_t st;
@@ -1921,26 +1982,36 @@ void batch_capture(scxpca_batch* b, int nb) {
     b->join.push_back(e);
   }
   const auto lists = batch_schedule(b, nb);
-  const scxpca_params p = b->params;
+  const scxpca_params& p = b->params;
   CK(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeRelaxed));
   try {
-    CK(cudaEventRecord(b->fork, b->main));
-    for (int t = 0; t < nb; ++t) {
-      cudaStream_t st = b->branch[t];
-      CK(cudaStreamWaitEvent(st, b->fork, 0));
-      for (int q : lists[t]) {
-        scxpca_plan* pl = b->plans[q];
-        pl->stream = st;
-        enqueue_run(pl, p, b->emb.as<float>() + b->offsets[q] * b->nc);
-        CK(cudaMemcpyAsync(b->h_status + 4 * q, pl->status.p, sizeof(int) * 3, cudaMemcpyDeviceToHost, st));
-        if (pl->use_tc)
-          CK(cudaMemcpyAsync(b->h_status + 4 * q + 3, pl->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(b->h_sigma + b->k * q, pl->sigma.p, sizeof(double) * pl->k, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(b->h_comps + (size_t)b->nc * b->n_vars * q, pl->comps.p,
-                           sizeof(float) * pl->nc * pl->g, cudaMemcpyDeviceToHost, st));
+    if (lockstep) {
+      BatchOperator bop{b, {}, std::vector<int>(b->plans.size(), 0), nb};
+      for (int t = 0; t < nb; ++t)
+        for (int q : lists[t]) bop.branch_of[q] = t;
+      for (scxpca_plan* pl : b->plans) bop.ops.push_back(device_operator(pl, p));
+      bop.each([&](int, DeviceOperator& o) {
+        CK(cudaMemsetAsync(o.pl->status.p, 0, sizeof(int) * 4, o.pl->stream));
+      });
+      run_power_loop(bop, p.n_power_iterations);
+      bop.each([&](int q, DeviceOperator& o) {
+        enqueue_finish(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
+        batch_copy_out(b, q);
+      });
+    } else {
+      CK(cudaEventRecord(b->fork, b->main));
+      for (int t = 0; t < nb; ++t) {
+        cudaStream_t st = b->branch[t];
+        CK(cudaStreamWaitEvent(st, b->fork, 0));
+        for (int q : lists[t]) {
+          scxpca_plan* pl = b->plans[q];
+          pl->stream = st;
+          enqueue_run(pl, p, b->emb.as<float>() + b->offsets[q] * b->nc);
+          batch_copy_out(b, q);
+        }
+        CK(cudaEventRecord(b->join[t], st));
+        CK(cudaStreamWaitEvent(b->main, b->join[t], 0));
       }
-      CK(cudaEventRecord(b->join[t], st));
-      CK(cudaStreamWaitEvent(b->main, b->join[t], 0));
     }
   } catch (...) {
     cudaGraph_t g = nullptr;
@@ -1957,6 +2028,7 @@ void batch_capture(scxpca_batch* b, int nb) {
   CK(cudaGraphGetNodes(b->graph, nullptr, &nodes));
   b->graph_nodes = nodes;
   b->branches = nb;
+  b->lockstep = lockstep;
 }
 
 // One graph launch; returns its device time in ms.
@@ -2051,8 +2123,9 @@ scxpca_batch* create_batch(const scxpca_csr* x, const int64_t* offsets, int64_t 
                            const scxpca_params* p, int32_t branches) {
   if (!x || !offsets || !p) fail(SCXPCA_INVALID_ARGUMENT, "null csr, offsets or params");
   if (n_segments <= 0) fail(SCXPCA_INVALID_ARGUMENT, "n_segments must be > 0");
-  if (branches < 0 || branches > kMaxBranches)
-    fail(SCXPCA_INVALID_ARGUMENT, "branches must be in [0, " + std::to_string(kMaxBranches) + "] (0 = autotune)");
+  if (branches < -kMaxBranches || branches > kMaxBranches)
+    fail(SCXPCA_INVALID_ARGUMENT, "branches must be in [-" + std::to_string(kMaxBranches) + ", " +
+                                      std::to_string(kMaxBranches) + "] (0 = autotune, negative = lockstep)");
   if (p->omega && p->omega_memory != SCXPCA_MEM_DEVICE)
     fail(SCXPCA_INVALID_ARGUMENT, "a batch takes a device omega (or NULL for the seeded test matrix)");
   if (p->stream) fail(SCXPCA_INVALID_ARGUMENT, "a batch owns its streams: params.stream must be NULL");
@@ -2116,26 +2189,32 @@ scxpca_batch* create_batch(const scxpca_csr* x, const int64_t* offsets, int64_t 
     CK(cudaMallocHost(&b->h_comps, sizeof(float) * (size_t)b->nc * b->n_vars * n_segments));
     // measured per-segment times: one plain pass (warms every plan up too)
     batch_run_plain(b, b->emb.as<float>(), nullptr, nullptr, nullptr, nullptr, true);
-    if (branches > 0) {
-      batch_capture(b, branches);
+    if (branches != 0) {
+      batch_capture(b, std::abs(branches), branches < 0);
     } else {
-      // autotune the branch count: time one launch of each candidate graph
+      // autotune the schedule and the branch count: time one launch of each
+      // candidate graph, keep the fastest
       double best = 0.0;
       int best_nb = 1;
+      bool best_lock = false, first = true;
       const int cands[6] = {1, 2, 4, 8, 16, 32};
-      for (int i = 0; i < 6; ++i) {
-        const int nb = cands[i];
-        if (nb > n_segments) break;
-        batch_capture(b, nb);
-        batch_launch_timed(b);  // warm
-        const double ms = batch_launch_timed(b);
-        b->tuned_ms[i] = ms;
-        if (i == 0 || ms < best) {
-          best = ms;
-          best_nb = nb;
+      for (int lock = 0; lock < 2; ++lock) {
+        for (int i = 0; i < 6; ++i) {
+          const int nb = cands[i];
+          if (nb > n_segments) break;
+          batch_capture(b, nb, lock != 0);
+          batch_launch_timed(b);  // warm
+          const double ms = batch_launch_timed(b);
+          b->tuned_ms[6 * lock + i] = ms;
+          if (first || ms < best) {
+            best = ms;
+            best_nb = nb;
+            best_lock = lock != 0;
+            first = false;
+          }
         }
       }
-      if (b->branches != best_nb) batch_capture(b, best_nb);
+      if (b->branches != best_nb || b->lockstep != best_lock) batch_capture(b, best_nb, best_lock);
     }
     return b;
   } catch (...) {
@@ -2200,10 +2279,10 @@ int32_t scxpca_batch_run(scxpca_batch* batch, int32_t use_graph, float* embeddin
 int32_t scxpca_batch_info(const scxpca_batch* batch, int32_t* branches, int64_t* graph_nodes,
                           double* tuned_ms) {
   if (!batch) return SCXPCA_INVALID_ARGUMENT;
-  if (branches) *branches = batch->branches;
+  if (branches) *branches = batch->lockstep ? -batch->branches : batch->branches;
   if (graph_nodes) *graph_nodes = (int64_t)batch->graph_nodes;
   if (tuned_ms)
-    for (int i = 0; i < 6; ++i) tuned_ms[i] = batch->tuned_ms[i];
+    for (int i = 0; i < 12; ++i) tuned_ms[i] = batch->tuned_ms[i];
   return SCXPCA_OK;
 }
 
