@@ -562,12 +562,13 @@ def streamed_leg(args, host_csr, n_obs, local, res_resident):
 
     h_ip = torch.from_numpy(np.asarray(host_csr[0])).pin_memory()
     h_ix = torch.from_numpy(np.asarray(host_csr[1])).pin_memory()
-    vdt = {"mixed_bf16": torch.bfloat16, "mixed_f16": torch.float16, "strict_fp32": torch.float32}[args.mode]
-    h_vv = torch.from_numpy(np.asarray(host_csr[2])).to(vdt).pin_memory()
-    a_vv = h_vv if vdt == torch.bfloat16 else h_vv.numpy()
+    # FP32 host values, as the resident plan was built from: the statistics and
+    # the value transform then see the same inputs and the singular values
+    # differ only by the order of the per-shard partial sums.
+    h_vv = torch.from_numpy(np.asarray(host_csr[2], dtype=np.float32)).pin_memory()
 
     def one():
-        return accel.randomized_pca(h_ip.numpy(), h_ix.numpy(), a_vv, (n_obs, N_VARS), n_components=N_COMPS,
+        return accel.randomized_pca(h_ip.numpy(), h_ix.numpy(), h_vv.numpy(), (n_obs, N_VARS), n_components=N_COMPS,
                                     n_oversamples=N_OVERSAMPLES, n_power_iterations=N_POWER, zero_center=True,
                                     scale=True, clip_max=CLIP, seed=SEED, qr_method="cholesky",
                                     math_mode=args.mode, device=local, device_budget=STREAM_BUDGET)
@@ -582,6 +583,7 @@ def streamed_leg(args, host_csr, n_obs, local, res_resident):
     return {"ms": round(statistics.median(times), 2), "steps": len(times), "device_budget_bytes": STREAM_BUDGET,
             "resident_csr": bool(r.resident_csr), "n_shards": int(r.n_shards),
             "sigma_max_rel_diff_vs_resident": float(np.max(np.abs(np.asarray(r.singular_values) - sv) / sv)),
+            "values_on_host": "float32",
             "path": "scxpca_randomized on pinned host CSR, streamed in row shards"}
 
 

@@ -447,6 +447,15 @@ int32_t scxpca_synth_nb_csr(int32_t device_ordinal, uint64_t seed, int64_t n_obs
                             int32_t* indices, float* values, int64_t* nnz_out, char* err,
                             size_t err_len);
 
+/* Self-test of the bounded pipeline wait (diagnostics; no reference
+ * counterpart).  Runs one block on `device_ordinal` whose mbarrier wait can
+ * never complete (no thread arrives), under the same bounded wait the
+ * tensor-core kernels use.  Returns SCXPCA_TIMEOUT, with the site in the
+ * message, once the wait's limit (about 1 s) has passed; the context stays
+ * usable and the next call runs normally.  Any other status means the
+ * give-up path is broken. */
+int32_t scxpca_wait_selftest(int32_t device_ordinal, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

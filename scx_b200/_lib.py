@@ -56,6 +56,7 @@ EXPORTED = (
     "scxpca_plan_get_profile",
     "scxpca_gaussian",
     "scxpca_synth_nb_csr",
+    "scxpca_wait_selftest",
     "scxpca_last_call_phases",
     "scxpca_preprocess",
     "scxpca_project_columns",
@@ -180,6 +181,7 @@ def load() -> C.CDLL:
         "scxpca_gaussian": (C.c_int32, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, P, *E]),
         "scxpca_synth_nb_csr": (C.c_int32, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, C.c_double,
                                             C.c_double, P, P, P, C.POINTER(C.c_int64), *E]),
+        "scxpca_wait_selftest": (C.c_int32, [C.c_int32, *E]),
         "scxpca_last_call_phases": (C.c_int32, [P, C.c_int32, C.POINTER(C.c_double)]),
         "scxpca_preprocess": (C.c_int32, [C.c_int32, C.POINTER(Csr), P, C.c_double, C.c_int32, P, P, *E]),
         "scxpca_project_columns": (C.c_int32, [C.c_int32, C.POINTER(Csr), P, C.c_int64, P, P, P,

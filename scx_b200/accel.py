@@ -659,6 +659,15 @@ def gaussian(n_rows: int, n_cols: int, seed: int, device: int = 0):
     return out.t()
 
 
+def wait_selftest(device: int = 0) -> None:
+    """Run the give-up path of the bounded pipeline wait: a block whose
+    mbarrier wait never completes.  Raises ScxPcaError with status TIMEOUT
+    after about 1 s (the expected outcome); the device stays usable."""
+    err = _lib.errbuf()
+    st = _lib.load().scxpca_wait_selftest(device, err, len(err))
+    _lib.check(st, err)
+
+
 def synth_nb_csr_device(n_obs: int, n_vars: int, seed: int = 0, loc: float = -3.0,
                         dispersion: float = 0.3, device: int = 0):
     """Generate the synthetic NB CSR on the device; returns torch CUDA tensors."""

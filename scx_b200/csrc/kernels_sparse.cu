@@ -41,8 +41,8 @@ constexpr int kStatsPassGenes = (int)((kStatsSmemMax - (size_t)kStatsWindow * 8)
 template <typename ValT>
 __global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* __restrict__ idx,
                                                                 const ValT* __restrict__ val, int64_t nnz,
-                                                                int32_t g, int32_t pass_genes,
-                                                                double* __restrict__ partial) {
+                                                                int32_t g, int32_t pass_genes, int nparts,
+                                                                int block0, double* __restrict__ partial) {
   extern __shared__ double sm[];  // [2][pass_genes] accumulators, then the window
   double* acc = sm;
   int32_t* w_idx = reinterpret_cast<int32_t*>(sm + 2 * (int64_t)pass_genes);
@@ -50,23 +50,32 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* _
   constexpr int kPer = kStatsWindow / (kStatsWarps * 32);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lanemask_le = 0xffffffffu >> (31 - lane);
-  const int64_t per = (nnz + gridDim.x - 1) / gridDim.x;
-  const int64_t s = min(nnz, (int64_t)blockIdx.x * per);
+  // partition block b of nparts owns entries [b per, (b + 1) per); this
+  // launch runs blocks block0 .. block0 + gridDim.x - 1 of it
+  const int b = block0 + (int)blockIdx.x;
+  const int64_t per = (nnz + nparts - 1) / nparts;
+  const int64_t s = min(nnz, (int64_t)b * per);
   const int64_t e = min(nnz, s + per);
-  double* out = partial + (int64_t)blockIdx.x * 2 * g;
+  double* out = partial + (int64_t)b * 2 * g;
   for (int32_t lo = 0; lo < g; lo += pass_genes) {
     const int32_t gp = min(pass_genes, g - lo);
     for (int i = threadIdx.x; i < 2 * gp; i += blockDim.x) acc[i] = 0.0;
-    for (int64_t w0 = s; w0 < e; w0 += kStatsWindow) {
-      const int cnt = (int)min((int64_t)kStatsWindow, e - w0);
-      int32_t ri[kPer];
-      float rv[kPer];
+    // the window's entries are loaded into registers one window ahead, so
+    // their loads are in flight while the block works on the previous window
+    int32_t ri[kPer];
+    float rv[kPer];
+    auto load = [&](int64_t w) {
+      const int c = (int)min((int64_t)kStatsWindow, e - w);
 #pragma unroll
       for (int u = 0; u < kPer; ++u) {
         const int t = threadIdx.x + u * kStatsWarps * 32;
-        ri[u] = t < cnt ? __ldg(idx + w0 + t) : -1;
-        rv[u] = t < cnt ? to_f32(val[w0 + t]) : 0.f;
+        ri[u] = t < c ? __ldg(idx + w + t) : -1;
+        rv[u] = t < c ? to_f32(val[w + t]) : 0.f;
       }
+    };
+    if (s < e) load(s);
+    for (int64_t w0 = s; w0 < e; w0 += kStatsWindow) {
+      const int cnt = (int)min((int64_t)kStatsWindow, e - w0);
       __syncthreads();  // the previous window is consumed (and the accumulators zeroed)
 #pragma unroll
       for (int u = 0; u < kPer; ++u) {
@@ -75,6 +84,7 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* _
         w_val[t] = rv[u];
       }
       __syncthreads();
+      if (w0 + kStatsWindow < e) load(w0 + kStatsWindow);
       for (int b = 0; b < cnt; b += 32) {
         const int t = b + lane;
         const int32_t j = t < cnt ? w_idx[t] : -1;
@@ -336,9 +346,9 @@ __global__ void __launch_bounds__(512) k_spmm_t(const int64_t* __restrict__ indp
 // Host launchers
 // ---------------------------------------------------------------------------
 template <typename ValT>
-static cudaError_t col_stats_t(const int32_t* idx, const void* val, int64_t nnz, int32_t g,
-                               double* partial, int nparts, double* out, cudaStream_t st,
-                               int num_sms, int accumulate) {
+static cudaError_t col_stats_blocks_t(const int32_t* idx, const void* val, int64_t nnz, int32_t g,
+                                      double* partial, int nparts, int block0, int nblocks, cudaStream_t st) {
+  if (nblocks <= 0) return cudaSuccess;
   const ValT* v = static_cast<const ValT*>(val);
   const int32_t pass_genes = std::min<int32_t>(g, kStatsPassGenes);
   const size_t smem = (size_t)2 * pass_genes * sizeof(double) + (size_t)kStatsWindow * 8;
@@ -346,20 +356,39 @@ static cudaError_t col_stats_t(const int32_t* idx, const void* val, int64_t nnz,
     cudaError_t e = cudaFuncSetAttribute(k_col_stats<ValT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_col_stats<ValT><<<nparts, kStatsWarps * 32, smem, st>>>(idx, v, nnz, g, pass_genes, partial);
-  k_reduce_rows<double><<<grid_for(2 * g, 256, num_sms), 256, 0, st>>>(partial, nparts, 2 * g, out, accumulate);
-  note_launches(2);
+  k_col_stats<ValT><<<nblocks, kStatsWarps * 32, smem, st>>>(idx, v, nnz, g, pass_genes, nparts, block0, partial);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+int64_t col_stats_block_begin(int64_t nnz, int nparts, int b) {
+  const int64_t per = (nnz + nparts - 1) / nparts;
+  return std::min(nnz, (int64_t)b * per);
+}
+
+cudaError_t launch_col_stats_blocks(int dtype, const int32_t* idx, const void* val, int64_t nnz, int32_t g,
+                                    double* partial, int nparts, int block0, int nblocks, cudaStream_t st) {
+  switch (dtype) {
+    case 0: return col_stats_blocks_t<float>(idx, val, nnz, g, partial, nparts, block0, nblocks, st);
+    case 1: return col_stats_blocks_t<__nv_bfloat16>(idx, val, nnz, g, partial, nparts, block0, nblocks, st);
+    default: return col_stats_blocks_t<__half>(idx, val, nnz, g, partial, nparts, block0, nblocks, st);
+  }
+}
+
+cudaError_t launch_col_stats_reduce(const double* partial, int nparts, int32_t g, double* out, cudaStream_t st,
+                                    int num_sms, int accumulate) {
+  k_reduce_rows<double><<<grid_for(2 * g, 256, num_sms), 256, 0, st>>>(partial, nparts, 2 * (int64_t)g, out,
+                                                                      accumulate);
+  note_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_col_stats(int dtype, const int32_t* idx, const void* val, int64_t nnz,
                              int32_t g, double* partial, int nparts, double* out,
                              cudaStream_t st, int num_sms, int accumulate) {
-  switch (dtype) {
-    case 0: return col_stats_t<float>(idx, val, nnz, g, partial, nparts, out, st, num_sms, accumulate);
-    case 1: return col_stats_t<__nv_bfloat16>(idx, val, nnz, g, partial, nparts, out, st, num_sms, accumulate);
-    default: return col_stats_t<__half>(idx, val, nnz, g, partial, nparts, out, st, num_sms, accumulate);
-  }
+  cudaError_t e = launch_col_stats_blocks(dtype, idx, val, nnz, g, partial, nparts, 0, nparts, st);
+  if (e != cudaSuccess) return e;
+  return launch_col_stats_reduce(partial, nparts, g, out, st, num_sms, accumulate);
 }
 
 template <typename InT>

@@ -201,15 +201,29 @@ __global__ void __launch_bounds__(256, 2) k_fwd_strict(const int64_t* __restrict
         if (m) {
           const int t0 = __ffs(m) - 1;
           const int t1 = t0 + __popc(m);
-          for (int t = t0; t < t1; ++t) {
-            const int32_t j = __shfl_sync(0xffffffffu, wi[r], t);
-            const float x = __shfl_sync(0xffffffffu, wv[r], t);
-            // j is in [g0, g1) for a sorted row; the clamp keeps any other
-            // index inside the staged chunk
-            const unsigned jl = min((unsigned)(j - g0), (unsigned)(GC - 1));
-            const float* vr = vc + jl * LD;
+          // four entries per iteration, so their shuffles and shared loads
+          // are in flight together; an entry past t1 enters with x = 0
+          for (int t = t0; t < t1; t += 4) {
+            float xs[4];
+            const float* vr[4];
 #pragma unroll
-            for (int c = 0; c < C; ++c) acc[r][c] = fmaf(x, vr[32 * c], acc[r][c]);
+            for (int u = 0; u < 4; ++u) {
+              const int tu = min(t + u, 31);
+              const int32_t j = __shfl_sync(0xffffffffu, wi[r], tu);
+              const float x = __shfl_sync(0xffffffffu, wv[r], tu);
+              const bool in = t + u < t1;
+              xs[u] = in ? x : 0.f;
+              // j is in [g0, g1) for a taken entry; the clamp keeps any other
+              // index inside the staged chunk.  An entry past t1 reads row 0 of
+              // the chunk (always a staged gene): a row past g1 may hold stale
+              // shared memory, and 0 * NaN would poison the sum.
+              const unsigned jl = in ? min((unsigned)(j - g0), (unsigned)(GC - 1)) : 0u;
+              vr[u] = vc + jl * LD;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+              for (int c = 0; c < C; ++c) acc[r][c] = fmaf(xs[u], vr[u][32 * c], acc[r][c]);
           }
           if (take) wi[r] = kDone;
         }
@@ -305,12 +319,23 @@ __global__ void __launch_bounds__(256, 2) k_rmat_strict(const int64_t* __restric
             cl = __ldg(cell + tb + q);
             x = to_f32(cval[tb + q]);
           }
-          for (int u = 0; u < cnt; ++u) {
-            const int cu = __shfl_sync(0xffffffffu, cl, u) & (T - 1);
-            const float xu = __shfl_sync(0xffffffffu, x, u);
-            const float* qr = qt + cu * LD;
+          // four entries per iteration (lanes past cnt hold x = 0 and cell 0,
+          // a staged row, so their zero products add nothing)
+          for (int u = 0; u < cnt; u += 4) {
+            float xs[4];
+            const float* qr[4];
 #pragma unroll
-            for (int c = 0; c < C; ++c) acc[jj][c] = fmaf(xu, qr[32 * c], acc[jj][c]);
+            for (int v = 0; v < 4; ++v) {
+              const int uv = min(u + v, 31);
+              const int cu = __shfl_sync(0xffffffffu, cl, uv) & (T - 1);
+              const float xu = __shfl_sync(0xffffffffu, x, uv);
+              xs[v] = u + v < cnt ? xu : 0.f;
+              qr[v] = qt + cu * LD;
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+#pragma unroll
+              for (int c = 0; c < C; ++c) acc[jj][c] = fmaf(xs[v], qr[v][32 * c], acc[jj][c]);
           }
         }
       }

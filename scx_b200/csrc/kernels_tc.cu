@@ -1509,6 +1509,41 @@ int launch_gram_tc(int64_t n, const CUtensorMap* qmap, double* part, int fmt, in
   return cudaGetLastError() == cudaSuccess ? grid : -1;
 }
 
+// ---------------------------------------------------------------------------
+// The give-up path of the bounded pipeline wait, on its own.  One block; the
+// barrier expects one arrival and no thread ever arrives, so thread 0's wait
+// (the same mbar_wait the tensor-core kernels use) runs to its limit, raises
+// the block's abort flag and records `code` in err.  Every other warp then
+// sees the abort flag in its own wait and leaves at once, as the roles of a
+// tensor-core kernel do.  No copy or MMA is in flight, so the block ends
+// cleanly and the context stays usable.
+// ---------------------------------------------------------------------------
+__global__ void k_wait_selftest(int* err, int code) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int abort_s;
+  volatile int* abort_flag = &abort_s;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+    *abort_flag = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_wait(&bar, 0u, abort_flag, err, code);
+  } else if ((threadIdx.x & 31) == 0) {
+    // wait for the abort (bounded as well: twice the limit of thread 0)
+    const long long t0 = clock64();
+    while (!*abort_flag && clock64() - t0 < 2 * kWaitCycles) __nanosleep(20000);
+  }
+  __syncthreads();
+}
+
+cudaError_t launch_wait_selftest(int* err, int code, cudaStream_t st) {
+  note_launches(1);
+  k_wait_selftest<<<1, 128, 0, st>>>(err, code);
+  return cudaGetLastError();
+}
+
 size_t fwd_tc_smem_bytes(int ld) { return ld == 64 ? fwd_swap_smem() : fwd_smem(ld); }
 size_t rmat_tc_smem_bytes(int ld) { return ld == 64 ? rmat_swap_smem() : rmat_smem(ld); }
 

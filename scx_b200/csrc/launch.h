@@ -25,6 +25,15 @@ constexpr int kTransposeGeneBlock = 256;       // genes per block, CUDA-core tra
 cudaError_t launch_col_stats(int dtype, const int32_t* idx, const void* val, int64_t nnz,
                              int32_t g, double* partial, int nparts, double* out,
                              cudaStream_t st, int num_sms, int accumulate = 0);
+// The same statistics in two halves: blocks [block0, block0 + nblocks) of the
+// nparts-block partition write their partials (block b reads entries
+// [col_stats_block_begin(b), col_stats_block_begin(b + 1))), then one reduce.
+// Launching the partition in pieces gives the bits of one launch.
+int64_t col_stats_block_begin(int64_t nnz, int nparts, int b);
+cudaError_t launch_col_stats_blocks(int dtype, const int32_t* idx, const void* val, int64_t nnz, int32_t g,
+                                    double* partial, int nparts, int block0, int nblocks, cudaStream_t st);
+cudaError_t launch_col_stats_reduce(const double* partial, int nparts, int32_t g, double* out, cudaStream_t st,
+                                    int num_sms, int accumulate = 0);
 cudaError_t launch_transform_values(int in_dtype, int out_dtype, const int32_t* idx,
                                     const void* in, void* out, int64_t nnz, int mode,
                                     const double* mu, const double* inv_std,
@@ -164,6 +173,9 @@ cudaError_t launch_rmat_tc(int ld, const uint32_t* ent, const void* meta, int64_
 int launch_gram_tc(int64_t n, const CUtensorMap* qmap, double* part, int fmt, int* err, cudaStream_t st, int num_sms);
 size_t fwd_tc_smem_bytes(int ld);
 size_t rmat_tc_smem_bytes(int ld);
+// One block whose pipeline wait never completes: the bounded wait gives up
+// after its limit (about 1 s) and writes `code` to err.
+cudaError_t launch_wait_selftest(int* err, int code, cudaStream_t st);
 // Image of count floats: img[2 i] = round16(x_i), img[2 i + 1] = round16(x_i - img[2 i]).
 cudaError_t launch_split16(const float* in, int64_t count, uint16_t* img, int fmt, cudaStream_t st, int num_sms);
 

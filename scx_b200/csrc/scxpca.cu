@@ -400,6 +400,22 @@ void validate_params(const scxpca_csr* x, const scxpca_params* p) {
                                  std::to_string(kMaxK));
 }
 
+// Pieces a host matrix's entries are copied in (statistics overlap the copy).
+constexpr int kUploadPieces = 8;
+
+// Reduce the statistics partials already written to stats_part and bring
+// the column sums and sums of squares to the host.
+void stats_finish(scxpca_plan* pl, std::vector<double>& sums, std::vector<double>& sq) {
+  CK(launch_col_stats_reduce(pl->stats_part.as<double>(), pl->stats_parts, (int32_t)pl->g,
+                             pl->stats_out.as<double>(), pl->stream, pl->num_sms));
+  std::vector<double> host(2 * pl->g);
+  CK(cudaMemcpyAsync(host.data(), pl->stats_out.p, sizeof(double) * 2 * pl->g,
+                     cudaMemcpyDeviceToHost, pl->stream));
+  CK(cudaStreamSynchronize(pl->stream));
+  sums.assign(host.begin(), host.begin() + pl->g);
+  sq.assign(host.begin() + pl->g, host.end());
+}
+
 void stats_pass(scxpca_plan* pl, const void* val, int dtype, std::vector<double>& sums,
                 std::vector<double>& sq) {
   CK(launch_col_stats(dtype, pl->idx, val, pl->nnz, (int32_t)pl->g, pl->stats_part.as<double>(),
@@ -786,7 +802,7 @@ void setup_streaming(scxpca_plan* pl, const scxpca_csr* x, size_t limit) {
   phase_mark(SCXPCA_PHASE_UPLOAD, st);
 
   // ---- validation, input statistics (and gene counts) over the shards ----
-  pl->stats_parts = 2 * pl->num_sms;
+  pl->stats_parts = 4 * pl->num_sms;
   pl->stats_part.alloc(sizeof(double) * 2 * g * pl->stats_parts);
   pl->stats_out.alloc(sizeof(double) * 2 * g);
   DevBuf flags, counts;
@@ -1073,6 +1089,11 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
 
     // ---- resident CSR ----
     const bool dev_in = x->memory == SCXPCA_MEM_DEVICE;
+    pl->stats_parts = 4 * pl->num_sms;
+    pl->stats_part.alloc(sizeof(double) * 2 * g * pl->stats_parts);
+    pl->stats_out.alloc(sizeof(double) * 2 * g);
+    const void* vin = x->values;
+    bool stats_queued = false;  // the statistics blocks already ran under the copy
     if (dev_in) {
       pl->indptr = x->indptr;
       pl->idx = x->indices;
@@ -1080,16 +1101,44 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       pl->b_indptr.alloc(sizeof(int64_t) * (n + 1));
       pl->b_idx.alloc(sizeof(int32_t) * std::max<int64_t>(nnz, 1));
       CK(cudaMemcpyAsync(pl->b_indptr.p, x->indptr, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
-      if (nnz) CK(cudaMemcpyAsync(pl->b_idx.p, x->indices, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
       pl->indptr = pl->b_indptr.as<int64_t>();
       pl->idx = pl->b_idx.as<int32_t>();
-    }
-    const void* vin = x->values;
-    if (!dev_in && nnz) {
-      pl->b_stage.alloc(dtype_size(pl->in_dtype) * nnz);
-      CK(cudaMemcpyAsync(pl->b_stage.p, x->values, dtype_size(pl->in_dtype) * nnz,
-                         cudaMemcpyHostToDevice, st));
-      vin = pl->b_stage.p;
+      if (nnz) {
+        // The entries cross in pieces on a copy stream, each piece a run of
+        // whole blocks of the statistics partition; the plan's stream runs a
+        // piece's statistics blocks as soon as it has landed, so the column
+        // sums are computed under the copy and equal (bit for bit) those of
+        // one launch over the whole matrix.  The statistics kernel checks
+        // every index it reads; validation follows the copy.
+        const size_t vs = dtype_size(pl->in_dtype);
+        pl->b_stage.alloc(vs * nnz);
+        vin = pl->b_stage.p;
+        if (!pl->copy_stream) CK(cudaStreamCreateWithFlags(&pl->copy_stream, cudaStreamNonBlocking));
+        cudaStream_t cs = pl->copy_stream;
+        const int parts = pl->stats_parts;
+        const int pieces = std::min(kUploadPieces, parts);
+        std::vector<cudaEvent_t> landed(pieces + 1, nullptr);
+        for (auto& e : landed) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        CK(cudaEventRecord(landed[pieces], st));  // the buffers exist before the copies start
+        CK(cudaStreamWaitEvent(cs, landed[pieces], 0));
+        for (int c = 0; c < pieces; ++c) {
+          const int b0 = (int)((int64_t)c * parts / pieces), b1 = (int)((int64_t)(c + 1) * parts / pieces);
+          const int64_t e0 = col_stats_block_begin(nnz, parts, b0), e1 = col_stats_block_begin(nnz, parts, b1);
+          if (e1 > e0) {
+            CK(cudaMemcpyAsync(pl->b_idx.as<int32_t>() + e0, x->indices + e0, sizeof(int32_t) * (e1 - e0),
+                               cudaMemcpyHostToDevice, cs));
+            CK(cudaMemcpyAsync(static_cast<char*>(pl->b_stage.p) + vs * e0,
+                               static_cast<const char*>(x->values) + vs * e0, vs * (e1 - e0),
+                               cudaMemcpyHostToDevice, cs));
+          }
+          CK(cudaEventRecord(landed[c], cs));
+          CK(cudaStreamWaitEvent(st, landed[c], 0));
+          CK(launch_col_stats_blocks(pl->in_dtype, pl->idx, vin, nnz, (int32_t)g, pl->stats_part.as<double>(),
+                                     parts, b0, b1 - b0, st));
+        }
+        for (auto& e : landed) CK(cudaEventDestroy(e));  // released once the pending work completes
+        stats_queued = true;
+      }
     }
     phase_mark(SCXPCA_PHASE_UPLOAD, st);
 
@@ -1140,11 +1189,11 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
     phase_mark(SCXPCA_PHASE_VALIDATE, st);
 
     // ---- statistics of the input ----
-    pl->stats_parts = 2 * pl->num_sms;
-    pl->stats_part.alloc(sizeof(double) * 2 * g * pl->stats_parts);
-    pl->stats_out.alloc(sizeof(double) * 2 * g);
     std::vector<double> sx, sxx;
-    stats_pass(pl, vin, pl->in_dtype, sx, sxx);
+    if (stats_queued && !pl->rows_resorted)
+      stats_finish(pl, sx, sxx);
+    else
+      stats_pass(pl, vin, pl->in_dtype, sx, sxx);
     pl->mean_x.resize(g);
     for (int64_t j = 0; j < g; ++j) pl->mean_x[j] = sx[j] / (double)n;
     phase_mark(SCXPCA_PHASE_STATS, st);
@@ -2561,6 +2610,21 @@ int32_t scxpca_gaussian(int32_t device_ordinal, uint64_t seed, int64_t n_rows, i
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal));
     CK(launch_gaussian(seed, n_rows, n_cols, out, 0, nullptr, sms));
     CK(cudaStreamSynchronize(nullptr));
+  });
+}
+
+int32_t scxpca_wait_selftest(int32_t device_ordinal, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    DeviceGuard dg(device_ordinal);
+    constexpr int kSelftestSite = 99;
+    DevBuf code;
+    code.alloc(sizeof(int));
+    CK(cudaMemsetAsync(code.p, 0, sizeof(int), nullptr));
+    CK(launch_wait_selftest(code.as<int>(), kSelftestSite, nullptr));
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, code.p, sizeof(int), cudaMemcpyDeviceToHost, nullptr));
+    CK(cudaStreamSynchronize(nullptr));
+    if (e != 0) fail(SCXPCA_TIMEOUT, "pipeline wait timed out (site " + std::to_string(e) + ")");
   });
 }
 
