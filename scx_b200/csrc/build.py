@@ -34,6 +34,7 @@ SOURCES = [
     "noalloc.cu",
     "kernels_strict.cu",
     "kernels_preprocess.cu",
+    "kernels_wide.cu",
 ]
 EXTRA_SOURCES_OPTIONAL = ["kernels_tc.cu"]
 

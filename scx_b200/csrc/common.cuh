@@ -9,11 +9,16 @@
 namespace scx {
 
 constexpr int kWarp = 32;
-constexpr int kMaxK = 128;  // widest sketch (n_components + n_oversamples) supported
+constexpr int kMaxK = 128;      // widest sketch (n_components + n_oversamples) of the single-panel kernels
+constexpr int kPanel = 128;     // column panel of a wider sketch
+constexpr int kMaxKWide = 256;  // widest sketch supported (two panels)
 
 // Padded row stride of the tall (n_obs x k) and gene (n_vars x k) buffers:
-// k rounded up to a whole warp so each lane owns ld/32 columns.
-inline int64_t padded_k(int64_t k) { return (k + 31) / 32 * 32; }
+// k rounded up to a whole warp so each lane owns ld/32 columns; a sketch
+// wider than one panel is padded to whole panels.
+inline int64_t padded_k(int64_t k) {
+  return k <= kMaxK ? (k + 31) / 32 * 32 : (k + kPanel - 1) / kPanel * kPanel;
+}
 
 __device__ __forceinline__ float to_f32(float x) { return x; }
 __device__ __forceinline__ float to_f32(__nv_bfloat16 x) { return __bfloat162float(x); }

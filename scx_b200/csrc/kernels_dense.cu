@@ -68,6 +68,10 @@ __global__ void __launch_bounds__(256) k_gram(const T* __restrict__ A, int64_t n
 
 template <typename T>
 static cudaError_t gram_t(const T* A, int64_t n, int ld, double* part, int nparts, cudaStream_t st) {
+  if (ld > kMaxK) {
+    if constexpr (sizeof(T) == 4) return launch_gram_wide_f32(reinterpret_cast<const float*>(A), n, ld, part, nparts, st);
+    else return launch_gram_wide_f64(reinterpret_cast<const double*>(A), n, ld, part, nparts, st);
+  }
   note_launches(1);
   switch (ld) {
     case 32: k_gram<T, 32><<<nparts, 256, 0, st>>>(A, n, part); break;
@@ -252,6 +256,7 @@ __global__ void __launch_bounds__(T * T) k_cholesky(const double* __restrict__ G
 
 cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shift_on_fail,
                             double* R, double* Rinv, float* Rinv_f, int* status, cudaStream_t st) {
+  if (ld > kMaxK) return launch_cholesky_wide(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status, st);
   if (k > kMaxK) return cudaErrorInvalidValue;
   note_launches(1);
   // 16 x 16 threads with 4 x 4 entries each for k <= 64: every owner reads the
@@ -424,11 +429,21 @@ static cudaError_t tall_mm(const float* In, int64_t n, int K, int ldi, const flo
 
 cudaError_t launch_apply_right_f32(const float* In, int64_t n, int ld, const float* M, float* Out,
                                    cudaStream_t st, int num_sms) {
+  if (ld > kMaxK) {
+    // wider than one panel: in place for an upper-triangular M, else panel by panel into Out
+    if (In == Out) return launch_apply_upper_wide(Out, n, ld, M, st, num_sms);
+    for (int c0 = 0; c0 < ld; c0 += kPanel) {
+      cudaError_t e = launch_tall_mm_wide(In, n, ld, ld, M, ld, c0, kPanel, Out, ld, st, num_sms);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
   return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, nullptr, 0, st, num_sms);
 }
 
 cudaError_t launch_apply_right_split(const float* In, int64_t n, int ld, const float* M, float* Out,
                                      uint16_t* img, int fmt, cudaStream_t st, int num_sms) {
+  if (ld > kMaxK) return cudaErrorInvalidValue;  // the 16-bit image belongs to the tensor-core path (ld <= 128)
   return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, img, fmt, st, num_sms);
 }
 
@@ -463,6 +478,7 @@ __global__ void k_center_apply(const double* __restrict__ W, int64_t g, int ld,
 
 cudaError_t launch_center_apply(const double* W, int64_t g, int ld, const double* mu,
                                 const double* s, const double* M, double* Z, cudaStream_t st) {
+  if (ld > kMaxK) return launch_center_apply_wide(W, g, ld, mu, s, M, Z, st);
   size_t smem = (size_t)(ld * ld + 256) * sizeof(double);
   cudaFuncSetAttribute(k_center_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int rpb = 256 / ld;
@@ -544,15 +560,19 @@ cudaError_t launch_round_v(const double* A, int64_t g, int ld, const double* mu,
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, int k, int ld,
                                                  double* __restrict__ evals, double* __restrict__ evecs,
-                                                 double* __restrict__ Eglob, int* sweeps_out) {
+                                                 double* __restrict__ Eglob, double* __restrict__ Rglob,
+                                                 int* sweeps_out) {
   extern __shared__ double sm[];
   const int kk = (k + 1) & ~1;  // even number of columns; column k (if odd) is a zero dummy
   const int S = kk + 1;
   const int npair = kk / 2, m = kk - 1;
-  double* R = sm;                                              // [kk cols][S]: R[c * S + r]
-  uint16_t* sched = reinterpret_cast<uint16_t*>(sm + kk * S);  // [m][npair]: p | q << 8
-  double* V = (Eglob != nullptr) ? Eglob : sm + kk * S + (m * npair + 3) / 4;  // [kk cols][S]: R0, then V
-  __shared__ double colnorm[kMaxK];
+  // R, and V after it, in shared memory when they fit, else in the global
+  // scratch the launcher passes (a sketch wider than one panel)
+  double* R = Rglob != nullptr ? Rglob : sm;                   // [kk cols][S]: R[c * S + r]
+  double* sm_rest = Rglob != nullptr ? sm : sm + kk * S;
+  uint16_t* sched = reinterpret_cast<uint16_t*>(sm_rest);      // [m][npair]: p | q << 8
+  double* V = (Eglob != nullptr) ? Eglob : sm_rest + (m * npair + 3) / 4;  // [kk cols][S]: R0, then V
+  __shared__ double colnorm[kMaxKWide];
   __shared__ int done;
   __shared__ unsigned long long maxt_bits;  // largest |t| of the sweep (non-negative doubles order as integers)
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
@@ -718,17 +738,26 @@ cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, dou
   const size_t one = (size_t)kk * (kk + 1) * sizeof(double);
   const size_t sched = ((size_t)(kk - 1) * (kk / 2) + 3) / 4 * sizeof(double);
   // V lives in shared memory when both matrices fit, else in the scratch that
-  // follows evecs (the plan allocates ld * ld + ld * (ld + 1) doubles there).
+  // follows evecs (the plan allocates ld * ld + ld * (ld + 1) doubles there;
+  // ld * ld + 2 ld (ld + 1) for a sketch wider than one panel, whose R goes
+  // to global memory too).
+  if (kk > 256) return cudaErrorInvalidValue;  // the schedule packs a column pair into 8 + 8 bits
   double* eglob = nullptr;
+  double* rglob = nullptr;
   size_t smem = 2 * one + sched;
   if (smem > 200 * 1024) {
     eglob = evecs + (size_t)ld * ld;
     smem = one + sched;
   }
-  cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > 200 * 1024) {
+    rglob = evecs + (size_t)ld * ld + (size_t)ld * (ld + 1);
+    smem = sched;
+  }
+  cudaError_t e = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   const int warps = std::min(32, std::max(1, (kk / 2 + 1) / 2));  // one half-warp per column pair
   note_launches(1);
-  k_jacobi<<<1, 32 * warps, smem, st>>>(C, k, ld, evals, evecs, eglob, sweeps);
+  k_jacobi<<<1, 32 * warps, smem, st>>>(C, k, ld, evals, evecs, eglob, rglob, sweeps);
   return cudaGetLastError();
 }
 
@@ -736,35 +765,37 @@ cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, dou
 // Rayleigh-Ritz finish (single kernel, one block per gene row for the
 // components plus block 0 building M_emb).
 // ---------------------------------------------------------------------------
+// Components c0 .. c0 + ncc - 1 of nc per launch (E's columns staged in
+// shared memory); one launch takes them all when E[:, :nc] fits.
 __global__ void __launch_bounds__(128) k_ritz_finish(const double* __restrict__ B, int64_t g, int ld, int k,
-                                                     int nc, const double* __restrict__ evals,
+                                                     int nc, int c0, int ncc, const double* __restrict__ evals,
                                                      const double* __restrict__ E,
                                                      const double* __restrict__ Rinv2, double* __restrict__ sigma,
                                                      float* __restrict__ comps, float* __restrict__ M_emb) {
   extern __shared__ double sm[];
-  double* Es = sm;             // [ld][nc]
-  double* sg = sm + ld * nc;   // [nc]
-  for (int t = threadIdx.x; t < ld * nc; t += blockDim.x) {
-    const int l = t / nc, c = t - l * nc;
-    Es[t] = E[l * ld + c];
+  double* Es = sm;              // [ld][ncc]: columns c0 .. c0 + ncc - 1 of E
+  double* sg = sm + ld * ncc;   // [ncc]
+  for (int t = threadIdx.x; t < ld * ncc; t += blockDim.x) {
+    const int l = t / ncc, c = t - l * ncc;
+    Es[t] = E[l * ld + c0 + c];
   }
-  for (int c = threadIdx.x; c < nc; c += blockDim.x) sg[c] = sqrt(fmax(evals[c], 0.0));
+  for (int c = threadIdx.x; c < ncc; c += blockDim.x) sg[c] = sqrt(fmax(evals[c0 + c], 0.0));
   __syncthreads();
-  if (blockIdx.x == 0)
+  if (blockIdx.x == 0 && c0 == 0)
     for (int c = threadIdx.x; c < k; c += blockDim.x) sigma[c] = sqrt(fmax(evals[c], 0.0));
   // M_emb row l (one row per block in turn) = Rinv2[l, :] E[:, :nc] diag(sigma)
   for (int l = blockIdx.x; l < ld; l += gridDim.x)
-    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    for (int c = threadIdx.x; c < ncc; c += blockDim.x) {
       double acc = 0.0;
-      for (int m = 0; m < ld; ++m) acc = fma(Rinv2[l * ld + m], Es[m * nc + c], acc);
-      M_emb[l * nc + c] = (float)(acc * sg[c]);
+      for (int m = 0; m < ld; ++m) acc = fma(Rinv2[l * ld + m], Es[m * ncc + c], acc);
+      M_emb[l * nc + c0 + c] = (float)(acc * sg[c]);
     }
   // components[c][j] = (B E)[j][c] / sigma_c
   for (int64_t j = blockIdx.x; j < g; j += gridDim.x) {
-    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    for (int c = threadIdx.x; c < ncc; c += blockDim.x) {
       double acc = 0.0;
-      for (int l = 0; l < k; ++l) acc = fma(B[j * ld + l], Es[l * nc + c], acc);
-      comps[(int64_t)c * g + j] = sg[c] > 0.0 ? (float)(acc / sg[c]) : 0.f;
+      for (int l = 0; l < k; ++l) acc = fma(B[j * ld + l], Es[l * ncc + c], acc);
+      comps[(int64_t)(c0 + c) * g + j] = sg[c] > 0.0 ? (float)(acc / sg[c]) : 0.f;
     }
   }
 }
@@ -772,13 +803,18 @@ __global__ void __launch_bounds__(128) k_ritz_finish(const double* __restrict__ 
 cudaError_t launch_ritz_finish(const double* B, int64_t g, int ld, int k, int nc,
                                const double* evals, const double* evecs, const double* Rinv2,
                                double* sigma, float* components, float* M_emb, cudaStream_t st) {
-  size_t smem = (size_t)(ld * nc + nc) * sizeof(double);
-  cudaFuncSetAttribute(k_ritz_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  constexpr size_t kStage = 160 * 1024;  // shared bytes for the staged columns of E
+  const int ncc = (int)std::max<size_t>(1, std::min<size_t>(nc, kStage / ((size_t)(ld + 1) * sizeof(double))));
+  const size_t smem = (size_t)(ld * ncc + ncc) * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(k_ritz_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   // Few blocks: each stages E once and then takes a run of genes.
   const int grid = (int)std::max<int64_t>(std::min<int64_t>(g, 296), std::min<int64_t>(ld, 296));
-  note_launches(1);
-  k_ritz_finish<<<grid, 128, smem, st>>>(B, g, ld, k, nc, evals, evecs, Rinv2, sigma, components,
-                                         M_emb);
+  for (int c0 = 0; c0 < nc; c0 += ncc) {
+    note_launches(1);
+    k_ritz_finish<<<grid, 128, smem, st>>>(B, g, ld, k, nc, c0, std::min(ncc, nc - c0), evals, evecs, Rinv2,
+                                           sigma, components, M_emb);
+  }
   return cudaGetLastError();
 }
 
@@ -786,6 +822,14 @@ cudaError_t launch_ritz_finish(const double* B, int64_t g, int ld, int k, int nc
 cudaError_t launch_embed(const float* Q, int64_t n, int ld, int k, const float* M_emb, int nc,
                          float* U, cudaStream_t st, int num_sms) {
   (void)k;  // rows k..ld-1 of M_emb are zero
+  if (ld > kMaxK) {
+    for (int c0 = 0; c0 < nc; c0 += kPanel) {
+      cudaError_t e = launch_tall_mm_wide(Q, n, ld, ld, M_emb, nc, c0, std::min(kPanel, nc - c0), U, nc, st,
+                                          num_sms);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
   return tall_mm(Q, n, ld, ld, M_emb, nc, nc, U, nc, nullptr, 0, st, num_sms);
 }
 

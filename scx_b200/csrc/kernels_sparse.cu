@@ -126,9 +126,12 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* _
 // consecutive outputs (one per lane, coalesced); warp w sums the partials
 // b = w, w + 8, ... with four loads in flight, and warp 0 adds the eight warp
 // sums in warp order: a fixed order, so the result is deterministic.
+// With width > 0 the output is a column panel of a wider matrix: element i
+// goes to out[(i / width) * ldo + i % width].
 template <typename T>
 __global__ void __launch_bounds__(256) k_reduce_rows(const T* __restrict__ part, int nparts, int64_t len,
-                                                     double* __restrict__ out, int accumulate) {
+                                                     double* __restrict__ out, int accumulate, int width = 0,
+                                                     int ldo = 0) {
   __shared__ double red[8][33];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int64_t base = (int64_t)blockIdx.x * 32; base < len; base += (int64_t)gridDim.x * 32) {
@@ -151,10 +154,11 @@ __global__ void __launch_bounds__(256) k_reduce_rows(const T* __restrict__ part,
     red[w][lane] = acc;
     __syncthreads();
     if (w == 0 && i < len) {
-      double s = accumulate ? out[i] : 0.0;
+      const int64_t oi = width > 0 ? (i / width) * ldo + i % width : i;
+      double s = accumulate ? out[oi] : 0.0;
 #pragma unroll
       for (int u = 0; u < 8; ++u) s += red[u][lane];
-      out[i] = s;
+      out[oi] = s;
     }
     __syncthreads();
   }
@@ -503,6 +507,14 @@ cudaError_t launch_reduce_rows_f32(const float* part, int nparts, int64_t len, d
                                    int accumulate, cudaStream_t st, int num_sms) {
   note_launches(1);
   k_reduce_rows<float><<<grid_for(len, 32, num_sms), 256, 0, st>>>(part, nparts, len, out, accumulate);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_panel_f32(const float* part, int nparts, int64_t rows, int width, double* out, int ldo,
+                                    cudaStream_t st, int num_sms) {
+  const int64_t len = rows * width;
+  note_launches(1);
+  k_reduce_rows<float><<<grid_for(len, 32, num_sms), 256, 0, st>>>(part, nparts, len, out, 0, width, ldo);
   return cudaGetLastError();
 }
 

@@ -52,6 +52,22 @@ __device__ __forceinline__ void block_copy_async(void* smem, const void* gmem, i
     cp_async16(static_cast<char*>(smem) + o, static_cast<const char*>(gmem) + o);
 }
 
+// Copy `rows` rows of LD floats, row stride `lds` floats in global memory
+// (a column panel of a wider matrix), to consecutive rows in shared memory.
+// With lds == LD it is the contiguous copy.
+template <int LD>
+__device__ __forceinline__ void block_copy_rows_async(float* smem, const float* gmem, int rows, int lds) {
+  if (lds == LD) {
+    block_copy_async(smem, gmem, rows * LD * 4);
+    return;
+  }
+  constexpr int Q = LD / 4;  // 16-byte pieces per row
+  for (int o = threadIdx.x; o < rows * Q; o += blockDim.x) {
+    const int r = o / Q, q = o - r * Q;
+    cp_async16(smem + r * LD + 4 * q, gmem + (int64_t)r * lds + 4 * q);
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -154,7 +170,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_strict(const int64_t* __restrict
                                                        const int32_t* __restrict__ idx,
                                                        const ValT* __restrict__ val, int64_t n, int32_t g,
                                                        const float* __restrict__ V, const float* __restrict__ mc,
-                                                       float* __restrict__ Y) {
+                                                       float* __restrict__ Y, int lds) {
   constexpr int C = LD / 32;
   constexpr int32_t kDone = -1;
   extern __shared__ __align__(16) float vs[];  // [2][GC][LD]
@@ -180,14 +196,14 @@ __global__ void __launch_bounds__(256, 2) k_fwd_strict(const int64_t* __restrict
     wv[r] = p < end ? to_f32(val[p]) : 0.f;
   }
   const int nchunk = (g + GC - 1) / GC;
-  block_copy_async(vs, V, min(GC, (int)g) * LD * 4);
+  block_copy_rows_async<LD>(vs, V, min(GC, (int)g), lds);
   cp_async_commit();
   for (int ch = 0; ch < nchunk; ++ch) {
     const int g0 = ch * GC;
     const int g1 = min((int)g, g0 + GC);
     if (ch + 1 < nchunk) {
       const int n1 = min(GC, (int)g - g1);
-      block_copy_async(vs + ((ch + 1) & 1) * GC * LD, V + (int64_t)g1 * LD, n1 * LD * 4);
+      block_copy_rows_async<LD>(vs + ((ch + 1) & 1) * GC * LD, V + (int64_t)g1 * lds, n1, lds);
     }
     cp_async_commit();
     cp_async_wait<1>();
@@ -248,7 +264,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_strict(const int64_t* __restrict
     const int64_t row = row0 + r;
     if (row < n) {
 #pragma unroll
-      for (int c = 0; c < C; ++c) Y[row * LD + lane + 32 * c] = acc[r][c] - m[c];
+      for (int c = 0; c < C; ++c) Y[row * lds + lane + 32 * c] = acc[r][c] - m[c];
     }
   }
 }
@@ -269,7 +285,7 @@ __global__ void __launch_bounds__(256, 2) k_rmat_strict(const int64_t* __restric
                                                         const ValT* __restrict__ cval, int64_t n, int32_t g,
                                                         int32_t nslots, const int32_t* __restrict__ slot2gene,
                                                         int64_t tiles_per_range, const float* __restrict__ Q,
-                                                        float* __restrict__ part) {
+                                                        int lds, float* __restrict__ part) {
   constexpr int C = LD / 32;
   constexpr int T = kStrictTile;
   extern __shared__ __align__(16) float qs[];  // [2][T][LD]
@@ -289,7 +305,7 @@ __global__ void __launch_bounds__(256, 2) k_rmat_strict(const int64_t* __restric
     auto stage = [&](int64_t t, int buf) {
       const int64_t r0 = t * T;
       const int rows = (int)min((int64_t)T, n - r0);
-      block_copy_async(qs + buf * T * LD, Q + r0 * LD, rows * LD * 4);
+      block_copy_rows_async<LD>(qs + buf * T * LD, Q + r0 * lds, rows, lds);
     };
     stage(t0, 0);
     cp_async_commit();
@@ -439,7 +455,7 @@ cudaError_t launch_tile_csc(int dtype, const int64_t* indptr, const int32_t* idx
 
 template <int LD, typename ValT>
 static cudaError_t fwd_strict_t(const int64_t* indptr, const int32_t* idx, const void* val, int64_t n, int32_t g,
-                                const float* V, const float* mc, float* Y, cudaStream_t st) {
+                                const float* V, const float* mc, float* Y, int lds, cudaStream_t st) {
   constexpr int RPW = LD <= 64 ? 16 : 8;
   constexpr int GC = (8192 / LD) & ~7;
   const size_t smem = (size_t)2 * GC * LD * sizeof(float);
@@ -450,37 +466,40 @@ static cudaError_t fwd_strict_t(const int64_t* indptr, const int32_t* idx, const
   }
   const int64_t rows_per_block = 8 * RPW;
   const int64_t grid = (n + rows_per_block - 1) / rows_per_block;
-  kern<<<(unsigned)grid, 256, smem, st>>>(indptr, idx, static_cast<const ValT*>(val), n, g, V, mc, Y);
+  kern<<<(unsigned)grid, 256, smem, st>>>(indptr, idx, static_cast<const ValT*>(val), n, g, V, mc, Y, lds);
   note_launches(1);
   return cudaGetLastError();
 }
 
 template <typename ValT>
 static cudaError_t fwd_strict_v(int ld, const int64_t* indptr, const int32_t* idx, const void* val, int64_t n,
-                                int32_t g, const float* V, const float* mc, float* Y, cudaStream_t st) {
+                                int32_t g, const float* V, const float* mc, float* Y, int lds, cudaStream_t st) {
   switch (ld) {
-    case 32: return fwd_strict_t<32, ValT>(indptr, idx, val, n, g, V, mc, Y, st);
-    case 64: return fwd_strict_t<64, ValT>(indptr, idx, val, n, g, V, mc, Y, st);
-    case 96: return fwd_strict_t<96, ValT>(indptr, idx, val, n, g, V, mc, Y, st);
-    case 128: return fwd_strict_t<128, ValT>(indptr, idx, val, n, g, V, mc, Y, st);
+    case 32: return fwd_strict_t<32, ValT>(indptr, idx, val, n, g, V, mc, Y, lds, st);
+    case 64: return fwd_strict_t<64, ValT>(indptr, idx, val, n, g, V, mc, Y, lds, st);
+    case 96: return fwd_strict_t<96, ValT>(indptr, idx, val, n, g, V, mc, Y, lds, st);
+    case 128: return fwd_strict_t<128, ValT>(indptr, idx, val, n, g, V, mc, Y, lds, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t launch_fwd_strict(int dtype, int ld, const int64_t* indptr, const int32_t* idx, const void* val,
-                              int64_t n, int32_t g, const float* V, const float* mc, float* Y, cudaStream_t st) {
+                              int64_t n, int32_t g, const float* V, const float* mc, float* Y, cudaStream_t st,
+                              int lds) {
   if (n == 0) return cudaSuccess;
+  if (lds == 0) lds = ld;
+  if (lds < ld || (lds & 3)) return cudaErrorInvalidValue;
   switch (dtype) {
-    case 0: return fwd_strict_v<float>(ld, indptr, idx, val, n, g, V, mc, Y, st);
-    case 1: return fwd_strict_v<__nv_bfloat16>(ld, indptr, idx, val, n, g, V, mc, Y, st);
-    default: return fwd_strict_v<__half>(ld, indptr, idx, val, n, g, V, mc, Y, st);
+    case 0: return fwd_strict_v<float>(ld, indptr, idx, val, n, g, V, mc, Y, lds, st);
+    case 1: return fwd_strict_v<__nv_bfloat16>(ld, indptr, idx, val, n, g, V, mc, Y, lds, st);
+    default: return fwd_strict_v<__half>(ld, indptr, idx, val, n, g, V, mc, Y, lds, st);
   }
 }
 
 template <int LD, typename ValT>
 static cudaError_t rmat_strict_t(const int64_t* indptr, const int32_t* tptr, const uint8_t* cell, const void* cval,
                                  int64_t n, int32_t g, int32_t nslots, const int32_t* slot2gene, int ranges,
-                                 const float* Q, float* part, cudaStream_t st) {
+                                 const float* Q, int lds, float* part, cudaStream_t st) {
   constexpr int GPW = LD <= 64 ? 32 : 16;
   const size_t smem = (size_t)2 * kStrictTile * LD * sizeof(float);
   auto kern = k_rmat_strict<LD, GPW, ValT>;
@@ -493,7 +512,7 @@ static cudaError_t rmat_strict_t(const int64_t* indptr, const int32_t* tptr, con
   const int64_t per = (n_tiles + ranges - 1) / ranges;
   dim3 grid((unsigned)ranges, (unsigned)(nslots / (8 * GPW)));
   kern<<<grid, 256, smem, st>>>(indptr, tptr, cell, static_cast<const ValT*>(cval), n, g, nslots, slot2gene, per, Q,
-                                part);
+                                lds, part);
   note_launches(1);
   return cudaGetLastError();
 }
@@ -501,24 +520,30 @@ static cudaError_t rmat_strict_t(const int64_t* indptr, const int32_t* tptr, con
 template <typename ValT>
 static cudaError_t rmat_strict_v(int ld, const int64_t* indptr, const int32_t* tptr, const uint8_t* cell,
                                  const void* cval, int64_t n, int32_t g, int32_t nslots, const int32_t* slot2gene,
-                                 int ranges, const float* Q, float* part, cudaStream_t st) {
+                                 int ranges, const float* Q, int lds, float* part, cudaStream_t st) {
   switch (ld) {
-    case 32: return rmat_strict_t<32, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
-    case 64: return rmat_strict_t<64, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
-    case 96: return rmat_strict_t<96, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
-    case 128: return rmat_strict_t<128, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
+    case 32: return rmat_strict_t<32, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, lds, part, st);
+    case 64: return rmat_strict_t<64, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, lds, part, st);
+    case 96: return rmat_strict_t<96, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, lds, part, st);
+    case 128:
+      return rmat_strict_t<128, ValT>(indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, lds, part, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t launch_rmat_strict(int dtype, int ld, const int64_t* indptr, const int32_t* tptr, const uint8_t* cell,
                                const void* cval, int64_t n, int32_t g, int32_t nslots, const int32_t* slot2gene,
-                               int ranges, const float* Q, float* part, cudaStream_t st) {
+                               int ranges, const float* Q, float* part, cudaStream_t st, int lds) {
+  if (lds == 0) lds = ld;
+  if (lds < ld || (lds & 3)) return cudaErrorInvalidValue;
   switch (dtype) {
-    case 0: return rmat_strict_v<float>(ld, indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
+    case 0:
+      return rmat_strict_v<float>(ld, indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, lds, part, st);
     case 1:
-      return rmat_strict_v<__nv_bfloat16>(ld, indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
-    default: return rmat_strict_v<__half>(ld, indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, part, st);
+      return rmat_strict_v<__nv_bfloat16>(ld, indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, lds,
+                                          part, st);
+    default:
+      return rmat_strict_v<__half>(ld, indptr, tptr, cell, cval, n, g, nslots, slot2gene, ranges, Q, lds, part, st);
   }
 }
 

@@ -50,6 +50,10 @@ cudaError_t launch_spmm_t(int dtype, int ld, const int64_t* indptr, const int32_
                           cudaStream_t st);
 cudaError_t launch_reduce_rows_f32(const float* part, int nparts, int64_t len, double* out,
                                    int accumulate, cudaStream_t st, int num_sms);
+// The same over partials of a column panel: part[b] is rows x width; row r
+// of the sum goes to out + r * ldo (a panel of a wider matrix).
+cudaError_t launch_reduce_panel_f32(const float* part, int nparts, int64_t rows, int width, double* out, int ldo,
+                                    cudaStream_t st, int num_sms);
 
 // ---- CUDA-core SpMM pair in a fixed summation order (kernels_strict.cu) ----
 constexpr int kStrictTile = 128;  // rows per tile of the tile-CSC copy (a power of two <= 256)
@@ -65,13 +69,18 @@ cudaError_t launch_gene_counts(const int32_t* idx, int64_t nnz, int32_t* counts,
 cudaError_t launch_tile_csc(int dtype, const int64_t* indptr, const int32_t* idx, const void* val, int64_t n,
                             const int32_t* gene2slot, int32_t nslots, int32_t* tptr, uint8_t* cell, void* cval,
                             cudaStream_t st, int num_sms);
-// Y (n x ld) = P V - 1 mc^T (mc may be null) from a row-sorted CSR; ld in {32, 64, 96, 128}.
+// Y (n x ld) = P V - 1 mc^T (mc may be null) from a row-sorted CSR.  `ld` is
+// the width of the column panel taken (32, 64, 96 or 128); V, mc and Y point
+// at its first column and `lds` is the row stride of V and Y in floats
+// (0: lds = ld, the whole matrix).
 cudaError_t launch_fwd_strict(int dtype, int ld, const int64_t* indptr, const int32_t* idx, const void* val,
-                              int64_t n, int32_t g, const float* V, const float* mc, float* Y, cudaStream_t st);
-// part[range][g][ld] = partial P^T Q over the row tiles of each of `ranges` contiguous ranges.
+                              int64_t n, int32_t g, const float* V, const float* mc, float* Y, cudaStream_t st,
+                              int lds = 0);
+// part[range][g][ld] = partial P^T Q over the row tiles of each of `ranges`
+// contiguous ranges; Q is a column panel of width ld and row stride lds (0: ld).
 cudaError_t launch_rmat_strict(int dtype, int ld, const int64_t* indptr, const int32_t* tptr, const uint8_t* cell,
                                const void* cval, int64_t n, int32_t g, int32_t nslots, const int32_t* slot2gene,
-                               int ranges, const float* Q, float* part, cudaStream_t st);
+                               int ranges, const float* Q, float* part, cudaStream_t st, int lds = 0);
 cudaError_t launch_reduce_rows_f64(const double* part, int nparts, int64_t len, double* out,
                                    int accumulate, cudaStream_t st, int num_sms);
 
@@ -85,6 +94,19 @@ cudaError_t launch_validate_csr(int dtype, const int64_t* indptr, const int32_t*
 // Sort every row by gene in place (values follow), one warp per row.
 cudaError_t launch_sort_rows(int dtype, const int64_t* indptr, int32_t* idx, void* val,
                              int64_t n, cudaStream_t st, int num_sms);
+
+// ---- sketches wider than one 128-column panel (kernels_wide.cu; ld = 256) ----
+cudaError_t launch_gram_wide_f32(const float* A, int64_t n, int ld, double* part, int nparts, cudaStream_t st);
+cudaError_t launch_gram_wide_f64(const double* A, int64_t n, int ld, double* part, int nparts, cudaStream_t st);
+cudaError_t launch_cholesky_wide(const double* G, int k, int ld, double tau, int shift_on_fail, double* R,
+                                 double* Rinv, float* Rinv_f, int* status, cudaStream_t st);
+// Out[:, c0 .. c0 + cnt) = In[:, :K] M[:K, c0 .. c0 + cnt), cnt <= 128.
+cudaError_t launch_tall_mm_wide(const float* In, int64_t n, int K, int ldi, const float* M, int ldm, int c0,
+                                int cnt, float* Out, int ldo, cudaStream_t st, int num_sms);
+// A <- A M in place for an upper-triangular M (ld x ld).
+cudaError_t launch_apply_upper_wide(float* A, int64_t n, int ld, const float* M, cudaStream_t st, int num_sms);
+cudaError_t launch_center_apply_wide(const double* W, int64_t g, int ld, const double* mu, const double* s,
+                                     const double* M, double* Z, cudaStream_t st);
 
 // ---- dense side (kernels_dense.cu) ----
 // Gram partials of a tall row-major matrix A (n x ld, first k columns used):

@@ -394,10 +394,10 @@ void validate_params(const scxpca_csr* x, const scxpca_params* p) {
   if (!x->indptr) fail(SCXPCA_INVALID_ARGUMENT, "null indptr");
   if (!std::isfinite(p->clip_max)) fail(SCXPCA_INVALID_ARGUMENT, "clip_max must be finite");
   int64_t k = std::min({p->n_components + p->n_oversamples, x->n_vars, x->n_obs});
-  if (k > kMaxK)
+  if (k > kMaxKWide)
     fail(SCXPCA_UNSUPPORTED, "sketch width k = min(n_components + n_oversamples, n_vars, n_obs) = " +
                                  std::to_string(k) + " exceeds the supported maximum " +
-                                 std::to_string(kMaxK));
+                                 std::to_string(kMaxKWide));
 }
 
 // Pieces a host matrix's entries are copied in (statistics overlap the copy).
@@ -514,6 +514,10 @@ void ensure_rbp(scxpca_plan* pl) {
 // Tile-CSC copy of the working matrix for the CUDA-core transposed product:
 // per-gene stored-entry counts -> balanced slot assignment (host) -> the
 // copy, and the per-range partial buffer.
+// Column panel the CUDA-core SpMM pair takes per launch: the whole sketch up
+// to 128 columns, else 128-column panels of it.
+int panel_width(const scxpca_plan* pl) { return (int)std::min<int64_t>(pl->ld, kPanel); }
+
 void build_tile_csc(scxpca_plan* pl) {
   cudaStream_t st = pl->stream;
   const int64_t n = pl->n, g = pl->g, nnz = pl->nnz;
@@ -525,7 +529,8 @@ void build_tile_csc(scxpca_plan* pl) {
   CK(cudaMemcpyAsync(hc.data(), counts.p, sizeof(int32_t) * g, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   std::vector<int32_t> gene2slot, slot2gene;
-  strict_assign_slots(hc, (int)pl->ld, gene2slot, slot2gene);
+  const int pw = panel_width(pl);
+  strict_assign_slots(hc, pw, gene2slot, slot2gene);
   DevBuf d_g2s;
   d_g2s.alloc(sizeof(int32_t) * g);
   CK(cudaMemcpyAsync(d_g2s.p, gene2slot.data(), sizeof(int32_t) * g, cudaMemcpyHostToDevice, st));
@@ -539,9 +544,9 @@ void build_tile_csc(scxpca_plan* pl) {
   CK(launch_tile_csc(pl->dtype, pl->indptr, pl->idx, pl->val, n, d_g2s.as<int32_t>(), pl->nslots,
                      pl->csc_tptr.as<int32_t>(), pl->csc_cell.as<uint8_t>(), pl->csc_val.p, st, pl->num_sms));
   // ranges: about four blocks per SM over all gene blocks, for balance
-  const int gblocks = pl->nslots / (8 * strict_genes_per_warp((int)pl->ld));
+  const int gblocks = pl->nslots / (8 * strict_genes_per_warp(pw));
   pl->strict_ranges = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, (4 * pl->num_sms + gblocks - 1) / gblocks));
-  pl->wpart.alloc(sizeof(float) * (size_t)pl->strict_ranges * g * pl->ld);
+  pl->wpart.alloc(sizeof(float) * (size_t)pl->strict_ranges * g * pw);
   CK(cudaStreamSynchronize(st));  // the host vectors above go out of scope
 }
 
@@ -993,7 +998,7 @@ void alloc_work_buffers(scxpca_plan* pl) {
   pl->Rinv_f.alloc(sizeof(float) * ld * ld);
   pl->R2inv.alloc(sizeof(double) * ld * ld);
   pl->evals.alloc(sizeof(double) * ld);
-  pl->evecs.alloc(sizeof(double) * (ld * ld + ld * (ld + 1)));  // + eigensolver scratch
+  pl->evecs.alloc(sizeof(double) * (ld * ld + 2 * ld * (ld + 1)));  // + eigensolver scratch
   pl->sigma.alloc(sizeof(double) * ld);
   pl->comps.alloc(sizeof(float) * pl->nc * g);
   pl->M_emb.alloc(sizeof(float) * ld * pl->nc);
@@ -1070,6 +1075,9 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       const char* res_env = getenv("SCXPCA_RESIDENT");
       const bool force_stream = res_env && res_env[0] == '0';
       if (x->memory != SCXPCA_MEM_DEVICE && !aff && !pf && (force_stream || with_headroom > (double)limit)) {
+        if (pl->k > kMaxK)
+          fail(SCXPCA_UNSUPPORTED, "a sketch wider than " + std::to_string(kMaxK) +
+                                       " columns needs the matrix resident on the device (it is not streamed)");
         setup_streaming(pl, x, limit);
         phase_mark(SCXPCA_PHASE_BUFFERS, st);
         CK(cudaStreamSynchronize(st));
@@ -1181,7 +1189,7 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
       // most 128 gene chunks (8,192 genes); SCXPCA_TC=0 forces the CUDA cores.
       const char* env = getenv("SCXPCA_TC");
       const bool tc_allowed = !(env && env[0] == '0');
-      pl->use_tc = tc_allowed && pl->dtype != SCXPCA_F32 && !duplicates && g <= 64 * 128;
+      pl->use_tc = tc_allowed && pl->dtype != SCXPCA_F32 && !duplicates && g <= 64 * 128 && pl->k <= kMaxK;
       if (pl->use_tc) pl->ld = (pl->k + 63) / 64 * 64;
       pl->fmt16 = pl->dtype == SCXPCA_BF16 ? 1 : 0;
     }
@@ -1351,9 +1359,12 @@ scxpca_plan* create_plan(const scxpca_csr* x, const scxpca_params* p, const Affi
     pl->nchunks = (int)std::min<int64_t>(pl->nchunks, n);
     pl->rows_per_chunk = (n + pl->nchunks - 1) / pl->nchunks;
     if (!pl->use_tc) {
-      pl->nslots = strict_slot_count(g, (int)ld);
+      pl->nslots = strict_slot_count(g, panel_width(pl));
       pl->strict_csc = strict_tile_smem_bytes(pl->nslots) <= kStatsSmemMax;
     }
+    if (pl->ld > kMaxK && !pl->strict_csc)
+      fail(SCXPCA_UNSUPPORTED, "a sketch wider than " + std::to_string(kMaxK) + " columns needs the tile-CSC "
+                               "copy, whose per-gene offsets exceed shared memory at n_vars = " + std::to_string(g));
     if (pl->strict_csc) build_tile_csc(pl);
     else if (!pl->use_tc) ensure_rbp(pl);
     phase_mark(SCXPCA_PHASE_PACK, st);
@@ -1486,6 +1497,23 @@ void rmatmat_raw(scxpca_plan* pl, float* A, int split) {
     stage_end(pl, SCXPCA_STAGE_REDUCE, s);
     return;
   }
+  if (pl->strict_csc && pl->ld > kMaxK) {
+    // one 128-column panel of A per launch, each panel's partials reduced
+    // into its columns of W
+    const int ld = (int)pl->ld, pw = panel_width(pl);
+    for (int c0 = 0; c0 < ld; c0 += pw) {
+      int s = stage_begin(pl);
+      CK(launch_rmat_strict(pl->dtype, pw, pl->indptr, pl->csc_tptr.as<int32_t>(), pl->csc_cell.as<uint8_t>(),
+                            pl->csc_val.p, pl->n, (int32_t)pl->g, pl->nslots, pl->d_slot2gene.as<int32_t>(),
+                            pl->strict_ranges, A + c0, pl->wpart.as<float>(), st, ld));
+      stage_end(pl, SCXPCA_STAGE_TRANSPOSE, s);
+      s = stage_begin(pl);
+      CK(launch_reduce_panel_f32(pl->wpart.as<float>(), pl->strict_ranges, pl->g, pw, pl->W.as<double>() + c0, ld,
+                                 st, pl->num_sms));
+      stage_end(pl, SCXPCA_STAGE_REDUCE, s);
+    }
+    return;
+  }
   int s = stage_begin(pl);
   int parts = pl->nchunks;
   if (pl->strict_csc) {
@@ -1533,8 +1561,10 @@ void forward(scxpca_plan* pl, bool f32 = true) {
     return;
   }
   int s = stage_begin(pl);
-  CK(launch_fwd_strict(pl->dtype, (int)pl->ld, pl->indptr, pl->idx, pl->val, pl->n, (int32_t)pl->g,
-                       pl->V.as<float>(), pl->centered ? pl->mc.as<float>() : nullptr, pl->Y.as<float>(), st));
+  const int ld = (int)pl->ld, pw = panel_width(pl);
+  for (int c0 = 0; c0 < ld; c0 += pw)
+    CK(launch_fwd_strict(pl->dtype, pw, pl->indptr, pl->idx, pl->val, pl->n, (int32_t)pl->g, pl->V.as<float>() + c0,
+                         pl->centered ? pl->mc.as<float>() + c0 : nullptr, pl->Y.as<float>() + c0, st, ld));
   stage_end(pl, SCXPCA_STAGE_FORWARD, s);
 }
 
@@ -1777,6 +1807,8 @@ void backward(scxpca_plan* pl, const float* S, const float* GS, int iters, float
   if (pl->streaming)
     fail(SCXPCA_UNSUPPORTED, "the backward pass needs the matrix resident on the device; this plan streams it "
                              "from host memory");
+  if (pl->ld > kMaxK)
+    fail(SCXPCA_UNSUPPORTED, "the backward pass takes sketches of at most " + std::to_string(kMaxK) + " columns");
   if (iters < 0 || iters > 1000) fail(SCXPCA_INVALID_ARGUMENT, "solve_iterations must be in [0, 1000]");
   if (!S || !GS || !gvals) fail(SCXPCA_INVALID_ARGUMENT, "null scores, grad_scores or grad_values");
   pl->run_valid = false;

@@ -92,18 +92,20 @@ def test_argument_validation_statuses(kw, status, msg):
 
 
 def test_sketch_width_limit_is_reported():
+    """k = min(n_components + n_oversamples, n_vars, n_obs) up to 256 is taken
+    (two 128-column panels); a wider sketch is reported before any device work."""
     lib = _lib.load()
-    n, g = 300, 300
+    n, g = 400, 400
     indptr = np.zeros(n + 1, dtype=np.int64)
     csr = _lib.Csr(n, g, 0, indptr.ctypes.data, None, None, 0, 0)
     p = _lib.Params()
-    p.n_components, p.n_oversamples = 130, 10
-    emb = np.zeros((n, 130), dtype=np.float32)
+    p.n_components, p.n_oversamples = 250, 10
+    emb = np.zeros((n, 250), dtype=np.float32)
     res = _lib.Result()
     res.embeddings = emb.ctypes.data
     err = _lib.errbuf()
     st = lib.scxpca_randomized(C.byref(csr), C.byref(p), C.byref(res), err, len(err))
-    assert st == _lib.UNSUPPORTED and "128" in err.value.decode()
+    assert st == _lib.UNSUPPORTED and "256" in err.value.decode()
 
 
 def test_python_layer_maps_statuses():
