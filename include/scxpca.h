@@ -87,7 +87,10 @@ typedef struct {
  * and pyscx.accel.pca (pyscx/src/accel/pca.rs:573-605), plus the explicit
  * test matrix and per-gene scaling, which have no reference counterpart. */
 typedef struct {
-  int64_t n_components;
+  int64_t n_components;   /* the sketch k = min(n_components + n_oversamples,
+                             n_vars, n_obs) may be up to 256; wider returns
+                             SCXPCA_UNSUPPORTED.  128 < k <= 256 runs on the
+                             CUDA cores, resident plans only, no backward. */
   int64_t n_oversamples;
   int64_t n_power_iterations;
   int32_t zero_center;    /* subtract per-gene means implicitly */

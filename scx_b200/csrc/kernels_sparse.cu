@@ -20,35 +20,47 @@ namespace scx {
 // (scx-sparse/src/csr.rs:570-580).
 //
 // Block b owns the stored entries [b * per, (b + 1) * per) and walks them in
-// windows of kStatsWindow entries staged in shared memory.  Its kStatsWarps
-// warps share one FP64 accumulator pair per gene, and warp w owns the genes
-// j with (j - lo) % kStatsWarps == w: every warp scans the whole window
-// (32 consecutive entries per step) and adds only its own genes, so no two
-// warps touch one accumulator and no atomics are needed.  Inside one step two
-// lanes may name the same gene only across a row boundary (a sorted row
-// holds a gene once); the step is cut into runs of strictly increasing gene
-// index, within which every gene is distinct, and the runs are applied one
-// after another in lane order.  Unsorted rows and duplicates are handled the
-// same way.  Genes beyond the shared-memory accumulator take further passes
-// over the block's entries, kStatsPassGenes at a time.  Each block writes one
-// partial row pair [sum | sum sq] (n_vars each); reduce_rows_f64 adds the
-// partials in block order.
+// windows of kStatsWindow entries.  Its kStatsWarps warps share one FP64
+// accumulator pair per gene, and warp w owns the genes j with (j - lo) %
+// kStatsWarps == w, so no two warps touch one accumulator and no atomics are
+// needed.  Each window is read into registers one window ahead (thread t of
+// warp w holds the window's 32-entry steps w, w + 4, ...), then bucketed by
+// owning warp with a stable partition (ballot counts per step, one scan, a
+// scatter into shared memory), so each warp then walks only its own entries,
+// in window order.  Inside one 32-entry step of a bucket two lanes may name
+// the same gene only across a row boundary (a sorted row holds a gene once);
+// the step is cut into runs of strictly increasing gene index, applied one
+// after another in lane order.  Every gene's adds therefore happen in entry
+// order, whatever the rows look like (unsorted rows and duplicates included).
+// Genes beyond the shared-memory accumulator take further passes over the
+// block's entries, kStatsPassGenes at a time.  Each block writes one partial
+// row pair [sum | sum sq] (n_vars each); reduce_rows_f64 adds the partials in
+// block order.
 // ---------------------------------------------------------------------------
 constexpr int kStatsWarps = 4;
 constexpr int kStatsWindow = 1024;
-constexpr int kStatsPassGenes = (int)((kStatsSmemMax - (size_t)kStatsWindow * 8) / 16);
+constexpr int kStatsSteps = kStatsWindow / 32;  // 32-entry steps per window
+// shared bytes besides the accumulators: the bucketed window (index + value)
+// and the per-step bucket offsets
+constexpr size_t kStatsWindowBytes = (size_t)kStatsWindow * 8 + (size_t)kStatsSteps * kStatsWarps * 4 + 64;
+constexpr int kStatsPassGenes = (int)((kStatsSmemMax - kStatsWindowBytes) / 16);
+static_assert(kStatsSteps == 32, "the bucket scan gives one window step to each lane of a warp");
+static_assert(kStatsSteps % kStatsWarps == 0, "every warp holds the same number of window steps");
 
 template <typename ValT>
 __global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* __restrict__ idx,
                                                                 const ValT* __restrict__ val, int64_t nnz,
                                                                 int32_t g, int32_t pass_genes, int nparts,
                                                                 int block0, double* __restrict__ partial) {
-  extern __shared__ double sm[];  // [2][pass_genes] accumulators, then the window
+  extern __shared__ double sm[];  // [2][pass_genes] accumulators, then the bucketed window
   double* acc = sm;
-  int32_t* w_idx = reinterpret_cast<int32_t*>(sm + 2 * (int64_t)pass_genes);
-  float* w_val = reinterpret_cast<float*>(w_idx + kStatsWindow);
-  constexpr int kPer = kStatsWindow / (kStatsWarps * 32);
+  int32_t* b_idx = reinterpret_cast<int32_t*>(sm + 2 * (int64_t)pass_genes);
+  float* b_val = reinterpret_cast<float*>(b_idx + kStatsWindow);
+  int32_t* base = reinterpret_cast<int32_t*>(b_val + kStatsWindow);  // [kStatsSteps][kStatsWarps]
+  int32_t* qbase = base + kStatsSteps * kStatsWarps;                 // [kStatsWarps + 1]
+  constexpr int kPer = kStatsSteps / kStatsWarps;                    // steps per warp
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lanemask_lt = (1u << lane) - 1u;
   const unsigned lanemask_le = 0xffffffffu >> (31 - lane);
   // partition block b of nparts owns entries [b per, (b + 1) per); this
   // launch runs blocks block0 .. block0 + gridDim.x - 1 of it
@@ -60,41 +72,88 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* _
   for (int32_t lo = 0; lo < g; lo += pass_genes) {
     const int32_t gp = min(pass_genes, g - lo);
     for (int i = threadIdx.x; i < 2 * gp; i += blockDim.x) acc[i] = 0.0;
-    // the window's entries are loaded into registers one window ahead, so
-    // their loads are in flight while the block works on the previous window
+    // step u of this thread is the window's step kStatsWarps u + warp
     int32_t ri[kPer];
     float rv[kPer];
     auto load = [&](int64_t w) {
       const int c = (int)min((int64_t)kStatsWindow, e - w);
 #pragma unroll
       for (int u = 0; u < kPer; ++u) {
-        const int t = threadIdx.x + u * kStatsWarps * 32;
+        const int t = (kStatsWarps * u + warp) * 32 + lane;
         ri[u] = t < c ? __ldg(idx + w + t) : -1;
         rv[u] = t < c ? to_f32(val[w + t]) : 0.f;
       }
     };
     if (s < e) load(s);
     for (int64_t w0 = s; w0 < e; w0 += kStatsWindow) {
-      const int cnt = (int)min((int64_t)kStatsWindow, e - w0);
-      __syncthreads();  // the previous window is consumed (and the accumulators zeroed)
+      // owning warp of each held entry (kStatsWarps: not in this pass)
+      int own[kPer];
 #pragma unroll
       for (int u = 0; u < kPer; ++u) {
-        const int t = threadIdx.x + u * kStatsWarps * 32;
-        w_idx[t] = ri[u];
-        w_val[t] = rv[u];
+        const int32_t jr = ri[u] - lo;
+        own[u] = (ri[u] >= 0 && jr >= 0 && jr < gp) ? jr % kStatsWarps : kStatsWarps;
+      }
+      __syncthreads();  // the previous window's buckets are consumed (and the accumulators zeroed)
+      // per-step bucket sizes
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int step = kStatsWarps * u + warp;
+#pragma unroll
+        for (int q = 0; q < kStatsWarps; ++q) {
+          const unsigned m = __ballot_sync(0xffffffffu, own[u] == q);
+          if (lane == 0) base[step * kStatsWarps + q] = __popc(m);
+        }
       }
       __syncthreads();
+      // exclusive scan over the steps, bucket by bucket (warp 0; lane = step)
+      if (warp == 0) {
+        int cnt[kStatsWarps], inc[kStatsWarps];
+#pragma unroll
+        for (int q = 0; q < kStatsWarps; ++q) {
+          cnt[q] = base[lane * kStatsWarps + q];
+          inc[q] = cnt[q];
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc[q], o);
+            if (lane >= o) inc[q] += y;
+          }
+        }
+        int off = 0;
+#pragma unroll
+        for (int q = 0; q < kStatsWarps; ++q) {
+          const int total = __shfl_sync(0xffffffffu, inc[q], 31);
+          base[lane * kStatsWarps + q] = off + inc[q] - cnt[q];
+          if (lane == 0) qbase[q] = off;
+          off += total;
+        }
+        if (lane == 0) qbase[kStatsWarps] = off;
+      }
+      __syncthreads();
+      // stable scatter into the buckets
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int step = kStatsWarps * u + warp;
+        const int q = own[u];
+        const unsigned m = __match_any_sync(0xffffffffu, q);
+        if (q < kStatsWarps) {
+          const int pos = base[step * kStatsWarps + q] + __popc(m & lanemask_lt);
+          b_idx[pos] = ri[u] - lo;
+          b_val[pos] = rv[u];
+        }
+      }
+      __syncthreads();
+      // the next window's loads are in flight while the buckets are applied
       if (w0 + kStatsWindow < e) load(w0 + kStatsWindow);
-      for (int b = 0; b < cnt; b += 32) {
-        const int t = b + lane;
-        const int32_t j = t < cnt ? w_idx[t] : -1;
-        const int32_t jl = __shfl_up_sync(0xffffffffu, j, 1);
-        const unsigned starts = __ballot_sync(0xffffffffu, lane > 0 && t < cnt && j <= jl);
-        const int32_t jr = j - lo;
-        const bool own = t < cnt && jr >= 0 && jr < gp && (jr % kStatsWarps) == warp;
+      const int q0 = qbase[warp], q1 = qbase[warp + 1];
+      for (int p0 = q0; p0 < q1; p0 += 32) {
+        const int t = p0 + lane;
+        const bool in = t < q1;
+        const int32_t jr = in ? b_idx[t] : -1;
+        const int32_t jl = __shfl_up_sync(0xffffffffu, jr, 1);
+        const unsigned starts = __ballot_sync(0xffffffffu, lane > 0 && in && jr <= jl);
+        const double x = in ? (double)b_val[t] : 0.0;
         if (starts == 0) {
-          if (own) {
-            const double x = (double)w_val[t];
+          if (in) {
             acc[jr] += x;
             acc[gp + jr] += x * x;
           }
@@ -103,8 +162,7 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* _
           const int run = __popc(starts & lanemask_le);
           const int runs = __popc(starts) + 1;
           for (int r = 0; r < runs; ++r) {
-            if (own && run == r) {
-              const double x = (double)w_val[t];
+            if (in && run == r) {
               acc[jr] += x;
               acc[gp + jr] += x * x;
             }
@@ -355,7 +413,7 @@ static cudaError_t col_stats_blocks_t(const int32_t* idx, const void* val, int64
   if (nblocks <= 0) return cudaSuccess;
   const ValT* v = static_cast<const ValT*>(val);
   const int32_t pass_genes = std::min<int32_t>(g, kStatsPassGenes);
-  const size_t smem = (size_t)2 * pass_genes * sizeof(double) + (size_t)kStatsWindow * 8;
+  const size_t smem = (size_t)2 * pass_genes * sizeof(double) + kStatsWindowBytes;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_col_stats<ValT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

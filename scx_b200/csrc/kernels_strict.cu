@@ -335,23 +335,15 @@ __global__ void __launch_bounds__(256, 2) k_rmat_strict(const int64_t* __restric
             cl = __ldg(cell + tb + q);
             x = to_f32(cval[tb + q]);
           }
-          // four entries per iteration (lanes past cnt hold x = 0 and cell 0,
-          // a staged row, so their zero products add nothing)
-          for (int u = 0; u < cnt; u += 4) {
-            float xs[4];
-            const float* qr[4];
+          // one entry per step: the jj loop is unrolled over the warp's
+          // GPW slots, so a wider body here would overflow the instruction
+          // cache (measured: four entries per step ran 30 % slower)
+          for (int u = 0; u < cnt; ++u) {
+            const int cu = __shfl_sync(0xffffffffu, cl, u) & (T - 1);
+            const float xu = __shfl_sync(0xffffffffu, x, u);
+            const float* qr = qt + cu * LD;
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-              const int uv = min(u + v, 31);
-              const int cu = __shfl_sync(0xffffffffu, cl, uv) & (T - 1);
-              const float xu = __shfl_sync(0xffffffffu, x, uv);
-              xs[v] = u + v < cnt ? xu : 0.f;
-              qr[v] = qt + cu * LD;
-            }
-#pragma unroll
-            for (int v = 0; v < 4; ++v)
-#pragma unroll
-              for (int c = 0; c < C; ++c) acc[jj][c] = fmaf(xs[v], qr[v][32 * c], acc[jj][c]);
+            for (int c = 0; c < C; ++c) acc[jj][c] = fmaf(xu, qr[32 * c], acc[jj][c]);
           }
         }
       }
