@@ -254,133 +254,14 @@ __global__ void __launch_bounds__(T * T) k_cholesky(const double* __restrict__ G
     }
 }
 
-// ---------------------------------------------------------------------------
-// The same elimination with the augmented matrix in shared memory and few
-// threads: M holds A's upper triangle (c >= a) and X's strict lower triangle
-// (c < a) in one k x k array.  Warp w updates rows a = j + 1 + w, j + 1 + w +
-// NW, ... of step j, its lanes over the columns; warp 0 takes row j + 1 first
-// and its lane 0 computes the next pivot as soon as that row's diagonal entry
-// is updated.  Every entry receives the same operations in the same order as
-// in k_cholesky (A_ac -= (A_ja / d_j) A_jc, X_ac -= (A_ja / d_j) X_jc with
-// X_jj = 1), so the factors are bit-identical; a step issues far fewer
-// instructions than 1024 threads walking their register tiles do.
-// ---------------------------------------------------------------------------
-template <int NW>
-__global__ void __launch_bounds__(NW * 32) k_cholesky_rows(const double* __restrict__ G, int k, int ld, double tau,
-                                                           int shift_on_fail, double* __restrict__ R,
-                                                           double* __restrict__ Rinv, float* __restrict__ Rinv_f,
-                                                           int* __restrict__ status) {
-  extern __shared__ double smc[];
-  double* M = smc;                  // [k][ld]
-  double* pv_rinv = M + k * ld;     // [k]
-  double* pv_di = pv_rinv + k;      // [k]
-  double* dg = pv_di + k;           // [k]
-  int* pv_ok = reinterpret_cast<int*>(dg + k);
-  __shared__ double maxdiag_s;
-  __shared__ int fail_s;
-  constexpr int NT = NW * 32;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int j = tid; j < k; j += NT) dg[j] = G[(int64_t)j * ld + j];
-  for (int t = tid; t < ld * ld; t += NT) {
-    R[t] = 0.0;
-    Rinv[t] = 0.0;
-    Rinv_f[t] = 0.f;
-  }
-  __syncthreads();
-  if (tid < 32) {
-    double m = 0.0;
-    for (int j = tid; j < k; j += 32) m = fmax(m, dg[j]);
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (tid == 0) maxdiag_s = m;
-  }
-  double shift = 0.0;
-  int fail = -1;
-  for (int attempt = 0; attempt < 2; ++attempt) {
-    auto pivot = [&](int j, double d) {
-      const bool ok = isfinite(d) && d > 0.0 && (attempt == 1 || d > tau * (dg[j] + shift));
-      pv_ok[j] = ok ? 1 : 0;
-      if (ok) {
-        const double rinv = d >= 1e-300 ? rsqrt_nr(d) : rsqrt(d);
-        pv_rinv[j] = rinv;
-        pv_di[j] = rinv * rinv;
-      }
-    };
-    for (int t = tid; t < k * k; t += NT) {
-      const int a = t / k, c = t - a * k;
-      M[a * ld + c] = c >= a ? G[(int64_t)a * ld + c] + (a == c ? shift : 0.0) : 0.0;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      fail_s = -1;
-      pivot(0, M[0]);
-    }
-    __syncthreads();
-    for (int j = 0; j < k; ++j) {
-      if (!pv_ok[j]) {  // every thread reads the same flag: uniform exit
-        if (tid == 0) fail_s = j;
-        break;
-      }
-      const double di = pv_di[j], rj = pv_rinv[j];
-      const double* rowj = M + j * ld;
-      for (int a = j + 1 + warp; a < k; a += NW) {
-        double* rowa = M + a * ld;
-        const double m = rowj[a] * di;
-        for (int c = a + lane; c < k; c += 32) rowa[c] -= m * rowj[c];
-        if (a == j + 1 && lane == 0) pivot(a, rowa[a]);
-        for (int c = lane; c <= j; c += 32) rowa[c] -= m * (c == j ? 1.0 : rowj[c]);
-      }
-      // row j is final: R_jc = A_jc / sqrt(d_j)
-      for (int c = j + tid; c < k; c += NT) R[(int64_t)j * ld + c] = rowj[c] * rj;
-      __syncthreads();
-    }
-    __syncthreads();
-    fail = fail_s;
-    if (fail < 0) break;
-    if (!shift_on_fail || attempt == 1) {
-      if (tid == 0) status[0] = -(fail + 1);
-      // Leave well-defined (identity) factors so downstream kernels stay finite.
-      for (int t = tid; t < ld * ld; t += NT) {
-        const int r = t / ld, c = t % ld;
-        const double v = (r == c && r < k) ? 1.0 : 0.0;
-        R[t] = v;
-        Rinv[t] = v;
-        Rinv_f[t] = (float)v;
-      }
-      return;
-    }
-    if (tid == 0) status[0] += 1;
-    shift = 10.0 * tau * fmax(maxdiag_s, 1e-300);
-    __syncthreads();
-  }
-  // R^{-1}_ca = X_ac / sqrt(d_a), c <= a.
-  for (int t = tid; t < k * k; t += NT) {
-    const int a = t / k, c = t - a * k;
-    if (c <= a) {
-      const double x = (c == a ? 1.0 : M[a * ld + c]) * pv_rinv[a];
-      Rinv[(int64_t)c * ld + a] = x;
-      Rinv_f[(int64_t)c * ld + a] = (float)x;
-    }
-  }
-}
-
 cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shift_on_fail,
                             double* R, double* Rinv, float* Rinv_f, int* status, cudaStream_t st) {
   if (ld > kMaxK) return launch_cholesky_wide(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status, st);
   if (k > kMaxK) return cudaErrorInvalidValue;
   note_launches(1);
-  // 8 warps over the rows, the matrix in shared memory
-  const size_t smem = ((size_t)k * ld + 3 * (size_t)k) * sizeof(double) + (size_t)k * sizeof(int);
-  cudaError_t e = cudaFuncSetAttribute(k_cholesky_rows<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  k_cholesky_rows<8><<<1, 256, smem, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
-  return cudaGetLastError();
-}
-
-// The register-tile variant (1024 threads): kept for comparison timings.
-cudaError_t launch_cholesky_tiles(const double* G, int k, int ld, double tau, int shift_on_fail,
-                                  double* R, double* Rinv, float* Rinv_f, int* status, cudaStream_t st) {
-  if (k > kMaxK) return cudaErrorInvalidValue;
-  note_launches(1);
+  // 32 x 32 threads, 2 x 2 entries each for k <= 64 (measured per 60 x 60
+  // factor: 51 us, against 61 us for 16 x 16 threads with 4 x 4 entries, and
+  // 94 us for 8 warps updating rows of the matrix held in shared memory)
   if (k <= 64)
     k_cholesky<2, 32><<<1, 1024, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
   else
@@ -677,6 +558,7 @@ cudaError_t launch_round_v(const double* A, int64_t g, int ld, const double* mu,
 // sweeps.  FP64 issue bandwidth (one warp instruction per ~4 cycles per SM
 // sub-partition) bounds a round, so the work per round is kept minimal.
 // ---------------------------------------------------------------------------
+template <int NR>  // column entries a lane holds in registers: kk <= 16 NR
 __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, int k, int ld,
                                                  double* __restrict__ evals, double* __restrict__ evecs,
                                                  double* __restrict__ Eglob, double* __restrict__ Rglob,
@@ -760,8 +642,18 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, i
         const int p = pr[i] & 0xff, q = pr[i] >> 8;
         double* rp = R + p * S;
         double* rq = R + q * S;
+        // the pair's columns stay in registers from the dot product to the
+        // rotation: shared-memory traffic bounds a round, so each column is
+        // read once and written once
+        double xp[NR], xq[NR];
         double c = 0.0;
-        for (int r = hl; r < kk; r += 16) c = fma(rp[r], rq[r], c);
+#pragma unroll
+        for (int u = 0; u < NR; ++u) {
+          const int r = hl + 16 * u;
+          xp[u] = r < kk ? rp[r] : 0.0;
+          xq[u] = r < kk ? rq[r] : 0.0;
+          c = fma(xp[u], xq[u], c);
+        }
 #pragma unroll
         for (int o = 8; o > 0; o >>= 1) c += __shfl_xor_sync(hmask, c, o);
         const double a = colnorm[p], b = colnorm[q];
@@ -780,10 +672,13 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, i
         const double t = (double)(__fdividef(tf >= 0.f ? cf : -cf, den));
         if (t == 0.0) continue;  // below FP32 resolution: nothing to rotate
         const double cs = rsqrt_nr(fma(t, t, 1.0)), sn = t * cs;
-        for (int r = hl; r < kk; r += 16) {
-          const double xp = rp[r], xq = rq[r];
-          rp[r] = cs * xp - sn * xq;
-          rq[r] = sn * xp + cs * xq;
+#pragma unroll
+        for (int u = 0; u < NR; ++u) {
+          const int r = hl + 16 * u;
+          if (r < kk) {
+            rp[r] = cs * xp[u] - sn * xq[u];
+            rq[r] = sn * xp[u] + cs * xq[u];
+          }
         }
         if (hl == 0) {
           const double cc = cs * cs, ss = sn * sn, x2 = 2.0 * cs * sn * c;
@@ -872,12 +767,17 @@ cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, dou
     rglob = evecs + (size_t)ld * ld + (size_t)ld * (ld + 1);
     smem = sched;
   }
-  cudaError_t e = cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
   const int warps = std::min(32, std::max(1, (kk / 2 + 1) / 2));  // one half-warp per column pair
-  note_launches(1);
-  k_jacobi<<<1, 32 * warps, smem, st>>>(C, k, ld, evals, evecs, eglob, rglob, sweeps);
-  return cudaGetLastError();
+  auto go = [&](auto kern) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    note_launches(1);
+    kern<<<1, 32 * warps, smem, st>>>(C, k, ld, evals, evecs, eglob, rglob, sweeps);
+    return cudaGetLastError();
+  };
+  if (kk <= 64) return go(k_jacobi<4>);
+  if (kk <= 128) return go(k_jacobi<8>);
+  return go(k_jacobi<16>);
 }
 
 // ---------------------------------------------------------------------------

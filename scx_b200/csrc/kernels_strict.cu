@@ -153,47 +153,58 @@ __global__ void k_tile_csc(const int64_t* __restrict__ indptr, const int32_t* __
 }
 
 // ---------------------------------------------------------------------------
-// Forward product.  A block owns a tile of 8 * RPW rows (RPW per warp) and
-// walks the genes in chunks of GC, each chunk of V (GC x LD floats) staged in
-// shared memory by asynchronous copies, double-buffered.  A warp keeps, for
-// each of its rows, a 32-entry window of the row (one entry per lane) in
-// registers and consumes the window entries whose gene falls in the current
-// chunk (rows are sorted, so they are the next unconsumed ones); lane l
-// accumulates columns l, l + 32, ... of every row in registers.  A consumed
-// entry is marked by gene -1 (0xffffffff as unsigned, above every chunk
-// bound), an entry past the row's end by INT32_MAX; the window is reloaded
-// once all 32 of its entries are consumed.  The window position and end of
-// row r live in lane r.  Each stored entry is loaded from memory once.
+// Forward product, quarter-warp layout.  A quarter (8 lanes) owns RPQ rows and
+// lane l8 of it the columns 4 l8 + 32 s + e (s < LD / 32, e < 4) of each:
+// an entry's V row is read as LD / 32 16-byte loads per lane, the quarter's
+// eight lanes covering 128 consecutive bytes, so the four quarters of a warp
+// read four V rows in four shared-memory wavefronts, conflict-free.  Each
+// entry is broadcast to the 8 lanes of its quarter only (the four quarters
+// take four entries with one shuffle), and every lane does 4 LD / 32 FMAs per
+// entry, against 2 shuffles for LD / 32 FMAs when a whole warp owns a row
+// (measured at 250,000 cells, LD 64: 1.51 ms against 1.85 ms per launch).
+//
+// Per gene chunk and row, each quarter keeps an 8-entry window of the row
+// (one entry per lane; consumed entries marked -1, entries past the row's
+// end INT32_MAX), takes the entries whose gene falls in the chunk (the next
+// unconsumed ones: rows are sorted), and reloads the window once all 8 are
+// consumed.  The four quarters step together: a step runs the largest take
+// count of the four, and a quarter past its own count adds 0 x (a staged row
+// of V), so every shuffle is warp-uniform.  Entries are added in row order.
 // ---------------------------------------------------------------------------
-template <int LD, int RPW, int GC, typename ValT>
-__global__ void __launch_bounds__(256, 2) k_fwd_strict(const int64_t* __restrict__ indptr,
-                                                       const int32_t* __restrict__ idx,
-                                                       const ValT* __restrict__ val, int64_t n, int32_t g,
-                                                       const float* __restrict__ V, const float* __restrict__ mc,
-                                                       float* __restrict__ Y, int lds) {
-  constexpr int C = LD / 32;
+template <int LD, int RPQ, int GC, typename ValT>
+__global__ void __launch_bounds__(256, 2) k_fwd_strict_q(const int64_t* __restrict__ indptr,
+                                                         const int32_t* __restrict__ idx,
+                                                         const ValT* __restrict__ val, int64_t n, int32_t g,
+                                                         const float* __restrict__ V, const float* __restrict__ mc,
+                                                         float* __restrict__ Y, int lds) {
+  constexpr int S4 = LD / 32;  // 16-byte column groups per lane
   constexpr int32_t kDone = -1;
+  constexpr unsigned FULL = 0xffffffffu;
+  static_assert(RPQ <= 8, "a quarter holds the window bounds of its rows in its 8 lanes");
   extern __shared__ __align__(16) float vs[];  // [2][GC][LD]
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int64_t row0 = (int64_t)blockIdx.x * (8 * RPW) + (int64_t)wib * RPW;
-  // lane r < RPW: window start and end of row row0 + r
+  const int qw = lane >> 3, l8 = lane & 7;
+  const int64_t row0 = (int64_t)blockIdx.x * (32 * RPQ) + (int64_t)wib * (4 * RPQ) + qw * RPQ;
+  // lane l8 < RPQ of a quarter: window start and end of its row row0 + l8
   int64_t my_base = 0, my_end = 0;
-  if (lane < RPW && row0 + lane < n) {
-    my_base = indptr[row0 + lane];
-    my_end = indptr[row0 + lane + 1];
+  if (l8 < RPQ && row0 + l8 < n) {
+    my_base = indptr[row0 + l8];
+    my_end = indptr[row0 + l8 + 1];
   }
-  float acc[RPW][C];
-  int32_t wi[RPW];
-  float wv[RPW];
+  float acc[RPQ][4 * S4];
+  int32_t wi[RPQ], ni[RPQ];  // the window, and the next 8 entries of the row already loaded
+  float wv[RPQ], nv[RPQ];
 #pragma unroll
-  for (int r = 0; r < RPW; ++r) {
+  for (int r = 0; r < RPQ; ++r) {
 #pragma unroll
-    for (int c = 0; c < C; ++c) acc[r][c] = 0.f;
-    const int64_t base = __shfl_sync(0xffffffffu, my_base, r);
-    const int64_t end = __shfl_sync(0xffffffffu, my_end, r);
-    const int64_t p = base + lane;
+    for (int c = 0; c < 4 * S4; ++c) acc[r][c] = 0.f;
+    const int64_t base = __shfl_sync(FULL, my_base, r, 8);
+    const int64_t end = __shfl_sync(FULL, my_end, r, 8);
+    const int64_t p = base + l8;
     wi[r] = p < end ? __ldg(idx + p) : INT32_MAX;
     wv[r] = p < end ? to_f32(val[p]) : 0.f;
+    ni[r] = p + 8 < end ? __ldg(idx + p + 8) : INT32_MAX;
+    nv[r] = p + 8 < end ? to_f32(val[p + 8]) : 0.f;
   }
   const int nchunk = (g + GC - 1) / GC;
   block_copy_rows_async<LD>(vs, V, min(GC, (int)g), lds);
@@ -208,99 +219,115 @@ __global__ void __launch_bounds__(256, 2) k_fwd_strict(const int64_t* __restrict
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
-    const float* vc = vs + (ch & 1) * GC * LD + lane;
+    const float* vc = vs + (ch & 1) * GC * LD + 4 * l8;
 #pragma unroll
-    for (int r = 0; r < RPW; ++r) {
+    for (int r = 0; r < RPQ; ++r) {
       while (true) {
         const bool take = (unsigned)wi[r] < (unsigned)g1;
-        const unsigned m = __ballot_sync(0xffffffffu, take);
-        if (m) {
-          const int t0 = __ffs(m) - 1;
-          const int t1 = t0 + __popc(m);
-          // four entries per iteration, so their shuffles and shared loads
-          // are in flight together; an entry past t1 enters with x = 0
-          for (int t = t0; t < t1; t += 4) {
-            float xs[4];
-            const float* vr[4];
+        const unsigned mq = (__ballot_sync(FULL, take) >> (8 * qw)) & 0xffu;
+        const int cnt = __popc(mq);
+        const int t0 = cnt ? __ffs(mq) - 1 : 0;
+        const int steps = (int)__reduce_max_sync(FULL, (unsigned)cnt);
+        for (int t = 0; t < steps; ++t) {
+          const int src = min(t0 + t, 7);
+          const int32_t j = __shfl_sync(FULL, wi[r], src, 8);
+          const float x = __shfl_sync(FULL, wv[r], src, 8);
+          const bool in = t < cnt;
+          const float xs = in ? x : 0.f;
+          // a taken gene is in [g0, g1); a step past the quarter's count
+          // reads row 0 of the chunk (always staged) and adds zero
+          const unsigned jl = in ? min((unsigned)(j - g0), (unsigned)(GC - 1)) : 0u;
+          const float* vr = vc + jl * LD;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int tu = min(t + u, 31);
-              const int32_t j = __shfl_sync(0xffffffffu, wi[r], tu);
-              const float x = __shfl_sync(0xffffffffu, wv[r], tu);
-              const bool in = t + u < t1;
-              xs[u] = in ? x : 0.f;
-              // j is in [g0, g1) for a taken entry; the clamp keeps any other
-              // index inside the staged chunk.  An entry past t1 reads row 0 of
-              // the chunk (always a staged gene): a row past g1 may hold stale
-              // shared memory, and 0 * NaN would poison the sum.
-              const unsigned jl = in ? min((unsigned)(j - g0), (unsigned)(GC - 1)) : 0u;
-              vr[u] = vc + jl * LD;
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-              for (int c = 0; c < C; ++c) acc[r][c] = fmaf(xs[u], vr[u][32 * c], acc[r][c]);
+          for (int s4 = 0; s4 < S4; ++s4) {
+            const float4 v = *reinterpret_cast<const float4*>(vr + 32 * s4);
+            acc[r][4 * s4 + 0] = fmaf(xs, v.x, acc[r][4 * s4 + 0]);
+            acc[r][4 * s4 + 1] = fmaf(xs, v.y, acc[r][4 * s4 + 1]);
+            acc[r][4 * s4 + 2] = fmaf(xs, v.z, acc[r][4 * s4 + 2]);
+            acc[r][4 * s4 + 3] = fmaf(xs, v.w, acc[r][4 * s4 + 3]);
           }
-          if (take) wi[r] = kDone;
         }
-        if (__ballot_sync(0xffffffffu, wi[r] == kDone) != 0xffffffffu) break;
-        // all 32 window entries consumed: load the next 32 entries of the row
-        if (lane == r) my_base += 32;
-        const int64_t base = __shfl_sync(0xffffffffu, my_base, r);
-        const int64_t end = __shfl_sync(0xffffffffu, my_end, r);
-        const int64_t p = base + lane;
-        wi[r] = p < end ? __ldg(idx + p) : INT32_MAX;
-        wv[r] = p < end ? to_f32(val[p]) : 0.f;
+        if (take) wi[r] = kDone;
+        // a quarter whose 8 window entries are all consumed loads the next 8
+        const unsigned dq = (__ballot_sync(FULL, wi[r] == kDone) >> (8 * qw)) & 0xffu;
+        const bool reload = dq == 0xffu;
+        if (!__any_sync(FULL, reload)) break;
+        if (reload && l8 == r) my_base += 8;
+        const int64_t base = __shfl_sync(FULL, my_base, r, 8);
+        const int64_t end = __shfl_sync(FULL, my_end, r, 8);
+        if (reload) {
+          // the next window was loaded a window ahead; fetch the one after it
+          wi[r] = ni[r];
+          wv[r] = nv[r];
+          const int64_t p = base + 8 + l8;
+          ni[r] = p < end ? __ldg(idx + p) : INT32_MAX;
+          nv[r] = p < end ? to_f32(val[p]) : 0.f;
+        }
       }
     }
     __syncthreads();  // everyone is done with this buffer before it is refilled
   }
   cp_async_wait<0>();
-  float m[C];
+  float m[4 * S4];
 #pragma unroll
-  for (int c = 0; c < C; ++c) m[c] = mc ? mc[lane + 32 * c] : 0.f;
+  for (int s4 = 0; s4 < S4; ++s4)
 #pragma unroll
-  for (int r = 0; r < RPW; ++r) {
+    for (int e = 0; e < 4; ++e) m[4 * s4 + e] = mc ? mc[4 * l8 + 32 * s4 + e] : 0.f;
+#pragma unroll
+  for (int r = 0; r < RPQ; ++r) {
     const int64_t row = row0 + r;
     if (row < n) {
 #pragma unroll
-      for (int c = 0; c < C; ++c) Y[row * lds + lane + 32 * c] = acc[r][c] - m[c];
+      for (int s4 = 0; s4 < S4; ++s4)
+        *reinterpret_cast<float4*>(Y + row * lds + 4 * l8 + 32 * s4) =
+            make_float4(acc[r][4 * s4 + 0] - m[4 * s4 + 0], acc[r][4 * s4 + 1] - m[4 * s4 + 1],
+                        acc[r][4 * s4 + 2] - m[4 * s4 + 2], acc[r][4 * s4 + 3] - m[4 * s4 + 3]);
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Transposed product.  Block (range, b) owns the slots [b * 8 GPW, (b + 1) *
-// 8 GPW) -- warp w the GPW consecutive slots from b * 8 GPW + w GPW -- and the
-// row tiles of one contiguous range.  For each tile, Q's rows (kStrictTile x
-// LD floats) are staged in shared memory (double-buffered, asynchronous
-// copies); a warp walks the tile-CSC entries of each of its slots in row
-// order and lane l accumulates columns l, l + 32, ... of every slot in
-// registers.  The block writes one partial row per gene it owns.
+// Transposed product, quarter-warp layout.  Block (range, b) owns the slots
+// [b 32 GPQ, (b + 1) 32 GPQ) and the row tiles of one contiguous range; warp
+// w owns the GPW = 4 GPQ slots of one group of the slot assignment
+// (strict_genes_per_warp), and its quarter qw the slots slot0 + 4 i + qw
+// (i < GPQ), so the group's heaviest genes, which fill its first slots,
+// spread over the four quarters.  For each tile, Q's rows (kStrictTile x LD
+// floats) are staged in shared memory (double-buffered, asynchronous
+// copies).  The block writes one partial row per gene it owns.  Lane l8 owns
+// the columns 4 l8 + 32 s + e: a cell's Q row is read as LD / 32 16-byte
+// loads per lane, the quarter covering 128 consecutive bytes, and each entry
+// is broadcast within its quarter only.  For each slot the four quarters walk
+// their entry lists 8 at a time in step (the longest list sets the count; a
+// lane past its list holds x = 0 and cell 0, a staged row).  Entries are added
+// in tile-CSC order, so the partials do not depend on the schedule.
 // ---------------------------------------------------------------------------
-template <int LD, int GPW, typename ValT>
-__global__ void __launch_bounds__(256, 2) k_rmat_strict(const int64_t* __restrict__ indptr,
-                                                        const int32_t* __restrict__ tptr,
-                                                        const uint8_t* __restrict__ cell,
-                                                        const ValT* __restrict__ cval, int64_t n, int32_t g,
-                                                        int32_t nslots, const int32_t* __restrict__ slot2gene,
-                                                        int64_t tiles_per_range, const float* __restrict__ Q,
-                                                        int lds, float* __restrict__ part) {
-  constexpr int C = LD / 32;
+template <int LD, int GPQ, typename ValT>
+__global__ void __launch_bounds__(256, 2) k_rmat_strict_q(const int64_t* __restrict__ indptr,
+                                                          const int32_t* __restrict__ tptr,
+                                                          const uint8_t* __restrict__ cell,
+                                                          const ValT* __restrict__ cval, int64_t n, int32_t g,
+                                                          int32_t nslots, const int32_t* __restrict__ slot2gene,
+                                                          int64_t tiles_per_range, const float* __restrict__ Q,
+                                                          int lds, float* __restrict__ part) {
+  constexpr int S4 = LD / 32;
   constexpr int T = kStrictTile;
+  constexpr unsigned FULL = 0xffffffffu;
+  static_assert(GPQ <= 8, "a quarter holds the list bounds of its slots in its 8 lanes");
   extern __shared__ __align__(16) float qs[];  // [2][T][LD]
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int qw = lane >> 3, l8 = lane & 7;
   const int64_t n_tiles = (n + T - 1) / T;
   const int64_t t0 = (int64_t)blockIdx.x * tiles_per_range;
   const int64_t t1 = min(n_tiles, t0 + tiles_per_range);
-  const int slot0 = (blockIdx.y * 8 + wib) * GPW;
-  // lane jj < GPW reads the pointers of slot slot0 + jj (coalesced)
-  const int my_slot = slot0 + (lane % GPW);
-  float acc[GPW][C];
+  const int slot0 = (blockIdx.y * 8 + wib) * (4 * GPQ);
+  // lane l8 < GPQ of a quarter reads the list bounds of its slot i = l8
+  const int my_slot = slot0 + 4 * (l8 % GPQ) + qw;
+  float acc[GPQ][4 * S4];
 #pragma unroll
-  for (int jj = 0; jj < GPW; ++jj)
+  for (int i = 0; i < GPQ; ++i)
 #pragma unroll
-    for (int c = 0; c < C; ++c) acc[jj][c] = 0.f;
+    for (int c = 0; c < 4 * S4; ++c) acc[i][c] = 0.f;
   if (t0 < t1) {
     auto stage = [&](int64_t t, int buf) {
       const int64_t r0 = t * T;
@@ -321,29 +348,33 @@ __global__ void __launch_bounds__(256, 2) k_rmat_strict(const int64_t* __restric
       }
       cp_async_wait<1>();
       __syncthreads();
-      const float* qt = qs + buf * T * LD + lane;
+      const float* qt = qs + buf * T * LD + 4 * l8;
 #pragma unroll
-      for (int jj = 0; jj < GPW; ++jj) {
-        const int32_t s = __shfl_sync(0xffffffffu, p0, jj);
-        const int32_t e = __shfl_sync(0xffffffffu, p1, jj);
-        for (int32_t b = s; b < e; b += 32) {
-          const int32_t q = b + lane;
-          const int cnt = min(32, e - b);
+      for (int i = 0; i < GPQ; ++i) {
+        const int32_t s = __shfl_sync(FULL, p0, i, 8);
+        const int32_t len = __shfl_sync(FULL, p1, i, 8) - s;
+        const int32_t longest = (int32_t)__reduce_max_sync(FULL, (unsigned)max(len, 0));
+        for (int32_t b = 0; b < longest; b += 8) {
+          const int32_t q = b + l8;
           int cl = 0;
           float x = 0.f;
-          if (q < e) {
-            cl = __ldg(cell + tb + q);
-            x = to_f32(cval[tb + q]);
+          if (q < len) {
+            cl = __ldg(cell + tb + s + q);
+            x = to_f32(cval[tb + s + q]);
           }
-          // one entry per step: the jj loop is unrolled over the warp's
-          // GPW slots, so a wider body here would overflow the instruction
-          // cache (measured: four entries per step ran 30 % slower)
-          for (int u = 0; u < cnt; ++u) {
-            const int cu = __shfl_sync(0xffffffffu, cl, u) & (T - 1);
-            const float xu = __shfl_sync(0xffffffffu, x, u);
+          const int steps = min(8, longest - b);
+          for (int u = 0; u < steps; ++u) {
+            const int cu = __shfl_sync(FULL, cl, u, 8) & (T - 1);
+            const float xu = __shfl_sync(FULL, x, u, 8);
             const float* qr = qt + cu * LD;
 #pragma unroll
-            for (int c = 0; c < C; ++c) acc[jj][c] = fmaf(xu, qr[32 * c], acc[jj][c]);
+            for (int s4 = 0; s4 < S4; ++s4) {
+              const float4 v = *reinterpret_cast<const float4*>(qr + 32 * s4);
+              acc[i][4 * s4 + 0] = fmaf(xu, v.x, acc[i][4 * s4 + 0]);
+              acc[i][4 * s4 + 1] = fmaf(xu, v.y, acc[i][4 * s4 + 1]);
+              acc[i][4 * s4 + 2] = fmaf(xu, v.z, acc[i][4 * s4 + 2]);
+              acc[i][4 * s4 + 3] = fmaf(xu, v.w, acc[i][4 * s4 + 3]);
+            }
           }
         }
       }
@@ -353,12 +384,14 @@ __global__ void __launch_bounds__(256, 2) k_rmat_strict(const int64_t* __restric
   }
   float* out = part + (int64_t)blockIdx.x * g * LD;
 #pragma unroll
-  for (int jj = 0; jj < GPW; ++jj) {
-    const int slot = slot0 + jj;
+  for (int i = 0; i < GPQ; ++i) {
+    const int slot = slot0 + 4 * i + qw;
     const int j = slot < nslots ? __ldg(slot2gene + slot) : -1;
     if (j >= 0) {
 #pragma unroll
-      for (int c = 0; c < C; ++c) out[(int64_t)j * LD + lane + 32 * c] = acc[jj][c];
+      for (int s4 = 0; s4 < S4; ++s4)
+        *reinterpret_cast<float4*>(out + (int64_t)j * LD + 4 * l8 + 32 * s4) =
+            make_float4(acc[i][4 * s4 + 0], acc[i][4 * s4 + 1], acc[i][4 * s4 + 2], acc[i][4 * s4 + 3]);
     }
   }
 }
@@ -448,15 +481,15 @@ cudaError_t launch_tile_csc(int dtype, const int64_t* indptr, const int32_t* idx
 template <int LD, typename ValT>
 static cudaError_t fwd_strict_t(const int64_t* indptr, const int32_t* idx, const void* val, int64_t n, int32_t g,
                                 const float* V, const float* mc, float* Y, int lds, cudaStream_t st) {
-  constexpr int RPW = LD <= 64 ? 16 : 8;
+  constexpr int RPQ = LD <= 32 ? 8 : 4;  // rows per quarter-warp: RPQ x LD / 8 accumulators per lane
   constexpr int GC = (8192 / LD) & ~7;
   const size_t smem = (size_t)2 * GC * LD * sizeof(float);
-  auto kern = k_fwd_strict<LD, RPW, GC, ValT>;
+  auto kern = k_fwd_strict_q<LD, RPQ, GC, ValT>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  const int64_t rows_per_block = 8 * RPW;
+  const int64_t rows_per_block = 32 * RPQ;
   const int64_t grid = (n + rows_per_block - 1) / rows_per_block;
   kern<<<(unsigned)grid, 256, smem, st>>>(indptr, idx, static_cast<const ValT*>(val), n, g, V, mc, Y, lds);
   note_launches(1);
@@ -492,9 +525,9 @@ template <int LD, typename ValT>
 static cudaError_t rmat_strict_t(const int64_t* indptr, const int32_t* tptr, const uint8_t* cell, const void* cval,
                                  int64_t n, int32_t g, int32_t nslots, const int32_t* slot2gene, int ranges,
                                  const float* Q, int lds, float* part, cudaStream_t st) {
-  constexpr int GPW = LD <= 64 ? 32 : 16;
+  constexpr int GPW = LD <= 64 ? 32 : 16;  // slots per warp (strict_genes_per_warp)
   const size_t smem = (size_t)2 * kStrictTile * LD * sizeof(float);
-  auto kern = k_rmat_strict<LD, GPW, ValT>;
+  auto kern = k_rmat_strict_q<LD, GPW / 4, ValT>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
