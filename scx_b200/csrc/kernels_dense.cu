@@ -111,11 +111,22 @@ cudaError_t launch_gram_f64(const double* A, int64_t n, int ld, double* part, in
 // next diagonal entry computes the next pivot's reciprocals, so a step is
 // one barrier plus a short dependent chain.
 // ---------------------------------------------------------------------------
+// With `tasks` set, block b factors the matrix of tasks[b] (many segments'
+// factorisations in one launch, one block each) and the pointer arguments are
+// ignored.
 template <int U, int T>
 __global__ void __launch_bounds__(T * T) k_cholesky(const double* __restrict__ G, int k, int ld, double tau,
                                                    int shift_on_fail, double* __restrict__ R,
                                                    double* __restrict__ Rinv, float* __restrict__ Rinv_f,
-                                                   int* __restrict__ status) {
+                                                   int* __restrict__ status, const CholTask* __restrict__ tasks) {
+  if (tasks) {
+    const CholTask t = tasks[blockIdx.x];
+    G = t.G;
+    R = t.R;
+    Rinv = t.Rinv;
+    Rinv_f = t.Rinv_f;
+    status = t.status;
+  }
   __shared__ double rowA[2][kMaxK], rowX[2][kMaxK];
   __shared__ double pv_rinv[kMaxK], pv_di[kMaxK], dg[kMaxK];
   __shared__ int pv_ok[kMaxK];
@@ -263,9 +274,23 @@ cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shif
   // factor: 51 us, against 61 us for 16 x 16 threads with 4 x 4 entries, and
   // 94 us for 8 warps updating rows of the matrix held in shared memory)
   if (k <= 64)
-    k_cholesky<2, 32><<<1, 1024, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
+    k_cholesky<2, 32><<<1, 1024, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status, nullptr);
   else
-    k_cholesky<4, 32><<<1, 1024, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status);
+    k_cholesky<4, 32><<<1, 1024, 0, st>>>(G, k, ld, tau, shift_on_fail, R, Rinv, Rinv_f, status, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cholesky_batch(const CholTask* tasks, int ntasks, int k, int ld, double tau, int shift_on_fail,
+                                  cudaStream_t st) {
+  if (k > kMaxK || ld > kMaxK) return cudaErrorInvalidValue;
+  if (ntasks <= 0) return cudaSuccess;
+  note_launches(1);
+  if (k <= 64)
+    k_cholesky<2, 32><<<ntasks, 1024, 0, st>>>(nullptr, k, ld, tau, shift_on_fail, nullptr, nullptr, nullptr, nullptr,
+                                               tasks);
+  else
+    k_cholesky<4, 32><<<ntasks, 1024, 0, st>>>(nullptr, k, ld, tau, shift_on_fail, nullptr, nullptr, nullptr, nullptr,
+                                               tasks);
   return cudaGetLastError();
 }
 
@@ -558,11 +583,23 @@ cudaError_t launch_round_v(const double* A, int64_t g, int ld, const double* mu,
 // sweeps.  FP64 issue bandwidth (one warp instruction per ~4 cycles per SM
 // sub-partition) bounds a round, so the work per round is kept minimal.
 // ---------------------------------------------------------------------------
+// V (use_eglob) and R (use_rglob) go to the scratch that follows evecs when
+// they do not fit shared memory.  With `tasks` set, block b solves tasks[b]
+// (one launch for many segments) and C, evals, evecs, sweeps_out are ignored.
 template <int NR>  // column entries a lane holds in registers: kk <= 16 NR
 __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, int k, int ld,
                                                  double* __restrict__ evals, double* __restrict__ evecs,
-                                                 double* __restrict__ Eglob, double* __restrict__ Rglob,
-                                                 int* sweeps_out) {
+                                                 int use_eglob, int use_rglob, int* sweeps_out,
+                                                 const JacobiTask* __restrict__ tasks) {
+  if (tasks) {
+    const JacobiTask t = tasks[blockIdx.x];
+    C = t.C;
+    evals = t.evals;
+    evecs = t.evecs;
+    sweeps_out = t.sweeps;
+  }
+  double* Eglob = use_eglob ? evecs + (size_t)ld * ld : nullptr;
+  double* Rglob = use_rglob ? evecs + (size_t)ld * ld + (size_t)ld * (ld + 1) : nullptr;
   extern __shared__ double sm[];
   const int kk = (k + 1) & ~1;  // even number of columns; column k (if odd) is a zero dummy
   const int S = kk + 1;
@@ -746,25 +783,23 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, i
   if (tid == 0 && sweeps_out) *sweeps_out = sweep;
 }
 
-cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, double* evecs,
-                              int* sweeps, cudaStream_t st) {
+static cudaError_t jacobi_go(const double* C, int k, int ld, double* evals, double* evecs, int* sweeps,
+                             const JacobiTask* tasks, int nblocks, cudaStream_t st) {
   const int kk = (k + 1) & ~1;
   const size_t one = (size_t)kk * (kk + 1) * sizeof(double);
   const size_t sched = ((size_t)(kk - 1) * (kk / 2) + 3) / 4 * sizeof(double);
   // V lives in shared memory when both matrices fit, else in the scratch that
-  // follows evecs (the plan allocates ld * ld + ld * (ld + 1) doubles there;
-  // ld * ld + 2 ld (ld + 1) for a sketch wider than one panel, whose R goes
-  // to global memory too).
+  // follows evecs (the plan allocates ld * ld + 2 ld (ld + 1) doubles there),
+  // and R too when even one does not fit (a sketch wider than one panel).
   if (kk > 256) return cudaErrorInvalidValue;  // the schedule packs a column pair into 8 + 8 bits
-  double* eglob = nullptr;
-  double* rglob = nullptr;
+  int use_e = 0, use_r = 0;
   size_t smem = 2 * one + sched;
   if (smem > 200 * 1024) {
-    eglob = evecs + (size_t)ld * ld;
+    use_e = 1;
     smem = one + sched;
   }
   if (smem > 200 * 1024) {
-    rglob = evecs + (size_t)ld * ld + (size_t)ld * (ld + 1);
+    use_r = 1;
     smem = sched;
   }
   const int warps = std::min(32, std::max(1, (kk / 2 + 1) / 2));  // one half-warp per column pair
@@ -772,12 +807,22 @@ cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, dou
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     note_launches(1);
-    kern<<<1, 32 * warps, smem, st>>>(C, k, ld, evals, evecs, eglob, rglob, sweeps);
+    kern<<<nblocks, 32 * warps, smem, st>>>(C, k, ld, evals, evecs, use_e, use_r, sweeps, tasks);
     return cudaGetLastError();
   };
   if (kk <= 64) return go(k_jacobi<4>);
   if (kk <= 128) return go(k_jacobi<8>);
   return go(k_jacobi<16>);
+}
+
+cudaError_t launch_jacobi_eig(const double* C, int k, int ld, double* evals, double* evecs,
+                              int* sweeps, cudaStream_t st) {
+  return jacobi_go(C, k, ld, evals, evecs, sweeps, nullptr, 1, st);
+}
+
+cudaError_t launch_jacobi_eig_batch(const JacobiTask* tasks, int ntasks, int k, int ld, cudaStream_t st) {
+  if (ntasks <= 0) return cudaSuccess;
+  return jacobi_go(nullptr, k, ld, nullptr, nullptr, nullptr, tasks, ntasks, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -109,6 +109,25 @@ cudaError_t launch_center_apply_wide(const double* W, int64_t g, int ld, const d
                                      const double* M, double* Z, cudaStream_t st);
 
 // ---- dense side (kernels_dense.cu) ----
+// One k x k factorisation (Cholesky) or eigensolve (Jacobi) of a segment of a
+// batch: its arguments, read by one block of a batched launch.
+struct CholTask {
+  const double* G;
+  double* R;
+  double* Rinv;
+  float* Rinv_f;
+  int* status;
+};
+struct JacobiTask {
+  const double* C;
+  double* evals;
+  double* evecs;
+  int* sweeps;
+};
+// ntasks factorisations of one launch, one block each (k, ld <= 128).
+cudaError_t launch_cholesky_batch(const CholTask* tasks, int ntasks, int k, int ld, double tau, int shift_on_fail,
+                                  cudaStream_t st);
+cudaError_t launch_jacobi_eig_batch(const JacobiTask* tasks, int ntasks, int k, int ld, cudaStream_t st);
 // Gram partials of a tall row-major matrix A (n x ld, first k columns used):
 // part[b] = [A_b^T A_b (ld x ld), colsum(A_b) (ld)] in FP64.
 cudaError_t launch_gram_f32(const float* A, int64_t n, int ld, double* part, int nparts,

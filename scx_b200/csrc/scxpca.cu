@@ -1424,11 +1424,10 @@ void collect_stages(scxpca_plan* pl) {
   pl->events_used = 0;
 }
 
-// Tall Gram + Cholesky (FP64) of a tall matrix A.  With `from_image` (tensor-core
-// path, ld 64) the Gram is taken on tensor cores from the 16-bit image of A
-// held in Yimg; otherwise from the FP32 A with FP64 FMAs.
-void tall_chol(scxpca_plan* pl, const float* A, int64_t rows, double* Rinv, float* Rinv_f,
-               int shift, bool from_image = false) {
+// The Gram (FP64, with column sums after it) of a tall A into G.  With
+// `from_image` (tensor-core path, ld 64) it is taken on tensor cores from the
+// 16-bit image of A held in Yimg; otherwise from the FP32 A with FP64 FMAs.
+void tall_gram(scxpca_plan* pl, const float* A, int64_t rows, bool from_image) {
   cudaStream_t st = pl->stream;
   const int ld = (int)pl->ld;
   int parts = (int)std::max<int64_t>(1, std::min<int64_t>(pl->gram_parts, (rows + 31) / 32));
@@ -1442,26 +1441,51 @@ void tall_chol(scxpca_plan* pl, const float* A, int64_t rows, double* Rinv, floa
   CK(launch_reduce_rows_f64(pl->gpart.as<double>(), parts, (int64_t)ld * ld + ld, pl->G.as<double>(), 0,
                             st, pl->num_sms));
   stage_end(pl, SCXPCA_STAGE_GRAM, s);
-  s = stage_begin(pl);
-  CK(launch_cholesky(pl->G.as<double>(), (int)pl->k, ld, pl->tau, shift, pl->R.as<double>(), Rinv,
-                     Rinv_f, pl->status.as<int>(), st));
+}
+
+// The k x k Cholesky of G: R, and R^{-1} into Rinv / Rinv_f.
+void gram_chol(scxpca_plan* pl, double* Rinv, float* Rinv_f, int shift) {
+  int s = stage_begin(pl);
+  CK(launch_cholesky(pl->G.as<double>(), (int)pl->k, (int)pl->ld, pl->tau, shift, pl->R.as<double>(), Rinv,
+                     Rinv_f, pl->status.as<int>(), pl->stream));
   stage_end(pl, SCXPCA_STAGE_SMALL, s);
 }
 
-// CholeskyQR2 of a gene-side FP64 matrix in place.
-// One CholeskyQR pass.  The Gram and the triangular apply are both FP64, so the
-// loss of orthogonality is about cond(A)^2 * 1e-16: the second pass of
-// CholeskyQR2, which repairs a Gram formed in working precision, is not needed
-// on this FP64 gene-side matrix (the tall FP32 Q keeps its second pass).
-void small_qr(scxpca_plan* pl, double* A, int shift) {
+// The same factorisation as one task of a batched launch.
+CholTask gram_chol_task(scxpca_plan* pl, double* Rinv, float* Rinv_f) {
+  return CholTask{pl->G.as<double>(), pl->R.as<double>(), Rinv, Rinv_f, pl->status.as<int>()};
+}
+
+// Tall Gram + Cholesky (FP64) of a tall matrix A.
+void tall_chol(scxpca_plan* pl, const float* A, int64_t rows, double* Rinv, float* Rinv_f,
+               int shift, bool from_image = false) {
+  tall_gram(pl, A, rows, from_image);
+  gram_chol(pl, Rinv, Rinv_f, shift);
+}
+
+// One CholeskyQR pass of a gene-side FP64 matrix in place.  The Gram and the
+// triangular apply are both FP64, so the loss of orthogonality is about
+// cond(A)^2 * 1e-16: the second pass of CholeskyQR2, which repairs a Gram
+// formed in working precision, is not needed on this FP64 gene-side matrix
+// (the tall FP32 Q keeps its second pass).  In halves: small_gram, the
+// Cholesky, small_apply.
+void small_gram(scxpca_plan* pl, const double* A) {
   cudaStream_t st = pl->stream;
   const int ld = (int)pl->ld;
   CK(launch_gram_f64(A, pl->g, ld, pl->gpart.as<double>(), pl->gram_parts_small, st));
   CK(launch_reduce_rows_f64(pl->gpart.as<double>(), pl->gram_parts_small, (int64_t)ld * ld + ld,
                             pl->G.as<double>(), 0, st, pl->num_sms));
-  CK(launch_cholesky(pl->G.as<double>(), (int)pl->k, ld, pl->tau, shift, pl->R.as<double>(),
-                     pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), pl->status.as<int>(), st));
-  CK(launch_apply_right_f64(A, pl->g, ld, pl->Rinv.as<double>(), st));
+}
+
+void small_apply(scxpca_plan* pl, double* A) {
+  CK(launch_apply_right_f64(A, pl->g, (int)pl->ld, pl->Rinv.as<double>(), pl->stream));
+}
+
+void small_qr(scxpca_plan* pl, double* A, int shift) {
+  small_gram(pl, A);
+  CK(launch_cholesky(pl->G.as<double>(), (int)pl->k, (int)pl->ld, pl->tau, shift, pl->R.as<double>(),
+                     pl->Rinv.as<double>(), pl->Rinv_f.as<float>(), pl->status.as<int>(), pl->stream));
+  small_apply(pl, A);
 }
 
 // W = X^T A (raw, uncentred), FP64, for a tall float A (n x ld).
@@ -1671,6 +1695,35 @@ struct DeviceOperator {
                                 pl->num_sms));
     stage_end(pl, SCXPCA_STAGE_APPLY, s);
   }
+  // qr(b) around its k x k Cholesky, for a batch that factors every
+  // segment's Gram in one launch: qr_gram, then the factorisation of
+  // qr_task(), then qr_after.
+  void qr_gram(Buf b) {
+    if (b == Buf::kY) {
+      tall_gram(pl, pl->Y.as<float>(), pl->n, true);
+      return;
+    }
+    int s = stage_begin(pl);
+    small_gram(pl, pl->Z.as<double>());
+    stage_end(pl, SCXPCA_STAGE_SMALL, s);
+  }
+  CholTask qr_task() { return gram_chol_task(pl, pl->Rinv.as<double>(), pl->Rinv_f.as<float>()); }
+  void qr_after(Buf b) {
+    if (b == Buf::kY) return;
+    const int ld = (int)pl->ld;
+    int s = stage_begin(pl);
+    small_apply(pl, pl->Z.as<double>());
+    CK(launch_round_v(pl->Z.as<double>(), pl->g, ld, mu, pl->V.as<float>(), pl->mc.as<float>(), pl->stream));
+    if (pl->pflog) CK(launch_aug_colsum(pl->V.as<float>(), (int32_t)pl->g_user, ld, pl->stream));
+    stage_end(pl, SCXPCA_STAGE_SMALL, s);
+  }
+  // finalize_q in the same way: each pass is finalize_gram, then the
+  // factorisation of finalize_task(); then the operator is closing.
+  void finalize_gram() {
+    apply_q();
+    tall_gram(pl, pl->Y.as<float>(), pl->n, true);
+  }
+  CholTask finalize_task() { return gram_chol_task(pl, pl->R2inv.as<double>(), pl->Rinv_f.as<float>()); }
   void finalize_q() {
     // Explicit Q = Y R^{-1}, re-orthonormalised by a second FP64 Cholesky pass.
     apply_q();
@@ -1709,16 +1762,23 @@ void enqueue_run(scxpca_plan* pl, const scxpca_params& p, float* U) {
 }
 
 // After the loop: the SVD of B (in Z) through the FP64 eigendecomposition of
-// B^T B, the components, and the embeddings U = Q R2^{-1} E Sigma.
-void enqueue_finish(scxpca_plan* pl, float* U) {
+// B^T B, the components, and the embeddings U = Q R2^{-1} E Sigma.  In parts
+// (finish_gram, the eigensolve of finish_task, finish_after) for a batch that
+// solves every segment's eigenproblem in one launch.
+void finish_gram(scxpca_plan* pl) {
+  int s = stage_begin(pl);
+  small_gram(pl, pl->Z.as<double>());
+  stage_end(pl, SCXPCA_STAGE_SMALL, s);
+}
+
+JacobiTask finish_task(scxpca_plan* pl) {
+  return JacobiTask{pl->G.as<double>(), pl->evals.as<double>(), pl->evecs.as<double>(), pl->status.as<int>() + 2};
+}
+
+void finish_after(scxpca_plan* pl, float* U) {
   cudaStream_t st = pl->stream;
   const int ld = (int)pl->ld;
   int s = stage_begin(pl);
-  CK(launch_gram_f64(pl->Z.as<double>(), pl->g, ld, pl->gpart.as<double>(), pl->gram_parts_small, st));
-  CK(launch_reduce_rows_f64(pl->gpart.as<double>(), pl->gram_parts_small, (int64_t)ld * ld + ld,
-                            pl->G.as<double>(), 0, st, pl->num_sms));
-  CK(launch_jacobi_eig(pl->G.as<double>(), (int)pl->k, ld, pl->evals.as<double>(), pl->evecs.as<double>(),
-                       pl->status.as<int>() + 2, st));
   CK(launch_ritz_finish(pl->Z.as<double>(), pl->g, ld, (int)pl->k, (int)pl->nc, pl->evals.as<double>(),
                         pl->evecs.as<double>(), pl->R2inv.as<double>(), pl->sigma.as<double>(),
                         pl->comps.as<float>(), pl->M_emb.as<float>(), st));
@@ -1728,6 +1788,15 @@ void enqueue_finish(scxpca_plan* pl, float* U) {
   CK(launch_embed(pl->Y.as<float>(), pl->n, ld, (int)pl->k, pl->M_emb.as<float>(), (int)pl->nc, U, st,
                   pl->num_sms));
   stage_end(pl, SCXPCA_STAGE_EMBED, s);
+}
+
+void enqueue_finish(scxpca_plan* pl, float* U) {
+  finish_gram(pl);
+  int s = stage_begin(pl);
+  CK(launch_jacobi_eig(pl->G.as<double>(), (int)pl->k, (int)pl->ld, pl->evals.as<double>(), pl->evecs.as<double>(),
+                       pl->status.as<int>() + 2, pl->stream));
+  stage_end(pl, SCXPCA_STAGE_SMALL, s);
+  finish_after(pl, U);
 }
 
 // Host side of a finished run: the status words and singular values copied
@@ -1957,6 +2026,9 @@ struct scxpca_batch {
   // 16, 32 branches; [6..11] lockstep over as many streams
   double tuned_ms[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   scxpca_params params{};
+  // the lockstep schedule's batched k x k launches: one task per segment for
+  // the loop's Cholesky (R^{-1}), the closing one (R2^{-1}) and the eigensolve
+  DevBuf task_qr, task_fin, task_eig;
 
   ~scxpca_batch() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -1965,6 +2037,9 @@ struct scxpca_batch {
     for (scxpca_plan* pl : plans) delete pl;
     for (DevBuf* b : indptrs) delete b;
     emb.release();
+    task_qr.release();
+    task_fin.release();
+    task_eig.release();
     for (cudaStream_t st : branch) cudaStreamDestroy(st);
     for (cudaEvent_t e : join) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
@@ -2026,6 +2101,10 @@ struct BatchOperator {
   std::vector<DeviceOperator> ops;  // one per segment
   std::vector<int> branch_of;       // segment -> branch
   int nb;
+  // every segment's k x k Cholesky of a step in ONE launch on the main
+  // stream (one block per segment) between the step's two forked halves,
+  // instead of one single-block launch per segment on its branch
+  bool small_batched = false;
 
   template <class F>
   void each(F&& f) {
@@ -2042,9 +2121,59 @@ struct BatchOperator {
   }
   void matmat(Operand src, bool last) { each([&](int, DeviceOperator& o) { o.matmat(src, last); }); }
   void rmatmat() { each([&](int, DeviceOperator& o) { o.rmatmat(); }); }
-  void qr(Buf x) { each([&](int, DeviceOperator& o) { o.qr(x); }); }
-  void finalize_q() { each([&](int, DeviceOperator& o) { o.finalize_q(); }); }
+  void chol_all(const DevBuf& tasks) {
+    const scxpca_plan* p0 = ops[0].pl;
+    CK(launch_cholesky_batch(tasks.as<CholTask>(), (int)ops.size(), (int)p0->k, (int)p0->ld, p0->tau,
+                             ops[0].shift, b->main));
+  }
+  void qr(Buf x) {
+    if (!small_batched) {
+      each([&](int, DeviceOperator& o) { o.qr(x); });
+      return;
+    }
+    each([&](int, DeviceOperator& o) { o.qr_gram(x); });
+    chol_all(b->task_qr);
+    if (x == Buf::kZ) each([&](int, DeviceOperator& o) { o.qr_after(x); });
+  }
+  void finalize_q() {
+    if (!small_batched) {
+      each([&](int, DeviceOperator& o) { o.finalize_q(); });
+      return;
+    }
+    const int passes = ops[0].shift ? 2 : 1;  // the Householder contract's third pass (DeviceOperator::finalize_q)
+    for (int pass = 0; pass < passes; ++pass) {
+      each([&](int, DeviceOperator& o) { o.finalize_gram(); });
+      chol_all(b->task_fin);
+    }
+    for (DeviceOperator& o : ops) o.closing = true;
+  }
 };
+
+// Upload the batched launches' task tables (before a capture).  The batched
+// kernels take k, ld <= 128 and one (k, ld) for all segments; otherwise the
+// lockstep schedule keeps one launch per segment.
+bool batch_prepare_tasks(scxpca_batch* b, BatchOperator& bop) {
+  const scxpca_plan* p0 = b->plans[0];
+  for (const scxpca_plan* pl : b->plans)
+    if (pl->k != p0->k || pl->ld != p0->ld) return false;
+  if (p0->ld > kMaxK) return false;
+  const size_t ns = b->plans.size();
+  std::vector<CholTask> tq(ns), tf(ns);
+  std::vector<JacobiTask> te(ns);
+  for (size_t q = 0; q < ns; ++q) {
+    tq[q] = bop.ops[q].qr_task();
+    tf[q] = bop.ops[q].finalize_task();
+    te[q] = finish_task(b->plans[q]);
+  }
+  b->task_qr.alloc(sizeof(CholTask) * ns);
+  b->task_fin.alloc(sizeof(CholTask) * ns);
+  b->task_eig.alloc(sizeof(JacobiTask) * ns);
+  CK(cudaMemcpyAsync(b->task_qr.p, tq.data(), sizeof(CholTask) * ns, cudaMemcpyHostToDevice, b->main));
+  CK(cudaMemcpyAsync(b->task_fin.p, tf.data(), sizeof(CholTask) * ns, cudaMemcpyHostToDevice, b->main));
+  CK(cudaMemcpyAsync(b->task_eig.p, te.data(), sizeof(JacobiTask) * ns, cudaMemcpyHostToDevice, b->main));
+  CK(cudaStreamSynchronize(b->main));
+  return true;
+}
 
 // Record every segment's run (and the copies of its status, singular values
 // and components to pinned host memory) into one graph over `nb` branches.
@@ -2064,21 +2193,35 @@ void batch_capture(scxpca_batch* b, int nb, bool lockstep) {
   }
   const auto lists = batch_schedule(b, nb);
   const scxpca_params& p = b->params;
+  BatchOperator bop{b, {}, std::vector<int>(b->plans.size(), 0), nb};
+  if (lockstep) {
+    for (int t = 0; t < nb; ++t)
+      for (int q : lists[t]) bop.branch_of[q] = t;
+    for (scxpca_plan* pl : b->plans) bop.ops.push_back(device_operator(pl, p));
+    bop.small_batched = batch_prepare_tasks(b, bop);
+  }
   CK(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeRelaxed));
   try {
     if (lockstep) {
-      BatchOperator bop{b, {}, std::vector<int>(b->plans.size(), 0), nb};
-      for (int t = 0; t < nb; ++t)
-        for (int q : lists[t]) bop.branch_of[q] = t;
-      for (scxpca_plan* pl : b->plans) bop.ops.push_back(device_operator(pl, p));
       bop.each([&](int, DeviceOperator& o) {
         CK(cudaMemsetAsync(o.pl->status.p, 0, sizeof(int) * 4, o.pl->stream));
       });
       run_power_loop(bop, p.n_power_iterations);
-      bop.each([&](int q, DeviceOperator& o) {
-        enqueue_finish(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
-        batch_copy_out(b, q);
-      });
+      if (bop.small_batched) {
+        bop.each([&](int, DeviceOperator& o) { finish_gram(o.pl); });
+        const scxpca_plan* p0 = b->plans[0];
+        CK(launch_jacobi_eig_batch(b->task_eig.as<JacobiTask>(), (int)b->plans.size(), (int)p0->k, (int)p0->ld,
+                                   b->main));
+        bop.each([&](int q, DeviceOperator& o) {
+          finish_after(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
+          batch_copy_out(b, q);
+        });
+      } else {
+        bop.each([&](int q, DeviceOperator& o) {
+          enqueue_finish(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
+          batch_copy_out(b, q);
+        });
+      }
     } else {
       CK(cudaEventRecord(b->fork, b->main));
       for (int t = 0; t < nb; ++t) {
