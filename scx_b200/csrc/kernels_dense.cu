@@ -21,8 +21,8 @@ namespace scx {
 // exact in FP64; accumulation is FP64.
 // ---------------------------------------------------------------------------
 template <typename T, int LD>
-__global__ void __launch_bounds__(256) k_gram(const T* __restrict__ A, int64_t n,
-                                              double* __restrict__ part) {
+__device__ __forceinline__ void gram_body(const T* __restrict__ A, int64_t n, double* __restrict__ part, int b,
+                                          int nb) {
   constexpr int TT = LD / 16;
   constexpr int R = 32;  // rows staged per step
   __shared__ double sh[R][LD];
@@ -33,8 +33,8 @@ __global__ void __launch_bounds__(256) k_gram(const T* __restrict__ A, int64_t n
 #pragma unroll
     for (int j = 0; j < TT; ++j) acc[i][j] = 0.0;
   double csum = 0.0;
-  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
-  const int64_t r0 = (int64_t)blockIdx.x * per;
+  const int64_t per = (n + nb - 1) / nb;
+  const int64_t r0 = (int64_t)b * per;
   const int64_t r1 = min(n, r0 + per);
   for (int64_t base = r0; base < r1; base += R) {
     const int rows = (int)min((int64_t)R, r1 - base);
@@ -58,12 +58,41 @@ __global__ void __launch_bounds__(256) k_gram(const T* __restrict__ A, int64_t n
       for (int r = 0; r < rows; ++r) csum += sh[r][threadIdx.x];
     __syncthreads();
   }
-  double* out = part + (int64_t)blockIdx.x * (LD * LD + LD);
+  double* out = part + (int64_t)b * (LD * LD + LD);
 #pragma unroll
   for (int i = 0; i < TT; ++i)
 #pragma unroll
     for (int j = 0; j < TT; ++j) out[(ty + 16 * i) * LD + tx + 16 * j] = acc[i][j];
   if (threadIdx.x < LD) out[LD * LD + threadIdx.x] = csum;
+}
+
+template <typename T, int LD>
+__global__ void __launch_bounds__(256) k_gram(const T* __restrict__ A, int64_t n, double* __restrict__ part) {
+  gram_body<T, LD>(A, n, part, blockIdx.x, gridDim.x);
+}
+
+// One FP64 matrix per grid row y (batched segments): partials into the task's part.
+template <int LD>
+__global__ void __launch_bounds__(256) k_gram_batch(const GramTask* __restrict__ tasks, int64_t n) {
+  const GramTask t = tasks[blockIdx.y];
+  gram_body<double, LD>(t.A, n, t.part, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_gram_f64_batch(const GramTask* tasks, int ntasks, int64_t n, int ld, int nparts,
+                                  cudaStream_t st, int num_sms) {
+  if (ntasks <= 0) return cudaSuccess;
+  const dim3 grid((unsigned)nparts, (unsigned)ntasks);
+  note_launches(1);
+  switch (ld) {
+    case 32: k_gram_batch<32><<<grid, 256, 0, st>>>(tasks, n); break;
+    case 64: k_gram_batch<64><<<grid, 256, 0, st>>>(tasks, n); break;
+    case 96: k_gram_batch<96><<<grid, 256, 0, st>>>(tasks, n); break;
+    case 128: k_gram_batch<128><<<grid, 256, 0, st>>>(tasks, n); break;
+    default: return cudaErrorInvalidValue;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_reduce_rows_f64_batch(tasks, ntasks, nparts, (int64_t)ld * ld + ld, st, num_sms);
 }
 
 template <typename T>
@@ -432,6 +461,105 @@ __global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, 
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// ---------------------------------------------------------------------------
+// Y <- Y M at ld 64 for an upper-triangular M (the Cholesky inverse), with the
+// optional 16-bit image: output column c takes only rows l <= c of M, half
+// the FMAs of the full product.  Warp w computes the column groups w and
+// 15 - w (4 columns each: 4 (w + 1) + 4 (16 - w) = 68 terms, the same for
+// every warp), lane r the rows r + 32 i (i < 4) of a 128-row tile.  The tile
+// is staged as in k_tall_mm (padded rows, cp.async double buffering, loaded
+// whole before any of its rows is written, so Out may alias In).  The terms
+// dropped are exact zeros, so the result equals the full product's.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256, 2) k_tall_mm_upper64(const float* In, int64_t n,
+                                                            const float* __restrict__ M, float* Out,
+                                                            uint16_t* __restrict__ img, int fmt) {
+  constexpr int K = 64, KP = K + 4;
+  extern __shared__ __align__(16) float sm_u[];
+  float* Ms = sm_u;                    // [K][K]
+  float* T0 = sm_u + K * K;
+  float* T1 = T0 + kTallRows * KP;
+  for (int t = threadIdx.x; t < K * K; t += blockDim.x) Ms[t] = M[t];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t n_tiles = (n + kTallRows - 1) / kTallRows;
+  auto issue = [&](int64_t tile, float* T) {
+    const int64_t r0 = tile * kTallRows;
+    for (int t = threadIdx.x; t < kTallRows * (K / 4); t += blockDim.x) {
+      const int r = t / (K / 4), c4 = t - r * (K / 4);
+      float* dst = T + r * KP + 4 * c4;
+      if (r0 + r < n) cp_async16(dst, In + (r0 + r) * K + 4 * c4);
+      else *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  int64_t tile = blockIdx.x;
+  if (tile < n_tiles) issue(tile, T0);
+  cp_async_commit();
+  for (int it = 0; tile < n_tiles; tile += gridDim.x, ++it) {
+    float* T = (it & 1) ? T1 : T0;
+    const int64_t next = tile + gridDim.x;
+    if (next < n_tiles) issue(next, (it & 1) ? T0 : T1);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    const int64_t r0 = tile * kTallRows;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int cg = h == 0 ? w : 15 - w;  // column group: columns 4 cg .. 4 cg + 3
+      float acc[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int o = 0; o < 4; ++o) acc[i][o] = 0.f;
+      for (int l = 0; l < 4 * (cg + 1); l += 4) {
+        float4 a[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = *reinterpret_cast<const float4*>(T + (lane + 32 * i) * KP + l);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const float4 m = *reinterpret_cast<const float4*>(Ms + (l + u) * K + 4 * cg);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float x = u == 0 ? a[i].x : u == 1 ? a[i].y : u == 2 ? a[i].z : a[i].w;
+            acc[i][0] = fmaf(x, m.x, acc[i][0]);
+            acc[i][1] = fmaf(x, m.y, acc[i][1]);
+            acc[i][2] = fmaf(x, m.z, acc[i][2]);
+            acc[i][3] = fmaf(x, m.w, acc[i][3]);
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int64_t row = r0 + lane + 32 * i;
+        if (row >= n) continue;
+        const int col = 4 * cg;
+        *reinterpret_cast<float4*>(Out + row * K + col) = make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+        if (img) {
+          uint16_t hh[4], ll[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) split16(acc[i][j], fmt, hh[j], ll[j]);
+          *reinterpret_cast<uint4*>(img + (row * K + col) * 2) =
+              make_uint4(hh[0] | ((uint32_t)ll[0] << 16), hh[1] | ((uint32_t)ll[1] << 16),
+                         hh[2] | ((uint32_t)ll[2] << 16), hh[3] | ((uint32_t)ll[3] << 16));
+        }
+      }
+    }
+    __syncthreads();  // every thread is done with T before it is refilled
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+static cudaError_t tall_mm_upper64(const float* In, int64_t n, const float* M, float* Out, uint16_t* img, int fmt,
+                                   cudaStream_t st, int num_sms) {
+  if (n == 0) return cudaSuccess;
+  const size_t smem = ((size_t)64 * 64 + 2 * (size_t)kTallRows * 68) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(k_tall_mm_upper64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int grid = grid_for(n, kTallRows, num_sms, 2);
+  note_launches(1);
+  k_tall_mm_upper64<<<grid, 256, smem, st>>>(In, n, M, Out, img, fmt);
+  return cudaGetLastError();
+}
+
 static cudaError_t tall_mm(const float* In, int64_t n, int K, int ldi, const float* M, int ldm, int cnt,
                            float* Out, int ldo, uint16_t* img, int fmt, cudaStream_t st,
                            int num_sms) {
@@ -463,28 +591,30 @@ cudaError_t launch_apply_right_f32(const float* In, int64_t n, int ld, const flo
     }
     return cudaSuccess;
   }
+  if (ld == 64) return tall_mm_upper64(In, n, M, Out, nullptr, 0, st, num_sms);
   return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, nullptr, 0, st, num_sms);
 }
 
 cudaError_t launch_apply_right_split(const float* In, int64_t n, int ld, const float* M, float* Out,
                                      uint16_t* img, int fmt, cudaStream_t st, int num_sms) {
   if (ld > kMaxK) return cudaErrorInvalidValue;  // the 16-bit image belongs to the tensor-core path (ld <= 128)
+  if (ld == 64) return tall_mm_upper64(In, n, M, Out, img, fmt, st, num_sms);
   return tall_mm(In, n, ld, ld, M, ld, ld, Out, ld, img, fmt, st, num_sms);
 }
 
 // ---------------------------------------------------------------------------
 // Gene-side FP64 ops.  Block = 256 threads handles 256 / ld rows at a time.
 // ---------------------------------------------------------------------------
-__global__ void k_center_apply(const double* __restrict__ W, int64_t g, int ld,
-                               const double* __restrict__ mu, const double* __restrict__ s,
-                               const double* __restrict__ M, double* __restrict__ Z) {
+// Block b of nb (of one matrix's grid) takes rows b rpb, (b + nb) rpb, ...
+__device__ __forceinline__ void center_apply_body(const double* W, int64_t g, int ld, const double* mu,
+                                                  const double* s, const double* M, double* Z, int b, int nb) {
   extern __shared__ double sm[];  // M [ld][ld], rows [256/ld][ld]
   double* Ms = sm;
   double* rows = sm + ld * ld;
   for (int t = threadIdx.x; t < ld * ld; t += blockDim.x) Ms[t] = M[t];
   const int rpb = blockDim.x / ld;
   const int r = threadIdx.x / ld, c = threadIdx.x % ld;
-  for (int64_t j0 = (int64_t)blockIdx.x * rpb; j0 < g; j0 += (int64_t)gridDim.x * rpb) {
+  for (int64_t j0 = (int64_t)b * rpb; j0 < g; j0 += (int64_t)nb * rpb) {
     __syncthreads();
     const int64_t j = j0 + r;
     if (r < rpb && j < g) {
@@ -499,6 +629,30 @@ __global__ void k_center_apply(const double* __restrict__ W, int64_t g, int ld,
       Z[j * ld + c] = acc;
     }
   }
+}
+
+__global__ void k_center_apply(const double* W, int64_t g, int ld, const double* __restrict__ mu,
+                               const double* __restrict__ s, const double* __restrict__ M, double* Z) {
+  center_apply_body(W, g, ld, mu, s, M, Z, blockIdx.x, gridDim.x);
+}
+
+// One matrix per grid row y (batched segments).
+__global__ void k_center_apply_batch(const ApplyTask* __restrict__ tasks, int64_t g, int ld) {
+  const ApplyTask t = tasks[blockIdx.y];
+  center_apply_body(t.W, g, ld, t.mu, t.s, t.M, t.Z, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_center_apply_batch(const ApplyTask* tasks, int ntasks, int64_t g, int ld, cudaStream_t st) {
+  if (ld > kMaxK) return cudaErrorInvalidValue;
+  if (ntasks <= 0) return cudaSuccess;
+  size_t smem = (size_t)(ld * ld + 256) * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(k_center_apply_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int rpb = 256 / ld;
+  const int grid = (int)std::min<int64_t>((g + rpb - 1) / rpb, 8);  // 8 blocks per matrix, ntasks matrices
+  note_launches(1);
+  k_center_apply_batch<<<dim3((unsigned)grid, (unsigned)ntasks), 256, smem, st>>>(tasks, g, ld);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_center_apply(const double* W, int64_t g, int ld, const double* mu,
@@ -523,11 +677,17 @@ __global__ void k_round_v(const double* __restrict__ A, int64_t g, int ld, float
     Vf[t] = (float)A[t];
 }
 
+__global__ void k_round_v_batch(const RoundTask* __restrict__ tasks, int64_t g, int ld) {
+  const RoundTask tk = tasks[blockIdx.y];
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < g * ld;
+       t += (int64_t)gridDim.x * blockDim.x)
+    tk.Vf[t] = (float)tk.A[t];
+}
+
 // mc[c] = sum_j mu_j Vf[j][c], FP64 accumulation, one block per column.
-__global__ void k_mean_prefactor(const float* __restrict__ Vf, int64_t g, int ld,
-                                 const double* __restrict__ mu, float* __restrict__ mc) {
+__device__ __forceinline__ void mean_prefactor_body(const float* Vf, int64_t g, int ld, const double* mu,
+                                                    float* mc, int c) {
   __shared__ double red[256];
-  const int c = blockIdx.x;
   double acc = 0.0;
   if (mu)
     for (int64_t j = threadIdx.x; j < g; j += blockDim.x) acc += mu[j] * (double)Vf[j * ld + c];
@@ -538,6 +698,25 @@ __global__ void k_mean_prefactor(const float* __restrict__ Vf, int64_t g, int ld
     __syncthreads();
   }
   if (threadIdx.x == 0) mc[c] = (float)red[0];
+}
+
+__global__ void k_mean_prefactor(const float* __restrict__ Vf, int64_t g, int ld,
+                                 const double* __restrict__ mu, float* __restrict__ mc) {
+  mean_prefactor_body(Vf, g, ld, mu, mc, blockIdx.x);
+}
+
+__global__ void k_mean_prefactor_batch(const RoundTask* __restrict__ tasks, int64_t g, int ld) {
+  const RoundTask tk = tasks[blockIdx.y];
+  mean_prefactor_body(tk.Vf, g, ld, tk.mu, tk.mc, blockIdx.x);
+}
+
+cudaError_t launch_round_v_batch(const RoundTask* tasks, int ntasks, int64_t g, int ld, cudaStream_t st) {
+  if (ntasks <= 0) return cudaSuccess;
+  note_launches(2);
+  const int gx = (int)std::min<int64_t>((g * ld + 255) / 256, 64);
+  k_round_v_batch<<<dim3((unsigned)gx, (unsigned)ntasks), 256, 0, st>>>(tasks, g, ld);
+  k_mean_prefactor_batch<<<dim3((unsigned)ld, (unsigned)ntasks), 256, 0, st>>>(tasks, g, ld);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_mean_prefactor(const float* Vf, int64_t g, int ld, const double* mu, float* mc,

@@ -187,12 +187,12 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* _
 // With width > 0 the output is a column panel of a wider matrix: element i
 // goes to out[(i / width) * ldo + i % width].
 template <typename T>
-__global__ void __launch_bounds__(256) k_reduce_rows(const T* __restrict__ part, int nparts, int64_t len,
-                                                     double* __restrict__ out, int accumulate, int width = 0,
-                                                     int ldo = 0) {
+__device__ __forceinline__ void reduce_rows_body(const T* __restrict__ part, int nparts, int64_t len,
+                                                 double* __restrict__ out, int accumulate, int width, int ldo,
+                                                 int blk, int nblk) {
   __shared__ double red[8][33];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int64_t base = (int64_t)blockIdx.x * 32; base < len; base += (int64_t)gridDim.x * 32) {
+  for (int64_t base = (int64_t)blk * 32; base < len; base += (int64_t)nblk * 32) {
     const int64_t i = base + lane;
     double acc = 0.0;
     if (i < len) {
@@ -220,6 +220,30 @@ __global__ void __launch_bounds__(256) k_reduce_rows(const T* __restrict__ part,
     }
     __syncthreads();
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_reduce_rows(const T* __restrict__ part, int nparts, int64_t len,
+                                                     double* __restrict__ out, int accumulate, int width = 0,
+                                                     int ldo = 0) {
+  reduce_rows_body<T>(part, nparts, len, out, accumulate, width, ldo, blockIdx.x, gridDim.x);
+}
+
+// One reduction per grid row y (batched segments): the task's part into its G.
+__global__ void __launch_bounds__(256) k_reduce_rows_batch(const GramTask* __restrict__ tasks, int nparts,
+                                                           int64_t len) {
+  const GramTask t = tasks[blockIdx.y];
+  reduce_rows_body<double>(t.part, nparts, len, t.G, 0, 0, 0, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_reduce_rows_f64_batch(const GramTask* tasks, int ntasks, int nparts, int64_t len, cudaStream_t st,
+                                         int num_sms) {
+  if (ntasks <= 0) return cudaSuccess;
+  const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((len + 31) / 32, 16));
+  note_launches(1);
+  k_reduce_rows_batch<<<dim3((unsigned)gx, (unsigned)ntasks), 256, 0, st>>>(tasks, nparts, len);
+  (void)num_sms;
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

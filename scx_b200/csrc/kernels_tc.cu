@@ -883,6 +883,15 @@ __global__ void k_split16(const float* __restrict__ in, int64_t count, uint32_t*
     img[i] = hilo16(in[i], fmt);
 }
 
+// One matrix per grid row y (batched segments).
+__global__ void k_split16_batch(const SplitTask* __restrict__ tasks, int64_t count, int fmt) {
+  const SplitTask t = tasks[blockIdx.y];
+  uint32_t* img = reinterpret_cast<uint32_t*>(t.img);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x)
+    img[i] = hilo16(t.in[i], fmt);
+}
+
 // ---------------------------------------------------------------------------
 // ld 64: the two products with the dense operand's image as the MMA's A and
 // the densified tiles as its B, so one instruction spans N = 256 cells (two
@@ -1489,6 +1498,14 @@ cudaError_t launch_rmat_tc(int ld, const uint32_t* ent, const void* meta, int64_
     cudaFuncSetAttribute(k_rmat_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_rmat_tc<128><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, g, gene_groups, *qmap, part, fmt, err);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_split16_batch(const SplitTask* tasks, int ntasks, int64_t count, int fmt, cudaStream_t st) {
+  if (ntasks <= 0 || count <= 0) return cudaSuccess;
+  const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((count + 255) / 256, 64));
+  note_launches(1);
+  k_split16_batch<<<dim3((unsigned)gx, (unsigned)ntasks), 256, 0, st>>>(tasks, count, fmt);
   return cudaGetLastError();
 }
 

@@ -124,6 +124,36 @@ struct JacobiTask {
   double* evecs;
   int* sweeps;
 };
+// Per-segment arguments of the batched gene-side launches (one grid row per segment).
+struct ApplyTask {  // Z = (W - mu s^T) M (mu may be null)
+  const double* W;
+  const double* mu;
+  const double* s;
+  const double* M;
+  double* Z;
+};
+struct GramTask {  // Gram partials of A into part, then their sum into G
+  const double* A;
+  double* part;
+  double* G;
+};
+struct RoundTask {  // Vf = (float) A, mc = mu^T Vf
+  const double* A;
+  const double* mu;
+  float* Vf;
+  float* mc;
+};
+struct SplitTask {  // 16-bit image of a float matrix
+  const float* in;
+  uint16_t* img;
+};
+cudaError_t launch_center_apply_batch(const ApplyTask* tasks, int ntasks, int64_t g, int ld, cudaStream_t st);
+cudaError_t launch_gram_f64_batch(const GramTask* tasks, int ntasks, int64_t n, int ld, int nparts,
+                                  cudaStream_t st, int num_sms);
+cudaError_t launch_reduce_rows_f64_batch(const GramTask* tasks, int ntasks, int nparts, int64_t len, cudaStream_t st,
+                                         int num_sms);
+cudaError_t launch_round_v_batch(const RoundTask* tasks, int ntasks, int64_t g, int ld, cudaStream_t st);
+cudaError_t launch_split16_batch(const SplitTask* tasks, int ntasks, int64_t count, int fmt, cudaStream_t st);
 // ntasks factorisations of one launch, one block each (k, ld <= 128).
 cudaError_t launch_cholesky_batch(const CholTask* tasks, int ntasks, int k, int ld, double tau, int shift_on_fail,
                                   cudaStream_t st);
@@ -140,7 +170,7 @@ cudaError_t launch_gram_f64(const double* A, int64_t n, int ld, double* part, in
 // factorisation (shift_on_fail) or is set to -(j+1) on a failed pivot j.
 cudaError_t launch_cholesky(const double* G, int k, int ld, double tau, int shift_on_fail,
                             double* R, double* Rinv, float* Rinv_f, int* status, cudaStream_t st);
-// Tall apply: Out[i, :] = In[i, :] * M (ld x ld float, upper-triangular or full).
+// Tall apply: Out[i, :] = In[i, :] * M (ld x ld float, upper-triangular: the Cholesky inverse).
 cudaError_t launch_apply_right_f32(const float* In, int64_t n, int ld, const float* M,
                                    float* Out, cudaStream_t st, int num_sms);
 // Same, also writing the 16-bit image of Out (n x 2 ld; fmt 1 = bf16, 0 = f16).

@@ -1561,7 +1561,9 @@ void rmatmat_raw(scxpca_plan* pl, float* A, int split) {
 // the product also leaves the image of Y for the Gram and the transposed
 // product; `f32` = false skips the FP32 copy of Y when nothing reads it
 // (inside the power loop at ld 64, whose Gram uses the image).
-void forward(scxpca_plan* pl, bool f32 = true) {
+// `split_v` = false: V's 16-bit image is already written (a batch writes all
+// segments' images in one launch).
+void forward(scxpca_plan* pl, bool f32 = true, bool split_v = true) {
   cudaStream_t st = pl->stream;
   if (pl->streaming) {
     int s = stage_begin(pl);
@@ -1575,7 +1577,8 @@ void forward(scxpca_plan* pl, bool f32 = true) {
   }
   if (pl->use_tc) {
     int s = stage_begin(pl);
-    CK(launch_split16(pl->V.as<float>(), pl->g * pl->ld, pl->Vimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
+    if (split_v)
+      CK(launch_split16(pl->V.as<float>(), pl->g * pl->ld, pl->Vimg.as<uint16_t>(), pl->fmt16, st, pl->num_sms));
     stage_end(pl, SCXPCA_STAGE_SMALL, s);
     s = stage_begin(pl);
     CK(launch_fwd_tc((int)pl->ld, pl->tf_ent.as<uint32_t>(), pl->tf_meta.p, pl->n, pl->n_chunks, &pl->vmap,
@@ -1662,6 +1665,18 @@ struct DeviceOperator {
     // Only the last forward product's FP32 Y is read (by finalize_q); the
     // tensor-core Gram at ld 64 reads the 16-bit image.
     forward(pl, !image_only || last);
+  }
+  // The size-proportional halves of matmat and rmatmat, for a batch that runs
+  // the gene-side halves (V's image; the centring and R^{-1} apply) of all
+  // segments in one launch each.
+  void matmat_products(bool last) { forward(pl, !image_only || last, false); }
+  void rmatmat_products() {
+    rmatmat_raw(pl, pl->Y.as<float>(), 0);
+    if (pl->pflog) CK(launch_aug_fold(pl->W.as<double>(), (int32_t)pl->g_user, (int)pl->ld, pl->stream, pl->num_sms));
+  }
+  ApplyTask rmatmat_task() const {
+    return ApplyTask{pl->W.as<double>(), mu, sY, closing ? pl->R2inv.as<double>() : pl->Rinv.as<double>(),
+                     pl->Z.as<double>()};
   }
   void qr(Buf b) {
     if (b == Buf::kY) {
@@ -2026,9 +2041,13 @@ struct scxpca_batch {
   // 16, 32 branches; [6..11] lockstep over as many streams
   double tuned_ms[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   scxpca_params params{};
-  // the lockstep schedule's batched k x k launches: one task per segment for
-  // the loop's Cholesky (R^{-1}), the closing one (R2^{-1}) and the eigensolve
+  // the lockstep schedule's batched launches: one task per segment for the
+  // loop's Cholesky (R^{-1}), the closing one (R2^{-1}) and the eigensolve;
+  // and for the gene-side work (V's image, the centring + R^{-1} apply of the
+  // transposed product in the loop and at the close, Z's Gram, Z R^{-1},
+  // the rounding of Z into V)
   DevBuf task_qr, task_fin, task_eig;
+  DevBuf task_split, task_apply_loop, task_apply_close, task_small_apply, task_gram_z, task_round;
 
   ~scxpca_batch() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -2037,9 +2056,9 @@ struct scxpca_batch {
     for (scxpca_plan* pl : plans) delete pl;
     for (DevBuf* b : indptrs) delete b;
     emb.release();
-    task_qr.release();
-    task_fin.release();
-    task_eig.release();
+    for (DevBuf* t : {&task_qr, &task_fin, &task_eig, &task_split, &task_apply_loop, &task_apply_close,
+                      &task_small_apply, &task_gram_z, &task_round})
+      t->release();
     for (cudaStream_t st : branch) cudaStreamDestroy(st);
     for (cudaEvent_t e : join) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
@@ -2105,6 +2124,9 @@ struct BatchOperator {
   // stream (one block per segment) between the step's two forked halves,
   // instead of one single-block launch per segment on its branch
   bool small_batched = false;
+  // the gene-side work of every segment (n_vars x k, the same size for all)
+  // in one launch per kernel on the main stream as well
+  bool gene_batched = false;
 
   template <class F>
   void each(F&& f) {
@@ -2119,8 +2141,31 @@ struct BatchOperator {
       CK(cudaStreamWaitEvent(b->main, b->join[t], 0));
     }
   }
-  void matmat(Operand src, bool last) { each([&](int, DeviceOperator& o) { o.matmat(src, last); }); }
-  void rmatmat() { each([&](int, DeviceOperator& o) { o.rmatmat(); }); }
+  const scxpca_plan* p0() const { return ops[0].pl; }
+  int ns() const { return (int)ops.size(); }
+  void matmat(Operand src, bool last) {
+    if (!gene_batched || src == Operand::kOmega) {
+      each([&](int, DeviceOperator& o) { o.matmat(src, last); });
+      return;
+    }
+    if (p0()->use_tc)
+      CK(launch_split16_batch(b->task_split.as<SplitTask>(), ns(), p0()->g * p0()->ld, p0()->fmt16, b->main));
+    each([&](int, DeviceOperator& o) { o.matmat_products(last); });
+  }
+  void rmatmat() {
+    if (!gene_batched) {
+      each([&](int, DeviceOperator& o) { o.rmatmat(); });
+      return;
+    }
+    each([&](int, DeviceOperator& o) { o.rmatmat_products(); });
+    const DevBuf& t = ops[0].closing ? b->task_apply_close : b->task_apply_loop;
+    CK(launch_center_apply_batch(t.as<ApplyTask>(), ns(), p0()->g, (int)p0()->ld, b->main));
+  }
+  // Z's Gram for every segment (the closing one, or qr(Z)'s), on the main stream
+  void gram_z_all() {
+    CK(launch_gram_f64_batch(b->task_gram_z.as<GramTask>(), ns(), p0()->g, (int)p0()->ld, p0()->gram_parts_small,
+                             b->main, p0()->num_sms));
+  }
   void chol_all(const DevBuf& tasks) {
     const scxpca_plan* p0 = ops[0].pl;
     CK(launch_cholesky_batch(tasks.as<CholTask>(), (int)ops.size(), (int)p0->k, (int)p0->ld, p0->tau,
@@ -2129,6 +2174,14 @@ struct BatchOperator {
   void qr(Buf x) {
     if (!small_batched) {
       each([&](int, DeviceOperator& o) { o.qr(x); });
+      return;
+    }
+    if (x == Buf::kZ && gene_batched) {
+      // all on the main stream: Gram, factor, Z R^{-1}, rounding into V
+      gram_z_all();
+      chol_all(b->task_qr);
+      CK(launch_center_apply_batch(b->task_small_apply.as<ApplyTask>(), ns(), p0()->g, (int)p0()->ld, b->main));
+      CK(launch_round_v_batch(b->task_round.as<RoundTask>(), ns(), p0()->g, (int)p0()->ld, b->main));
       return;
     }
     each([&](int, DeviceOperator& o) { o.qr_gram(x); });
@@ -2165,12 +2218,41 @@ bool batch_prepare_tasks(scxpca_batch* b, BatchOperator& bop) {
     tf[q] = bop.ops[q].finalize_task();
     te[q] = finish_task(b->plans[q]);
   }
-  b->task_qr.alloc(sizeof(CholTask) * ns);
-  b->task_fin.alloc(sizeof(CholTask) * ns);
-  b->task_eig.alloc(sizeof(JacobiTask) * ns);
-  CK(cudaMemcpyAsync(b->task_qr.p, tq.data(), sizeof(CholTask) * ns, cudaMemcpyHostToDevice, b->main));
-  CK(cudaMemcpyAsync(b->task_fin.p, tf.data(), sizeof(CholTask) * ns, cudaMemcpyHostToDevice, b->main));
-  CK(cudaMemcpyAsync(b->task_eig.p, te.data(), sizeof(JacobiTask) * ns, cudaMemcpyHostToDevice, b->main));
+  auto put = [&](DevBuf& buf, const void* src, size_t bytes) {
+    buf.alloc(bytes);
+    CK(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, b->main));
+  };
+  put(b->task_qr, tq.data(), sizeof(CholTask) * ns);
+  put(b->task_fin, tf.data(), sizeof(CholTask) * ns);
+  put(b->task_eig, te.data(), sizeof(JacobiTask) * ns);
+  // the gene-side tables: every segment has n_vars rows of the same k columns
+  bool gene = true;
+  for (const scxpca_plan* pl : b->plans)
+    gene = gene && pl->use_tc == p0->use_tc && pl->fmt16 == p0->fmt16 && !pl->pflog && !pl->streaming &&
+           pl->gram_parts_small == p0->gram_parts_small;
+  if (gene) {
+    std::vector<SplitTask> tsp(ns);
+    std::vector<ApplyTask> tal(ns), tac(ns), tsa(ns);
+    std::vector<GramTask> tg(ns);
+    std::vector<RoundTask> tr(ns);
+    for (size_t q = 0; q < ns; ++q) {
+      scxpca_plan* pl = b->plans[q];
+      const DeviceOperator& o = bop.ops[q];
+      tsp[q] = SplitTask{pl->V.as<float>(), pl->Vimg.as<uint16_t>()};
+      tal[q] = ApplyTask{pl->W.as<double>(), o.mu, o.sY, pl->Rinv.as<double>(), pl->Z.as<double>()};
+      tac[q] = ApplyTask{pl->W.as<double>(), o.mu, o.sY, pl->R2inv.as<double>(), pl->Z.as<double>()};
+      tsa[q] = ApplyTask{pl->Z.as<double>(), nullptr, nullptr, pl->Rinv.as<double>(), pl->Z.as<double>()};
+      tg[q] = GramTask{pl->Z.as<double>(), pl->gpart.as<double>(), pl->G.as<double>()};
+      tr[q] = RoundTask{pl->Z.as<double>(), o.mu, pl->V.as<float>(), pl->mc.as<float>()};
+    }
+    if (p0->use_tc) put(b->task_split, tsp.data(), sizeof(SplitTask) * ns);
+    put(b->task_apply_loop, tal.data(), sizeof(ApplyTask) * ns);
+    put(b->task_apply_close, tac.data(), sizeof(ApplyTask) * ns);
+    put(b->task_small_apply, tsa.data(), sizeof(ApplyTask) * ns);
+    put(b->task_gram_z, tg.data(), sizeof(GramTask) * ns);
+    put(b->task_round, tr.data(), sizeof(RoundTask) * ns);
+  }
+  bop.gene_batched = gene;
   CK(cudaStreamSynchronize(b->main));
   return true;
 }
@@ -2208,7 +2290,10 @@ void batch_capture(scxpca_batch* b, int nb, bool lockstep) {
       });
       run_power_loop(bop, p.n_power_iterations);
       if (bop.small_batched) {
-        bop.each([&](int, DeviceOperator& o) { finish_gram(o.pl); });
+        if (bop.gene_batched)
+          bop.gram_z_all();
+        else
+          bop.each([&](int, DeviceOperator& o) { finish_gram(o.pl); });
         const scxpca_plan* p0 = b->plans[0];
         CK(launch_jacobi_eig_batch(b->task_eig.as<JacobiTask>(), (int)b->plans.size(), (int)p0->k, (int)p0->ld,
                                    b->main));
