@@ -47,11 +47,12 @@ constexpr int kStatsPassGenes = (int)((kStatsSmemMax - kStatsWindowBytes) / 16);
 static_assert(kStatsSteps == 32, "the bucket scan gives one window step to each lane of a warp");
 static_assert(kStatsSteps % kStatsWarps == 0, "every warp holds the same number of window steps");
 
-template <typename ValT>
-__global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* __restrict__ idx,
-                                                                const ValT* __restrict__ val, int64_t nnz,
-                                                                int32_t g, int32_t pass_genes, int nparts,
-                                                                int block0, double* __restrict__ partial) {
+// `value(p, j, first)` gives entry p's value (gene j) as float; `first` is
+// true in the first gene pass.
+template <typename Value>
+__device__ __forceinline__ void col_stats_body(const int32_t* __restrict__ idx, Value value, int64_t nnz, int32_t g,
+                                               int32_t pass_genes, int nparts, int block0,
+                                               double* __restrict__ partial) {
   extern __shared__ double sm[];  // [2][pass_genes] accumulators, then the bucketed window
   double* acc = sm;
   int32_t* b_idx = reinterpret_cast<int32_t*>(sm + 2 * (int64_t)pass_genes);
@@ -81,7 +82,7 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* _
       for (int u = 0; u < kPer; ++u) {
         const int t = (kStatsWarps * u + warp) * 32 + lane;
         ri[u] = t < c ? __ldg(idx + w + t) : -1;
-        rv[u] = t < c ? to_f32(val[w + t]) : 0.f;
+        rv[u] = t < c ? value(w + t, ri[u], lo == 0) : 0.f;
       }
     };
     if (s < e) load(s);
@@ -180,6 +181,36 @@ __global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* _
   }
 }
 
+template <typename ValT>
+__global__ void __launch_bounds__(kStatsWarps * 32) k_col_stats(const int32_t* __restrict__ idx,
+                                                                const ValT* __restrict__ val, int64_t nnz,
+                                                                int32_t g, int32_t pass_genes, int nparts,
+                                                                int block0, double* __restrict__ partial) {
+  col_stats_body(idx, [&](int64_t p, int32_t, bool) { return to_f32(val[p]); }, nnz, g, pass_genes, nparts, block0,
+                 partial);
+}
+
+// The value transform of one entry (k_transform_values, below): the working
+// value as stored.
+template <typename InT, typename OutT>
+__device__ __forceinline__ OutT transform_value(InT v, int32_t j, int mode, const double* __restrict__ mu,
+                                                const double* __restrict__ inv_std,
+                                                const double* __restrict__ cshift, double clip) {
+  double x = (double)to_f32(v);
+  if (mode != 0) {
+    const double is = __ldg(inv_std + j);
+    if (mode == 1) {
+      double sv = (x - __ldg(mu + j)) * is;
+      if (clip > 0.0) sv = fmin(fmax(sv, -clip), clip);
+      x = sv - __ldg(cshift + j);
+    } else {
+      x = x * is;
+      if (clip > 0.0) x = fmin(x, clip);
+    }
+  }
+  return from_f32<OutT>((float)x);
+}
+
 // out[i] (+)= sum_{b < nparts} part[b * len + i] in FP64.  A block takes 32
 // consecutive outputs (one per lane, coalesced); warp w sums the partials
 // b = w, w + 8, ... with four loads in flight, and warp 0 adds the eight warp
@@ -260,22 +291,8 @@ __global__ void k_transform_values(const int32_t* __restrict__ idx, const InT* _
                                    const double* __restrict__ mu, const double* __restrict__ inv_std,
                                    const double* __restrict__ cshift, double clip) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nnz;
-       p += (int64_t)gridDim.x * blockDim.x) {
-    double x = (double)to_f32(in[p]);
-    if (mode != 0) {
-      int32_t j = __ldg(idx + p);
-      double is = __ldg(inv_std + j);
-      if (mode == 1) {
-        double s = (x - __ldg(mu + j)) * is;
-        if (clip > 0.0) s = fmin(fmax(s, -clip), clip);
-        x = s - __ldg(cshift + j);
-      } else {
-        x = x * is;
-        if (clip > 0.0) x = fmin(x, clip);
-      }
-    }
-    out[p] = from_f32<OutT>((float)x);
-  }
+       p += (int64_t)gridDim.x * blockDim.x)
+    out[p] = transform_value<InT, OutT>(in[p], mode != 0 ? __ldg(idx + p) : 0, mode, mu, inv_std, cshift, clip);
 }
 
 // ---------------------------------------------------------------------------
