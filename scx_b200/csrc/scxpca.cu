@@ -350,12 +350,26 @@ struct scxpca_plan {
 
   // opt-in stage timing
   bool profiling = false;
+
+  // A plan run replayed as a CUDA graph: recorded on the second run with the
+  // same (power iterations, seed, omega, embeddings buffer), replayed while
+  // they stay the same (one launch instead of ~375).
+  struct RunGraph {
+    cudaGraphExec_t exec = nullptr;
+    int64_t q = -1;
+    uint64_t seed = 0;
+    const float* omega = nullptr;
+    float* U = nullptr;
+    int64_t launches = 0;  // kernels in the graph
+    bool seen = false;     // the key was run once without a graph
+  } rg;
   std::vector<cudaEvent_t> events;
   std::vector<std::pair<int, int>> marks;  // (stage, index of the begin event)
   int events_used = 0;
   scxpca_profile prof{};
 
   ~scxpca_plan() {
+    if (rg.exec) cudaGraphExecDestroy(rg.exec);
     for (cudaEvent_t e : events) cudaEventDestroy(e);
     if (copy_stream) {
       cudaStreamSynchronize(copy_stream);
@@ -1841,6 +1855,60 @@ void finish_result(scxpca_plan* pl, const int* hstatus, const double* sigma, scx
   pl->run_valid = true;
 }
 
+// One run on the plan's stream.  A plan run again with the same power
+// iterations, seed, omega and embeddings buffer replays the graph of that run
+// (recorded on its second occurrence); stage profiling, a host omega (staged
+// by an allocation) and SCXPCA_GRAPH=0 keep the plain launches.
+void enqueue_run_replayed(scxpca_plan* pl, const scxpca_params& p, float* U) {
+  const char* env = getenv("SCXPCA_GRAPH");
+  const bool allowed = !(env && env[0] == '0') && !pl->profiling && !pl->streaming &&
+                       (!p.omega || p.omega_memory == SCXPCA_MEM_DEVICE);
+  scxpca_plan::RunGraph& g = pl->rg;
+  const bool same = g.q == p.n_power_iterations && g.seed == p.seed && g.omega == p.omega && g.U == U;
+  if (allowed && same && g.exec) {
+    CK(cudaGraphLaunch(g.exec, pl->stream));
+    pl->prof.kernel_launches += g.launches;
+    return;
+  }
+  if (!allowed || !same || !g.seen) {
+    if (!same) {
+      if (g.exec) CK(cudaGraphExecDestroy(g.exec));
+      g = scxpca_plan::RunGraph{};
+      g.q = p.n_power_iterations;
+      g.seed = p.seed;
+      g.omega = p.omega;
+      g.U = U;
+    }
+    g.seen = true;
+    const int64_t launches0 = launches_total();
+    enqueue_run(pl, p, U);
+    pl->prof.kernel_launches += launches_total() - launches0;
+    return;
+  }
+  // second run with this key: record it, then replay
+  cudaGraph_t graph = nullptr;
+  const int64_t launches0 = launches_total();
+  CK(cudaStreamBeginCapture(pl->stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    enqueue_run(pl, p, U);
+  } catch (...) {
+    cudaStreamEndCapture(pl->stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    throw;
+  }
+  g.launches = launches_total() - launches0;
+  CK(cudaStreamEndCapture(pl->stream, &graph));
+  cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    g.exec = nullptr;
+    CK(e);
+  }
+  CK(cudaGraphLaunch(g.exec, pl->stream));
+  pl->prof.kernel_launches += g.launches;
+}
+
 void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
   if (!out) fail(SCXPCA_INVALID_ARGUMENT, "null result");
   if (!out->embeddings) fail(SCXPCA_INVALID_ARGUMENT, "null embeddings output");
@@ -1852,9 +1920,7 @@ void run_plan(scxpca_plan* pl, const scxpca_params* over, scxpca_result* out) {
     pl->U.alloc(sizeof(float) * pl->n * pl->nc);
     U = pl->U.as<float>();
   }
-  const int64_t launches0 = launches_total();
-  enqueue_run(pl, p, U);
-  pl->prof.kernel_launches += launches_total() - launches0;
+  enqueue_run_replayed(pl, p, U);
   pl->prof.runs += 1;
   phase_mark(SCXPCA_PHASE_PCA, st);
   if (host_out)
