@@ -182,7 +182,13 @@ int32_t scxpca_plan_create(const scxpca_csr* x, const scxpca_params* params,
  * (run_resident_power_loop, gpu_pca_resident.rs:295-347, then
  * randomized_pca_core steps 7-8, gpu_pca.rs:590-697).  Only `seed`, `omega`,
  * `omega_memory` and `n_power_iterations` of `params` may differ from the
- * values the plan was created with; NULL reuses the creation parameters. */
+ * values the plan was created with; NULL reuses the creation parameters.
+ * A plan run again with the same n_power_iterations, seed, omega pointer and
+ * embeddings buffer records that run as a CUDA graph on its second
+ * occurrence and replays it afterwards (same results, one launch); stage
+ * profiling, a host omega or the environment variable SCXPCA_GRAPH=0 keep
+ * plain kernel launches.  The graph reads omega and writes the embeddings
+ * at the pointers given, so their contents may change between runs. */
 int32_t scxpca_plan_run(scxpca_plan* plan, const scxpca_params* params,
                         scxpca_result* out, char* err, size_t err_len);
 
