@@ -63,6 +63,14 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
   return y * pow2_int(-h);
 }
 
+// Opts kernel `kern` in to `smem` bytes of dynamic shared memory.  A refused
+// opt-in is returned to the launcher, so the caller sees its cause rather than
+// the launch failure that would follow it.
+template <typename Kernel>
+inline cudaError_t allow_smem(Kernel* kern, size_t smem) {
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
 // Grid size for a grid-stride loop over `work` items at `per_block` items per
 // block: a multiple of the SM count, never more blocks than there is work.
 inline int grid_for(int64_t work, int per_block, int num_sms, int blocks_per_sm = 8) {

@@ -350,7 +350,7 @@ static cudaError_t sddmm_t(const int64_t* indptr, const int32_t* idx, const void
                            int ldv, int cs, const double* scale, int accumulate, float* grad, double* part,
                            cudaStream_t st) {
   const size_t smem = sddmm_smem_bytes(cs);
-  cudaFuncSetAttribute(k_sddmm<ValT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaError_t e = allow_smem(k_sddmm<ValT>, smem); e != cudaSuccess) return e;
   dim3 grid(nchunks, nb);
   note_launches(1);
   k_sddmm<ValT><<<grid, 512, smem, st>>>(indptr, idx, static_cast<const ValT*>(val), n, g, rbp, nb, rows_per_chunk,

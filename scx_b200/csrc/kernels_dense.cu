@@ -571,10 +571,10 @@ static cudaError_t tall_mm(const float* In, int64_t n, int K, int ldi, const flo
   const int grid = grid_for(n, kTallRows, num_sms, per_sm);
   note_launches(1);
   if (outb == 64) {
-    cudaFuncSetAttribute(k_tall_mm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaError_t e = allow_smem(k_tall_mm<64>, smem); e != cudaSuccess) return e;
     k_tall_mm<64><<<grid, 256, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo, img, fmt);
   } else {
-    cudaFuncSetAttribute(k_tall_mm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaError_t e = allow_smem(k_tall_mm<128>, smem); e != cudaSuccess) return e;
     k_tall_mm<128><<<grid, 256, smem, st>>>(In, n, K, ldi, M, ldm, cnt, Out, ldo, img, fmt);
   }
   return cudaGetLastError();
@@ -659,7 +659,7 @@ cudaError_t launch_center_apply(const double* W, int64_t g, int ld, const double
                                 const double* s, const double* M, double* Z, cudaStream_t st) {
   if (ld > kMaxK) return launch_center_apply_wide(W, g, ld, mu, s, M, Z, st);
   size_t smem = (size_t)(ld * ld + 256) * sizeof(double);
-  cudaFuncSetAttribute(k_center_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaError_t e = allow_smem(k_center_apply, smem); e != cudaSuccess) return e;
   int rpb = 256 / ld;
   int grid = (int)std::min<int64_t>((g + rpb - 1) / rpb, 160);  // M is staged once per block
   note_launches(1);

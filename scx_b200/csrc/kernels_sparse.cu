@@ -456,8 +456,7 @@ static cudaError_t col_stats_blocks_t(const int32_t* idx, const void* val, int64
   const int32_t pass_genes = std::min<int32_t>(g, kStatsPassGenes);
   const size_t smem = (size_t)2 * pass_genes * sizeof(double) + kStatsWindowBytes;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_col_stats<ValT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    if (cudaError_t e = allow_smem(k_col_stats<ValT>, smem); e != cudaSuccess) return e;
   }
   k_col_stats<ValT><<<nblocks, kStatsWarps * 32, smem, st>>>(idx, v, nnz, g, pass_genes, nparts, block0, partial);
   note_launches(1);
@@ -571,7 +570,7 @@ static cudaError_t spmm_t_c(const int64_t* indptr, const int32_t* idx, const voi
   constexpr int GB = kTransposeGeneBlock;
   size_t smem = (size_t)GB * 32 * C * sizeof(float);
   auto kern = k_spmm_t<C, ValT, GB>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaError_t e = allow_smem(kern, smem); e != cudaSuccess) return e;
   dim3 grid(nchunks, nb);
   note_launches(1);
   kern<<<grid, 512, smem, st>>>(indptr, idx, static_cast<const ValT*>(val), n, g, rbp, nb,

@@ -1408,7 +1408,7 @@ cudaError_t tile_format_fill(const int64_t* indptr, const int32_t* idx, const vo
                              int num_sms) {
   const int64_t n_tiles = (n + TM - 1) / TM;
   size_t smem = (size_t)2 * TM * nc * sizeof(int);
-  cudaFuncSetAttribute(k_tile_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaError_t e = allow_smem(k_tile_fill, smem); e != cudaSuccess) return e;
   note_launches(1);
   k_tile_fill<<<grid_for(n_tiles, 1, num_sms, 2), 512, smem, st>>>(
       indptr, idx, static_cast<const uint16_t*>(val16), n, n_tiles, nc, seg, ent,
@@ -1459,12 +1459,12 @@ cudaError_t launch_fwd_tc(int ld, const uint32_t* ent, const void* meta, int64_t
   if (ld == 64) {
     const int grid = (int)std::min<int64_t>((n_tiles + 1) / 2, (int64_t)num_sms);
     const size_t smem = fwd_swap_smem();
-    cudaFuncSetAttribute(k_fwd_swap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaError_t e = allow_smem(k_fwd_swap, smem); e != cudaSuccess) return e;
     k_fwd_swap<<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, n, *vmap, mc, Y, Yimg, fmt, err);
   } else {
     const int grid = (int)std::min<int64_t>(n_tiles, (int64_t)num_sms);
     const size_t smem = fwd_smem(128);
-    cudaFuncSetAttribute(k_fwd_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaError_t e = allow_smem(k_fwd_tc<128>, smem); e != cudaSuccess) return e;
     k_fwd_tc<128><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, n, *vmap, mc, Y, Yimg, fmt, err);
   }
   return cudaGetLastError();
@@ -1491,11 +1491,11 @@ cudaError_t launch_rmat_tc(int ld, const uint32_t* ent, const void* meta, int64_
   note_launches(1);
   if (ld == 64) {
     const size_t smem = rmat_swap_smem();
-    cudaFuncSetAttribute(k_rmat_swap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaError_t e = allow_smem(k_rmat_swap, smem); e != cudaSuccess) return e;
     k_rmat_swap<<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, g, gene_groups, *qmap, part, fmt, err);
   } else {
     const size_t smem = rmat_smem(128);
-    cudaFuncSetAttribute(k_rmat_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaError_t e = allow_smem(k_rmat_tc<128>, smem); e != cudaSuccess) return e;
     k_rmat_tc<128><<<grid, kThreads, smem, st>>>(ent, m, n_tiles, nc, g, gene_groups, *qmap, part, fmt, err);
   }
   return cudaGetLastError();
@@ -1520,7 +1520,7 @@ int launch_gram_tc(int64_t n, const CUtensorMap* qmap, double* part, int fmt, in
   const int64_t n_tiles = (n + TM - 1) / TM;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, num_sms));
   const size_t smem = 1024 + (size_t)kGramStages * 2 * TM * 64 * 2 + TM * 64 * 2 + TM * 64 * 4 + 256;
-  cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (allow_smem(k_gram_tc, smem) != cudaSuccess) return -1;
   note_launches(1);
   k_gram_tc<<<grid, 128, smem, st>>>(n_tiles, *qmap, part, fmt, err);
   return cudaGetLastError() == cudaSuccess ? grid : -1;
