@@ -603,68 +603,124 @@ cudaError_t launch_apply_right_split(const float* In, int64_t n, int ld, const f
 }
 
 // ---------------------------------------------------------------------------
-// Gene-side FP64 ops.  Block = 256 threads handles 256 / ld rows at a time.
+// Gene-side FP64 ops: Z = (W - mu s^T) M for a g x LD matrix W and an LD x LD
+// M (mu null: Z = W M; Z may be W).  A block of 256 threads stages M once and
+// then 64 rows of W at a time; thread (ty, tx) of the 16 x 16 grid owns rows
+// ty + 16 i (i < 4) and columns tx + 16 v (v < LD / 16) of the 64-row block,
+// so every shared value it reads feeds 4 or LD / 16 FMAs (one value per FMA
+// made the kernel shared-memory bound at 256 segments).  Each output is one
+// FMA chain over l = 0 .. LD-1 in order.
 // ---------------------------------------------------------------------------
-// Block b of nb (of one matrix's grid) takes rows b rpb, (b + nb) rpb, ...
-__device__ __forceinline__ void center_apply_body(const double* W, int64_t g, int ld, const double* mu,
-                                                  const double* s, const double* M, double* Z, int b, int nb) {
-  extern __shared__ double sm[];  // M [ld][ld], rows [256/ld][ld]
-  double* Ms = sm;
-  double* rows = sm + ld * ld;
-  for (int t = threadIdx.x; t < ld * ld; t += blockDim.x) Ms[t] = M[t];
-  const int rpb = blockDim.x / ld;
-  const int r = threadIdx.x / ld, c = threadIdx.x % ld;
-  for (int64_t j0 = (int64_t)b * rpb; j0 < g; j0 += (int64_t)nb * rpb) {
-    __syncthreads();
-    const int64_t j = j0 + r;
-    if (r < rpb && j < g) {
-      double v = W[j * ld + c];
-      if (mu) v -= mu[j] * s[c];
-      rows[r * ld + c] = v;
+constexpr int kApplyRows = 64;
+
+__host__ __device__ constexpr size_t center_apply_smem(int ld) {
+  return ((size_t)ld * ld + (size_t)kApplyRows * (ld + 1)) * sizeof(double);
+}
+
+// Block b of nb (of one matrix's grid) takes the row blocks b, b + nb, ...
+template <int LD>
+__device__ __forceinline__ void center_apply_body(const double* W, int64_t g, const double* mu, const double* s,
+                                                  const double* M, double* Z, int b, int nb) {
+  constexpr int TT = LD / 16, RP = LD + 1;  // odd row stride: rows ty and ty + 1 sit in different banks
+  extern __shared__ double sm[];
+  double* Ms = sm;             // [LD][LD]
+  double* rows = sm + LD * LD;  // [kApplyRows][LD + 1]
+  for (int t = threadIdx.x; t < LD * LD; t += 256) Ms[t] = M[t];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int64_t j0 = (int64_t)b * kApplyRows; j0 < g; j0 += (int64_t)nb * kApplyRows) {
+    __syncthreads();  // M staged; the previous block's rows consumed
+    for (int t = threadIdx.x; t < kApplyRows * LD; t += 256) {
+      const int r = t / LD, c = t % LD;
+      const int64_t j = j0 + r;
+      double v = 0.0;
+      if (j < g) {
+        v = W[j * LD + c];
+        if (mu) v -= mu[j] * s[c];
+      }
+      rows[r * RP + c] = v;
     }
     __syncthreads();
-    if (r < rpb && j < g) {
-      double acc = 0.0;
-      for (int l = 0; l < ld; ++l) acc = fma(rows[r * ld + l], Ms[l * ld + c], acc);
-      Z[j * ld + c] = acc;
+    double acc[4][TT];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int v = 0; v < TT; ++v) acc[i][v] = 0.0;
+#pragma unroll 4
+    for (int l = 0; l < LD; ++l) {
+      double a[4], m[TT];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = rows[(ty + 16 * i) * RP + l];
+#pragma unroll
+      for (int v = 0; v < TT; ++v) m[v] = Ms[l * LD + tx + 16 * v];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int v = 0; v < TT; ++v) acc[i][v] = fma(a[i], m[v], acc[i][v]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int64_t j = j0 + ty + 16 * i;
+      if (j < g)
+#pragma unroll
+        for (int v = 0; v < TT; ++v) Z[j * LD + tx + 16 * v] = acc[i][v];
     }
   }
 }
 
-__global__ void k_center_apply(const double* W, int64_t g, int ld, const double* __restrict__ mu,
-                               const double* __restrict__ s, const double* __restrict__ M, double* Z) {
-  center_apply_body(W, g, ld, mu, s, M, Z, blockIdx.x, gridDim.x);
+template <int LD>
+__global__ void __launch_bounds__(256) k_center_apply(const double* W, int64_t g, const double* __restrict__ mu,
+                                                      const double* __restrict__ s, const double* __restrict__ M,
+                                                      double* Z) {
+  center_apply_body<LD>(W, g, mu, s, M, Z, blockIdx.x, gridDim.x);
 }
 
 // One matrix per grid row y (batched segments).
-__global__ void k_center_apply_batch(const ApplyTask* __restrict__ tasks, int64_t g, int ld) {
+template <int LD>
+__global__ void __launch_bounds__(256) k_center_apply_batch(const ApplyTask* __restrict__ tasks, int64_t g) {
   const ApplyTask t = tasks[blockIdx.y];
-  center_apply_body(t.W, g, ld, t.mu, t.s, t.M, t.Z, blockIdx.x, gridDim.x);
+  center_apply_body<LD>(t.W, g, t.mu, t.s, t.M, t.Z, blockIdx.x, gridDim.x);
+}
+
+template <int LD>
+static cudaError_t center_apply_t(const ApplyTask* tasks, int ntasks, const double* W, int64_t g, const double* mu,
+                                  const double* s, const double* M, double* Z, cudaStream_t st) {
+  const size_t smem = center_apply_smem(LD);
+  const int64_t blocks = (g + kApplyRows - 1) / kApplyRows;
+  if (blocks == 0) return cudaSuccess;
+  note_launches(1);
+  if (tasks) {
+    if (cudaError_t e = allow_smem(k_center_apply_batch<LD>, smem); e != cudaSuccess) return e;
+    // up to 8 blocks per matrix, M staged once per block
+    const dim3 grid((unsigned)std::min<int64_t>(blocks, 8), (unsigned)ntasks);
+    k_center_apply_batch<LD><<<grid, 256, smem, st>>>(tasks, g);
+  } else {
+    if (cudaError_t e = allow_smem(k_center_apply<LD>, smem); e != cudaSuccess) return e;
+    k_center_apply<LD><<<(unsigned)std::min<int64_t>(blocks, 160), 256, smem, st>>>(W, g, mu, s, M, Z);
+  }
+  return cudaGetLastError();
+}
+
+static cudaError_t center_apply_ld(const ApplyTask* tasks, int ntasks, const double* W, int64_t g, int ld,
+                                   const double* mu, const double* s, const double* M, double* Z, cudaStream_t st) {
+  switch (ld) {
+    case 32: return center_apply_t<32>(tasks, ntasks, W, g, mu, s, M, Z, st);
+    case 64: return center_apply_t<64>(tasks, ntasks, W, g, mu, s, M, Z, st);
+    case 96: return center_apply_t<96>(tasks, ntasks, W, g, mu, s, M, Z, st);
+    case 128: return center_apply_t<128>(tasks, ntasks, W, g, mu, s, M, Z, st);
+    default: return cudaErrorInvalidValue;  // ld is a multiple of 32 up to kMaxK here
+  }
 }
 
 cudaError_t launch_center_apply_batch(const ApplyTask* tasks, int ntasks, int64_t g, int ld, cudaStream_t st) {
   if (ld > kMaxK) return cudaErrorInvalidValue;
   if (ntasks <= 0) return cudaSuccess;
-  size_t smem = (size_t)(ld * ld + 256) * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(k_center_apply_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const int rpb = 256 / ld;
-  const int grid = (int)std::min<int64_t>((g + rpb - 1) / rpb, 8);  // 8 blocks per matrix, ntasks matrices
-  note_launches(1);
-  k_center_apply_batch<<<dim3((unsigned)grid, (unsigned)ntasks), 256, smem, st>>>(tasks, g, ld);
-  return cudaGetLastError();
+  return center_apply_ld(tasks, ntasks, nullptr, g, ld, nullptr, nullptr, nullptr, nullptr, st);
 }
 
 cudaError_t launch_center_apply(const double* W, int64_t g, int ld, const double* mu,
                                 const double* s, const double* M, double* Z, cudaStream_t st) {
   if (ld > kMaxK) return launch_center_apply_wide(W, g, ld, mu, s, M, Z, st);
-  size_t smem = (size_t)(ld * ld + 256) * sizeof(double);
-  if (cudaError_t e = allow_smem(k_center_apply, smem); e != cudaSuccess) return e;
-  int rpb = 256 / ld;
-  int grid = (int)std::min<int64_t>((g + rpb - 1) / rpb, 160);  // M is staged once per block
-  note_launches(1);
-  k_center_apply<<<grid, 256, smem, st>>>(W, g, ld, mu, s, M, Z);
-  return cudaGetLastError();
+  return center_apply_ld(nullptr, 0, W, g, ld, mu, s, M, Z, st);
 }
 
 cudaError_t launch_apply_right_f64(double* A, int64_t g, int ld, const double* M, cudaStream_t st) {
@@ -1005,16 +1061,19 @@ cudaError_t launch_jacobi_eig_batch(const JacobiTask* tasks, int ntasks, int k, 
 }
 
 // ---------------------------------------------------------------------------
-// Rayleigh-Ritz finish (single kernel, one block per gene row for the
-// components plus block 0 building M_emb).
+// Rayleigh-Ritz finish: sigma, the components and M_emb from B (g x k, in
+// Z), the eigenpairs of B^T B and R2^{-1}.
 // ---------------------------------------------------------------------------
 // Components c0 .. c0 + ncc - 1 of nc per launch (E's columns staged in
-// shared memory); one launch takes them all when E[:, :nc] fits.
-__global__ void __launch_bounds__(128) k_ritz_finish(const double* __restrict__ B, int64_t g, int ld, int k,
-                                                     int nc, int c0, int ncc, const double* __restrict__ evals,
-                                                     const double* __restrict__ E,
-                                                     const double* __restrict__ Rinv2, double* __restrict__ sigma,
-                                                     float* __restrict__ comps, float* __restrict__ M_emb) {
+// shared memory); one launch takes them all when E[:, :nc] fits.  Block b of
+// nb takes the rows l = b, b + nb, ... of M_emb and the genes j = b, b + nb,
+// ... of the components, its 128 threads spread over (row, component) pairs.
+// Each output is one FMA chain in index order.
+__device__ __forceinline__ void ritz_finish_body(const double* __restrict__ B, int64_t g, int ld, int k, int nc,
+                                                 int c0, int ncc, const double* __restrict__ evals,
+                                                 const double* __restrict__ E, const double* __restrict__ Rinv2,
+                                                 double* __restrict__ sigma, float* __restrict__ comps,
+                                                 float* __restrict__ M_emb, int b, int nb) {
   extern __shared__ double sm[];
   double* Es = sm;              // [ld][ncc]: columns c0 .. c0 + ncc - 1 of E
   double* sg = sm + ld * ncc;   // [ncc]
@@ -1024,39 +1083,78 @@ __global__ void __launch_bounds__(128) k_ritz_finish(const double* __restrict__ 
   }
   for (int c = threadIdx.x; c < ncc; c += blockDim.x) sg[c] = sqrt(fmax(evals[c0 + c], 0.0));
   __syncthreads();
-  if (blockIdx.x == 0 && c0 == 0)
+  if (b == 0 && c0 == 0)
     for (int c = threadIdx.x; c < k; c += blockDim.x) sigma[c] = sqrt(fmax(evals[c], 0.0));
-  // M_emb row l (one row per block in turn) = Rinv2[l, :] E[:, :nc] diag(sigma)
-  for (int l = blockIdx.x; l < ld; l += gridDim.x)
-    for (int c = threadIdx.x; c < ncc; c += blockDim.x) {
-      double acc = 0.0;
-      for (int m = 0; m < ld; ++m) acc = fma(Rinv2[l * ld + m], Es[m * ncc + c], acc);
-      M_emb[l * nc + c0 + c] = (float)(acc * sg[c]);
-    }
-  // components[c][j] = (B E)[j][c] / sigma_c
-  for (int64_t j = blockIdx.x; j < g; j += gridDim.x) {
-    for (int c = threadIdx.x; c < ncc; c += blockDim.x) {
-      double acc = 0.0;
-      for (int l = 0; l < k; ++l) acc = fma(B[j * ld + l], Es[l * ncc + c], acc);
-      comps[(int64_t)(c0 + c) * g + j] = sg[c] > 0.0 ? (float)(acc / sg[c]) : 0.f;
-    }
+  // M_emb row l = Rinv2[l, :] E[:, :nc] diag(sigma)
+  const int64_t rows_m = b < ld ? (ld - 1 - b) / nb + 1 : 0;
+  for (int64_t t = threadIdx.x; t < rows_m * ncc; t += blockDim.x) {
+    const int l = b + (int)(t / ncc) * nb, c = (int)(t % ncc);
+    double acc = 0.0;
+    for (int m = 0; m < ld; ++m) acc = fma(Rinv2[l * ld + m], Es[m * ncc + c], acc);
+    M_emb[l * nc + c0 + c] = (float)(acc * sg[c]);
   }
+  // components[c][j] = (B E)[j][c] / sigma_c
+  const int64_t rows_g = b < g ? (g - 1 - b) / nb + 1 : 0;
+  for (int64_t t = threadIdx.x; t < rows_g * ncc; t += blockDim.x) {
+    const int64_t j = b + (t / ncc) * nb;
+    const int c = (int)(t % ncc);
+    double acc = 0.0;
+    for (int l = 0; l < k; ++l) acc = fma(B[j * ld + l], Es[l * ncc + c], acc);
+    comps[(int64_t)(c0 + c) * g + j] = sg[c] > 0.0 ? (float)(acc / sg[c]) : 0.f;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_ritz_finish(const double* __restrict__ B, int64_t g, int ld, int k,
+                                                     int nc, int c0, int ncc, const double* __restrict__ evals,
+                                                     const double* __restrict__ E,
+                                                     const double* __restrict__ Rinv2, double* __restrict__ sigma,
+                                                     float* __restrict__ comps, float* __restrict__ M_emb) {
+  ritz_finish_body(B, g, ld, k, nc, c0, ncc, evals, E, Rinv2, sigma, comps, M_emb, blockIdx.x, gridDim.x);
+}
+
+// One segment per grid row y (batched segments).
+__global__ void __launch_bounds__(128) k_ritz_finish_batch(const RitzTask* __restrict__ tasks, int64_t g, int ld,
+                                                           int k, int nc, int c0, int ncc) {
+  const RitzTask t = tasks[blockIdx.y];
+  ritz_finish_body(t.B, g, ld, k, nc, c0, ncc, t.evals, t.evecs, t.Rinv2, t.sigma, t.comps, t.M_emb, blockIdx.x,
+                   gridDim.x);
+}
+
+// Components staged per launch, and the launch's shared bytes.
+static int ritz_cols(int ld, int nc, size_t* smem) {
+  constexpr size_t kStage = 160 * 1024;  // shared bytes for the staged columns of E
+  const int ncc = (int)std::max<size_t>(1, std::min<size_t>(nc, kStage / ((size_t)(ld + 1) * sizeof(double))));
+  *smem = (size_t)(ld * ncc + ncc) * sizeof(double);
+  return ncc;
 }
 
 cudaError_t launch_ritz_finish(const double* B, int64_t g, int ld, int k, int nc,
                                const double* evals, const double* evecs, const double* Rinv2,
                                double* sigma, float* components, float* M_emb, cudaStream_t st) {
-  constexpr size_t kStage = 160 * 1024;  // shared bytes for the staged columns of E
-  const int ncc = (int)std::max<size_t>(1, std::min<size_t>(nc, kStage / ((size_t)(ld + 1) * sizeof(double))));
-  const size_t smem = (size_t)(ld * ncc + ncc) * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(k_ritz_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
+  size_t smem = 0;
+  const int ncc = ritz_cols(ld, nc, &smem);
+  if (cudaError_t e = allow_smem(k_ritz_finish, smem); e != cudaSuccess) return e;
   // Few blocks: each stages E once and then takes a run of genes.
   const int grid = (int)std::max<int64_t>(std::min<int64_t>(g, 296), std::min<int64_t>(ld, 296));
   for (int c0 = 0; c0 < nc; c0 += ncc) {
     note_launches(1);
     k_ritz_finish<<<grid, 128, smem, st>>>(B, g, ld, k, nc, c0, std::min(ncc, nc - c0), evals, evecs, Rinv2,
                                            sigma, components, M_emb);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ritz_finish_batch(const RitzTask* tasks, int ntasks, int64_t g, int ld, int k, int nc,
+                                     cudaStream_t st) {
+  if (ntasks <= 0) return cudaSuccess;
+  size_t smem = 0;
+  const int ncc = ritz_cols(ld, nc, &smem);
+  if (cudaError_t e = allow_smem(k_ritz_finish_batch, smem); e != cudaSuccess) return e;
+  const int gx = (int)std::max<int64_t>(1, std::min<int64_t>(std::max<int64_t>(g, ld), 8));
+  for (int c0 = 0; c0 < nc; c0 += ncc) {
+    note_launches(1);
+    k_ritz_finish_batch<<<dim3((unsigned)gx, (unsigned)ntasks), 128, smem, st>>>(tasks, g, ld, k, nc, c0,
+                                                                                  std::min(ncc, nc - c0));
   }
   return cudaGetLastError();
 }

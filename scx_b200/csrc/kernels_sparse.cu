@@ -267,6 +267,26 @@ __global__ void __launch_bounds__(256) k_reduce_rows_batch(const GramTask* __res
   reduce_rows_body<double>(t.part, nparts, len, t.G, 0, 0, 0, blockIdx.x, gridDim.x);
 }
 
+// One reduction per grid row y with its own part count (the segments of a
+// batch); the sums have the bits of k_reduce_rows on the same partials.
+template <typename T>
+__global__ void __launch_bounds__(256) k_reduce_rows_sum(const SumTask* __restrict__ tasks, int64_t len) {
+  const SumTask t = tasks[blockIdx.y];
+  reduce_rows_body<T>(static_cast<const T*>(t.part), t.nparts, len, t.out, 0, 0, 0, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_reduce_rows_batch(int part_dtype_f32, const SumTask* tasks, int ntasks, int64_t len,
+                                     cudaStream_t st) {
+  if (ntasks <= 0 || len <= 0) return cudaSuccess;
+  const dim3 grid((unsigned)std::max<int64_t>(1, std::min<int64_t>((len + 31) / 32, 64)), (unsigned)ntasks);
+  note_launches(1);
+  if (part_dtype_f32)
+    k_reduce_rows_sum<float><<<grid, 256, 0, st>>>(tasks, len);
+  else
+    k_reduce_rows_sum<double><<<grid, 256, 0, st>>>(tasks, len);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_reduce_rows_f64_batch(const GramTask* tasks, int ntasks, int nparts, int64_t len, cudaStream_t st,
                                          int num_sms) {
   if (ntasks <= 0) return cudaSuccess;

@@ -742,9 +742,16 @@ done:
 // ---------------------------------------------------------------------------
 constexpr int kGramStages = 4;
 
-__global__ void __launch_bounds__(128, 1)
-    k_gram_tc(int64_t n_tiles, const __grid_constant__ CUtensorMap qmap, double* __restrict__ part, int fmt,
-              int* err) {
+// One CTA's work: the row tiles [t0, t1) of one image, into the partial at `out`.
+struct GramJob {
+  const CUtensorMap* qmap;
+  double* out;
+  int* err;
+  int64_t t0, t1;
+};
+
+template <bool kGlobalMaps>
+__device__ __forceinline__ void gram_tc_body(const GramJob& job, int fmt) {
   constexpr int LD = 64;
   constexpr int PLANE = TM * LD * 2;  // 64 image columns of 128 rows, 16 KB
   constexpr int TILE = 2 * PLANE;     // the 128 image columns of a row tile
@@ -762,8 +769,8 @@ __global__ void __launch_bounds__(128, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t t0 = (int64_t)blockIdx.x * n_tiles / gridDim.x;
-  const int64_t t1 = (int64_t)(blockIdx.x + 1) * n_tiles / gridDim.x;
+  const int64_t t0 = job.t0, t1 = job.t1;
+  int* err = job.err;
   const uint16_t one16 = fmt ? (uint16_t)0x3F80u : (uint16_t)0x3C00u;
   {
     const uint32_t w = (uint32_t)one16 | ((uint32_t)one16 << 16);
@@ -792,14 +799,15 @@ __global__ void __launch_bounds__(128, 1)
 
   if (threadIdx.x == 0 && have_work) {
     // loader
+    if (kGlobalMaps) tmap_acquire(job.qmap);
     uint32_t it = 0;
     for (int64_t t = t0; t < t1; ++t, ++it) {
       const int s = it % S;
       if (!mbar_wait(&empty[s], ((it / S) & 1u) ^ 1u, abort_flag, err, 41)) break;
       uint8_t* tile = tiles + s * TILE;
       mbar_arrive_expect_tx(&full[s], TILE);
-      tma_load_2d(tile, &qmap, &full[s], 0, (int)(t * TM));
-      tma_load_2d(tile + PLANE, &qmap, &full[s], 64, (int)(t * TM));
+      tma_load_2d(tile, job.qmap, &full[s], 0, (int)(t * TM));
+      tma_load_2d(tile + PLANE, job.qmap, &full[s], 64, (int)(t * TM));
     }
   } else if (threadIdx.x == 32 && have_work) {
     // MMA issuer
@@ -852,7 +860,7 @@ __global__ void __launch_bounds__(128, 1)
   }
   __syncthreads();
   {
-    double* out = part + (int64_t)blockIdx.x * (LD * LD + LD);
+    double* out = job.out;
     // image rows 2 i (hi) and 2 i + 1 (lo) belong to column i
     for (int t = threadIdx.x; t < LD * LD; t += blockDim.x) {
       const int i = t / LD, j = t % LD;
@@ -862,7 +870,7 @@ __global__ void __launch_bounds__(128, 1)
   }
   __syncthreads();
   if (threadIdx.x < LD) {
-    double* out = part + (int64_t)blockIdx.x * (LD * LD + LD);
+    double* out = job.out;
     out[LD * LD + threadIdx.x] = (double)pbuf[(2 * threadIdx.x) * LD] + (double)pbuf[(2 * threadIdx.x + 1) * LD];
   }
 done:
@@ -873,6 +881,24 @@ done:
     tc_fence_after();
     tmem_dealloc(tmem, 256);
   }
+}
+
+// CTA b takes the tiles [tc_range_begin(b), tc_range_begin(b + 1)) and writes partial b.
+__global__ void __launch_bounds__(128, 1)
+    k_gram_tc(int64_t n_tiles, const __grid_constant__ CUtensorMap qmap, double* __restrict__ part, int fmt,
+              int* err) {
+  const GramJob job{&qmap, part + (int64_t)blockIdx.x * (64 * 64 + 64), err,
+                    tc_range_begin(blockIdx.x, gridDim.x, n_tiles), tc_range_begin(blockIdx.x + 1, gridDim.x, n_tiles)};
+  gram_tc_body<false>(job, fmt);
+}
+
+// One item (segment, tile range, partial) per CTA, over every segment of a batch.
+__global__ void __launch_bounds__(128, 1)
+    k_gram_tc_batch(const TcSegment* __restrict__ segs, const TcItem* __restrict__ items, int fmt) {
+  const TcItem it = items[blockIdx.x];
+  const TcSegment& sg = segs[it.seg];
+  const GramJob job{sg.qmap, sg.gpart + (int64_t)it.slot * (64 * 64 + 64), sg.err, it.t0, it.t1};
+  gram_tc_body<true>(job, fmt);
 }
 
 // 16-bit image of x: words (hi | lo << 16), hi = round16(x), lo = round16(x - hi)
@@ -910,12 +936,59 @@ __host__ __device__ constexpr size_t fwd_swap_smem() {
          2 * 2 * (size_t)kMaxChunks * sizeof(SegMeta) + 64 * sizeof(uint64_t) + 64;
 }
 
+// The operands of one band: of the one matrix of k_fwd_swap (FwdOne), or of
+// the segment it belongs to in k_fwd_swap_batch (FwdBatch).
+struct FwdBand {
+  const uint32_t* ent;
+  const SegMeta* meta;  // the band's first metadata record
+  const CUtensorMap* vmap;
+  const float* mc;
+  float* Y;             // null: no FP32 copy
+  uint16_t* Yimg;
+  int* err;
+  int64_t row0;         // the band's first row in its matrix
+  int64_t n;            // rows of its matrix
+  int tiles;            // 1 or 2
+};
+
+struct FwdOne {
+  const uint32_t* ent;
+  const SegMeta* meta;
+  const CUtensorMap* vmap;
+  const float* mc;
+  float* Y;
+  uint16_t* Yimg;
+  int* err;
+  int64_t n_tiles, n;
+  int nc;
+  static constexpr bool kGlobalMaps = false;
+  __device__ int64_t bands() const { return (n_tiles + 1) / 2; }
+  __device__ FwdBand band(int64_t b) const {
+    return FwdBand{ent, meta + b * 2 * nc, vmap, mc, Y, Yimg, err, b * 2 * TM, n,
+                   (int)min((int64_t)2, n_tiles - b * 2)};
+  }
+};
+
+struct FwdBatch {
+  const TcSegment* segs;
+  const int32_t* band_seg;
+  int64_t n_bands;
+  int nc, write_y;
+  static constexpr bool kGlobalMaps = true;  // tensor maps in global memory
+  __device__ int64_t bands() const { return n_bands; }
+  __device__ FwdBand band(int64_t b) const {
+    const TcSegment& sg = segs[__ldg(band_seg + b)];
+    const int64_t lb = b - sg.band0, n_tiles = (sg.n + TM - 1) / TM;
+    return FwdBand{sg.ent, static_cast<const SegMeta*>(sg.meta) + lb * 2 * nc, sg.vmap, sg.mc,
+                   write_y ? sg.Y : nullptr, sg.Yimg, sg.err, lb * 2 * TM, sg.n,
+                   (int)min((int64_t)2, n_tiles - lb * 2)};
+  }
+};
+
 // A band is two consecutive row tiles.  Per band:
 // Y^T[m, its 256 cells] = sum over chunks c of Vimg_c^T (m x 64 genes) [A_(t0,c) | A_(t1,c)]^T.
-__global__ void __launch_bounds__(kThreads, 1)
-    k_fwd_swap(const uint32_t* __restrict__ ent, const SegMeta* __restrict__ meta, int64_t n_tiles, int nc,
-               int64_t n, const __grid_constant__ CUtensorMap vmap, const float* __restrict__ mc,
-               float* __restrict__ Y, uint16_t* __restrict__ Yimg, int fmt, int* err) {
+template <class Src>
+__device__ __forceinline__ void fwd_swap_body(const Src& src, int nc, int fmt) {
   constexpr int LD = 64;
   constexpr int S = kSwapFwdStages;
   constexpr int NB = kSwapFwdSlots;
@@ -942,8 +1015,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t n_bands = (n_tiles + 1) / 2;
-  auto band_tiles = [&](int64_t band) { return (int)min((int64_t)2, n_tiles - band * 2); };
+  const int64_t n_bands = src.bands();
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 8);
@@ -979,34 +1051,44 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int par = group >> 1, u = group & 1;
     uint32_t cc = 0, bi = 0;
     uint4 w[kFwdRegs];
-    Span pre{-1, -1};  // span whose loads are in flight in w
+    Span pre{-1, -1};             // span whose loads are in flight in w
+    const uint32_t* pre_ent = nullptr;  // the entry array pre indexes
     for (int64_t band = blockIdx.x; band < n_bands; band += gridDim.x, ++bi) {
-      const int nt = band_tiles(band);
-      const bool has = u < nt;
+      const FwdBand bd = src.band(band);
+      int* err = bd.err;
+      const bool has = u < bd.tiles;
       if (!warp_wait(&mfull[bi & 1u], (bi >> 1) & 1u, abort_flag, err, 11)) goto done;
       const SegMeta* mt = mring + (bi & 1u) * MSLOT;
       for (int c = 0; c < nc; ++c, ++cc) {
         if ((int)(cc & 1u) != par) continue;
         // the span loaded ahead (pre) is this segment's whenever one was loaded
         const Span sp = !has ? Span{0, 0} : pre.lo >= 0 ? pre : quarter_span(mt[u * nc + c], q);
-        if (has && pre.lo < 0) span_load<kFwdRegs>(ent, sp, lane, w);
+        const uint32_t* sp_ent = pre.lo >= 0 ? pre_ent : bd.ent;
+        if (has && pre.lo < 0) span_load<kFwdRegs>(sp_ent, sp, lane, w);
         const int s = cc % S;
         if (!warp_wait(&empty[s], ((cc / S) & 1u) ^ 1u, abort_flag, err, 12)) goto done;
         if (has) {
           const uint32_t tile = smem_u32(As + s * STAGE + u * TILE);
           zero_rows(tile, q, lane);
           __syncwarp();
-          span_scatter<kFwdRegs>(tile, ent, sp, lane, w);
+          span_scatter<kFwdRegs>(tile, sp_ent, sp, lane, w);
         }
         // the group's next segment: chunk c + 2 of this band, or of the next
         pre = Span{-1, -1};
         if (c + 2 < nc) {
-          if (has) pre = quarter_span(mt[u * nc + c + 2], q);
-        } else if (band + gridDim.x < n_bands && c + 2 - nc < nc && u < band_tiles(band + gridDim.x)) {
-          if (!warp_wait(&mfull[(bi + 1) & 1u], ((bi + 1) >> 1) & 1u, abort_flag, err, 11)) goto done;
-          pre = quarter_span(mring[((bi + 1) & 1u) * MSLOT + u * nc + (c + 2 - nc)], q);
+          if (has) {
+            pre = quarter_span(mt[u * nc + c + 2], q);
+            pre_ent = bd.ent;
+          }
+        } else if (band + gridDim.x < n_bands && c + 2 - nc < nc) {
+          const FwdBand nx = src.band(band + gridDim.x);
+          if (u < nx.tiles) {
+            if (!warp_wait(&mfull[(bi + 1) & 1u], ((bi + 1) >> 1) & 1u, abort_flag, err, 11)) goto done;
+            pre = quarter_span(mring[((bi + 1) & 1u) * MSLOT + u * nc + (c + 2 - nc)], q);
+            pre_ent = nx.ent;
+          }
         }
-        if (pre.lo >= 0) span_load<kFwdRegs>(ent, pre, lane, w);
+        if (pre.lo >= 0) span_load<kFwdRegs>(pre_ent, pre, lane, w);
         fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) mbar_arrive(&full[s]);
@@ -1018,16 +1100,20 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---- epilogue: lane pair (2 j, 2 j + 1) -> column j of Y and its image ----
     const int q = warp & 3;
     const int p = lane & 1, j = 16 * q + (lane >> 1);
-    const float mcj = __ldg(mc + j);
     uint32_t k = 0;
     for (int64_t band = blockIdx.x; band < n_bands; band += gridDim.x, ++k) {
-      const int nt = band_tiles(band);
+      const FwdBand bd = src.band(band);
+      int* err = bd.err;
+      const int64_t n = bd.n;
+      const float mcj = __ldg(bd.mc + j);
+      uint16_t* Yimg = bd.Yimg;
+      float* Y = bd.Y;
       const uint32_t a = k & 1u, ph = (k >> 1) & 1u;
       if (!warp_wait(&acc_full[a], ph, abort_flag, err, 14)) goto done;
       tc_fence_after();
-      for (int u = 0; u < nt; ++u) {
+      for (int u = 0; u < bd.tiles; ++u) {
         const uint32_t tbase = tmem + ((32u * q) << 16) + a * 256 + u * 128;
-        const int64_t row0 = (band * 2 + u) * TM;
+        const int64_t row0 = bd.row0 + u * TM;
 #pragma unroll 1
         for (int cb = 0; cb < TM / 32; ++cb) {  // 32 cells per TMEM load
           uint32_t r[32];
@@ -1065,7 +1151,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t cc = 0, k = 0;
       bool ok = true;
       for (int64_t band = blockIdx.x; band < n_bands && ok; band += gridDim.x, ++k) {
-        const uint32_t idesc = band_tiles(band) == 2 ? idesc2 : idesc1;
+        const FwdBand bd = src.band(band);
+        int* err = bd.err;
+        const uint32_t idesc = bd.tiles == 2 ? idesc2 : idesc1;
         const uint32_t a = k & 1u, ph = (k >> 1) & 1u;
         if (!mbar_wait(&acc_empty[a], ph ^ 1u, abort_flag, err, 15)) break;
         tc_fence_after();
@@ -1097,6 +1185,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t cc = 0;
       bool ok = true;
       for (int64_t band = blockIdx.x; band < n_bands && ok; band += gridDim.x) {
+        const FwdBand bd = src.band(band);
+        int* err = bd.err;
+        if (Src::kGlobalMaps) tmap_acquire(bd.vmap);
         for (int c = 0; c < nc; ++c, ++cc) {
           const int b = cc % NB;
           if (!mbar_wait(&bempty[b], ((cc / NB) & 1u) ^ 1u, abort_flag, err, 19)) {
@@ -1105,8 +1196,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           uint8_t* bb = Bs + b * B_BYTES;
           mbar_arrive_expect_tx(&bfull[b], B_BYTES);
-          tma_load_2d(bb, &vmap, &bfull[b], 0, CW * c);
-          tma_load_2d(bb + CW * 128, &vmap, &bfull[b], 64, CW * c);
+          tma_load_2d(bb, bd.vmap, &bfull[b], 0, CW * c);
+          tma_load_2d(bb + CW * 128, bd.vmap, &bfull[b], 64, CW * c);
         }
       }
     }
@@ -1116,11 +1207,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (lane == 0) {
       uint32_t bi = 0;
       for (int64_t band = blockIdx.x; band < n_bands; band += gridDim.x, ++bi) {
-        const int records = band_tiles(band) * nc;  // the band's tiles are consecutive in `meta`
-        if (!load_meta(meta + band * 2 * nc, records, mring, MSLOT, mfull, mempty, bi, abort_flag, err, 17))
-          break;
+        const FwdBand bd = src.band(band);
+        int* err = bd.err;
+        const int records = bd.tiles * nc;  // the band's tiles are consecutive in `meta`
+        if (!load_meta(bd.meta, records, mring, MSLOT, mfull, mempty, bi, abort_flag, err, 17)) break;
         if (!mbar_wait(&mfull[bi & 1u], (bi >> 1) & 1u, abort_flag, err, 18)) break;
-        prefetch_segments(ent, mring + (bi & 1u) * MSLOT, 0, records);
+        prefetch_segments(bd.ent, mring + (bi & 1u) * MSLOT, 0, records);
       }
     }
     __syncwarp();
@@ -1133,6 +1225,20 @@ done:
     tc_fence_after();
     tmem_dealloc(tmem, 512);
   }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_fwd_swap(const uint32_t* __restrict__ ent, const SegMeta* __restrict__ meta, int64_t n_tiles, int nc,
+               int64_t n, const __grid_constant__ CUtensorMap vmap, const float* __restrict__ mc,
+               float* __restrict__ Y, uint16_t* __restrict__ Yimg, int fmt, int* err) {
+  fwd_swap_body(FwdOne{ent, meta, &vmap, mc, Y, Yimg, err, n_tiles, n, nc}, nc, fmt);
+}
+
+// Every band of every segment of a batch in one persistent launch.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_fwd_swap_batch(const TcSegment* __restrict__ segs, const int32_t* __restrict__ band_seg, int64_t n_bands,
+                     int nc, int write_y, int fmt) {
+  fwd_swap_body(FwdBatch{segs, band_seg, n_bands, nc, write_y}, nc, fmt);
 }
 
 constexpr int kSwapRmatStages = 4;  // stages: one half tile (64 cells) of a quad's four chunks
@@ -1149,10 +1255,20 @@ __host__ __device__ constexpr size_t rmat_swap_smem() {
 // A stage holds one half (64 cells) of a tile for the quad's four chunks, so
 // K = 64 per stage and the densify warps split into two teams of eight, team
 // h filling the cells 64 h .. 64 h + 63 of every tile (warp = chunk x quarter).
-__global__ void __launch_bounds__(kThreads, 1)
-    k_rmat_swap(const uint32_t* __restrict__ ent, const SegMeta* __restrict__ meta, int64_t n_tiles, int nc,
-                int64_t g, int n_gene_groups, const __grid_constant__ CUtensorMap qmap, float* __restrict__ part,
-                int fmt, int* err) {
+// One CTA's work: gene group gg over the row tiles [t0, t1) of one matrix,
+// written as partial `rg` of `part`.
+struct RmatJob {
+  const uint32_t* ent;
+  const SegMeta* meta;
+  const CUtensorMap* qmap;
+  float* part;
+  int* err;
+  int64_t t0, t1;
+  int gg, rg;
+};
+
+template <bool kGlobalMaps>
+__device__ __forceinline__ void rmat_swap_body(const RmatJob& job, int nc, int64_t g, int fmt) {
   constexpr int LD = 64;
   constexpr int S = kSwapRmatStages;
   constexpr int HSUB = 64 * CW * 2;      // half a chunk tile (64 cells x 64 genes), 8 KB
@@ -1175,10 +1291,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gg = blockIdx.x % n_gene_groups;
-  const int rg = blockIdx.x / n_gene_groups;
-  const int R = gridDim.x / n_gene_groups;
-  const int64_t t0 = (int64_t)rg * n_tiles / R, t1 = (int64_t)(rg + 1) * n_tiles / R;
+  const uint32_t* ent = job.ent;
+  const SegMeta* meta = job.meta;
+  float* part = job.part;
+  int* err = job.err;
+  const int64_t t0 = job.t0, t1 = job.t1;
+  const int gg = job.gg, rg = job.rg;
   const int n_quads = (nc + 3) / 4;
   const int qd0 = gg * kSwapQuads, qd1 = min(n_quads, qd0 + kSwapQuads);
   const int nq = max(0, qd1 - qd0);
@@ -1346,14 +1464,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == W_DENSE) {
     // ---- dense loader: image tiles of Q, double-buffered per row tile ----
     if (lane == 0 && have_work) {
+      if (kGlobalMaps) tmap_acquire(job.qmap);
       uint32_t ti = 0;
       for (int64_t t = t0; t < t1; ++t, ++ti) {
         const uint32_t b = ti & 1u;
         if (!mbar_wait(&qempty[b], ((ti >> 1) & 1u) ^ 1u, abort_flag, err, 28)) break;
         uint8_t* qb = Qs + b * Q_BYTES;
         mbar_arrive_expect_tx(&qfull[b], Q_BYTES);
-        tma_load_2d(qb, &qmap, &qfull[b], 0, (int)(t * TM));
-        tma_load_2d(qb + TM * 128, &qmap, &qfull[b], 64, (int)(t * TM));
+        tma_load_2d(qb, job.qmap, &qfull[b], 0, (int)(t * TM));
+        tma_load_2d(qb + TM * 128, job.qmap, &qfull[b], 64, (int)(t * TM));
       }
     }
     __syncwarp();
@@ -1377,6 +1496,31 @@ done:
     tc_fence_after();
     tmem_dealloc(tmem, 512);
   }
+}
+
+// CTA b = (row group b / gene groups, gene group b % gene groups); the row
+// groups split the tiles evenly (tc_range_begin).
+__global__ void __launch_bounds__(kThreads, 1)
+    k_rmat_swap(const uint32_t* __restrict__ ent, const SegMeta* __restrict__ meta, int64_t n_tiles, int nc,
+                int64_t g, int n_gene_groups, const __grid_constant__ CUtensorMap qmap, float* __restrict__ part,
+                int fmt, int* err) {
+  const int gg = blockIdx.x % n_gene_groups, rg = blockIdx.x / n_gene_groups;
+  const int R = gridDim.x / n_gene_groups;
+  const RmatJob job{ent, meta, &qmap, part, err, tc_range_begin(rg, R, n_tiles), tc_range_begin(rg + 1, R, n_tiles),
+                    gg, rg};
+  rmat_swap_body<false>(job, nc, g, fmt);
+}
+
+// One item (segment, gene group, row group, tile range) per CTA, over every
+// segment of a batch.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_rmat_swap_batch(const TcSegment* __restrict__ segs, const TcItem* __restrict__ items, int nc, int64_t g,
+                      int fmt) {
+  const TcItem it = items[blockIdx.x];
+  const TcSegment& sg = segs[it.seg];
+  const RmatJob job{sg.ent, static_cast<const SegMeta*>(sg.meta), sg.qmap, sg.part, sg.err, it.t0, it.t1, it.gg,
+                    it.slot};
+  rmat_swap_body<true>(job, nc, g, fmt);
 }
 
 size_t smem_tail() { return 2 * kMaxChunks * sizeof(SegMeta) + 64 * sizeof(uint64_t) + 64; }
@@ -1515,15 +1659,53 @@ cudaError_t launch_split16(const float* in, int64_t count, uint16_t* img, int fm
   return cudaGetLastError();
 }
 
-int launch_gram_tc(int64_t n, const CUtensorMap* qmap, double* part, int fmt, int* err, cudaStream_t st,
-                   int num_sms) {
+int gram_tc_parts(int64_t n, int parts, int num_sms) {
   const int64_t n_tiles = (n + TM - 1) / TM;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, num_sms));
-  const size_t smem = 1024 + (size_t)kGramStages * 2 * TM * 64 * 2 + TM * 64 * 2 + TM * 64 * 4 + 256;
-  if (allow_smem(k_gram_tc, smem) != cudaSuccess) return -1;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(n_tiles, parts > 0 ? parts : num_sms));
+}
+
+static constexpr size_t gram_tc_smem() {
+  return 1024 + (size_t)kGramStages * 2 * TM * 64 * 2 + TM * 64 * 2 + TM * 64 * 4 + 256;
+}
+
+int launch_gram_tc(int64_t n, const CUtensorMap* qmap, double* part, int fmt, int* err, cudaStream_t st,
+                   int num_sms, int parts) {
+  const int64_t n_tiles = (n + TM - 1) / TM;
+  const int grid = gram_tc_parts(n, parts, num_sms);
+  if (allow_smem(k_gram_tc, gram_tc_smem()) != cudaSuccess) return -1;
   note_launches(1);
-  k_gram_tc<<<grid, 128, smem, st>>>(n_tiles, *qmap, part, fmt, err);
+  k_gram_tc<<<grid, 128, gram_tc_smem(), st>>>(n_tiles, *qmap, part, fmt, err);
   return cudaGetLastError() == cudaSuccess ? grid : -1;
+}
+
+cudaError_t launch_fwd_tc_batch(const TcSegment* segs, const int32_t* band_seg, int64_t n_bands, int nc,
+                                int write_y, int fmt, cudaStream_t st, int num_sms) {
+  if (n_bands <= 0) return cudaSuccess;
+  const int grid = (int)std::min<int64_t>(n_bands, (int64_t)num_sms);
+  const size_t smem = fwd_swap_smem();
+  if (cudaError_t e = allow_smem(k_fwd_swap_batch, smem); e != cudaSuccess) return e;
+  note_launches(1);
+  k_fwd_swap_batch<<<grid, kThreads, smem, st>>>(segs, band_seg, n_bands, nc, write_y, fmt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rmat_tc_batch(const TcSegment* segs, const TcItem* items, int n_items, int nc, int64_t g,
+                                 int gene_groups, int fmt, cudaStream_t st) {
+  (void)gene_groups;  // each item names its gene group
+  if (n_items <= 0) return cudaSuccess;
+  const size_t smem = rmat_swap_smem();
+  if (cudaError_t e = allow_smem(k_rmat_swap_batch, smem); e != cudaSuccess) return e;
+  note_launches(1);
+  k_rmat_swap_batch<<<n_items, kThreads, smem, st>>>(segs, items, nc, g, fmt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gram_tc_batch(const TcSegment* segs, const TcItem* items, int n_items, int fmt, cudaStream_t st) {
+  if (n_items <= 0) return cudaSuccess;
+  if (cudaError_t e = allow_smem(k_gram_tc_batch, gram_tc_smem()); e != cudaSuccess) return e;
+  note_launches(1);
+  k_gram_tc_batch<<<n_items, 128, gram_tc_smem(), st>>>(segs, items, fmt);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

@@ -147,6 +147,17 @@ struct SplitTask {  // 16-bit image of a float matrix
   const float* in;
   uint16_t* img;
 };
+struct RitzTask {  // the Rayleigh-Ritz finish of one segment (launch_ritz_finish's arguments)
+  const double* B;
+  const double* evals;
+  const double* evecs;
+  const double* Rinv2;
+  double* sigma;
+  float* comps;
+  float* M_emb;
+};
+cudaError_t launch_ritz_finish_batch(const RitzTask* tasks, int ntasks, int64_t g, int ld, int k, int nc,
+                                     cudaStream_t st);
 cudaError_t launch_center_apply_batch(const ApplyTask* tasks, int ntasks, int64_t g, int ld, cudaStream_t st);
 cudaError_t launch_gram_f64_batch(const GramTask* tasks, int ntasks, int64_t n, int ld, int nparts,
                                   cudaStream_t st, int num_sms);
@@ -241,9 +252,60 @@ cudaError_t launch_rmat_tc(int ld, const uint32_t* ent, const void* meta, int64_
 // Gram partials [G (64 x 64), colsum (64)] of hi + lo from the image (ld 64)
 // on tensor cores; returns the number of partials written, or -1 on a launch
 // error.
-int launch_gram_tc(int64_t n, const CUtensorMap* qmap, double* part, int fmt, int* err, cudaStream_t st, int num_sms);
+// `parts` > 0 asks for that many partials (at most one per row tile), 0 for
+// one per SM; gram_tc_parts gives the count a call writes.
+int gram_tc_parts(int64_t n, int parts, int num_sms);
+int launch_gram_tc(int64_t n, const CUtensorMap* qmap, double* part, int fmt, int* err, cudaStream_t st, int num_sms,
+                   int parts = 0);
 size_t fwd_tc_smem_bytes(int ld);
 size_t rmat_tc_smem_bytes(int ld);
+// The products and the Gram above over every segment of a batch in one
+// launch (ld 64).  A segment is one plan's packed matrix and buffers; its
+// tensor maps are device copies.  The forward kernel walks the bands (pairs
+// of row tiles) of all segments, numbered segment after segment
+// (band_seg[b] = the segment of band b, TcSegment::band0 its first band); the
+// transposed product and the Gram take one item (a tile range of one
+// segment, and the partial it writes) per CTA.  Each segment's results have
+// the bits of its own launch_*_tc call with the same partition.
+struct TcSegment {
+  const uint32_t* ent;
+  const void* meta;
+  const CUtensorMap* vmap;
+  const CUtensorMap* qmap;
+  const float* mc;
+  float* Y;        // FP32 copy of the forward product (written when asked)
+  uint16_t* Yimg;
+  float* part;     // transposed-product partials [row group][n_vars][64]
+  double* gpart;   // Gram partials [part][64 * 64 + 64]
+  int* err;
+  int64_t n;       // rows
+  int64_t band0;
+};
+struct TcItem {
+  int32_t seg;
+  int32_t gg;      // gene group (transposed product)
+  int32_t slot;    // partial written: row group (transposed) or part (Gram)
+  int32_t pad;
+  int64_t t0, t1;  // row tiles [t0, t1) of the segment
+};
+cudaError_t launch_fwd_tc_batch(const TcSegment* segs, const int32_t* band_seg, int64_t n_bands, int nc,
+                                int write_y, int fmt, cudaStream_t st, int num_sms);
+cudaError_t launch_rmat_tc_batch(const TcSegment* segs, const TcItem* items, int n_items, int nc, int64_t g,
+                                 int gene_groups, int fmt, cudaStream_t st);
+cudaError_t launch_gram_tc_batch(const TcSegment* segs, const TcItem* items, int n_items, int fmt, cudaStream_t st);
+// Tile range [t0, t1) of CTA b of nb over n_tiles row tiles: the split every
+// launcher above uses.
+__host__ __device__ inline int64_t tc_range_begin(int64_t b, int64_t nb, int64_t n_tiles) { return b * n_tiles / nb; }
+// Sums of per-segment partials: out = sum over nparts of part[p][len] (FP64,
+// fixed order), one task per segment, one launch.
+struct SumTask {
+  const void* part;
+  double* out;
+  int nparts;
+  int pad;
+};
+cudaError_t launch_reduce_rows_batch(int part_dtype_f32, const SumTask* tasks, int ntasks, int64_t len,
+                                     cudaStream_t st);
 // One block whose pipeline wait never completes: the bounded wait gives up
 // after its limit (about 1 s) and writes `code` to err.
 cudaError_t launch_wait_selftest(int* err, int code, cudaStream_t st);

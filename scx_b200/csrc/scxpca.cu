@@ -301,6 +301,7 @@ struct scxpca_plan {
   bool use_tc = false;
   int fmt16 = 1;  // 1 = bf16, 0 = f16
   int n_chunks = 0, tc_gene_groups = 0, tc_row_groups = 0;
+  int tc_gram_parts = 0;  // partials of the tensor-core Gram (0: one per SM)
   // 16-bit images (column 2 j = hi, 2 j + 1 = lo of column j) of the dense
   // operands of the tensor-core products: V (g x 2 ld) and the tall Y/Q (n x 2 ld)
   DevBuf tf_meta, tf_ent, Vimg, Yimg, tc_part, tc_err;
@@ -1448,7 +1449,7 @@ void tall_gram(scxpca_plan* pl, const float* A, int64_t rows, bool from_image) {
   int s = stage_begin(pl);
   if (from_image && pl->use_tc && ld == 64) {
     parts = launch_gram_tc(rows, &pl->qmap, pl->gpart.as<double>(), pl->fmt16,
-                           pl->tc_err.as<int>(), st, pl->num_sms);
+                           pl->tc_err.as<int>(), st, pl->num_sms, pl->tc_gram_parts);
     if (parts < 0) CK(cudaGetLastError());
   } else
   CK(launch_gram_f32(A, rows, ld, pl->gpart.as<double>(), parts, st));
@@ -1804,19 +1805,27 @@ JacobiTask finish_task(scxpca_plan* pl) {
   return JacobiTask{pl->G.as<double>(), pl->evals.as<double>(), pl->evecs.as<double>(), pl->status.as<int>() + 2};
 }
 
-void finish_after(scxpca_plan* pl, float* U) {
-  cudaStream_t st = pl->stream;
-  const int ld = (int)pl->ld;
+// The Rayleigh-Ritz finish's arguments, as one task of a batched launch.
+RitzTask ritz_task(scxpca_plan* pl) {
+  return RitzTask{pl->Z.as<double>(), pl->evals.as<double>(), pl->evecs.as<double>(), pl->R2inv.as<double>(),
+                  pl->sigma.as<double>(), pl->comps.as<float>(), pl->M_emb.as<float>()};
+}
+
+// Embeddings U = Q R2^{-1} E Sigma (first n_components).
+void finish_embed(scxpca_plan* pl, float* U) {
   int s = stage_begin(pl);
-  CK(launch_ritz_finish(pl->Z.as<double>(), pl->g, ld, (int)pl->k, (int)pl->nc, pl->evals.as<double>(),
-                        pl->evecs.as<double>(), pl->R2inv.as<double>(), pl->sigma.as<double>(),
-                        pl->comps.as<float>(), pl->M_emb.as<float>(), st));
-  stage_end(pl, SCXPCA_STAGE_SMALL, s);
-  // Embeddings U = Q R2^{-1} E Sigma (first n_components).
-  s = stage_begin(pl);
-  CK(launch_embed(pl->Y.as<float>(), pl->n, ld, (int)pl->k, pl->M_emb.as<float>(), (int)pl->nc, U, st,
-                  pl->num_sms));
+  CK(launch_embed(pl->Y.as<float>(), pl->n, (int)pl->ld, (int)pl->k, pl->M_emb.as<float>(), (int)pl->nc, U,
+                  pl->stream, pl->num_sms));
   stage_end(pl, SCXPCA_STAGE_EMBED, s);
+}
+
+void finish_after(scxpca_plan* pl, float* U) {
+  const RitzTask t = ritz_task(pl);
+  int s = stage_begin(pl);
+  CK(launch_ritz_finish(t.B, pl->g, (int)pl->ld, (int)pl->k, (int)pl->nc, t.evals, t.evecs, t.Rinv2, t.sigma,
+                        t.comps, t.M_emb, pl->stream));
+  stage_end(pl, SCXPCA_STAGE_SMALL, s);
+  finish_embed(pl, U);
 }
 
 void enqueue_finish(scxpca_plan* pl, float* U) {
@@ -2113,7 +2122,13 @@ struct scxpca_batch {
   // transposed product in the loop and at the close, Z's Gram, Z R^{-1},
   // the rounding of Z into V)
   DevBuf task_qr, task_fin, task_eig;
-  DevBuf task_split, task_apply_loop, task_apply_close, task_small_apply, task_gram_z, task_round;
+  DevBuf task_split, task_apply_loop, task_apply_close, task_small_apply, task_gram_z, task_round, task_ritz;
+  // the lockstep schedule's tensor-core products at ld 64: every segment's
+  // forward product, transposed product and Gram in one launch each, with
+  // the per-segment sums of their partials in one launch
+  DevBuf tc_segs, tc_maps, band_seg, rmat_items, gram_items, rmat_sums, gram_sums;
+  int64_t n_bands = 0;
+  int n_rmat_items = 0, n_gram_items = 0;
 
   ~scxpca_batch() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -2123,7 +2138,8 @@ struct scxpca_batch {
     for (DevBuf* b : indptrs) delete b;
     emb.release();
     for (DevBuf* t : {&task_qr, &task_fin, &task_eig, &task_split, &task_apply_loop, &task_apply_close,
-                      &task_small_apply, &task_gram_z, &task_round})
+                      &task_small_apply, &task_gram_z, &task_round, &task_ritz, &tc_segs, &tc_maps, &band_seg,
+                      &rmat_items, &gram_items, &rmat_sums, &gram_sums})
       t->release();
     for (cudaStream_t st : branch) cudaStreamDestroy(st);
     for (cudaEvent_t e : join) cudaEventDestroy(e);
@@ -2193,6 +2209,8 @@ struct BatchOperator {
   // the gene-side work of every segment (n_vars x k, the same size for all)
   // in one launch per kernel on the main stream as well
   bool gene_batched = false;
+  // the tensor-core products (ld 64) of every segment in one launch each
+  bool tc_batched = false;
 
   template <class F>
   void each(F&& f) {
@@ -2209,7 +2227,34 @@ struct BatchOperator {
   }
   const scxpca_plan* p0() const { return ops[0].pl; }
   int ns() const { return (int)ops.size(); }
+  // Y = (X - mu) V for every segment: V's images, then one launch over all
+  // bands; the FP32 Y only for the loop's last product (finalize_q reads it)
+  void fwd_all(bool last) {
+    const scxpca_plan* p = p0();
+    CK(launch_split16_batch(b->task_split.as<SplitTask>(), ns(), p->g * p->ld, p->fmt16, b->main));
+    CK(launch_fwd_tc_batch(b->tc_segs.as<TcSegment>(), b->band_seg.as<int32_t>(), b->n_bands, p->n_chunks,
+                           last ? 1 : 0, p->fmt16, b->main, p->num_sms));
+  }
+  // W = X^T Q (raw) for every segment: the partials, then their sums
+  void rmat_all() {
+    const scxpca_plan* p = p0();
+    CK(launch_rmat_tc_batch(b->tc_segs.as<TcSegment>(), b->rmat_items.as<TcItem>(), b->n_rmat_items, p->n_chunks,
+                            p->g, p->tc_gene_groups, p->fmt16, b->main));
+    CK(launch_reduce_rows_batch(1, b->rmat_sums.as<SumTask>(), ns(), p->g * p->ld, b->main));
+  }
+  // Y's Gram and column sums (from its image) for every segment
+  void gram_all() {
+    const scxpca_plan* p = p0();
+    CK(launch_gram_tc_batch(b->tc_segs.as<TcSegment>(), b->gram_items.as<TcItem>(), b->n_gram_items, p->fmt16,
+                            b->main));
+    CK(launch_reduce_rows_batch(0, b->gram_sums.as<SumTask>(), ns(), p->ld * p->ld + p->ld, b->main));
+  }
   void matmat(Operand src, bool last) {
+    if (tc_batched) {
+      if (src == Operand::kOmega) each([&](int, DeviceOperator& o) { load_omega(o.pl, &o.p); });
+      fwd_all(last);
+      return;
+    }
     if (!gene_batched || src == Operand::kOmega) {
       each([&](int, DeviceOperator& o) { o.matmat(src, last); });
       return;
@@ -2223,7 +2268,10 @@ struct BatchOperator {
       each([&](int, DeviceOperator& o) { o.rmatmat(); });
       return;
     }
-    each([&](int, DeviceOperator& o) { o.rmatmat_products(); });
+    if (tc_batched)
+      rmat_all();
+    else
+      each([&](int, DeviceOperator& o) { o.rmatmat_products(); });
     const DevBuf& t = ops[0].closing ? b->task_apply_close : b->task_apply_loop;
     CK(launch_center_apply_batch(t.as<ApplyTask>(), ns(), p0()->g, (int)p0()->ld, b->main));
   }
@@ -2250,7 +2298,10 @@ struct BatchOperator {
       CK(launch_round_v_batch(b->task_round.as<RoundTask>(), ns(), p0()->g, (int)p0()->ld, b->main));
       return;
     }
-    each([&](int, DeviceOperator& o) { o.qr_gram(x); });
+    if (x == Buf::kY && tc_batched)
+      gram_all();
+    else
+      each([&](int, DeviceOperator& o) { o.qr_gram(x); });
     chol_all(b->task_qr);
     if (x == Buf::kZ) each([&](int, DeviceOperator& o) { o.qr_after(x); });
   }
@@ -2261,7 +2312,12 @@ struct BatchOperator {
     }
     const int passes = ops[0].shift ? 2 : 1;  // the Householder contract's third pass (DeviceOperator::finalize_q)
     for (int pass = 0; pass < passes; ++pass) {
-      each([&](int, DeviceOperator& o) { o.finalize_gram(); });
+      if (tc_batched) {
+        each([&](int, DeviceOperator& o) { o.apply_q(); });
+        gram_all();
+      } else {
+        each([&](int, DeviceOperator& o) { o.finalize_gram(); });
+      }
       chol_all(b->task_fin);
     }
     for (DeviceOperator& o : ops) o.closing = true;
@@ -2301,6 +2357,7 @@ bool batch_prepare_tasks(scxpca_batch* b, BatchOperator& bop) {
     std::vector<ApplyTask> tal(ns), tac(ns), tsa(ns);
     std::vector<GramTask> tg(ns);
     std::vector<RoundTask> tr(ns);
+    std::vector<RitzTask> tz(ns);
     for (size_t q = 0; q < ns; ++q) {
       scxpca_plan* pl = b->plans[q];
       const DeviceOperator& o = bop.ops[q];
@@ -2310,6 +2367,7 @@ bool batch_prepare_tasks(scxpca_batch* b, BatchOperator& bop) {
       tsa[q] = ApplyTask{pl->Z.as<double>(), nullptr, nullptr, pl->Rinv.as<double>(), pl->Z.as<double>()};
       tg[q] = GramTask{pl->Z.as<double>(), pl->gpart.as<double>(), pl->G.as<double>()};
       tr[q] = RoundTask{pl->Z.as<double>(), o.mu, pl->V.as<float>(), pl->mc.as<float>()};
+      tz[q] = ritz_task(pl);
     }
     if (p0->use_tc) put(b->task_split, tsp.data(), sizeof(SplitTask) * ns);
     put(b->task_apply_loop, tal.data(), sizeof(ApplyTask) * ns);
@@ -2317,8 +2375,62 @@ bool batch_prepare_tasks(scxpca_batch* b, BatchOperator& bop) {
     put(b->task_small_apply, tsa.data(), sizeof(ApplyTask) * ns);
     put(b->task_gram_z, tg.data(), sizeof(GramTask) * ns);
     put(b->task_round, tr.data(), sizeof(RoundTask) * ns);
+    put(b->task_ritz, tz.data(), sizeof(RitzTask) * ns);
   }
   bop.gene_batched = gene;
+  // the tensor-core products: one segment table, the band numbering of the
+  // forward product, and one item per CTA of each segment's transposed
+  // product and Gram, partitioned exactly as the segment's own launches
+  bool tc = gene && p0->use_tc && p0->ld == 64;
+  for (const scxpca_plan* pl : b->plans)
+    tc = tc && pl->use_tc && pl->ld == 64 && pl->n_chunks == p0->n_chunks && pl->tc_gene_groups == p0->tc_gene_groups;
+  if (tc) {
+    b->tc_maps.alloc(sizeof(CUtensorMap) * 2 * ns);
+    const CUtensorMap* dmaps = b->tc_maps.as<CUtensorMap>();
+    std::vector<CUtensorMap> maps(2 * ns);
+    std::vector<TcSegment> segs(ns);
+    std::vector<int32_t> bseg;
+    std::vector<TcItem> ritems, gitems;
+    std::vector<SumTask> rs(ns), gs(ns);
+    int64_t band0 = 0;
+    for (size_t q = 0; q < ns; ++q) {
+      scxpca_plan* pl = b->plans[q];
+      maps[2 * q] = pl->vmap;
+      maps[2 * q + 1] = pl->qmap;
+      const int64_t n_tiles = (pl->n + 127) / 128, bands = (n_tiles + 1) / 2;
+      segs[q] = TcSegment{pl->tf_ent.as<uint32_t>(), pl->tf_meta.p, dmaps + 2 * q, dmaps + 2 * q + 1,
+                          pl->mc.as<float>(), pl->Y.as<float>(), pl->Yimg.as<uint16_t>(), pl->tc_part.as<float>(),
+                          pl->gpart.as<double>(), pl->tc_err.as<int>(), pl->n, band0};
+      bseg.insert(bseg.end(), (size_t)bands, (int32_t)q);
+      band0 += bands;
+      const int R = pl->tc_row_groups, G = pl->tc_gene_groups;
+      for (int rg = 0; rg < R; ++rg)
+        for (int gg = 0; gg < G; ++gg)
+          ritems.push_back(TcItem{(int32_t)q, gg, rg, 0, tc_range_begin(rg, R, n_tiles),
+                                  tc_range_begin(rg + 1, R, n_tiles)});
+      const int parts = gram_tc_parts(pl->n, pl->tc_gram_parts, pl->num_sms);
+      for (int part = 0; part < parts; ++part)
+        gitems.push_back(TcItem{(int32_t)q, 0, part, 0, tc_range_begin(part, parts, n_tiles),
+                                tc_range_begin(part + 1, parts, n_tiles)});
+      rs[q] = SumTask{pl->tc_part.p, pl->W.as<double>(), R, 0};
+      gs[q] = SumTask{pl->gpart.p, pl->G.as<double>(), parts, 0};
+    }
+    // the longest items first, so the short ones fill the tail
+    auto longer = [](const TcItem& x, const TcItem& y) { return x.t1 - x.t0 > y.t1 - y.t0; };
+    std::stable_sort(ritems.begin(), ritems.end(), longer);
+    std::stable_sort(gitems.begin(), gitems.end(), longer);
+    put(b->tc_maps, maps.data(), sizeof(CUtensorMap) * 2 * ns);
+    put(b->tc_segs, segs.data(), sizeof(TcSegment) * ns);
+    put(b->band_seg, bseg.data(), sizeof(int32_t) * bseg.size());
+    put(b->rmat_items, ritems.data(), sizeof(TcItem) * ritems.size());
+    put(b->gram_items, gitems.data(), sizeof(TcItem) * gitems.size());
+    put(b->rmat_sums, rs.data(), sizeof(SumTask) * ns);
+    put(b->gram_sums, gs.data(), sizeof(SumTask) * ns);
+    b->n_bands = band0;
+    b->n_rmat_items = (int)ritems.size();
+    b->n_gram_items = (int)gitems.size();
+  }
+  bop.tc_batched = tc;
   CK(cudaStreamSynchronize(b->main));
   return true;
 }
@@ -2363,10 +2475,19 @@ void batch_capture(scxpca_batch* b, int nb, bool lockstep) {
         const scxpca_plan* p0 = b->plans[0];
         CK(launch_jacobi_eig_batch(b->task_eig.as<JacobiTask>(), (int)b->plans.size(), (int)p0->k, (int)p0->ld,
                                    b->main));
-        bop.each([&](int q, DeviceOperator& o) {
-          finish_after(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
-          batch_copy_out(b, q);
-        });
+        if (bop.gene_batched) {
+          CK(launch_ritz_finish_batch(b->task_ritz.as<RitzTask>(), (int)b->plans.size(), p0->g, (int)p0->ld,
+                                      (int)p0->k, (int)p0->nc, b->main));
+          bop.each([&](int q, DeviceOperator& o) {
+            finish_embed(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
+            batch_copy_out(b, q);
+          });
+        } else {
+          bop.each([&](int q, DeviceOperator& o) {
+            finish_after(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
+            batch_copy_out(b, q);
+          });
+        }
       } else {
         bop.each([&](int q, DeviceOperator& o) {
           enqueue_finish(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
@@ -2556,6 +2677,21 @@ scxpca_batch* create_batch(const scxpca_csr* x, const int64_t* offsets, int64_t 
       kmax = std::max<int64_t>(kmax, b->plans.back()->k);
     }
     b->k = kmax;
+    // The gene-side Grams (n_vars x k, FP64) of all segments run together in
+    // the batched launches: split each into fewer row ranges than a lone plan
+    // does, so the partials written and summed stay small.  Every path of the
+    // batch (graph or plain launches) then sums in the same order.
+    // Likewise the transposed product's row groups: at least four row tiles
+    // each, so a small segment does not write (and sum) one n_vars x k
+    // partial per tile.
+    for (scxpca_plan* pl : b->plans) {
+      pl->gram_parts_small = (int)std::max<int64_t>(
+          1, std::min<int64_t>(pl->gram_parts_small, (2 * pl->num_sms + n_segments - 1) / n_segments));
+      if (pl->use_tc && !pl->streaming) {
+        pl->tc_row_groups = (int)std::max<int64_t>(1, std::min<int64_t>(pl->tc_row_groups, (pl->n + 511) / 512));
+        pl->tc_gram_parts = (int)std::max<int64_t>(1, (pl->n + 1023) / 1024);  // eight row tiles each
+      }
+    }
     b->seg_ms.assign(n_segments, 1.0);
     b->emb.alloc(sizeof(float) * b->n_obs * b->nc);
     CK(cudaMallocHost(&b->h_status, sizeof(int32_t) * 4 * n_segments));

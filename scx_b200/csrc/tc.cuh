@@ -118,6 +118,14 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
+// Before a TMA copy reads a tensor map that lives in global memory (copied
+// there by the host, one per segment of a batch): order the map's bytes,
+// seen through the generic proxy, before the tensor-map proxy reads them.
+__device__ __forceinline__ void tmap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
 // Bring [src, src + bytes) into L2 ahead of use (16-byte aligned address, size
 // a multiple of 16); no completion tracking, the later bulk copy finds it there.
 __device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {

@@ -96,3 +96,40 @@ def test_batch_rejects_bad_segments():
     bad[2] = bad[1]
     with pytest.raises(ValueError, match="increase strictly"):
         accel.Batch(*args, bad, n_components=5, math_mode="strict_fp32")
+
+
+@pytest.mark.parametrize("branches", [-1, -3])
+def test_lockstep_tensor_core_products_ld64(branches):
+    """k = 60 (ld 64) under the lockstep schedule: the forward product, the
+    transposed product and the Gram of all segments run as one launch each
+    (segments of 2 to 33 row tiles, odd and even).  Their results must equal
+    the plain per-segment launches bit for bit and match the FP64 oracle."""
+    import torch
+
+    ip, ix, vv, offs = _clusters()
+    n = int(offs[-1])
+    dev = "cuda:0"
+    tv = torch.from_numpy(vv).to(dev).to(torch.bfloat16)
+    tip, tix = torch.from_numpy(ip).to(dev), torch.from_numpy(ix).to(dev)
+    nc, over, q, seed = 50, 10, 2, 3
+    b = accel.Batch(tip, tix, tv, (n, N_VARS), offs, n_components=nc, n_oversamples=over,
+                    n_power_iterations=q, seed=seed, math_mode="mixed_bf16", branches=branches)
+    assert b.lockstep
+    emb_g, comp_g, sv_g, vr_g, _ = b.run(use_graph=True)
+    emb_p, comp_p, sv_p, _, _ = b.run(use_graph=False)
+    emb_g2, _, sv_g2, _, _ = b.run(use_graph=True)
+    b.close()
+    np.testing.assert_array_equal(sv_g, sv_p)
+    np.testing.assert_array_equal(sv_g2, sv_g)
+    np.testing.assert_array_equal(emb_g, emb_p)
+    np.testing.assert_array_equal(emb_g2, emb_g)
+    np.testing.assert_array_equal(comp_g, comp_p)
+    om = rpca.gaussian_omega(N_VARS, nc + over, seed)
+    for s in range(len(SIZES)):
+        r0, r1 = offs[s], offs[s + 1]
+        e0, e1 = ip[r0], ip[r1]
+        svv = torch.from_numpy(vv[e0:e1]).to(torch.bfloat16).float().numpy()
+        ref = rpca.randomized_pca(rpca.Csr(ip[r0:r1 + 1] - e0, ix[e0:e1], svv, (r1 - r0, N_VARS)), nc, over, q,
+                                  True, om)
+        rel = np.abs(sv_g[s] - ref["singular_values"]) / ref["singular_values"]
+        assert rel.max() < 1e-4, (s, rel.max())
