@@ -564,6 +564,7 @@ def e2e_leg(args, ip, ix, vv, n_obs, local, dev, world):
                        "max": round(max(per_step), 3)},
            "values_on_host": str(vdt).replace("torch.", ""),
            "phases_ms": med,
+           "slowest_step_phases_ms": {k: round(v, 3) for k, v in phases[per_step.index(max(per_step))].items()},
            "h2d_copy": {"ms": round(copy_ms, 3),
                         "gbs": round((h_ix.numel() * 4 + h_vv.numel() * h_vv.element_size()) / copy_ms / 1e6, 1)}}
     host_csr = (a_ip, a_ix, vv.cpu().numpy())

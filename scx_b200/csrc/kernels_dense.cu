@@ -502,6 +502,7 @@ __global__ void __launch_bounds__(256, 2) k_tall_mm_upper64(const float* In, int
     cp_async_wait1();
     __syncthreads();
     const int64_t r0 = tile * kTallRows;
+    float res[2][16];  // [column group][4 rows x 4 columns]
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int cg = h == 0 ? w : 15 - w;  // column group: columns 4 cg .. 4 cg + 3
@@ -527,20 +528,43 @@ __global__ void __launch_bounds__(256, 2) k_tall_mm_upper64(const float* In, int
           }
         }
       }
+      res[h][0] = acc[0][0]; res[h][1] = acc[0][1]; res[h][2] = acc[0][2]; res[h][3] = acc[0][3];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int64_t row = r0 + lane + 32 * i;
-        if (row >= n) continue;
-        const int col = 4 * cg;
-        *reinterpret_cast<float4*>(Out + row * K + col) = make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
-        if (img) {
-          uint16_t hh[4], ll[4];
+      for (int i = 1; i < 4; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) split16(acc[i][j], fmt, hh[j], ll[j]);
-          *reinterpret_cast<uint4*>(img + (row * K + col) * 2) =
-              make_uint4(hh[0] | ((uint32_t)ll[0] << 16), hh[1] | ((uint32_t)ll[1] << 16),
-                         hh[2] | ((uint32_t)ll[2] << 16), hh[3] | ((uint32_t)ll[3] << 16));
-        }
+        for (int j = 0; j < 4; ++j) res[h][4 * i + j] = acc[i][j];
+    }
+    // A lane holds rows of the tile, so storing from registers would put 32
+    // rows (32 sectors) in every warp store.  The results go back into T
+    // instead, and the tile leaves row-contiguous: each warp store covers two
+    // whole 256-byte rows.
+    __syncthreads();  // every warp is done reading T
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int cg = h == 0 ? w : 15 - w;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        *reinterpret_cast<float4*>(T + (lane + 32 * i) * KP + 4 * cg) =
+            make_float4(res[h][4 * i], res[h][4 * i + 1], res[h][4 * i + 2], res[h][4 * i + 3]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < kTallRows * (K / 4) / 256; ++u) {
+      const int f = threadIdx.x + 256 * u;
+      const int r = f >> 4, c4 = f & 15;
+      const int64_t row = r0 + r;
+      if (row >= n) continue;
+      const float4 v = *reinterpret_cast<const float4*>(T + r * KP + 4 * c4);
+      *reinterpret_cast<float4*>(Out + row * K + 4 * c4) = v;
+      if (img) {
+        uint16_t hh[4], ll[4];
+        split16(v.x, fmt, hh[0], ll[0]);
+        split16(v.y, fmt, hh[1], ll[1]);
+        split16(v.z, fmt, hh[2], ll[2]);
+        split16(v.w, fmt, hh[3], ll[3]);
+        *reinterpret_cast<uint4*>(img + (row * K + 4 * c4) * 2) =
+            make_uint4(hh[0] | ((uint32_t)ll[0] << 16), hh[1] | ((uint32_t)ll[1] << 16),
+                       hh[2] | ((uint32_t)ll[2] << 16), hh[3] | ((uint32_t)ll[3] << 16));
       }
     }
     __syncthreads();  // every thread is done with T before it is refilled
@@ -611,7 +635,7 @@ cudaError_t launch_apply_right_split(const float* In, int64_t n, int ld, const f
 // made the kernel shared-memory bound at 256 segments).  Each output is one
 // FMA chain over l = 0 .. LD-1 in order.
 // ---------------------------------------------------------------------------
-constexpr int kApplyRows = 64;
+constexpr int kApplyRows = 16;  // rows per block step: 125 blocks for 2,000 genes (latency-bound launch)
 
 __host__ __device__ constexpr size_t center_apply_smem(int ld) {
   return ((size_t)ld * ld + (size_t)kApplyRows * (ld + 1)) * sizeof(double);
@@ -625,40 +649,57 @@ __device__ __forceinline__ void center_apply_body(const double* W, int64_t g, co
   extern __shared__ double sm[];
   double* Ms = sm;             // [LD][LD]
   double* rows = sm + LD * LD;  // [kApplyRows][LD + 1]
-  for (int t = threadIdx.x; t < LD * LD; t += 256) Ms[t] = M[t];
+  {
+    // every load of M in flight before the first shared store: one L2 round
+    // trip per block instead of one per element the thread stages
+    constexpr int PT = LD * LD / 256;  // elements per thread
+    double mv[PT];
+#pragma unroll
+    for (int u = 0; u < PT; ++u) mv[u] = M[threadIdx.x + 256 * u];
+#pragma unroll
+    for (int u = 0; u < PT; ++u) Ms[threadIdx.x + 256 * u] = mv[u];
+  }
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   for (int64_t j0 = (int64_t)b * kApplyRows; j0 < g; j0 += (int64_t)nb * kApplyRows) {
     __syncthreads();  // M staged; the previous block's rows consumed
-    for (int t = threadIdx.x; t < kApplyRows * LD; t += 256) {
+    constexpr int RT = kApplyRows * LD / 256;  // row elements per thread
+    double wv[RT];
+#pragma unroll
+    for (int u = 0; u < RT; ++u) {
+      const int t = threadIdx.x + 256 * u;
+      const int64_t j = j0 + t / LD;
+      wv[u] = j < g ? W[j * LD + t % LD] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < RT; ++u) {
+      const int t = threadIdx.x + 256 * u;
       const int r = t / LD, c = t % LD;
       const int64_t j = j0 + r;
-      double v = 0.0;
-      if (j < g) {
-        v = W[j * LD + c];
-        if (mu) v -= mu[j] * s[c];
-      }
+      double v = wv[u];
+      if (j < g && mu) v -= mu[j] * s[c];
       rows[r * RP + c] = v;
     }
     __syncthreads();
-    double acc[4][TT];
+    constexpr int RI = kApplyRows / 16;  // rows per thread
+    double acc[RI][TT];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < RI; ++i)
 #pragma unroll
       for (int v = 0; v < TT; ++v) acc[i][v] = 0.0;
 #pragma unroll 4
     for (int l = 0; l < LD; ++l) {
-      double a[4], m[TT];
+      double a[RI], m[TT];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = rows[(ty + 16 * i) * RP + l];
+      for (int i = 0; i < RI; ++i) a[i] = rows[(ty + 16 * i) * RP + l];
 #pragma unroll
       for (int v = 0; v < TT; ++v) m[v] = Ms[l * LD + tx + 16 * v];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < RI; ++i)
 #pragma unroll
         for (int v = 0; v < TT; ++v) acc[i][v] = fma(a[i], m[v], acc[i][v]);
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < RI; ++i) {
       const int64_t j = j0 + ty + 16 * i;
       if (j < g)
 #pragma unroll
