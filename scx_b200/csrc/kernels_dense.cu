@@ -854,9 +854,13 @@ cudaError_t launch_round_v(const double* A, int64_t g, int ld, const double* mu,
 // needs one block barrier.  Columns are stored contiguously (column-major,
 // odd stride) so a column walk is conflict-free.  Stops after a sweep with no
 // rotation (|p.q| <= 1e-15 |p| |q| for every pair, or |p.q| <= 1e-150), after
-// a sweep whose largest rotation tangent is below 1e-8 (convergence is
-// quadratic: the next sweep would rotate by less than 1e-16), or after 40
-// sweeps.  FP64 issue bandwidth (one warp instruction per ~4 cycles per SM
+// a sweep whose largest rotation tangent is below 1e-4, or after 40 sweeps.
+// Convergence is quadratic: the sweep after one whose largest tangent is t
+// rotates by about t^2 / 4 at most (measured on power-iteration sketches of
+// the NB synthetic at k = 40 and 60: 3e-2 -> 2e-5 -> 9e-11), so stopping at
+// t < 1e-4 leaves every eigenvector within ~1e-9 of the next sweep's, below
+// the FP32 resolution of the components and embeddings, and the eigenvalues
+// (second order in the rotation) within ~1e-18.  FP64 issue bandwidth (one warp instruction per ~4 cycles per SM
 // sub-partition) bounds a round, so the work per round is kept minimal.
 // ---------------------------------------------------------------------------
 // V (use_eglob) and R (use_rglob) go to the scratch that follows evecs when
@@ -1003,7 +1007,7 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ C, i
       }
       __syncthreads();
     }
-    const int converged = done || __longlong_as_double((long long)maxt_bits) < 1e-8;
+    const int converged = done || __longlong_as_double((long long)maxt_bits) < 1e-4;
     __syncthreads();  // every thread has read the flags before they are reset
     if (converged) break;
     if (tid == 0) {
