@@ -360,10 +360,47 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-template <int OUTB>
-__global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, int K, int ldi,
-                                                    const float* __restrict__ M, int ldm, int cnt, float* Out,
-                                                    int ldo, uint16_t* __restrict__ img, int fmt) {
+// The matrices of one tall right-multiplication launch.  A task is one
+// matrix: In (n x ldi, rows in tiles of 128), Out, the optional image, and M;
+// tile0 numbers its first tile in the launch.
+// TallOne: one matrix, block b takes the tiles b, b + nb, ...
+// TallBatch: every matrix of a batch; block b takes a contiguous range of the
+// launch's tiles, so it restages M only where its range crosses into the
+// next matrix.
+struct TallOne {
+  TallTask t;
+  int64_t n_tiles;
+  __device__ int64_t first() const { return blockIdx.x; }
+  __device__ int64_t next(int64_t tile) const { return tile + gridDim.x; }
+  __device__ bool valid(int64_t tile) const { return tile < n_tiles; }
+  __device__ int task_of(int64_t) const { return 0; }
+  __device__ TallTask task(int) const { return t; }
+};
+struct TallBatch {
+  const TallTask* tasks;
+  int ntasks;
+  int64_t begin, end;  // this block's tiles
+  __device__ int64_t first() const { return begin; }
+  __device__ int64_t next(int64_t tile) const { return tile + 1; }
+  __device__ bool valid(int64_t tile) const { return tile < end; }
+  __device__ int task_of(int64_t tile) const {  // the last task whose first tile is <= tile
+    int lo = 0, hi = ntasks - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tasks[mid].tile0 <= tile) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  }
+  __device__ TallTask task(int q) const { return tasks[q]; }
+};
+__device__ __forceinline__ TallBatch tall_batch(const TallTask* tasks, int ntasks, int64_t total_tiles) {
+  return TallBatch{tasks, ntasks, (int64_t)blockIdx.x * total_tiles / gridDim.x,
+                   (int64_t)(blockIdx.x + 1) * total_tiles / gridDim.x};
+}
+
+template <int OUTB, class Src>
+__device__ __forceinline__ void tall_mm_body(const Src& src, int K, int ldi, int ldm, int cnt, int ldo, int fmt) {
   constexpr int H = OUTB / 64;
   constexpr int RPT = kTallRows / 16;  // rows per thread
   extern __shared__ __align__(16) float sm_f[];
@@ -371,34 +408,40 @@ __global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, 
   float* Ms = sm_f;  // [K][OUTB]
   float* T0 = sm_f + K * OUTB;
   float* T1 = T0 + kTallRows * KP;
-  for (int t = threadIdx.x; t < K * OUTB; t += blockDim.x) {
-    const int l = t / OUTB, o = t % OUTB;
-    Ms[t] = o < cnt ? M[l * ldm + o] : 0.f;
-  }
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int k4 = K >> 2;
   const bool vec_out = ((cnt & 3) == 0) && ((ldo & 3) == 0);
-  const int64_t n_tiles = (n + kTallRows - 1) / kTallRows;
 
   auto issue = [&](int64_t tile, float* T) {
-    const int64_t r0 = tile * kTallRows;
+    const TallTask tk = src.task(src.task_of(tile));
+    const int64_t r0 = (tile - tk.tile0) * kTallRows;
     for (int t = threadIdx.x; t < kTallRows * k4; t += blockDim.x) {
       const int r = t / k4, c4 = t - r * k4;
       float* dst = T + r * KP + 4 * c4;
-      if (r0 + r < n) cp_async16(dst, In + (r0 + r) * ldi + 4 * c4);
+      if (r0 + r < tk.n) cp_async16(dst, tk.In + (r0 + r) * ldi + 4 * c4);
       else *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
     }
   };
 
-  int64_t tile = blockIdx.x;
-  if (tile < n_tiles) issue(tile, T0);
+  int cur = -1;  // the task whose M is staged
+  int64_t tile = src.first();
+  if (src.valid(tile)) issue(tile, T0);
   cp_async_commit();
-  for (int it = 0; tile < n_tiles; tile += gridDim.x, ++it) {
+  for (int it = 0; src.valid(tile); tile = src.next(tile), ++it) {
     float* T = (it & 1) ? T1 : T0;
-    const int64_t next = tile + gridDim.x;
-    if (next < n_tiles) issue(next, (it & 1) ? T0 : T1);
+    const int64_t next = src.next(tile);
+    if (src.valid(next)) issue(next, (it & 1) ? T0 : T1);
     cp_async_commit();
     cp_async_wait1();  // this tile's copies are done (the next tile's may still run)
+    const int q = src.task_of(tile);
+    const TallTask tk = src.task(q);
+    if (q != cur) {  // every thread finished with Ms at the previous tile's last barrier
+      for (int t = threadIdx.x; t < K * OUTB; t += blockDim.x) {
+        const int l = t / OUTB, o = t % OUTB;
+        Ms[t] = o < cnt ? tk.M[l * ldm + o] : 0.f;
+      }
+      cur = q;
+    }
     __syncthreads();
     float acc[RPT][4 * H];
 #pragma unroll
@@ -425,11 +468,13 @@ __global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, 
         }
       }
     }
-    const int64_t r0 = tile * kTallRows;
+    const int64_t r0 = (tile - tk.tile0) * kTallRows;
+    float* Out = tk.Out;
+    uint16_t* img = tk.img;
 #pragma unroll
     for (int i = 0; i < RPT; ++i) {
       const int64_t row = r0 + ty + 16 * i;
-      if (row >= n) continue;
+      if (row >= tk.n) continue;
 #pragma unroll
       for (int h = 0; h < H; ++h) {
         const int col = 64 * h + 4 * tx;
@@ -456,9 +501,24 @@ __global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, 
         }
       }
     }
-    __syncthreads();  // every thread is done with T before it is refilled
+    __syncthreads();  // every thread is done with T (and Ms) before they are refilled
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+template <int OUTB>
+__global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, int K, int ldi,
+                                                    const float* __restrict__ M, int ldm, int cnt, float* Out,
+                                                    int ldo, uint16_t* __restrict__ img, int fmt) {
+  tall_mm_body<OUTB>(TallOne{TallTask{In, Out, img, M, n, 0}, (n + kTallRows - 1) / kTallRows}, K, ldi, ldm, cnt,
+                     ldo, fmt);
+}
+
+template <int OUTB>
+__global__ void __launch_bounds__(256, 2) k_tall_mm_batch(const TallTask* __restrict__ tasks, int ntasks,
+                                                          int64_t total_tiles, int K, int ldi, int ldm, int cnt,
+                                                          int ldo, int fmt) {
+  tall_mm_body<OUTB>(tall_batch(tasks, ntasks, total_tiles), K, ldi, ldm, cnt, ldo, fmt);
 }
 
 // ---------------------------------------------------------------------------
@@ -471,37 +531,44 @@ __global__ void __launch_bounds__(256, 2) k_tall_mm(const float* In, int64_t n, 
 // whole before any of its rows is written, so Out may alias In).  The terms
 // dropped are exact zeros, so the result equals the full product's.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 2) k_tall_mm_upper64(const float* In, int64_t n,
-                                                            const float* __restrict__ M, float* Out,
-                                                            uint16_t* __restrict__ img, int fmt) {
+template <class Src>
+__device__ __forceinline__ void upper64_body(const Src& src, int fmt) {
   constexpr int K = 64, KP = K + 4;
   extern __shared__ __align__(16) float sm_u[];
   float* Ms = sm_u;                    // [K][K]
   float* T0 = sm_u + K * K;
   float* T1 = T0 + kTallRows * KP;
-  for (int t = threadIdx.x; t < K * K; t += blockDim.x) Ms[t] = M[t];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int64_t n_tiles = (n + kTallRows - 1) / kTallRows;
   auto issue = [&](int64_t tile, float* T) {
-    const int64_t r0 = tile * kTallRows;
+    const TallTask tk = src.task(src.task_of(tile));
+    const int64_t r0 = (tile - tk.tile0) * kTallRows;
     for (int t = threadIdx.x; t < kTallRows * (K / 4); t += blockDim.x) {
       const int r = t / (K / 4), c4 = t - r * (K / 4);
       float* dst = T + r * KP + 4 * c4;
-      if (r0 + r < n) cp_async16(dst, In + (r0 + r) * K + 4 * c4);
+      if (r0 + r < tk.n) cp_async16(dst, tk.In + (r0 + r) * K + 4 * c4);
       else *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
     }
   };
-  int64_t tile = blockIdx.x;
-  if (tile < n_tiles) issue(tile, T0);
+  int cur = -1;  // the task whose M is staged
+  int64_t tile = src.first();
+  if (src.valid(tile)) issue(tile, T0);
   cp_async_commit();
-  for (int it = 0; tile < n_tiles; tile += gridDim.x, ++it) {
+  for (int it = 0; src.valid(tile); tile = src.next(tile), ++it) {
     float* T = (it & 1) ? T1 : T0;
-    const int64_t next = tile + gridDim.x;
-    if (next < n_tiles) issue(next, (it & 1) ? T0 : T1);
+    const int64_t next = src.next(tile);
+    if (src.valid(next)) issue(next, (it & 1) ? T0 : T1);
     cp_async_commit();
     cp_async_wait1();
+    const int q = src.task_of(tile);
+    const TallTask tk = src.task(q);
+    if (q != cur) {  // every thread finished with Ms at the previous tile's last barrier
+      for (int t = threadIdx.x; t < K * K; t += blockDim.x) Ms[t] = tk.M[t];
+      cur = q;
+    }
     __syncthreads();
-    const int64_t r0 = tile * kTallRows;
+    const int64_t r0 = (tile - tk.tile0) * kTallRows, n = tk.n;
+    float* Out = tk.Out;
+    uint16_t* img = tk.img;
     float res[2][16];  // [column group][4 rows x 4 columns]
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -572,6 +639,17 @@ __global__ void __launch_bounds__(256, 2) k_tall_mm_upper64(const float* In, int
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+__global__ void __launch_bounds__(256, 2) k_tall_mm_upper64(const float* In, int64_t n,
+                                                            const float* __restrict__ M, float* Out,
+                                                            uint16_t* __restrict__ img, int fmt) {
+  upper64_body(TallOne{TallTask{In, Out, img, M, n, 0}, (n + kTallRows - 1) / kTallRows}, fmt);
+}
+
+__global__ void __launch_bounds__(256, 2) k_tall_mm_upper64_batch(const TallTask* __restrict__ tasks, int ntasks,
+                                                                  int64_t total_tiles, int fmt) {
+  upper64_body(tall_batch(tasks, ntasks, total_tiles), fmt);
+}
+
 static cudaError_t tall_mm_upper64(const float* In, int64_t n, const float* M, float* Out, uint16_t* img, int fmt,
                                    cudaStream_t st, int num_sms) {
   if (n == 0) return cudaSuccess;
@@ -581,6 +659,30 @@ static cudaError_t tall_mm_upper64(const float* In, int64_t n, const float* M, f
   const int grid = grid_for(n, kTallRows, num_sms, 2);
   note_launches(1);
   k_tall_mm_upper64<<<grid, 256, smem, st>>>(In, n, M, Out, img, fmt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_apply_upper64_batch(const TallTask* tasks, int ntasks, int64_t total_tiles, int fmt,
+                                       cudaStream_t st, int num_sms) {
+  if (ntasks <= 0 || total_tiles <= 0) return cudaSuccess;
+  const size_t smem = ((size_t)64 * 64 + 2 * (size_t)kTallRows * 68) * sizeof(float);
+  if (cudaError_t e = allow_smem(k_tall_mm_upper64_batch, smem); e != cudaSuccess) return e;
+  const int grid = (int)std::min<int64_t>(total_tiles, 2 * (int64_t)num_sms);
+  note_launches(1);
+  k_tall_mm_upper64_batch<<<grid, 256, smem, st>>>(tasks, ntasks, total_tiles, fmt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_embed_batch(const TallTask* tasks, int ntasks, int64_t total_tiles, int ld, int nc,
+                               cudaStream_t st, int num_sms) {
+  if (ntasks <= 0 || total_tiles <= 0) return cudaSuccess;
+  if (ld > 64 || nc > 64 || (ld & 3)) return cudaErrorInvalidValue;  // one 64-column panel, as launch_embed at ld 64
+  const size_t smem = ((size_t)ld * 64 + 2 * (size_t)kTallRows * (ld + 4)) * sizeof(float);
+  if (cudaError_t e = allow_smem(k_tall_mm_batch<64>, smem); e != cudaSuccess) return e;
+  const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(2, (220 * 1024) / smem));
+  const int grid = (int)std::min<int64_t>(total_tiles, (int64_t)per_sm * num_sms);
+  note_launches(1);
+  k_tall_mm_batch<64><<<grid, 256, smem, st>>>(tasks, ntasks, total_tiles, ld, ld, nc, nc, nc, 0);
   return cudaGetLastError();
 }
 
@@ -635,14 +737,17 @@ cudaError_t launch_apply_right_split(const float* In, int64_t n, int ld, const f
 // made the kernel shared-memory bound at 256 segments).  Each output is one
 // FMA chain over l = 0 .. LD-1 in order.
 // ---------------------------------------------------------------------------
-constexpr int kApplyRows = 16;  // rows per block step: 125 blocks for 2,000 genes (latency-bound launch)
+// Rows per block step: 16 for one matrix (125 blocks at 2,000 genes, a
+// latency-bound launch); 64 when a launch covers the segments of a batch
+// (thousands of blocks: fewer, larger steps per staged M).
+constexpr int kApplyRows = 16, kApplyRowsBatch = 64;
 
-__host__ __device__ constexpr size_t center_apply_smem(int ld) {
-  return ((size_t)ld * ld + (size_t)kApplyRows * (ld + 1)) * sizeof(double);
+__host__ __device__ constexpr size_t center_apply_smem(int ld, int rb) {
+  return ((size_t)ld * ld + (size_t)rb * (ld + 1)) * sizeof(double);
 }
 
 // Block b of nb (of one matrix's grid) takes the row blocks b, b + nb, ...
-template <int LD>
+template <int LD, int kApplyRows>
 __device__ __forceinline__ void center_apply_body(const double* W, int64_t g, const double* mu, const double* s,
                                                   const double* M, double* Z, int b, int nb) {
   constexpr int TT = LD / 16, RP = LD + 1;  // odd row stride: rows ty and ty + 1 sit in different banks
@@ -712,29 +817,31 @@ template <int LD>
 __global__ void __launch_bounds__(256) k_center_apply(const double* W, int64_t g, const double* __restrict__ mu,
                                                       const double* __restrict__ s, const double* __restrict__ M,
                                                       double* Z) {
-  center_apply_body<LD>(W, g, mu, s, M, Z, blockIdx.x, gridDim.x);
+  center_apply_body<LD, kApplyRows>(W, g, mu, s, M, Z, blockIdx.x, gridDim.x);
 }
 
 // One matrix per grid row y (batched segments).
 template <int LD>
 __global__ void __launch_bounds__(256) k_center_apply_batch(const ApplyTask* __restrict__ tasks, int64_t g) {
   const ApplyTask t = tasks[blockIdx.y];
-  center_apply_body<LD>(t.W, g, t.mu, t.s, t.M, t.Z, blockIdx.x, gridDim.x);
+  center_apply_body<LD, kApplyRowsBatch>(t.W, g, t.mu, t.s, t.M, t.Z, blockIdx.x, gridDim.x);
 }
 
 template <int LD>
 static cudaError_t center_apply_t(const ApplyTask* tasks, int ntasks, const double* W, int64_t g, const double* mu,
                                   const double* s, const double* M, double* Z, cudaStream_t st) {
-  const size_t smem = center_apply_smem(LD);
-  const int64_t blocks = (g + kApplyRows - 1) / kApplyRows;
-  if (blocks == 0) return cudaSuccess;
+  if (g <= 0) return cudaSuccess;
   note_launches(1);
   if (tasks) {
+    const size_t smem = center_apply_smem(LD, kApplyRowsBatch);
     if (cudaError_t e = allow_smem(k_center_apply_batch<LD>, smem); e != cudaSuccess) return e;
-    // up to 8 blocks per matrix, M staged once per block
-    const dim3 grid((unsigned)std::min<int64_t>(blocks, 8), (unsigned)ntasks);
+    // up to 16 blocks per matrix (two 64-row steps each at 2,000 genes), M staged once per block
+    const int64_t blocks = (g + kApplyRowsBatch - 1) / kApplyRowsBatch;
+    const dim3 grid((unsigned)std::min<int64_t>(blocks, 16), (unsigned)ntasks);
     k_center_apply_batch<LD><<<grid, 256, smem, st>>>(tasks, g);
   } else {
+    const size_t smem = center_apply_smem(LD, kApplyRows);
+    const int64_t blocks = (g + kApplyRows - 1) / kApplyRows;
     if (cudaError_t e = allow_smem(k_center_apply<LD>, smem); e != cudaSuccess) return e;
     k_center_apply<LD><<<(unsigned)std::min<int64_t>(blocks, 160), 256, smem, st>>>(W, g, mu, s, M, Z);
   }
@@ -813,6 +920,71 @@ cudaError_t launch_round_v_batch(const RoundTask* tasks, int ntasks, int64_t g, 
   const int gx = (int)std::min<int64_t>((g * ld + 255) / 256, 64);
   k_round_v_batch<<<dim3((unsigned)gx, (unsigned)ntasks), 256, 0, st>>>(tasks, g, ld);
   k_mean_prefactor_batch<<<dim3((unsigned)ld, (unsigned)ntasks), 256, 0, st>>>(tasks, g, ld);
+  return cudaGetLastError();
+}
+
+// A batch's per-segment results gathered into contiguous buffers, so the
+// host takes them in three copies instead of four per segment: status[q] =
+// the segment's three status words and its tensor-core error word, sigma[q]
+// its k singular values, comps[q] its `count` component floats.
+__global__ void k_gather_out(const OutTask* __restrict__ tasks, int k, int64_t count, int* __restrict__ status,
+                             double* __restrict__ sigma, float* __restrict__ comps) {
+  const int q = blockIdx.y;
+  const OutTask t = tasks[q];
+  if (blockIdx.x == 0) {
+    if (threadIdx.x < 3) status[4 * q + threadIdx.x] = t.status[threadIdx.x];
+    if (threadIdx.x == 3) status[4 * q + 3] = t.tc_err ? t.tc_err[0] : 0;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) sigma[(int64_t)q * k + i] = t.sigma[i];
+  }
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x)
+    comps[(int64_t)q * count + e] = t.comps[e];
+}
+
+cudaError_t launch_gather_out(const OutTask* tasks, int ntasks, int k, int64_t count, int* status, double* sigma,
+                              float* comps, cudaStream_t st) {
+  if (ntasks <= 0) return cudaSuccess;
+  note_launches(1);
+  const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((count + 255) / 256, 16));
+  k_gather_out<<<dim3((unsigned)gx, (unsigned)ntasks), 256, 0, st>>>(tasks, k, count, status, sigma, comps);
+  return cudaGetLastError();
+}
+
+// The four status words of every task set to zero (the start of a batch run).
+__global__ void k_zero_status(const OutTask* __restrict__ tasks) {
+  if (threadIdx.x < 4) tasks[blockIdx.x].status[threadIdx.x] = 0;
+}
+
+cudaError_t launch_zero_status(const OutTask* tasks, int ntasks, cudaStream_t st) {
+  if (ntasks <= 0) return cudaSuccess;
+  note_launches(1);
+  k_zero_status<<<ntasks, 32, 0, st>>>(tasks);
+  return cudaGetLastError();
+}
+
+// mc = mu^T Vf for every task (the Vf and mu of each; A unused).
+cudaError_t launch_mean_prefactor_batch(const RoundTask* tasks, int ntasks, int64_t g, int ld, cudaStream_t st) {
+  if (ntasks <= 0) return cudaSuccess;
+  note_launches(1);
+  k_mean_prefactor_batch<<<dim3((unsigned)ld, (unsigned)ntasks), 256, 0, st>>>(tasks, g, ld);
+  return cudaGetLastError();
+}
+
+// tasks[q].Vf = src for q = 1 .. ntasks - 1 (count floats, a multiple of 4):
+// one segment's test matrix handed to the others of a batch.
+__global__ void k_broadcast_v(const float* __restrict__ src, int64_t count4, const RoundTask* __restrict__ tasks) {
+  float4* dst = reinterpret_cast<float4*>(tasks[blockIdx.y + 1].Vf);
+  const float4* s4 = reinterpret_cast<const float4*>(src);
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < count4; t += (int64_t)gridDim.x * blockDim.x)
+    dst[t] = s4[t];
+}
+
+cudaError_t launch_broadcast_v(const float* src, int64_t count, const RoundTask* tasks, int ntasks,
+                               cudaStream_t st) {
+  if (ntasks <= 1 || count <= 0) return cudaSuccess;
+  if (count & 3) return cudaErrorInvalidValue;
+  note_launches(1);
+  const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((count / 4 + 255) / 256, 32));
+  k_broadcast_v<<<dim3((unsigned)gx, (unsigned)(ntasks - 1)), 256, 0, st>>>(src, count / 4, tasks);
   return cudaGetLastError();
 }
 

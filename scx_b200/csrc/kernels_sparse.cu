@@ -217,10 +217,64 @@ __device__ __forceinline__ OutT transform_value(InT v, int32_t j, int mode, cons
 // sums in warp order: a fixed order, so the result is deterministic.
 // With width > 0 the output is a column panel of a wider matrix: element i
 // goes to out[(i / width) * ldo + i % width].
+// FP32 partials with len a multiple of 4: the same sums (warp w adds the
+// parts w, w + 8, ... in that order, warp 0 the eight warp sums), but a lane
+// takes four consecutive outputs with one 16-byte load per part, so a block
+// step covers 128 outputs.  A pass over many small partials (the segments of a
+// batch) is bound by the latency of its steps, not by bandwidth.
+__device__ __forceinline__ void reduce_rows_body_f4(const float* __restrict__ part, int nparts, int64_t len,
+                                                    double* __restrict__ out, int accumulate, int width, int ldo,
+                                                    int blk, int nblk) {
+  __shared__ double red4[8][4 * 32 + 1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int64_t base = (int64_t)blk * 128; base < len; base += (int64_t)nblk * 128) {
+    const int64_t i = base + 4 * lane;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (i < len) {
+      int b = w;
+      for (; b + 24 < nparts; b += 32) {
+        const float4 v0 = *reinterpret_cast<const float4*>(part + (int64_t)b * len + i);
+        const float4 v1 = *reinterpret_cast<const float4*>(part + (int64_t)(b + 8) * len + i);
+        const float4 v2 = *reinterpret_cast<const float4*>(part + (int64_t)(b + 16) * len + i);
+        const float4 v3 = *reinterpret_cast<const float4*>(part + (int64_t)(b + 24) * len + i);
+        acc[0] += (double)v0.x; acc[1] += (double)v0.y; acc[2] += (double)v0.z; acc[3] += (double)v0.w;
+        acc[0] += (double)v1.x; acc[1] += (double)v1.y; acc[2] += (double)v1.z; acc[3] += (double)v1.w;
+        acc[0] += (double)v2.x; acc[1] += (double)v2.y; acc[2] += (double)v2.z; acc[3] += (double)v2.w;
+        acc[0] += (double)v3.x; acc[1] += (double)v3.y; acc[2] += (double)v3.z; acc[3] += (double)v3.w;
+      }
+      for (; b < nparts; b += 8) {
+        const float4 v = *reinterpret_cast<const float4*>(part + (int64_t)b * len + i);
+        acc[0] += (double)v.x; acc[1] += (double)v.y; acc[2] += (double)v.z; acc[3] += (double)v.w;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) red4[w][4 * lane + e] = acc[e];
+    __syncthreads();
+    if (w == 0 && i < len) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int64_t ie = i + e;
+        const int64_t oi = width > 0 ? (ie / width) * ldo + ie % width : ie;
+        double s = accumulate ? out[oi] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s += red4[u][4 * lane + e];
+        out[oi] = s;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void reduce_rows_body(const T* __restrict__ part, int nparts, int64_t len,
                                                  double* __restrict__ out, int accumulate, int width, int ldo,
                                                  int blk, int nblk) {
+  if constexpr (sizeof(T) == 4) {
+    if ((len & 3) == 0 && (reinterpret_cast<uintptr_t>(part) & 15) == 0) {
+      reduce_rows_body_f4(part, nparts, len, out, accumulate, width, ldo, blk, nblk);
+      return;
+    }
+  }
   __shared__ double red[8][33];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int64_t base = (int64_t)blk * 32; base < len; base += (int64_t)nblk * 32) {

@@ -158,12 +158,46 @@ struct RitzTask {  // the Rayleigh-Ritz finish of one segment (launch_ritz_finis
 };
 cudaError_t launch_ritz_finish_batch(const RitzTask* tasks, int ntasks, int64_t g, int ld, int k, int nc,
                                      cudaStream_t st);
+// One matrix of a batched tall right-multiplication: Out = In M (In n x ld,
+// rows in tiles of 128; the 16-bit image of Out too when img is set).  tile0
+// is the matrix's first tile in the launch's numbering (the tiles of all
+// tasks, task after task).  Each output element gets the FMAs, in the same
+// order, of the matrix's own launch_apply_right_split / launch_embed call.
+struct TallTask {
+  const float* In;
+  float* Out;
+  uint16_t* img;
+  const float* M;
+  int64_t n;
+  int64_t tile0;
+};
+// Y <- Y M for an upper-triangular 64 x 64 M (Cholesky inverse), per task.
+cudaError_t launch_apply_upper64_batch(const TallTask* tasks, int ntasks, int64_t total_tiles, int fmt,
+                                       cudaStream_t st, int num_sms);
+// Embeddings U = Q M_emb per task (ld <= 64 and nc <= 64; M_emb ld x nc, U n x nc).
+cudaError_t launch_embed_batch(const TallTask* tasks, int ntasks, int64_t total_tiles, int ld, int nc,
+                               cudaStream_t st, int num_sms);
 cudaError_t launch_center_apply_batch(const ApplyTask* tasks, int ntasks, int64_t g, int ld, cudaStream_t st);
 cudaError_t launch_gram_f64_batch(const GramTask* tasks, int ntasks, int64_t n, int ld, int nparts,
                                   cudaStream_t st, int num_sms);
 cudaError_t launch_reduce_rows_f64_batch(const GramTask* tasks, int ntasks, int nparts, int64_t len, cudaStream_t st,
                                          int num_sms);
 cudaError_t launch_round_v_batch(const RoundTask* tasks, int ntasks, int64_t g, int ld, cudaStream_t st);
+// mc = mu^T Vf for every task; and the copy of one test matrix (count floats)
+// into the Vf of tasks 1 .. ntasks - 1.
+// Where one segment of a batch keeps its results: its status words (4), its
+// tensor-core error word (null without one), sigma (k) and components.
+struct OutTask {
+  int* status;
+  const int* tc_err;
+  const double* sigma;
+  const float* comps;
+};
+cudaError_t launch_gather_out(const OutTask* tasks, int ntasks, int k, int64_t count, int* status, double* sigma,
+                              float* comps, cudaStream_t st);
+cudaError_t launch_zero_status(const OutTask* tasks, int ntasks, cudaStream_t st);
+cudaError_t launch_mean_prefactor_batch(const RoundTask* tasks, int ntasks, int64_t g, int ld, cudaStream_t st);
+cudaError_t launch_broadcast_v(const float* src, int64_t count, const RoundTask* tasks, int ntasks, cudaStream_t st);
 cudaError_t launch_split16_batch(const SplitTask* tasks, int ntasks, int64_t count, int fmt, cudaStream_t st);
 // ntasks factorisations of one launch, one block each (k, ld <= 128).
 cudaError_t launch_cholesky_batch(const CholTask* tasks, int ntasks, int k, int ld, double tau, int shift_on_fail,

@@ -1622,7 +1622,9 @@ void check_tc_error(scxpca_plan* pl) {
   }
 }
 
-void load_omega(scxpca_plan* pl, const scxpca_params* p) {
+// V = Omega (seeded, or the caller's), zero-padded to g x ld; V's mean
+// prefactor is load_omega's.
+void load_omega_v(scxpca_plan* pl, const scxpca_params* p) {
   cudaStream_t st = pl->stream;
   const int64_t g = pl->g, gu = pl->g_user, k = pl->k, ld = pl->ld;
   CK(cudaMemsetAsync(pl->V.p, 0, sizeof(float) * g * ld, st));
@@ -1638,8 +1640,12 @@ void load_omega(scxpca_plan* pl, const scxpca_params* p) {
     CK(launch_gaussian(p->seed, gu, k, pl->V.as<float>(), (int)ld, st, pl->num_sms));
   }
   if (pl->pflog) CK(launch_aug_colsum(pl->V.as<float>(), (int32_t)gu, (int)ld, st));
-  CK(launch_mean_prefactor(pl->V.as<float>(), g, (int)ld, pl->centered ? pl->d_mu.as<double>() : nullptr,
-                           pl->mc.as<float>(), st));
+}
+
+void load_omega(scxpca_plan* pl, const scxpca_params* p) {
+  load_omega_v(pl, p);
+  CK(launch_mean_prefactor(pl->V.as<float>(), pl->g, (int)pl->ld, pl->centered ? pl->d_mu.as<double>() : nullptr,
+                           pl->mc.as<float>(), pl->stream));
 }
 
 // Parameters of one run: the plan's, with the per-run overrides of `over`.
@@ -2129,6 +2135,14 @@ struct scxpca_batch {
   DevBuf tc_segs, tc_maps, band_seg, rmat_items, gram_items, rmat_sums, gram_sums;
   int64_t n_bands = 0;
   int n_rmat_items = 0, n_gram_items = 0;
+  // and the tall right-multiplications (Y R^{-1} with its image, the
+  // embeddings) over the row tiles of every segment, one launch each
+  DevBuf task_tall_q, task_tall_emb;
+  int64_t tall_tiles = 0;
+  // and the results: every segment's status words zeroed by one launch at the
+  // start, its status, sigma and components gathered into the d_* buffers by
+  // one launch at the end and copied to the pinned host buffers in three
+  DevBuf task_out, d_status, d_sigma, d_comps;
 
   ~scxpca_batch() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -2139,7 +2153,8 @@ struct scxpca_batch {
     emb.release();
     for (DevBuf* t : {&task_qr, &task_fin, &task_eig, &task_split, &task_apply_loop, &task_apply_close,
                       &task_small_apply, &task_gram_z, &task_round, &task_ritz, &tc_segs, &tc_maps, &band_seg,
-                      &rmat_items, &gram_items, &rmat_sums, &gram_sums})
+                      &rmat_items, &gram_items, &rmat_sums, &gram_sums, &task_tall_q, &task_tall_emb, &task_out,
+                      &d_status, &d_sigma, &d_comps})
       t->release();
     for (cudaStream_t st : branch) cudaStreamDestroy(st);
     for (cudaEvent_t e : join) cudaEventDestroy(e);
@@ -2249,9 +2264,19 @@ struct BatchOperator {
                             b->main));
     CK(launch_reduce_rows_batch(0, b->gram_sums.as<SumTask>(), ns(), p->ld * p->ld + p->ld, b->main));
   }
+  // Omega for every segment: one batch has one (n_vars, k, seed or explicit
+  // Omega), so segment 0 fills its V as a lone plan would and the others copy
+  // it; then every segment's mean prefactor in one launch
+  void load_omega_all() {
+    scxpca_plan* p = ops[0].pl;
+    p->stream = b->main;
+    load_omega_v(p, &ops[0].p);
+    CK(launch_broadcast_v(p->V.as<float>(), p->g * p->ld, b->task_round.as<RoundTask>(), ns(), b->main));
+    CK(launch_mean_prefactor_batch(b->task_round.as<RoundTask>(), ns(), p->g, (int)p->ld, b->main));
+  }
   void matmat(Operand src, bool last) {
     if (tc_batched) {
-      if (src == Operand::kOmega) each([&](int, DeviceOperator& o) { load_omega(o.pl, &o.p); });
+      if (src == Operand::kOmega) load_omega_all();
       fwd_all(last);
       return;
     }
@@ -2313,7 +2338,8 @@ struct BatchOperator {
     const int passes = ops[0].shift ? 2 : 1;  // the Householder contract's third pass (DeviceOperator::finalize_q)
     for (int pass = 0; pass < passes; ++pass) {
       if (tc_batched) {
-        each([&](int, DeviceOperator& o) { o.apply_q(); });
+        CK(launch_apply_upper64_batch(b->task_tall_q.as<TallTask>(), ns(), b->tall_tiles, p0()->fmt16, b->main,
+                                      p0()->num_sms));
         gram_all();
       } else {
         each([&](int, DeviceOperator& o) { o.finalize_gram(); });
@@ -2392,6 +2418,29 @@ bool batch_prepare_tasks(scxpca_batch* b, BatchOperator& bop) {
     std::vector<int32_t> bseg;
     std::vector<TcItem> ritems, gitems;
     std::vector<SumTask> rs(ns), gs(ns);
+    std::vector<TallTask> tq_tall(ns), te_tall(ns);
+    int64_t tile0 = 0;
+    for (size_t q = 0; q < ns; ++q) {
+      scxpca_plan* pl = b->plans[q];
+      tq_tall[q] = TallTask{pl->Y.as<float>(), pl->Y.as<float>(), pl->Yimg.as<uint16_t>(), pl->Rinv_f.as<float>(),
+                            pl->n, tile0};
+      te_tall[q] = TallTask{pl->Y.as<float>(), b->emb.as<float>() + b->offsets[q] * b->nc, nullptr,
+                            pl->M_emb.as<float>(), pl->n, tile0};
+      tile0 += (pl->n + 127) / 128;
+    }
+    put(b->task_tall_q, tq_tall.data(), sizeof(TallTask) * ns);
+    put(b->task_tall_emb, te_tall.data(), sizeof(TallTask) * ns);
+    b->tall_tiles = tile0;
+    std::vector<OutTask> to(ns);
+    for (size_t q = 0; q < ns; ++q) {
+      scxpca_plan* pl = b->plans[q];
+      to[q] = OutTask{pl->status.as<int>(), pl->tc_err.as<int>(), pl->sigma.as<double>(), pl->comps.as<float>()};
+      tc = tc && pl->g == b->n_vars;  // the component slots of the host buffer are n_vars long
+    }
+    put(b->task_out, to.data(), sizeof(OutTask) * ns);
+    b->d_status.alloc(sizeof(int) * 4 * ns);
+    b->d_sigma.alloc(sizeof(double) * b->k * ns);
+    b->d_comps.alloc(sizeof(float) * (size_t)b->nc * b->n_vars * ns);
     int64_t band0 = 0;
     for (size_t q = 0; q < ns; ++q) {
       scxpca_plan* pl = b->plans[q];
@@ -2463,9 +2512,12 @@ void batch_capture(scxpca_batch* b, int nb, bool lockstep) {
   CK(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeRelaxed));
   try {
     if (lockstep) {
-      bop.each([&](int, DeviceOperator& o) {
-        CK(cudaMemsetAsync(o.pl->status.p, 0, sizeof(int) * 4, o.pl->stream));
-      });
+      if (bop.tc_batched)
+        CK(launch_zero_status(b->task_out.as<OutTask>(), (int)b->plans.size(), b->main));
+      else
+        bop.each([&](int, DeviceOperator& o) {
+          CK(cudaMemsetAsync(o.pl->status.p, 0, sizeof(int) * 4, o.pl->stream));
+        });
       run_power_loop(bop, p.n_power_iterations);
       if (bop.small_batched) {
         if (bop.gene_batched)
@@ -2478,10 +2530,23 @@ void batch_capture(scxpca_batch* b, int nb, bool lockstep) {
         if (bop.gene_batched) {
           CK(launch_ritz_finish_batch(b->task_ritz.as<RitzTask>(), (int)b->plans.size(), p0->g, (int)p0->ld,
                                       (int)p0->k, (int)p0->nc, b->main));
-          bop.each([&](int q, DeviceOperator& o) {
-            finish_embed(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
-            batch_copy_out(b, q);
-          });
+          if (bop.tc_batched) {
+            const int ns = (int)b->plans.size();
+            CK(launch_embed_batch(b->task_tall_emb.as<TallTask>(), ns, b->tall_tiles, (int)p0->ld, (int)p0->nc,
+                                  b->main, p0->num_sms));
+            CK(launch_gather_out(b->task_out.as<OutTask>(), ns, (int)b->k, b->nc * b->n_vars, b->d_status.as<int>(),
+                                 b->d_sigma.as<double>(), b->d_comps.as<float>(), b->main));
+            CK(cudaMemcpyAsync(b->h_status, b->d_status.p, sizeof(int) * 4 * ns, cudaMemcpyDeviceToHost, b->main));
+            CK(cudaMemcpyAsync(b->h_sigma, b->d_sigma.p, sizeof(double) * b->k * ns, cudaMemcpyDeviceToHost,
+                               b->main));
+            CK(cudaMemcpyAsync(b->h_comps, b->d_comps.p, sizeof(float) * (size_t)b->nc * b->n_vars * ns,
+                               cudaMemcpyDeviceToHost, b->main));
+          } else {
+            bop.each([&](int q, DeviceOperator& o) {
+              finish_embed(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
+              batch_copy_out(b, q);
+            });
+          }
         } else {
           bop.each([&](int q, DeviceOperator& o) {
             finish_after(o.pl, b->emb.as<float>() + b->offsets[q] * b->nc);
@@ -2681,14 +2746,15 @@ scxpca_batch* create_batch(const scxpca_csr* x, const int64_t* offsets, int64_t 
     // the batched launches: split each into fewer row ranges than a lone plan
     // does, so the partials written and summed stay small.  Every path of the
     // batch (graph or plain launches) then sums in the same order.
-    // Likewise the transposed product's row groups: at least four row tiles
-    // each, so a small segment does not write (and sum) one n_vars x k
-    // partial per tile.
+    // Likewise the transposed product's row groups: at least sixteen row
+    // tiles each.  Every row group writes (and the sum reads) one n_vars x k
+    // FP32 partial: at four tiles per group, 256 segments of 1.66M cells moved
+    // 1.8 GB of partials per product, more than the packed matrix itself.
     for (scxpca_plan* pl : b->plans) {
       pl->gram_parts_small = (int)std::max<int64_t>(
           1, std::min<int64_t>(pl->gram_parts_small, (2 * pl->num_sms + n_segments - 1) / n_segments));
       if (pl->use_tc && !pl->streaming) {
-        pl->tc_row_groups = (int)std::max<int64_t>(1, std::min<int64_t>(pl->tc_row_groups, (pl->n + 511) / 512));
+        pl->tc_row_groups = (int)std::max<int64_t>(1, std::min<int64_t>(pl->tc_row_groups, (pl->n + 2047) / 2048));
         pl->tc_gram_parts = (int)std::max<int64_t>(1, (pl->n + 1023) / 1024);  // eight row tiles each
       }
     }
