@@ -227,6 +227,31 @@ __device__ __forceinline__ void reduce_rows_body_f4(const float* __restrict__ pa
                                                     int blk, int nblk) {
   __shared__ double red4[8][4 * 32 + 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (nparts <= 8) {
+    // Warp w of the eight would hold part w alone, and warp 0 would add them
+    // in warp order: out + p_0 + p_1 + ... .  The same sums, each warp on its
+    // own 128 outputs: one step per chunk instead of a block-wide step with
+    // most warps idle (the partials of a batch's small segments).
+    for (int64_t base = ((int64_t)blk * 8 + w) * 128; base < len; base += (int64_t)nblk * 8 * 128) {
+      const int64_t i = base + 4 * lane;
+      if (i >= len) continue;
+      float4 v[8];
+#pragma unroll
+      for (int b = 0; b < 8; ++b)
+        if (b < nparts) v[b] = *reinterpret_cast<const float4*>(part + (int64_t)b * len + i);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int64_t ie = i + e;
+        const int64_t oi = width > 0 ? (ie / width) * ldo + ie % width : ie;
+        double acc = accumulate ? out[oi] : 0.0;
+#pragma unroll
+        for (int b = 0; b < 8; ++b)
+          if (b < nparts) acc += (double)(e == 0 ? v[b].x : e == 1 ? v[b].y : e == 2 ? v[b].z : v[b].w);
+        out[oi] = acc;
+      }
+    }
+    return;
+  }
   for (int64_t base = (int64_t)blk * 128; base < len; base += (int64_t)nblk * 128) {
     const int64_t i = base + 4 * lane;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
