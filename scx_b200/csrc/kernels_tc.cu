@@ -901,6 +901,159 @@ __global__ void __launch_bounds__(128, 1)
   gram_tc_body<true>(job, fmt);
 }
 
+// ---------------------------------------------------------------------------
+// Embeddings U = Q M (n x nc, nc <= 64) on tensor cores, from the 16-bit image
+// of Q (ld 64: columns 2 j, 2 j + 1 = hi, lo of Q[:, j], TMA-loaded in tiles
+// of 128 rows) and the image of M: B[n][2 j] = B[n][2 j + 1] = hi(M[j][n])
+// for n < 64 and lo(M[j][n - 64]) for 64 <= n < 128, so one MMA chain
+// (M = 128 rows, N = 128, K = 128 image columns) gives Q hi(M) in columns
+// 0..63 and Q lo(M) in 64..127, which the epilogue adds: about 16 mantissa
+// bits on both operands, FP32 accumulation.  A CTA walks a contiguous range
+// of row tiles: warp 4 loads image tiles into a four-stage ring, warp 5
+// issues the MMAs into one of two TMEM accumulators, and warps 0-3 (one TMEM
+// lane quarter each) drain the other, staging the tile's rows of U in shared
+// memory so they leave in whole contiguous rows.  All waits are bounded.
+// ---------------------------------------------------------------------------
+constexpr int kEmbedStages = 4;
+constexpr int kEmbedThreads = 192;
+
+__host__ __device__ constexpr size_t embed_tc_smem() {
+  return 1024 + (size_t)kEmbedStages * 2 * TM * 64 * 2 + 2 * 128 * 64 * 2 + (size_t)TM * 64 * 4 + 256;
+}
+
+__global__ void __launch_bounds__(kEmbedThreads, 1)
+    k_embed_tc(int64_t n, int64_t n_tiles, const __grid_constant__ CUtensorMap qmap, const float* __restrict__ M,
+               int nc, float* __restrict__ U, int fmt, int* err) {
+  constexpr int PLANE = TM * 64 * 2;  // 64 image columns of 128 rows, 16 KB
+  constexpr int TILE = 2 * PLANE;
+  constexpr int S = kEmbedStages;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = align1024(smem_raw);
+  uint8_t* tiles = smem;
+  uint8_t* Bs = tiles + S * TILE;                           // [2 planes][128 n][64 k], swizzled
+  float* Us = reinterpret_cast<float*>(Bs + 2 * PLANE);     // [128 rows][nc]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(Us + TM * 64);
+  uint64_t* full = bars;
+  uint64_t* empty = full + S;
+  uint64_t* acc_full = empty + S;
+  uint64_t* acc_empty = acc_full + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t t0 = tc_range_begin(blockIdx.x, gridDim.x, n_tiles), t1 = tc_range_begin(blockIdx.x + 1, gridDim.x, n_tiles);
+
+  // B from M (ld 64 rows, nc columns): element (n, k) of plane k / 64
+  for (int e = threadIdx.x; e < 128 * 128; e += blockDim.x) {
+    const int nn = e >> 7, k = e & 127, j = k >> 1;
+    const int col = nn & 63;
+    uint16_t v = 0;
+    if (col < nc) {
+      const uint32_t w = hilo16(M[j * nc + col], fmt);
+      v = (uint16_t)(nn < 64 ? (w & 0xFFFFu) : (w >> 16));
+    }
+    *reinterpret_cast<uint16_t*>(Bs + (k >> 6) * PLANE + sw128_offset((uint32_t)nn, (uint32_t)(k & 63))) = v;
+  }
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < S; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&acc_full[a], 1);
+      mbar_init(&acc_empty[a], 4);
+    }
+    *abort_flag = 0;
+    mbar_fence_init();
+  }
+  fence_proxy_async_smem();  // B, written by threads, is read by the tensor cores
+  if (warp == 5) {
+    tmem_alloc(tmem_slot, 256);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 4) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      for (int64_t t = t0; t < t1; ++t, ++it) {
+        const int st = it % S;
+        if (!mbar_wait(&empty[st], ((it / S) & 1u) ^ 1u, abort_flag, err, 51)) break;
+        uint8_t* tile = tiles + st * TILE;
+        mbar_arrive_expect_tx(&full[st], TILE);
+        tma_load_2d(tile, &qmap, &full[st], 0, (int)(t * TM));
+        tma_load_2d(tile + PLANE, &qmap, &full[st], 64, (int)(t * TM));
+      }
+    }
+    __syncwarp();
+  } else if (warp == 5) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_f16(128, 128, fmt, 0, 0);  // both K-major
+      const uint32_t bbase = smem_u32(Bs);
+      uint32_t it = 0;
+      for (int64_t t = t0; t < t1; ++t, ++it) {
+        const int st = it % S;
+        const uint32_t a = it & 1u, u = it >> 1;
+        if (!mbar_wait(&acc_empty[a], (u & 1u) ^ 1u, abort_flag, err, 52) ||
+            !mbar_wait(&full[st], (it / S) & 1u, abort_flag, err, 53))
+          break;
+        tc_fence_after();
+        const uint32_t abase = smem_u32(tiles + st * TILE);
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {  // K = 16 image columns per step: +32 B along a row, plane after 4
+          const uint32_t off = (uint32_t)(kk >> 2) * PLANE + (uint32_t)(kk & 3) * 32u;
+          umma_f16(tmem + a * 128, sdesc_sw128(abase + off, 16, 1024), sdesc_sw128(bbase + off, 16, 1024), idesc,
+                   kk != 0);
+        }
+        umma_commit(&empty[st]);
+        umma_commit(&acc_full[a]);
+      }
+    }
+    __syncwarp();
+  } else {
+    // epilogue: TMEM lane quarter = warp; row 32 warp + lane of the tile
+    const int row = 32 * warp + lane;
+    uint32_t it = 0;
+    for (int64_t t = t0; t < t1; ++t, ++it) {
+      const uint32_t a = it & 1u, u = it >> 1;
+      if (!warp_wait(&acc_full[a], u & 1u, abort_flag, err, 54)) break;
+      tc_fence_after();
+      const uint32_t tb = tmem + ((32u * warp) << 16) + a * 128;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {  // output columns 32 h .. 32 h + 31
+        uint32_t x[32], y[32];
+        tmem_ld32(tb + 32 * h, x);
+        tmem_ld32(tb + 64 + 32 * h, y);
+        tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+          if (32 * h + c < nc) Us[row * nc + 32 * h + c] = __uint_as_float(x[c]) + __uint_as_float(y[c]);
+      }
+      tc_fence_before();
+      __syncwarp();  // the warp's 32 rows of U are staged
+      if (lane == 0) mbar_arrive(&acc_empty[a]);
+      // the warp's rows are contiguous in U: it copies them out alone (no
+      // barrier with the other epilogue warps, which could wait on a warp that
+      // gave up on a timed-out wait)
+      const int64_t r0 = t * TM + 32 * warp;
+      const int64_t cnt = max((int64_t)0, min((int64_t)32, n - r0)) * nc;
+      float* dst = U + r0 * nc;
+      const float* src = Us + 32 * warp * nc;
+      for (int64_t e = lane; e < cnt; e += 32) dst[e] = src[e];
+      __syncwarp();  // the warp's rows of Us are free for the next tile
+    }
+  }
+  if (*abort_flag) __nanosleep(500000);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 256);
+  }
+}
+
 // 16-bit image of x: words (hi | lo << 16), hi = round16(x), lo = round16(x - hi)
 // (fmt 1 = bf16, 0 = f16).
 __global__ void k_split16(const float* __restrict__ in, int64_t count, uint32_t* __restrict__ img, int fmt) {
@@ -1676,6 +1829,18 @@ int launch_gram_tc(int64_t n, const CUtensorMap* qmap, double* part, int fmt, in
   note_launches(1);
   k_gram_tc<<<grid, 128, gram_tc_smem(), st>>>(n_tiles, *qmap, part, fmt, err);
   return cudaGetLastError() == cudaSuccess ? grid : -1;
+}
+
+cudaError_t launch_embed_tc(int64_t n, const CUtensorMap* qmap, const float* M, int nc, float* U, int fmt, int* err,
+                            cudaStream_t st, int num_sms) {
+  if (n <= 0) return cudaSuccess;
+  if (nc <= 0 || nc > 64) return cudaErrorInvalidValue;
+  const int64_t n_tiles = (n + TM - 1) / TM;
+  const int grid = (int)std::min<int64_t>(n_tiles, (int64_t)num_sms);
+  if (cudaError_t e = allow_smem(k_embed_tc, embed_tc_smem()); e != cudaSuccess) return e;
+  note_launches(1);
+  k_embed_tc<<<grid, kEmbedThreads, embed_tc_smem(), st>>>(n, n_tiles, *qmap, M, nc, U, fmt, err);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_fwd_tc_batch(const TcSegment* segs, const int32_t* band_seg, int64_t n_bands, int nc,

@@ -322,6 +322,10 @@ struct TcItem {
   int32_t pad;
   int64_t t0, t1;  // row tiles [t0, t1) of the segment
 };
+// Embeddings U = Q M (n x nc row-major, nc <= 64; M ld 64 x nc) on tensor
+// cores from the 16-bit image of Q (ld 64) behind qmap.
+cudaError_t launch_embed_tc(int64_t n, const CUtensorMap* qmap, const float* M, int nc, float* U, int fmt, int* err,
+                            cudaStream_t st, int num_sms);
 cudaError_t launch_fwd_tc_batch(const TcSegment* segs, const int32_t* band_seg, int64_t n_bands, int nc,
                                 int write_y, int fmt, cudaStream_t st, int num_sms);
 cudaError_t launch_rmat_tc_batch(const TcSegment* segs, const TcItem* items, int n_items, int nc, int64_t g,

@@ -302,6 +302,9 @@ struct scxpca_plan {
   int fmt16 = 1;  // 1 = bf16, 0 = f16
   int n_chunks = 0, tc_gene_groups = 0, tc_row_groups = 0;
   int tc_gram_parts = 0;  // partials of the tensor-core Gram (0: one per SM)
+  // embeddings on tensor cores from Q's 16-bit image (ld 64); a batch's plans
+  // keep the CUDA-core product, which its batched embedding launch shares
+  bool embed_tc = true;
   // 16-bit images (column 2 j = hi, 2 j + 1 = lo of column j) of the dense
   // operands of the tensor-core products: V (g x 2 ld) and the tall Y/Q (n x 2 ld)
   DevBuf tf_meta, tf_ent, Vimg, Yimg, tc_part, tc_err;
@@ -1820,8 +1823,12 @@ RitzTask ritz_task(scxpca_plan* pl) {
 // Embeddings U = Q R2^{-1} E Sigma (first n_components).
 void finish_embed(scxpca_plan* pl, float* U) {
   int s = stage_begin(pl);
-  CK(launch_embed(pl->Y.as<float>(), pl->n, (int)pl->ld, (int)pl->k, pl->M_emb.as<float>(), (int)pl->nc, U,
-                  pl->stream, pl->num_sms));
+  if (pl->use_tc && pl->ld == 64 && pl->embed_tc && !pl->streaming)
+    CK(launch_embed_tc(pl->n, &pl->qmap, pl->M_emb.as<float>(), (int)pl->nc, U, pl->fmt16, pl->tc_err.as<int>(),
+                       pl->stream, pl->num_sms));
+  else
+    CK(launch_embed(pl->Y.as<float>(), pl->n, (int)pl->ld, (int)pl->k, pl->M_emb.as<float>(), (int)pl->nc, U,
+                    pl->stream, pl->num_sms));
   stage_end(pl, SCXPCA_STAGE_EMBED, s);
 }
 
@@ -2751,6 +2758,7 @@ scxpca_batch* create_batch(const scxpca_csr* x, const int64_t* offsets, int64_t 
     // FP32 partial: at four tiles per group, 256 segments of 1.66M cells moved
     // 1.8 GB of partials per product, more than the packed matrix itself.
     for (scxpca_plan* pl : b->plans) {
+      pl->embed_tc = false;
       pl->gram_parts_small = (int)std::max<int64_t>(
           1, std::min<int64_t>(pl->gram_parts_small, (2 * pl->num_sms + n_segments - 1) / n_segments));
       if (pl->use_tc && !pl->streaming) {
