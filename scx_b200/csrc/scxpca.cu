@@ -303,8 +303,9 @@ struct scxpca_plan {
   int n_chunks = 0, tc_gene_groups = 0, tc_row_groups = 0;
   int tc_gram_parts = 0;  // partials of the tensor-core Gram (0: one per SM)
   // embeddings on tensor cores from Q's 16-bit image (ld 64); a batch's plans
-  // keep the CUDA-core product, which its batched embedding launch shares
-  bool embed_tc = true;
+  // keep the CUDA-core product, which its batched embedding launch shares, and
+  // SCXPCA_EMBED_TC=0 keeps it for any plan
+  bool embed_tc = !(getenv("SCXPCA_EMBED_TC") && getenv("SCXPCA_EMBED_TC")[0] == '0');
   // 16-bit images (column 2 j = hi, 2 j + 1 = lo of column j) of the dense
   // operands of the tensor-core products: V (g x 2 ld) and the tall Y/Q (n x 2 ld)
   DevBuf tf_meta, tf_ent, Vimg, Yimg, tc_part, tc_err;

@@ -115,3 +115,28 @@ def test_tc_duplicates_use_cuda_cores_and_stay_correct():
     ref = rpca.dense_pca(rpca.round_to_bf16(dense.astype(np.float32)), 10)
     rel = np.abs(res.singular_values - ref["singular_values"]) / ref["singular_values"]
     assert rel.max() < 5e-3
+
+
+@pytest.mark.parametrize("n,nc,over,mode", [(3000, 50, 10, "mixed_bf16"), (100, 40, 24, "mixed_f16"),
+                                            (20000, 64, 0, "mixed_bf16")])
+def test_tensor_core_embeddings_match_cuda_core_product(monkeypatch, n, nc, over, mode):
+    """The embeddings U = Q M on tensor cores (from Q's 16-bit image and the
+    hi/lo image of M) against the CUDA-core FP32 product of the same run:
+    a ragged last row tile, a single partial tile, more tiles than SMs, BF16
+    and FP16 images, 40 to 64 components.  Everything before the embedding is
+    the same launches, so sigma and the components are bit-identical."""
+    g = 700
+    c = _csr(n, g, seed=11)
+    om = rpca.gaussian_omega(g, nc + over, seed=1)
+    kw = dict(n_components=nc, n_oversamples=over, n_power_iterations=3, omega=om, math_mode=mode,
+              qr_method="cholesky")
+    tc = accel.randomized_pca(c.indptr, c.indices, c.data, c.shape, **kw)
+    monkeypatch.setenv("SCXPCA_EMBED_TC", "0")
+    cc = accel.randomized_pca(c.indptr, c.indices, c.data, c.shape, **kw)
+    np.testing.assert_array_equal(tc.singular_values, cc.singular_values)
+    np.testing.assert_array_equal(tc.components, cc.components)
+    assert np.isfinite(tc.embeddings).all() and tc.embeddings.shape == (n, nc)
+    # ~16 mantissa bits on both operands of the tensor-core product
+    err = np.linalg.norm(tc.embeddings - cc.embeddings) / np.linalg.norm(cc.embeddings)
+    assert err < 2e-4, err
+    assert np.abs(tc.embeddings - cc.embeddings).max() < 2e-3 * np.abs(cc.embeddings).max()
