@@ -16,8 +16,9 @@ namespace scx {
 
 // ---------------------------------------------------------------------------
 // Gram partials.  Block b owns a contiguous row range; the 16 x 16 thread grid
-// owns output entries (ty + 16 i, tx + 16 j), i, j < T = ld / 16, so the shared
-// row reads of a warp hit consecutive banks.  Products of float inputs are
+// owns output entries (ty + 16 i, tx + 16 j), i <= j < T = ld / 16 (the 16 x 16
+// blocks on and above the diagonal, mirrored below it), so the shared row
+// reads of a warp hit consecutive banks.  Products of float inputs are
 // exact in FP64; accumulation is FP64.
 // ---------------------------------------------------------------------------
 template <typename T, int LD>
@@ -52,17 +53,25 @@ __device__ __forceinline__ void gram_body(const T* __restrict__ A, int64_t n, do
 #pragma unroll
       for (int i = 0; i < TT; ++i)
 #pragma unroll
-        for (int j = 0; j < TT; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < TT; ++j)
+          if (i <= j) acc[i][j] = fma(a[i], b[j], acc[i][j]);  // blocks on and above the diagonal
     }
     if (threadIdx.x < LD)
       for (int r = 0; r < rows; ++r) csum += sh[r][threadIdx.x];
     __syncthreads();
   }
+  // The Gram is symmetric: block (j, i) below the diagonal is the transpose of
+  // block (i, j), whose entry (a, b) is the same FMA chain over the rows with
+  // the two factors of each product swapped, which fma rounds identically.
   double* out = part + (int64_t)b * (LD * LD + LD);
 #pragma unroll
   for (int i = 0; i < TT; ++i)
 #pragma unroll
-    for (int j = 0; j < TT; ++j) out[(ty + 16 * i) * LD + tx + 16 * j] = acc[i][j];
+    for (int j = 0; j < TT; ++j)
+      if (i <= j) {
+        out[(ty + 16 * i) * LD + tx + 16 * j] = acc[i][j];
+        if (i < j) out[(tx + 16 * j) * LD + ty + 16 * i] = acc[i][j];
+      }
   if (threadIdx.x < LD) out[LD * LD + threadIdx.x] = csum;
 }
 
