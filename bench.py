@@ -392,6 +392,8 @@ def run_ours(args):
     out["ms_per_step"] = round(ms_max, 4)
     out["eig_sweeps"] = int(res.eig_sweeps)
     out["value"] = round(ms_max / world, 4)
+    out["value_is"] = ("the job's time per PCA: ms_per_step (the slowest replica's step, one whole PCA per GPU) "
+                       f"/ {world} replica(s)")
 
     # roofline of the dominant kernel, from the live stage timing of the timed region
     peak, peak_kind = measured_hbm_peak()
