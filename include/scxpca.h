@@ -261,7 +261,13 @@ int32_t scxpca_plan_qr(scxpca_plan* plan, float* a, int64_t m, int64_t ld_a,
  * measured times.  Two schedules: segment per branch (each branch runs whole
  * segments one after another) or lockstep (all segments take each step of
  * the power loop together, so their products run together and then their
- * small factorisations run together).  `branches` = b in 1..32 fixes the
+ * small factorisations run together).  When every segment has the same
+ * sketch width at ld 64 on the tensor-core path, each lockstep step is ONE
+ * launch over all segments (products, Grams, factorisations, eigensolves,
+ * the tall right-multiplications, Omega and the result gathers: a graph of a
+ * few dozen nodes whatever the segment count); otherwise the branches launch
+ * per segment.  Both schedules give the bits of use_graph = 0.
+ * `branches` = b in 1..32 fixes the
  * segment-per-branch schedule over b branches, -b the lockstep schedule over
  * b streams; 0 lets an autotuner time both schedules for 1, 2, 4, ... 32 and
  * keep the fastest.  params->omega must be NULL (seeded) or device memory, and
